@@ -1,0 +1,392 @@
+"""Generate the golden fixtures in this folder by running the reference ``sttopt``.
+
+The reference is pure Python (torch + NumPy/SciPy); its own LFS fixtures are absent,
+so its FP64 CPU torch path is run here, seeded, and its outputs saved as ``.npz``.
+Run from the repository root with the reference checkout on ``REFERENCE_ROOT``
+(default ``/root/reference``)::
+
+    python tests/golden/make_golden.py
+
+The fixtures are inputs and outputs only; nothing here is imported at test time.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REFERENCE_ROOT = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+sys.path.insert(0, str(REFERENCE_ROOT))
+sys.path.insert(0, str(HERE.parents[1]))
+
+import torch  # noqa: E402
+
+import sttopt.compliance as compliance  # noqa: E402
+import sttopt.fem as fem  # noqa: E402
+import sttopt.gravity as gravity  # noqa: E402
+import sttopt.load_cases as load_cases  # noqa: E402
+import sttopt.sensitivity as sensitivity  # noqa: E402
+import sttopt.torch_fem as torch_fem  # noqa: E402
+import sttopt.torch_mg as torch_mg  # noqa: E402
+import sttopt.torch_solve as torch_solve  # noqa: E402
+import sttopt.torch_util as torch_util  # noqa: E402
+import sttopt.virtual_heat as vh  # noqa: E402
+from sttopt.run_config import HeatRunConfig  # noqa: E402
+
+from oracle.sttopt_oracle import smoothed_density  # noqa: E402  (seeded input recipe)
+
+F64 = torch.float64
+EMIN, EMAX, PENAL, NU = 1e-9, 1.0, 3.0, 0.3
+
+
+def t(a, dtype=F64):
+    return torch.as_tensor(np.asarray(a), dtype=dtype)
+
+
+def save(name, **arrays):
+    out = {k: (v.detach().cpu().numpy() if torch.is_tensor(v) else np.asarray(v)) for k, v in arrays.items()}
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    size = (HERE / f"{name}.npz").stat().st_size
+    print(f"{name}.npz: {len(out)} arrays, {size / 1024:.1f} KiB")
+
+
+def heat_config(nelx, nely, **kw):
+    """A HeatRunConfig-shaped object carrying only the fields heat_time_field reads."""
+
+    class Cfg:
+        pass
+
+    c = Cfg()
+    c.chi_contrast = kw.get("chi_contrast", 1000.0)
+    c.drain_beta = kw.get("drain_beta", 25.0)
+    c.time_map = kw.get("time_map", "one_minus")
+    c.heat_cg_rtol = kw.get("heat_cg_rtol", 1e-8)
+    c.poisson_cg_rtol = kw.get("poisson_cg_rtol", 1e-8)
+    return c
+
+
+def gen_fem_basic():
+    save(
+        "fem_basic",
+        KE=fem.plane_stress_KE(NU),
+        KE_nu0=fem.plane_stress_KE(0.0),
+        KEh=fem.diffusion_KE(),
+        edof_5x3_d2=fem.element_dof_map(5, 3, 2),
+        edof_5x3_d1=fem.element_dof_map(5, 3, 1),
+        edof_7x4_d2=fem.element_dof_map(7, 4, 2),
+        mbb_F=load_cases.load_case(load_cases.LoadCase.MBB, 12, 4, 0.0, 0.0, 1.0)[0],
+        mbb_free=load_cases.load_case(load_cases.LoadCase.MBB, 12, 4, 0.0, 0.0, 1.0)[1],
+        cant_F=load_cases.load_case(load_cases.LoadCase.CANTILEVER, 12, 4, 0.0, 0.0, 1.0)[0],
+        cant_free=load_cases.load_case(load_cases.LoadCase.CANTILEVER, 12, 4, 0.0, 0.0, 1.0)[1],
+        gravity_C=gravity.gravity_load_matrix(6, 4).toarray(),
+        coarsen=np.array([torch_mg.coarsening_factors(a, b) for a, b in
+                          [(180, 60), (45, 15), (15, 5), (5, 5), (2048, 1024), (120, 40),
+                           (30, 10), (7, 9), (6, 9), (768, 384)]]),
+        plate_bottom_6x4=vh.plate_nodes(6, 4, "bottom_edge"),
+        plate_left_6x4=vh.plate_nodes(6, 4, "left_edge"),
+    )
+
+
+def gen_operator():
+    rng = np.random.default_rng(11)
+    nelx, nely = 12, 8
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    KE = t(fem.plane_stress_KE(NU))
+    F, free = load_cases.load_case(load_cases.LoadCase.CANTILEVER, nelx, nely, 0.0, 0.0, 1.0)
+    mask = torch_fem.free_mask(ndof, t(free, torch.int64))
+    x = rng.uniform(0.0, 1.0, (3, nelx * nely))
+    x[2, : nelx * nely // 3] = 1e-6
+    dens = torch_fem.simp_density(t(x), EMIN, EMAX, PENAL)
+    U = t(rng.standard_normal((3, ndof)))
+    # scalar with reaction
+    hx, hy = 9, 7
+    hedof = t(fem.element_dof_map(hx, hy, 1), torch.int64)
+    KEh = t(fem.diffusion_KE())
+    hn = (hx + 1) * (hy + 1)
+    hchi = t(rng.uniform(0.01, 2.0, (2, hx * hy)))
+    hreac = t(rng.uniform(0.0, 0.5, (2, hx * hy)))
+    hmask = ~torch.as_tensor(vh.plate_nodes(hx, hy, "bottom_edge"))
+    hU = t(rng.standard_normal((2, hn)))
+    rd = torch_fem.lumped_reaction(hreac, hedof, hn)
+    save(
+        "operator",
+        x=x, U=U, mask=mask, dens=dens,
+        matvec=torch_fem.matvec(U, dens, edof, KE, ndof),
+        matvec_bcast=torch_fem.matvec(U, dens[0], edof, KE, ndof),
+        diag=torch_fem.matvec_diagonal(dens, edof, KE, ndof),
+        op=torch_fem.operator(U, dens, edof, KE, ndof, mask),
+        jdiag=torch_fem.jacobi_preconditioner_diag(dens, edof, KE, ndof, mask),
+        h_chi=hchi, h_reac=hreac, h_mask=hmask, h_U=hU,
+        h_rdiag=rd,
+        h_op=torch_fem.operator(hU, hchi, hedof, KEh, hn, hmask, rd),
+        h_jdiag=torch_fem.jacobi_preconditioner_diag(hchi, hedof, KEh, hn, hmask, rd),
+    )
+
+
+def gen_transfers():
+    rng = np.random.default_rng(12)
+    out = {}
+    for kx, ky in [(2, 2), (3, 3), (3, 1), (2, 3), (1, 2)]:
+        for d in (1, 2):
+            nCx, nCy = 3, 2
+            c = t(rng.standard_normal(d * (nCx + 1) * (nCy + 1)))
+            f = t(rng.standard_normal(d * (nCx * kx + 1) * (nCy * ky + 1)))
+            key = f"k{kx}{ky}_d{d}"
+            out[f"c_{key}"] = c
+            out[f"f_{key}"] = f
+            out[f"P_{key}"] = torch_mg._on_node_grid(c, nCx + 1, nCy + 1, kx, ky, torch_mg._interp_axis)
+            out[f"R_{key}"] = torch_mg._on_node_grid(f, nCx * kx + 1, nCy * ky + 1, kx, ky,
+                                                     torch_mg._restrict_axis)
+            out[f"S_{key}"] = torch_mg.child_interpolation_matrices(kx, ky, None, F64, d)
+        out[f"children_{kx}{ky}"] = torch_mg._child_elements(6 * kx, 2 * ky, kx, ky, "cpu")
+    save("transfers", **out)
+
+
+def _binary_design(nelx, nely):
+    rows, cols = np.mgrid[0:nely, 0:nelx]
+    x = np.zeros((nely, nelx))
+    x[np.abs(rows / max(nely - 1, 1) - cols / max(nelx - 1, 1)) < 0.15] = 1.0
+    x[:2, :] = 1.0
+    x[-2:, :] = 1.0
+    x[:, :2] = 1.0
+    return x.ravel()
+
+
+def gen_hierarchy():
+    rng = np.random.default_rng(13)
+    out = {}
+    # vector: 24x18 (factors 2, 3) batched over 2 density rows
+    nelx, nely = 24, 18
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    F, free = load_cases.load_case(load_cases.LoadCase.CANTILEVER, nelx, nely, 0.0, 0.0, 1.0)
+    mask = torch_fem.free_mask(ndof, t(free, torch.int64))
+    x = np.stack([_binary_design(nelx, nely), rng.uniform(0.05, 1.0, nelx * nely)])
+    dens = torch_fem.simp_density(t(x), EMIN, EMAX, PENAL)
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    KE = t(fem.plane_stress_KE(NU))
+    levels = torch_mg.build_hierarchy(dens, edof, KE, mask, nelx, nely, max_coarse_elements=10)
+    out["v_x"] = x
+    out["v_mask"] = mask
+    out["v_nlevels"] = len(levels)
+    for i, lv in enumerate(levels):
+        out[f"v_L{i}_shape"] = np.array([lv.nelx, lv.nely, lv.kx, lv.ky])
+        out[f"v_L{i}_diag"] = lv.diag
+        out[f"v_L{i}_mask"] = lv.mask
+        if lv.keff is not None:
+            out[f"v_L{i}_keff"] = lv.keff
+    out["v_chol"] = levels[-1].chol
+    r = torch_fem.project(t(rng.standard_normal((2, ndof))), mask)
+    M = torch_mg.VCycle(levels)
+    out["v_r"] = r
+    out["v_Mr"] = M(r)
+    out["v_Ar"] = levels[0](r)
+    # scalar with reaction, 18x12
+    hx, hy = 18, 12
+    hn = (hx + 1) * (hy + 1)
+    hedof = t(fem.element_dof_map(hx, hy, 1), torch.int64)
+    KEh = t(fem.diffusion_KE())
+    hmask = ~torch.as_tensor(vh.plate_nodes(hx, hy, "bottom_edge"))
+    hchi = t(rng.uniform(1e-3, 1.0, hx * hy))
+    hreac = torch.full((hx * hy,), 25.0 / (hx * hy), dtype=F64)
+    hl = torch_mg.build_hierarchy(hchi, hedof, KEh, hmask, hx, hy, reaction=hreac,
+                                  max_coarse_elements=10)
+    out["h_chi"] = hchi
+    out["h_nlevels"] = len(hl)
+    for i, lv in enumerate(hl):
+        out[f"h_L{i}_shape"] = np.array([lv.nelx, lv.nely, lv.kx, lv.ky])
+        out[f"h_L{i}_diag"] = lv.diag
+        out[f"h_L{i}_mask"] = lv.mask
+        if lv.keff is not None:
+            out[f"h_L{i}_keff"] = lv.keff
+    out["h_chol"] = hl[-1].chol
+    hr = torch_fem.project(t(rng.standard_normal(hn)), hmask)
+    out["h_r"] = hr
+    out["h_Mr"] = torch_mg.VCycle(hl)(hr)
+    save("hierarchy", **out)
+
+
+def gen_mbb_config():
+    """MBB 120x40, uniform 0.5, one MG-PCG solve, compliance and dc/dxPhys."""
+    nelx, nely = 120, 40
+    F, free = load_cases.load_case(load_cases.LoadCase.MBB, nelx, nely, 0.0, 0.0, 1.0)
+    ndof = len(F)
+    KE = t(fem.plane_stress_KE(NU))
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    mask = torch_fem.free_mask(ndof, t(free, torch.int64))
+    xPhys = torch.full((nely, nelx), 0.5, dtype=F64, requires_grad=True)
+    info = {}
+    density = torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL).flatten()
+    U = torch_solve.femsolve(density, t(F), edof, KE, mask, nelx, nely, info=info)
+    ce = compliance._element_strain_energy(U, edof, KE, nely, nelx)
+    c = torch.sum(torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL) * ce)
+    (dc,) = sensitivity.jacobian_rows(c[None], [xPhys])
+    levels = torch_mg.build_hierarchy(density.detach(), edof, KE, mask, nelx, nely)
+    save("mbb120x40", F=F, mask=mask, U=U, c=c, dc=dc.reshape(nely, nelx),
+         forward_n_iter=info["forward_n_iter"], backward_n_iter=info["backward_n_iter"],
+         level_shapes=np.array([[lv.nelx, lv.nely] for lv in levels]),
+         coarse_ndof=levels[-1].ndof)
+
+
+def gen_cantilever():
+    """Config-2 shape, reduced: mid-right load cantilever, smoothed density, FP64."""
+    out = {}
+    for nelx, nely, seed, mce in [(64, 32, 2, 700), (96, 48, 3, 60)]:
+        x = smoothed_density(nelx, nely, seed)
+        nodes = fem.node_grid(nelx, nely)
+        ndof = 2 * nodes.size
+        F = np.zeros(ndof)
+        F[2 * nodes[nely // 2, -1] + 1] = -1.0
+        mask = np.ones(ndof, bool)
+        mask[2 * nodes[:, 0]] = False
+        mask[2 * nodes[:, 0] + 1] = False
+        KE = t(fem.plane_stress_KE(NU))
+        edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+        xPhys = t(x).requires_grad_(True)
+        info = {}
+        density = torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL).flatten()
+        U = torch_solve.femsolve(density, t(F), edof, KE, torch.as_tensor(mask), nelx, nely,
+                                 info=info, max_coarse_elements=mce)
+        ce = compliance._element_strain_energy(U, edof, KE, nely, nelx)
+        c = torch.sum(torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL) * ce)
+        (dc,) = sensitivity.jacobian_rows(c[None], [xPhys])
+        k = f"{nelx}x{nely}"
+        out.update({f"{k}_x": x, f"{k}_F": F, f"{k}_mask": mask, f"{k}_U": U, f"{k}_c": c,
+                    f"{k}_dc": dc.reshape(nely, nelx), f"{k}_mce": mce,
+                    f"{k}_fwd_iter": info["forward_n_iter"], f"{k}_bwd_iter": info["backward_n_iter"]})
+    save("cantilever", **out)
+
+
+def _heat(nelx, nely, x, mu, w, conduction_penal=3.0, mce=700):
+    mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device("cpu"), F64)
+    cfg = heat_config(nelx, nely)
+    xPhys = t(x).requires_grad_(True)
+    muT = t(mu).requires_grad_(True)
+    orig = torch_mg.MAX_COARSE_ELEMENTS
+    sol = vh.heat_time_field(cfg, mesh, xPhys, muT, conduction_penal=conduction_penal)
+    J = torch.sum(t(w) * sol.tPhys)
+    gx, gmu = torch.autograd.grad(J, [xPhys, muT])
+    return sol, J, gx, gmu
+
+
+def gen_heat():
+    out = {}
+    for nelx, nely, seed in [(40, 20, 4), (60, 30, 5)]:
+        rng = np.random.default_rng(seed)
+        x = smoothed_density(nelx, nely, seed)
+        mu = rng.uniform(0.2, 0.8, (nely, nelx))
+        w = rng.uniform(-1, 1, (nely, nelx))
+        sol, J, gx, gmu = _heat(nelx, nely, x, mu, w)
+        k = f"{nelx}x{nely}"
+        out.update({f"{k}_x": x, f"{k}_mu": mu, f"{k}_w": w, f"{k}_tPhys": sol.tPhys,
+                    f"{k}_T": sol.primary, f"{k}_J": J, f"{k}_gx": gx, f"{k}_gmu": gmu})
+    save("heat", **out)
+
+
+def _hard_time_mask(tPhys, ti, beta):
+    return (tPhys <= ti).to(tPhys.dtype)
+
+
+def spacetime_reference(x, w, n_stage):
+    """The space-time objective of the configs, composed from reference functions.
+
+    ``compliance.time_mask`` is replaced by the hard threshold ``tPhys <= s/n_stage``;
+    the stage rows go through one batched ``femsolve`` exactly as
+    ``batched_whole_and_gravity_compliance`` stacks them (without its row 0).
+    """
+    nely, nelx = x.shape
+    mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device("cpu"), F64)
+    cfg = heat_config(nelx, nely)
+    xPhys = t(x).requires_grad_(True)
+    mu = torch.full((nely, nelx), 0.5, dtype=F64)
+    sol = vh.heat_time_field(cfg, mesh, xPhys, mu, conduction_penal=3.0)
+    tPhys = sol.tPhys
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    KE = t(fem.plane_stress_KE(NU))
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    nodes = fem.node_grid(nelx, nely)
+    mask = np.ones(ndof, bool)
+    mask[2 * nodes[-1, :]] = False
+    mask[2 * nodes[-1, :] + 1] = False
+    mask = torch.as_tensor(mask)
+    C = torch_util.csr_to_tensor(gravity.gravity_load_matrix(nelx, nely), "cpu", F64)
+    orig = compliance.time_mask
+    compliance.time_mask = _hard_time_mask
+    try:
+        rows, Fs, xts = [], [], []
+        for s in range(1, n_stage + 1):
+            _, xt, Fg = compliance._gravity_load(xPhys, tPhys, s / n_stage, C, 10.0, ndof)
+            rows.append(torch_fem.simp_density(xt, EMIN, EMAX, PENAL).flatten())
+            Fs.append(Fg)
+            xts.append(xt)
+    finally:
+        compliance.time_mask = orig
+    density = torch.stack(rows)
+    info = {}
+    U = torch_solve.femsolve(density, torch.stack(Fs), edof, KE, mask, nelx, nely, info=info)
+    cs = []
+    for i, xt in enumerate(xts):
+        ce = compliance._element_strain_energy(U[i], edof, KE, nely, nelx)
+        cs.append(torch.sum(torch_fem.simp_density(xt, EMIN, EMAX, PENAL) * ce))
+    cs = torch.stack(cs)
+    Jt = torch.sum(t(w) * tPhys)
+    L = cs.sum() + Jt
+    (g,) = sensitivity.jacobian_rows(L[None], [xPhys])
+    member = np.stack([(tPhys.detach().numpy().ravel() <= s / n_stage) for s in range(1, n_stage + 1)])
+    return dict(x=x, w=w, tPhys=tPhys, T=sol.primary, U=U, c_s=cs, J_t=Jt, L=L,
+                grad=g.reshape(nely, nelx), member=member.astype(np.uint8),
+                fwd_iter=info["forward_n_iter"], bwd_iter=info["backward_n_iter"])
+
+
+def gen_spacetime():
+    out = {}
+    for nelx, nely, n_stage, seed in [(48, 24, 4, 7), (64, 32, 16, 8)]:
+        rng = np.random.default_rng(seed)
+        x = smoothed_density(nelx, nely, seed)
+        w = rng.uniform(-1, 1, (nely, nelx))
+        res = spacetime_reference(x, w, n_stage)
+        k = f"{nelx}x{nely}s{n_stage}"
+        out.update({f"{k}_{name}": v for name, v in res.items()})
+    save("spacetime", **out)
+
+
+def gen_pcg_cases():
+    """Retirement, zero rows, warm starts and non-convergence, as the reference does them."""
+    nelx, nely = 18, 12
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    F, free = load_cases.load_case(load_cases.LoadCase.CANTILEVER, nelx, nely, 0.0, 0.0, 1.0)
+    mask = torch_fem.free_mask(ndof, t(free, torch.int64))
+    KE = t(fem.plane_stress_KE(NU))
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    x = np.stack([_binary_design(nelx, nely), np.full(nelx * nely, 0.4), np.full(nelx * nely, 0.9)])
+    Fb = t(F).expand(3, -1).clone()
+    Fb[1] = 0.0
+    info = {}
+    U, n = torch_mg.solve(Fb, t(x), edof, KE, EMIN, EMAX, PENAL, mask, nelx, nely,
+                          rtol=1e-11, max_coarse_elements=24, info=info)
+    try:
+        torch_mg.solve(Fb, t(x), edof, KE, EMIN, EMAX, PENAL, mask, nelx, nely,
+                       rtol=1e-14, max_iter=2, max_coarse_elements=24)
+        raise AssertionError("expected non-convergence")
+    except torch_fem.CGConvergenceError as e:
+        resid = e.residuals
+        msg = str(e)
+    save("pcg_cases", x=x, F=Fb, mask=mask, U=U, n_iter=n, row_iters=info["row_iters"],
+         fail_resid=resid, fail_msg=np.array(msg))
+
+
+if __name__ == "__main__":
+    torch.set_num_threads(os.cpu_count() or 1)
+    gen_fem_basic()
+    gen_operator()
+    gen_transfers()
+    gen_hierarchy()
+    gen_pcg_cases()
+    gen_mbb_config()
+    gen_cantilever()
+    gen_heat()
+    gen_spacetime()
