@@ -1,0 +1,186 @@
+/* sttb200.h -- C ABI of the B200 (sm_100a) matrix-free FEM solve path.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t, returns an
+ * int status (STT_OK or an STT_ERR_* code) and retains no pointer past the call, except
+ * through the explicit hierarchy handle (stt_hier_*), whose device memory is a
+ * caller-owned workspace.  No entry point allocates device memory.
+ *
+ * Conventions match the reference's tensors: nodes in C order row * (nelx + 1) + col
+ * with row 0 at the top, dofs interleaved d * node + i (d = 2 plane stress, d = 1 scalar
+ * heat), elements row * nelx + col with local corners BL, BR, TR, TL.  Vectors are
+ * batched as rows with an explicit row stride (in elements).  Boundary conditions are a
+ * per-node byte of "fixed" flags (bit i set = dof i fixed), the mask P of the reference's
+ * projected operator A(v) = P(K P v).
+ *
+ * Reference interfaces replaced (paths inside the sttopt project):
+ *   stt_q4_apply        sttopt/torch_fem.py:62-83 (matvec), :135-159 (operator)
+ *   stt_q4_diag         sttopt/torch_fem.py:86-98 (matvec_diagonal), :162-181 (jacobi diag)
+ *   stt_lumped_reaction sttopt/torch_fem.py:117-132
+ *   stt_hier_*          sttopt/torch_mg.py:293-400 (build_hierarchy), :257-266 (select)
+ *   stt_level_apply     sttopt/torch_mg.py:239-255 (_Level.__call__), :179-193 (keff_matvec)
+ *   stt_vcycle          sttopt/torch_mg.py:403-476 (VCycle.__call__)
+ *   stt_pcg_mg          sttopt/torch_fem.py:201-343 (pcg with a multigrid preconditioner)
+ *   stt_vec_*           sttopt/torch_fem.py:253-331 (the PCG vector updates, any operator)
+ *   stt_element_sens    sttopt/torch_solve.py:144-152 (FemSolve.backward element terms),
+ *                       sttopt/compliance.py:49-59 (_element_strain_energy)
+ *   stt_stage_*         sttopt/compliance.py:137-161,198-253 with a hard stage threshold
+ *   stt_heat_*          sttopt/virtual_heat.py:162-166,189-201,404-462
+ */
+#ifndef STTB200_H
+#define STTB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* stt_stream_t; /* == cudaStream_t */
+
+enum {
+  STT_OK = 0,
+  STT_ERR_INVALID = 1,       /* bad argument (size, pointer, precision) */
+  STT_ERR_NOT_CONVERGED = 2, /* PCG hit max_iter with a row above rtol */
+  STT_ERR_BREAKDOWN = 3,     /* a non-finite PCG scalar */
+  STT_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  STT_ERR_CUDA = 5,          /* a CUDA runtime call failed */
+  STT_ERR_WORKSPACE = 6      /* the workspace is smaller than required */
+};
+
+enum { STT_FP64 = 0, STT_FP32 = 1 };
+enum { STT_PROJECT_IN = 1, STT_PROJECT_OUT = 2 };
+
+/* Last CUDA / argument error message of this thread (never NULL). */
+const char* stt_last_error(void);
+
+/* ---- level-0 operator ---------------------------------------------------------- */
+
+/* out[s] = [P] (K(rho[h(s)]) [P] u[s] + rdiag[h(s)] * [P] u[s]) for s < nrows.
+ * precision selects double (STT_FP64) or float (STT_FP32) for u, out, rho and rdiag.
+ * rho_rs == 0 broadcasts one density field; rdiag may be NULL (no reaction term);
+ * fixed may be NULL (no projection).  KE is a host pointer to (4d)^2 doubles. */
+int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
+                 const void* u, long long u_rs, void* out, long long out_rs,
+                 const void* rho, long long rho_rs, const void* rdiag, long long rdiag_rs,
+                 const uint8_t* fixed, int flags, const double* KE, stt_stream_t stream);
+
+/* diag(K(rho)) (+ rdiag), with fixed dofs set to 1 when fixed != NULL.  FP64. */
+int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho, long long rho_rs,
+                const double* rdiag, long long rdiag_rs, const uint8_t* fixed,
+                double* out, long long out_rs, const double* KE, stt_stream_t stream);
+
+/* rdiag[n * d + i] = sum over elements e touching node n of reaction[e] / 4.  FP64. */
+int stt_lumped_reaction(int d, int nelx, int nely, int nrows, const double* reaction,
+                        long long r_rs, double* out, long long out_rs, stt_stream_t stream);
+
+/* ---- multigrid hierarchy ------------------------------------------------------- */
+
+typedef struct stt_hier stt_hier;
+
+/* Bytes of device workspace a hierarchy of hrows density fields needs. */
+long long stt_hier_workspace_bytes(int d, int nelx, int nely, int hrows,
+                                   int max_coarse_elements, int precision);
+
+/* Build the Galerkin hierarchy on the device (torch_mg.build_hierarchy): level 0 is
+ * K(rho) (+ lumped reaction), coarser levels the exact Galerkin products stored as
+ * symmetric 9-point block stencils, the coarsest factorised by FP64 Cholesky.
+ * precision STT_FP32 keeps FP32 copies for an FP32 V-cycle.  reaction may be NULL. */
+int stt_hier_create(stt_hier** out, void* workspace, long long ws_bytes, int d, int nelx,
+                    int nely, int hrows, const double* rho, long long rho_rs,
+                    const double* reaction, long long r_rs, const uint8_t* fixed,
+                    const double* KE, int max_coarse_elements, int precision,
+                    stt_stream_t stream);
+
+/* A view of h restricted to batch rows: batch row s uses hierarchy row row_map[s]
+ * (device int32, caller-owned, kept alive while the view is used). */
+int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier** out);
+int stt_hier_destroy(stt_hier* h);
+
+/* nlevels, and per level (nelx, nely, kx, ky) into dims[4 * level]. */
+int stt_hier_info(const stt_hier* h, int* nlevels, int* dims, int max_levels);
+
+/* Copies of a level's Jacobi diagonal (FP64, [hrows][ndof]) and fixed flags. */
+int stt_hier_level_diag(const stt_hier* h, int level, double* out, stt_stream_t stream);
+int stt_hier_level_fixed(const stt_hier* h, int level, uint8_t* out, stt_stream_t stream);
+
+/* out[s] = A_level v[s] (the projected level operator, FP64). */
+int stt_level_apply(const stt_hier* h, int level, int nrows, const double* v, long long v_rs,
+                    double* out, long long out_rs, stt_stream_t stream);
+
+/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
+long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int gamma);
+
+/* z[s] = M r[s], one V-cycle (damped Jacobi omega, n_smooth sweeps each way, gamma
+ * coarse visits).  r and z are FP64; the cycle runs in the hierarchy's precision. */
+int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
+               long long z_rs, double omega, int n_smooth, int gamma, void* workspace,
+               long long ws_bytes, stt_stream_t stream);
+
+/* MG-preconditioned CG on all batch rows, entirely on the device.  x holds the warm
+ * start when has_x0, else is zeroed; b must already be projected.  Outputs: rel_resid
+ * [nrows] (host), conv_iter [nrows] (host, -1 = not converged), *n_iter (host).
+ * flexible selects the Polak-Ribiere beta; replace_every > 0 recomputes the true
+ * residual b - A x every that many iterations.  Returns STT_ERR_NOT_CONVERGED when a
+ * row is above rtol after max_iter iterations. */
+int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long long b_rs, double* x,
+               long long x_rs, int has_x0, double rtol, int max_iter, double omega,
+               int n_smooth, int gamma, int flexible, int replace_every, double* rel_resid,
+               int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
+               stt_stream_t stream);
+
+/* ---- PCG vector steps for arbitrary operators (FP64) ---------------------------- */
+
+/* dots[s * k + j] = sum_i a_j[s, i] * b_j[s, i] for the k <= 3 pairs given (NULL ends). */
+int stt_vec_dots(int nrows, long long n, const double* a0, const double* b0, const double* a1,
+                 const double* b1, const double* a2, const double* b2, long long rs,
+                 double* dots, stt_stream_t stream);
+/* x += alpha[s] p; r -= alpha[s] Ap; rr[s] = ||r[s]||^2. */
+int stt_vec_cg_update(int nrows, long long n, const double* alpha, double* x, double* r,
+                      const double* p, const double* Ap, long long rs, double* rr,
+                      stt_stream_t stream);
+/* p = z + beta[s] p. */
+int stt_vec_xpay(int nrows, long long n, const double* z, const double* beta, double* p,
+                 long long rs, stt_stream_t stream);
+
+/* ---- element terms ------------------------------------------------------------- */
+
+/* Per element e and batch row s: ce = U_e^T KE U_e; gdens = -lam_e^T KE U_e;
+ * greac = -lam_e . U_e / 4.  Any of ce, gdens, greac may be NULL (lam too, if both
+ * gradients are NULL).  FP64. */
+int stt_element_sens(int d, int nelx, int nely, int nrows, const double* U, long long U_rs,
+                     const double* lam, long long lam_rs, const double* KE, double* ce,
+                     double* gdens, double* greac, long long e_rs, stt_stream_t stream);
+
+/* ---- space-time stage glue (hard threshold t <= s / n_stage) -------------------- */
+
+/* member[s * nel + e] = tPhys[e] <= (s + 1) / n_stage, bit-exact FP64 compare. */
+int stt_stage_membership(int nel, int n_stage, const double* tPhys, uint8_t* member,
+                         stt_stream_t stream);
+
+/* For each stage s: xt = x * m_s; rho = Emin + xt^penal (Emax - Emin) (FP64);
+ * F[2n+1] = -(fe / 4) sum of xt over the elements of node n, F[2n] = 0, masked by
+ * fixed; fe = 1 / (nelx nely). */
+int stt_stage_rows(int nelx, int nely, int n_stage, const double* x, const uint8_t* member,
+                   double Emin, double Emax, double penal, const uint8_t* fixed, double* rho,
+                   double* F, stt_stream_t stream);
+
+/* grad[e] += sum_s m_s[e] * ((ce_s + gdens_s) * penal * xt^(penal - 1) * (Emax - Emin)
+ *            - (fe / 4) * sum over corners of gF_s at the y dofs).  ce/gdens [n_stage][nel],
+ * gF [n_stage][2 nnode]. */
+int stt_stage_gradient(int nelx, int nely, int n_stage, const double* x,
+                       const uint8_t* member, const double* ce, const double* gdens,
+                       const double* gF, double Emin, double Emax, double penal, double* grad,
+                       stt_stream_t stream);
+
+/* Heat glue: t_e = mean over corners of (1 - T); and the adjoint load
+ * g[n] = -sum over elements of w[e] / (4 scale). */
+int stt_heat_element_means(int nelx, int nely, const double* T, double* t_e,
+                           stt_stream_t stream);
+int stt_heat_adjoint_load(int nelx, int nely, const double* w, double scale, double* g,
+                          stt_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STTB200_H */

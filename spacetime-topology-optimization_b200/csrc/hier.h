@@ -1,0 +1,68 @@
+// Host-side description of a device multigrid hierarchy (the object behind stt_hier*).
+//
+// All device arrays live in one caller-owned workspace, carved by plan_hierarchy().
+// Level 0 keeps the (copied) element densities and the lumped reaction diagonal;
+// every coarser level keeps its Galerkin operator as a symmetric 9-point block
+// stencil: per node the centre block and the E, S, SE, SW coupling blocks (the other
+// four couplings are the transposes of the neighbours' blocks), each D x D, stored
+// coefficient-major ([row][coef][node]) so a warp reads one coefficient coalesced.
+// The coarsest level is factorised by a block-banded FP64 Cholesky.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/sttb200.h"
+
+namespace stt {
+
+constexpr int kMaxLevels = 24;
+
+inline int stencil_coefs(int d) { return 5 * d * d; }
+
+struct LevelDesc {
+  int nelx, nely;  // elements of this level
+  int kx, ky;      // coarsening factors to the next level (1, 1 at the coarsest)
+  int nnx, nny;
+  long long nnode, ndof, nel;
+  uint8_t* fixed;  // [nnode] bit i = dof i fixed
+  // level 0 only
+  double* rho64;    // [hrows][nel]
+  float* rho32;     // [hrows][nel] (FP32 precision only)
+  double* rdiag64;  // [hrows][ndof] lumped reaction diagonal, or null
+  float* rdiag32;
+  // levels >= 1 (and level 0 when it is also the coarsest)
+  double* st64;  // [hrows][NS][nnode]
+  float* st32;   // [hrows][NS][nnode] (FP32 precision only)
+};
+
+struct CoarseDesc {
+  int n;             // dofs of the coarsest level
+  int B;             // block size (>= half bandwidth)
+  int nb;            // blocks, n padded to nb * B
+  int by_col;        // dof ordering: 1 = column-major nodes (nny < nnx), 0 = row-major
+  double* blocks;    // [hrows][nb][4][B][B]: Dinv, Dinv^T, E, E^T (E_k = L_{k,k-1})
+};
+
+struct stt_hier_impl {
+  int d, nelx, nely, hrows, precision, nlevels, mce;
+  LevelDesc lv[kMaxLevels];
+  CoarseDesc co;
+  double KE[64];
+  double* tables;    // device: per transition S[9][64], G[9][64], GM[9][64]
+  double* keffA;     // build temporaries
+  double* keffB;
+  const int* row_map;  // batch row -> hierarchy row (device), or null
+  int* status;         // device status word of the build (bit 0: pivot <= 0, bit 1: band)
+  long long ws_bytes;
+};
+
+inline int level_node_count(int nelx, int nely) { return (nelx + 1) * (nely + 1); }
+
+// Plans level shapes and carves the workspace (base may be null to only size it).
+// Returns the bytes needed.
+long long plan_hierarchy(stt_hier_impl& h, char* base);
+
+}  // namespace stt
+
+struct stt_hier : stt::stt_hier_impl {};

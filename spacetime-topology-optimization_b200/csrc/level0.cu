@@ -1,0 +1,174 @@
+// Level-0 operator entry points: K(rho) u (projected or not), diag(K), lumped reaction.
+#include <cstdio>
+#include <cstring>
+
+#include "errors.h"
+#include "q4.cuh"
+
+namespace stt {
+
+template <int D, typename T>
+__global__ void __launch_bounds__(kNT) q4_apply_kernel(
+    const T* __restrict__ u, long long u_rs, T* __restrict__ out, long long out_rs,
+    const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag, long long rdiag_rs,
+    const uint8_t* __restrict__ fixed, int proj_in, int proj_out, int nelx, int nely,
+    KEq<D, T> ke) {
+  __shared__ Q4Smem<D, T, T> s;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int row = blockIdx.z;
+  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
+  const T* ur = u + (size_t)row * u_rs;
+  load_rho_tile<D, T, T>(s, rho + (size_t)row * rho_rs, r0, c0, nelx, nely);
+  load_u_tile<D, T, T>(s, r0, c0, nnx, nny, [&](int node, T(&v)[D]) {
+    load_node<D, T>(ur, node, v);
+    if (proj_in) {
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        if (is_fixed(fixed, node, j)) v[j] = T(0);
+    }
+  });
+  __syncthreads();
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int r = r0 + ty, c = c0 + tx;
+  if (r >= nny || c >= nnx) return;
+  const int node = r * nnx + c;
+  T acc[D];
+  tile_Ku<D, T, T>(s, ty, tx, ke, acc);
+  if (rdiag) {
+    const T* rd = rdiag + (size_t)row * rdiag_rs + (size_t)node * D;
+#pragma unroll
+    for (int i = 0; i < D; ++i) acc[i] = fma(__ldg(rd + i), s.u[ty + 1][tx + 1][i], acc[i]);
+  }
+  if (proj_out) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+      if (is_fixed(fixed, node, i)) acc[i] = T(0);
+  }
+  store_node<D, T>(out + (size_t)row * out_rs, node, acc);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kNT) q4_diag_kernel(
+    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
+    long long rdiag_rs, const uint8_t* __restrict__ fixed, double* __restrict__ out,
+    long long out_rs, int nelx, int nely, KEq<D, double> ke) {
+  __shared__ Q4Smem<D, double, double> s;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int row = blockIdx.z;
+  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
+  load_rho_tile<D, double, double>(s, rho + (size_t)row * rho_rs, r0, c0, nelx, nely);
+  __syncthreads();
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int r = r0 + ty, c = c0 + tx;
+  if (r >= nny || c >= nnx) return;
+  const int node = r * nnx + c;
+  double dg[D];
+  tile_diag<D, double, double>(s, ty, tx, ke, dg);
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    if (rdiag) dg[i] += __ldg(rdiag + (size_t)row * rdiag_rs + (size_t)node * D + i);
+    if (is_fixed(fixed, node, i)) dg[i] = 1.0;
+  }
+  store_node<D, double>(out + (size_t)row * out_rs, node, dg);
+}
+
+// rdiag[node * D + i] = sum of reaction[e] / 4 over the elements around the node.
+template <int D>
+__global__ void lumped_reaction_kernel(const double* __restrict__ reac, long long r_rs,
+                                       double* __restrict__ out, long long out_rs, int nelx,
+                                       int nely) {
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (node >= nnx * nny) return;
+  const int r = node / nnx, c = node - r * nnx;
+  const double* rr = reac + (size_t)row * r_rs;
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int er = r - 1 + a, ec = c - 1 + b;
+      if (er >= 0 && er < nely && ec >= 0 && ec < nelx) acc += __ldg(rr + (size_t)er * nelx + ec) / 4;
+    }
+#pragma unroll
+  for (int i = 0; i < D; ++i) out[(size_t)row * out_rs + (size_t)node * D + i] = acc;
+}
+
+template <int D, typename T>
+KEq<D, T> make_ke(const double* KE) {
+  KEq<D, T> k;
+  for (int i = 0; i < 16 * D * D; ++i) k.v[i] = T(KE[i]);
+  return k;
+}
+
+template <int D, typename T>
+int launch_apply(int nelx, int nely, int nrows, const void* u, long long u_rs, void* out,
+                 long long out_rs, const void* rho, long long rho_rs, const void* rdiag,
+                 long long rdiag_rs, const uint8_t* fixed, int flags, const double* KE,
+                 cudaStream_t st) {
+  dim3 grid((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, nrows);
+  q4_apply_kernel<D, T><<<grid, kNT, 0, st>>>(
+      (const T*)u, u_rs, (T*)out, out_rs, (const T*)rho, rho_rs, (const T*)rdiag, rdiag_rs,
+      fixed, (flags & STT_PROJECT_IN) ? 1 : 0, (flags & STT_PROJECT_OUT) ? 1 : 0, nelx, nely,
+      make_ke<D, T>(KE));
+  return check_launch("q4_apply");
+}
+
+}  // namespace stt
+
+using namespace stt;
+
+extern "C" int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows, const void* u,
+                            long long u_rs, void* out, long long out_rs, const void* rho,
+                            long long rho_rs, const void* rdiag, long long rdiag_rs,
+                            const uint8_t* fixed, int flags, const double* KE,
+                            stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || !u || !out || !rho || !KE)
+    return set_error(STT_ERR_INVALID, "stt_q4_apply: bad sizes or null pointer");
+  if ((flags & STT_PROJECT_IN || flags & STT_PROJECT_OUT) && !fixed)
+    return set_error(STT_ERR_INVALID, "stt_q4_apply: projection needs the fixed flags");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == STT_FP64) {
+    if (d == 2) return launch_apply<2, double>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
+    if (d == 1) return launch_apply<1, double>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
+  } else if (precision == STT_FP32) {
+    if (d == 2) return launch_apply<2, float>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
+    if (d == 1) return launch_apply<1, float>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
+  }
+  return set_error(STT_ERR_INVALID, "stt_q4_apply: d must be 1 or 2, precision FP64 or FP32");
+}
+
+extern "C" int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho,
+                           long long rho_rs, const double* rdiag, long long rdiag_rs,
+                           const uint8_t* fixed, double* out, long long out_rs,
+                           const double* KE, stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || !rho || !out || !KE)
+    return set_error(STT_ERR_INVALID, "stt_q4_diag: bad sizes or null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, nrows);
+  if (d == 2)
+    q4_diag_kernel<2><<<grid, kNT, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<2, double>(KE));
+  else if (d == 1)
+    q4_diag_kernel<1><<<grid, kNT, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<1, double>(KE));
+  else
+    return set_error(STT_ERR_INVALID, "stt_q4_diag: d must be 1 or 2");
+  return check_launch("q4_diag");
+}
+
+extern "C" int stt_lumped_reaction(int d, int nelx, int nely, int nrows, const double* reaction,
+                                   long long r_rs, double* out, long long out_rs,
+                                   stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || !reaction || !out)
+    return set_error(STT_ERR_INVALID, "stt_lumped_reaction: bad sizes or null pointer");
+  const int nnode = (nelx + 1) * (nely + 1);
+  dim3 grid((nnode + 255) / 256, nrows);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (d == 2)
+    lumped_reaction_kernel<2><<<grid, 256, 0, st>>>(reaction, r_rs, out, out_rs, nelx, nely);
+  else if (d == 1)
+    lumped_reaction_kernel<1><<<grid, 256, 0, st>>>(reaction, r_rs, out, out_rs, nelx, nely);
+  else
+    return set_error(STT_ERR_INVALID, "stt_lumped_reaction: d must be 1 or 2");
+  return check_launch("lumped_reaction");
+}

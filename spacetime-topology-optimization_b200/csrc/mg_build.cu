@@ -1,0 +1,716 @@
+// Device construction of the Galerkin multigrid hierarchy (torch_mg.build_hierarchy,
+// sttopt/torch_mg.py:293-400) and the block-banded Cholesky factor of its coarsest
+// level (torch_mg._dense_cholesky, :269-290).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "errors.h"
+#include "hier.h"
+#include "q4.cuh"
+
+namespace stt {
+
+// ---- host tables --------------------------------------------------------------
+
+// Coarsening factor of one dimension: the smallest of 2, 3 dividing n, else 1
+// (torch_mg.coarsening_factors, :53-72).
+static int factor_of(int n) { return n % 2 == 0 ? 2 : (n % 3 == 0 ? 3 : 1); }
+
+// Piecewise-linear interpolation of two coarse values at fine offset j of k, in the
+// reference's operation order (torch_mg._interp_axis, :75-81).
+static double interp1(double a, double b, int j, int k) {
+  if (j == k) return b;
+  const double w = (double)j / k;
+  return a * (1 - w) + b * w;
+}
+
+// S[m][p][q]: weight of coarse local dof q on child m's local dof p
+// (torch_mg.child_interpolation_matrices, :140-165), derived by interpolating the
+// coarse element's unit basis vectors over its (ky+1) x (kx+1) fine nodes.
+static void child_interp(int kx, int ky, int d, double* S /* [kx*ky][4d][4d] */) {
+  const int nk = 4 * d;
+  std::memset(S, 0, sizeof(double) * kx * ky * nk * nk);
+  // coarse corners BL, BR, TR, TL at (row, col) of the 2x2 coarse node grid
+  for (int qc = 0; qc < 4; ++qc) {
+    const int cr = corner_dr(qc), cc = corner_dc(qc);
+    for (int my = 0; my < ky; ++my)
+      for (int mx = 0; mx < kx; ++mx) {
+        const int m = my * kx + mx;
+        for (int qf = 0; qf < 4; ++qf) {
+          const int fr = my + corner_dr(qf), fc = mx + corner_dc(qf);
+          // x pass on both coarse rows, then y pass
+          double g[2];
+          for (int R = 0; R < 2; ++R) {
+            const double a = (R == cr && cc == 0) ? 1.0 : 0.0;
+            const double b = (R == cr && cc == 1) ? 1.0 : 0.0;
+            g[R] = interp1(a, b, fc, kx);
+          }
+          const double v = interp1(g[0], g[1], fr, ky);
+          for (int i = 0; i < d; ++i) S[(m * nk + qf * d + i) * nk + qc * d + i] = v;
+        }
+      }
+  }
+}
+
+// G[m] = S_m^T K S_m for a fixed (nk x nk) K.
+static void galerkin_table(const double* S, const double* K, int nm, int nk, double* G) {
+  for (int m = 0; m < nm; ++m) {
+    const double* Sm = S + (size_t)m * nk * nk;
+    for (int i = 0; i < nk; ++i)
+      for (int j = 0; j < nk; ++j) {
+        double acc = 0.0;
+        for (int p = 0; p < nk; ++p) {
+          if (Sm[p * nk + i] == 0.0) continue;
+          double t = 0.0;
+          for (int q = 0; q < nk; ++q) t += K[p * nk + q] * Sm[q * nk + j];
+          acc += Sm[p * nk + i] * t;
+        }
+        G[((size_t)m * nk + i) * nk + j] = acc;
+      }
+  }
+}
+
+constexpr int kTableStride = 9 * 64;  // doubles per table (max 9 children x 8 x 8)
+
+static inline char* carve(char*& p, long long& used, long long bytes) {
+  const long long a = (bytes + 255) & ~255LL;
+  char* r = p ? p + used : nullptr;
+  used += a;
+  return r;
+}
+
+long long plan_hierarchy(stt_hier_impl& h, char* base) {
+  long long used = 0;
+  char* p = base;
+  const int d = h.d, NS = stencil_coefs(d), NK = 4 * d;
+  int nx = h.nelx, ny = h.nely, L = 0;
+  while (true) {
+    LevelDesc& lv = h.lv[L];
+    std::memset(&lv, 0, sizeof(lv));
+    lv.nelx = nx;
+    lv.nely = ny;
+    lv.nnx = nx + 1;
+    lv.nny = ny + 1;
+    lv.nnode = (long long)lv.nnx * lv.nny;
+    lv.ndof = lv.nnode * d;
+    lv.nel = (long long)nx * ny;
+    lv.kx = lv.ky = 1;
+    ++L;
+    if ((long long)nx * ny <= h.mce) break;
+    const int kx = factor_of(nx), ky = factor_of(ny);
+    if (kx == 1 && ky == 1) break;
+    if (L >= kMaxLevels) break;
+    lv.kx = kx;
+    lv.ky = ky;
+    nx /= kx;
+    ny /= ky;
+  }
+  h.nlevels = L;
+  const bool f32 = h.precision == STT_FP32;
+  for (int l = 0; l < L; ++l) {
+    LevelDesc& lv = h.lv[l];
+    lv.fixed = (uint8_t*)carve(p, used, lv.nnode);
+    if (l == 0) {
+      lv.rho64 = (double*)carve(p, used, 8LL * h.hrows * lv.nel);
+      if (f32) lv.rho32 = (float*)carve(p, used, 4LL * h.hrows * lv.nel);
+      lv.rdiag64 = (double*)carve(p, used, 8LL * h.hrows * lv.ndof);
+      if (f32) lv.rdiag32 = (float*)carve(p, used, 4LL * h.hrows * lv.ndof);
+    }
+    if (l > 0 || L == 1) {
+      lv.st64 = (double*)carve(p, used, 8LL * h.hrows * NS * lv.nnode);
+      if (f32 && l > 0) lv.st32 = (float*)carve(p, used, 4LL * h.hrows * NS * lv.nnode);
+    }
+  }
+  // coarse factor
+  {
+    const LevelDesc& c = h.lv[L - 1];
+    CoarseDesc& co = h.co;
+    co.n = (int)c.ndof;
+    co.by_col = c.nny < c.nnx ? 1 : 0;
+    const int nmin = co.by_col ? c.nny : c.nnx;
+    const int bw = d * (nmin + 2) - 1;  // max |P - Q| of a nonzero
+    co.B = ((bw + 31) / 32) * 32;
+    if (co.B < 32) co.B = 32;
+    co.nb = (co.n + co.B - 1) / co.B;
+    co.blocks = (double*)carve(p, used, 8LL * h.hrows * co.nb * 4 * co.B * co.B);
+  }
+  h.tables = (double*)carve(p, used, 8LL * kMaxLevels * 3 * kTableStride);
+  if (L > 1) {
+    h.keffA = (double*)carve(p, used, 8LL * h.hrows * h.lv[1].nel * NK * NK);
+    if (L > 2) h.keffB = (double*)carve(p, used, 8LL * h.hrows * h.lv[2].nel * NK * NK);
+  }
+  carve(p, used, 256);  // status word
+  h.ws_bytes = used;
+  return used;
+}
+
+// ---- build kernels -----------------------------------------------------------
+
+template <typename TI, typename TO>
+__global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (TO)in[i];
+}
+
+__global__ void copy_rows_kernel(const double* __restrict__ in, long long in_rs,
+                                 double* __restrict__ out, long long n) {
+  const int row = blockIdx.y;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[(size_t)row * n + i] = in[(size_t)row * in_rs + i];
+}
+
+// Coarse fixed flags: the fine flags at the collocated nodes (torch_mg.py:376).
+__global__ void coarse_fixed_kernel(const uint8_t* __restrict__ ff, int fnnx, int kx, int ky,
+                                    uint8_t* __restrict__ cf, int cnnx, int cnny) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= cnnx * cnny) return;
+  const int r = n / cnnx, c = n - r * cnnx;
+  cf[n] = ff[(size_t)(r * ky) * fnnx + c * kx];
+}
+
+// Level-1 element matrices from the fine densities: keff[E] = sum_m rho_m G_m
+// (+ sum_m reaction_m GM_m) (torch_mg.py:357-366).  One thread per (E, i).
+template <int D>
+__global__ void keff_from_density_kernel(const double* __restrict__ rho, long long rho_rs,
+                                         const double* __restrict__ reac, long long r_rs,
+                                         const double* __restrict__ G,
+                                         const double* __restrict__ GM, int fnelx, int kx,
+                                         int ky, int cnelx, int cnel, double* __restrict__ keff) {
+  constexpr int NK = 4 * D;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (t >= (long long)cnel * NK) return;
+  const int E = (int)(t / NK), i = (int)(t - (long long)E * NK);
+  const int R = E / cnelx, C = E - R * cnelx;
+  const double* rr = rho + (size_t)h * rho_rs;
+  double acc[NK], acc2[NK];
+#pragma unroll
+  for (int j = 0; j < NK; ++j) acc[j] = acc2[j] = 0.0;
+  const int nm = kx * ky;
+  for (int m = 0; m < nm; ++m) {
+    const int my = m / kx, mx = m - my * kx;
+    const size_t e = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
+    const double rv = __ldg(rr + e);
+    const double* g = G + ((size_t)m * NK + i) * NK;
+#pragma unroll
+    for (int j = 0; j < NK; ++j) acc[j] = fma(rv, __ldg(g + j), acc[j]);
+    if (reac) {
+      const double av = __ldg(reac + (size_t)h * r_rs + e);
+      const double* gm = GM + ((size_t)m * NK + i) * NK;
+#pragma unroll
+      for (int j = 0; j < NK; ++j) acc2[j] = fma(av, __ldg(gm + j), acc2[j]);
+    }
+  }
+  double* out = keff + (((size_t)h * cnel + E) * NK + i) * NK;
+#pragma unroll
+  for (int j = 0; j < NK; ++j) out[j] = reac ? acc[j] + acc2[j] : acc[j];
+}
+
+// Galerkin product of the level above: keff_c[E] = sum_m S_m^T keff_f[child m] S_m
+// (torch_mg.py:367-370).  One thread per (E, i).
+template <int D>
+__global__ void keff_galerkin_kernel(const double* __restrict__ kf, int fnelx, int fnel,
+                                     const double* __restrict__ S, int kx, int ky, int cnelx,
+                                     int cnel, double* __restrict__ kc) {
+  constexpr int NK = 4 * D;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (t >= (long long)cnel * NK) return;
+  const int E = (int)(t / NK), i = (int)(t - (long long)E * NK);
+  const int R = E / cnelx, C = E - R * cnelx;
+  double out[NK];
+#pragma unroll
+  for (int j = 0; j < NK; ++j) out[j] = 0.0;
+  const int nm = kx * ky;
+  for (int m = 0; m < nm; ++m) {
+    const int my = m / kx, mx = m - my * kx;
+    const size_t e = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
+    const double* K = kf + ((size_t)h * fnel + e) * NK * NK;
+    const double* Sm = S + (size_t)m * NK * NK;
+    double tq[NK];
+#pragma unroll
+    for (int q = 0; q < NK; ++q) tq[q] = 0.0;
+#pragma unroll
+    for (int p = 0; p < NK; ++p) {
+      const double s = __ldg(Sm + p * NK + i);
+      if (s != 0.0) {
+#pragma unroll
+        for (int q = 0; q < NK; ++q) tq[q] = fma(s, __ldg(K + p * NK + q), tq[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NK; ++q) {
+      if (tq[q] == 0.0) continue;
+#pragma unroll
+      for (int j = 0; j < NK; ++j) out[j] = fma(tq[q], __ldg(Sm + q * NK + j), out[j]);
+    }
+  }
+  double* o = kc + (((size_t)h * cnel + E) * NK + i) * NK;
+#pragma unroll
+  for (int j = 0; j < NK; ++j) o[j] = out[j];
+}
+
+// Element-matrix sources for the stencil assembly.
+template <int D>
+struct KeffSource {  // explicit element matrices
+  const double* keff;
+  int nel;
+  STT_DEV double operator()(int h, int e, int p, int q) const {
+    return __ldg(keff + (((size_t)h * nel + e) * (4 * D) + p) * (4 * D) + q);
+  }
+};
+template <int D>
+struct DensitySource {  // rho_e KE (+ reaction_e I / 4), level 0 used as the coarsest
+  const double* rho;
+  long long rho_rs;
+  const double* reac;
+  long long r_rs;
+  KEq<D, double> ke;
+  STT_DEV double operator()(int h, int e, int p, int q) const {
+    double v = __ldg(rho + (size_t)h * rho_rs + e) * ke.v[p * 4 * D + q];
+    if (reac) v += __ldg(reac + (size_t)h * r_rs + e) * (p == q ? 0.25 : 0.0);
+    return v;
+  }
+};
+
+// Symmetric, projected 9-point block stencil from element matrices: block (N, M)
+// sums the (corner N, corner M) blocks of the elements holding both nodes, averaged
+// with the transpose of (M, N) as the reference symmetrises its dense coarse matrix
+// (torch_mg.py:286), with rows and columns of fixed dofs zeroed.
+template <int D, typename Src>
+__global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int nelx, int nely,
+                               double* __restrict__ st) {
+  constexpr int NS = 5 * D * D;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (n >= nnx * nny) return;
+  const long long nnode = (long long)nnx * nny;
+  const int r = n / nnx, c = n - r * nnx;
+  const uint8_t fN = fixed[n];
+  auto elem_ok = [&](int er, int ec) { return er >= 0 && er < nely && ec >= 0 && ec < nelx; };
+  // (blk, neighbour offset, list of (element offset a,b), corner of N, corner of M)
+  double* out = st + (size_t)h * NS * nnode + n;
+#pragma unroll
+  for (int blk = 0; blk < 5; ++blk) {
+    const int dr = (blk == 0 || blk == 1) ? 0 : 1;
+    const int dc = blk == 0 ? 0 : (blk == 1 ? 1 : (blk == 2 ? 0 : (blk == 3 ? 1 : -1)));
+    const int mr = r + dr, mc = c + dc;
+    const bool m_ok = mr >= 0 && mr < nny && mc >= 0 && mc < nnx;
+    const uint8_t fM = m_ok ? fixed[mr * nnx + mc] : 0;
+    double A[D][D], AT[D][D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) A[i][j] = AT[i][j] = 0.0;
+    if (m_ok) {
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          const int er = r - 1 + a, ec = c - 1 + b;
+          if (!elem_ok(er, ec)) continue;
+          // corner of M in this element, if M belongs to it
+          const int ddr = mr - er, ddc = mc - ec;
+          if (ddr < 0 || ddr > 1 || ddc < 0 || ddc > 1) continue;
+          const int kN = corner_of(a, b);
+          const int kM = ddr == 1 ? (ddc == 0 ? 0 : 1) : (ddc == 1 ? 2 : 3);
+          const int e = er * nelx + ec;
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
+              A[i][j] += src(h, e, kN * D + i, kM * D + j);
+              AT[i][j] += src(h, e, kM * D + j, kN * D + i);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        double v = (A[i][j] + AT[i][j]) / 2;
+        if (((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
+        out[(size_t)(blk * D * D + i * D + j) * nnode] = v;
+      }
+  }
+}
+
+// Banded coarse matrix from the coarsest stencil, written into the factor's storage:
+// diagonal blocks in slot 0, sub-diagonal blocks A_{k,k-1} in slot 2.  Fixed dofs get
+// a unit diagonal (torch_mg.py:287-289); padding rows are identity.
+template <int D>
+__global__ void band_assemble_kernel(const double* __restrict__ st, const uint8_t* __restrict__ fixed,
+                                     int nnx, int nny, int by_col, int B, int nb,
+                                     double* __restrict__ blocks, int* __restrict__ status) {
+  constexpr int NS = 5 * D * D;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  const long long nnode = (long long)nnx * nny;
+  double* bh = blocks + (size_t)h * nb * 4 * B * B;
+  if (n >= nnode) {
+    // padding rows (beyond n dofs) get an identity diagonal
+    const long long pad = n - nnode;
+    const long long I = nnode * D + pad;
+    if (pad >= 0 && I < (long long)nb * B) {
+      const int k = (int)(I / B), ii = (int)(I % B);
+      bh[((size_t)k * 4 + 0) * B * B + (size_t)ii * B + ii] = 1.0;
+    }
+    return;
+  }
+  const int r = n / nnx, c = n - r * nnx;
+  auto perm = [&](int rr, int cc, int i) -> long long {
+    const long long node = by_col ? (long long)cc * nny + rr : (long long)rr * nnx + cc;
+    return node * D + i;
+  };
+  auto put = [&](long long I, long long J, double v) {
+    if (I < J) {
+      const long long t = I;
+      I = J;
+      J = t;
+    }
+    const int kI = (int)(I / B), kJ = (int)(J / B);
+    const int ii = (int)(I % B), jj = (int)(J % B);
+    if (kI == kJ)
+      bh[((size_t)kI * 4 + 0) * B * B + (size_t)ii * B + jj] = v;
+    else if (kI == kJ + 1)
+      bh[((size_t)kI * 4 + 2) * B * B + (size_t)ii * B + jj] = v;
+    else if (v != 0.0)
+      atomicOr(status, 2);
+  };
+  const double* sn = st + (size_t)h * NS * nnode + n;
+  const uint8_t fN = fixed[n];
+#pragma unroll
+  for (int blk = 0; blk < 5; ++blk) {
+    const int dr = (blk == 0 || blk == 1) ? 0 : 1;
+    const int dc = blk == 0 ? 0 : (blk == 1 ? 1 : (blk == 2 ? 0 : (blk == 3 ? 1 : -1)));
+    const int mr = r + dr, mc = c + dc;
+    if (mr < 0 || mr >= nny || mc < 0 || mc >= nnx) continue;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        if (blk == 0 && j > i) continue;  // centre block: lower triangle only
+        double v = sn[(size_t)(blk * D * D + i * D + j) * nnode];
+        if (blk == 0 && i == j && ((fN >> i) & 1)) v = 1.0;
+        put(perm(r, c, i), perm(mr, mc, j), v);
+      }
+  }
+}
+
+// Block-banded Cholesky of one hierarchy row's coarse matrix (one CTA):
+//   D_k D_k^T = A_kk - E_k E_k^T,  E_{k+1} = A_{k+1,k} D_k^{-T}.
+// Stores Dinv_k = D_k^{-1} and its transpose, and E_k and its transpose, so that the
+// per-cycle triangular solves are two dense GEMVs per block.
+__global__ void __launch_bounds__(256) band_factor_kernel(double* __restrict__ blocks, int B,
+                                                          int nb, int* __restrict__ status) {
+  extern __shared__ double sm[];
+  const int ld = B + 1;
+  double* A = sm;            // current diagonal block, then its Cholesky factor
+  double* X = A + B * ld;    // D_k^{-1}
+  double* Y = X + B * ld;    // E_k (from the previous step)
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int h = blockIdx.x;
+  double* bh = blocks + (size_t)h * nb * 4 * B * B;
+  __shared__ int bad;
+  if (tid == 0) bad = 0;
+  for (int k = 0; k < nb; ++k) {
+    double* Dk = bh + (size_t)k * 4 * B * B;
+    for (int t = tid; t < B * B; t += nt) {
+      const int i = t / B, j = t % B;
+      const double v = Dk[(size_t)i * B + j];
+      if (j <= i) A[i * ld + j] = v;
+    }
+    __syncthreads();
+    if (k > 0) {
+      for (int t = tid; t < B * B; t += nt) {
+        const int i = t / B, j = t % B;
+        if (j > i) continue;
+        double s = 0.0;
+        for (int l = 0; l < B; ++l) s = fma(Y[i * ld + l], Y[j * ld + l], s);
+        A[i * ld + j] -= s;
+      }
+      __syncthreads();
+    }
+    // unblocked right-looking Cholesky, lower triangle
+    for (int j = 0; j < B; ++j) {
+      if (tid == 0) {
+        const double p = A[j * ld + j];
+        if (!(p > 0.0)) bad = 1;
+        A[j * ld + j] = sqrt(p > 0.0 ? p : 1.0);
+      }
+      __syncthreads();
+      const double piv = A[j * ld + j];
+      for (int i = j + 1 + tid; i < B; i += nt) A[i * ld + j] /= piv;
+      __syncthreads();
+      const int m = B - j - 1;
+      for (int t = tid; t < m * m; t += nt) {
+        const int i = j + 1 + t / m, l = j + 1 + t % m;
+        if (l <= i) A[i * ld + l] = fma(-A[i * ld + j], A[l * ld + j], A[i * ld + l]);
+      }
+      __syncthreads();
+    }
+    // X = A^{-1}, one column per thread
+    for (int c = tid; c < B; c += nt) {
+      for (int i = 0; i < c; ++i) X[i * ld + c] = 0.0;
+      X[c * ld + c] = 1.0 / A[c * ld + c];
+      for (int i = c + 1; i < B; ++i) {
+        double s = 0.0;
+        for (int l = c; l < i; ++l) s = fma(A[i * ld + l], X[l * ld + c], s);
+        X[i * ld + c] = -s / A[i * ld + i];
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < B * B; t += nt) {
+      const int i = t / B, j = t % B;
+      Dk[(size_t)i * B + j] = X[i * ld + j];                        // Dinv
+      Dk[(size_t)B * B + (size_t)i * B + j] = X[j * ld + i];        // Dinv^T
+    }
+    if (k + 1 < nb) {
+      double* Dn = bh + (size_t)(k + 1) * 4 * B * B;
+      // A_{k+1,k} into A's storage (the factor is no longer needed)
+      for (int t = tid; t < B * B; t += nt) {
+        const int i = t / B, j = t % B;
+        A[i * ld + j] = Dn[(size_t)2 * B * B + (size_t)i * B + j];
+      }
+      __syncthreads();
+      // E = A_{k+1,k} X^T: E[i][j] = sum_{l <= j} A[i][l] X[j][l]
+      for (int t = tid; t < B * B; t += nt) {
+        const int i = t / B, j = t % B;
+        double s = 0.0;
+        for (int l = 0; l <= j; ++l) s = fma(A[i * ld + l], X[j * ld + l], s);
+        Y[i * ld + j] = s;
+      }
+      __syncthreads();
+      for (int t = tid; t < B * B; t += nt) {
+        const int i = t / B, j = t % B;
+        Dn[(size_t)2 * B * B + (size_t)i * B + j] = Y[i * ld + j];  // E
+        Dn[(size_t)3 * B * B + (size_t)i * B + j] = Y[j * ld + i];  // E^T
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0 && bad) atomicOr(status, 1);
+}
+
+}  // namespace stt
+
+using namespace stt;
+
+static int grid1(long long n, int bs = 256) {
+  long long g = (n + bs - 1) / bs;
+  if (g > 1 << 30) g = 1 << 30;
+  return (int)(g < 1 ? 1 : g);
+}
+
+extern "C" long long stt_hier_workspace_bytes(int d, int nelx, int nely, int hrows,
+                                              int max_coarse_elements, int precision) {
+  if ((d != 1 && d != 2) || nelx <= 0 || nely <= 0 || hrows <= 0) return -1;
+  stt_hier_impl h{};
+  h.d = d;
+  h.nelx = nelx;
+  h.nely = nely;
+  h.hrows = hrows;
+  h.precision = precision;
+  h.mce = max_coarse_elements;
+  return plan_hierarchy(h, nullptr);
+}
+
+template <int D>
+static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const double* reaction,
+                        long long r_rs, const uint8_t* fixed, cudaStream_t st) {
+  constexpr int NK = 4 * D, NS = 5 * D * D;
+  const int H = h->hrows;
+  LevelDesc& l0 = h->lv[0];
+  // level 0: copies of the densities, the lumped reaction diagonal, the flags
+  copy_rows_kernel<<<dim3(grid1(l0.nel), H), 256, 0, st>>>(rho, rho_rs, l0.rho64, l0.nel);
+  if (reaction) {
+    STT_TRY(stt_lumped_reaction(D, h->nelx, h->nely, H, reaction, r_rs, l0.rdiag64, l0.ndof,
+                                (stt_stream_t)st));
+  } else {
+    STT_TRY(check_cuda(cudaMemsetAsync(l0.rdiag64, 0, 8 * H * l0.ndof, st), "memset"));
+  }
+  if (fixed)
+    STT_TRY(check_cuda(cudaMemcpyAsync(l0.fixed, fixed, l0.nnode, cudaMemcpyDeviceToDevice, st), "copy fixed"));
+  else
+    STT_TRY(check_cuda(cudaMemsetAsync(l0.fixed, 0, l0.nnode, st), "memset"));
+  if (h->precision == STT_FP32) {
+    convert_kernel<double, float><<<grid1(H * l0.nel), 256, 0, st>>>(l0.rho64, l0.rho32, H * l0.nel);
+    convert_kernel<double, float><<<grid1(H * l0.ndof), 256, 0, st>>>(l0.rdiag64, l0.rdiag32, H * l0.ndof);
+  }
+  STT_TRY(check_launch("level0 copies"));
+
+  // tables: per transition S, and G/GM for the first
+  std::vector<double> tab((size_t)kMaxLevels * 3 * kTableStride, 0.0);
+  for (int l = 0; l + 1 < h->nlevels; ++l) {
+    double* S = &tab[(size_t)l * 3 * kTableStride];
+    child_interp(h->lv[l].kx, h->lv[l].ky, D, S);
+    if (l == 0) {
+      double ME[64] = {0};
+      for (int i = 0; i < NK; ++i) ME[i * NK + i] = 0.25;
+      galerkin_table(S, h->KE, h->lv[0].kx * h->lv[0].ky, NK, S + kTableStride);
+      galerkin_table(S, ME, h->lv[0].kx * h->lv[0].ky, NK, S + 2 * kTableStride);
+    }
+  }
+  STT_TRY(check_cuda(cudaMemcpyAsync(h->tables, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st), "tables"));
+
+  const double* kprev = nullptr;
+  for (int l = 1; l < h->nlevels; ++l) {
+    const LevelDesc& f = h->lv[l - 1];
+    LevelDesc& c = h->lv[l];
+    const double* S = h->tables + (size_t)(l - 1) * 3 * kTableStride;
+    double* kc = (l % 2 == 1) ? h->keffA : h->keffB;
+    const dim3 g(grid1(c.nel * NK), H);
+    if (l == 1)
+      keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.nel, reaction, r_rs, S + kTableStride,
+                                                     S + 2 * kTableStride, f.nelx, f.kx, f.ky, c.nelx,
+                                                     (int)c.nel, kc);
+    else
+      keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
+                                                 (int)c.nel, kc);
+    coarse_fixed_kernel<<<grid1(c.nnode), 256, 0, st>>>(f.fixed, f.nnx, f.kx, f.ky, c.fixed, c.nnx, c.nny);
+    stencil_kernel<D, KeffSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
+        KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64);
+    if (h->precision == STT_FP32)
+      convert_kernel<double, float><<<grid1(H * NS * c.nnode), 256, 0, st>>>(c.st64, c.st32, H * NS * c.nnode);
+    STT_TRY(check_launch("galerkin level"));
+    kprev = kc;
+  }
+  LevelDesc& cl = h->lv[h->nlevels - 1];
+  if (h->nlevels == 1) {
+    KEq<D, double> ke;
+    for (int i = 0; i < NK * NK; ++i) ke.v[i] = h->KE[i];
+    stencil_kernel<D, DensitySource<D>><<<dim3(grid1(cl.nnode), H), 256, 0, st>>>(
+        DensitySource<D>{l0.rho64, l0.nel, reaction, r_rs, ke}, cl.fixed, cl.nelx, cl.nely, cl.st64);
+  }
+  return STT_OK;
+}
+
+template <int D>
+static int build_coarse(stt_hier* h, cudaStream_t st) {
+  CoarseDesc& co = h->co;
+  const LevelDesc& cl = h->lv[h->nlevels - 1];
+  const int H = h->hrows;
+  const long long per = (long long)co.nb * 4 * co.B * co.B;
+  STT_TRY(check_cuda(cudaMemsetAsync(co.blocks, 0, 8 * H * per, st), "memset coarse"));
+  const long long threads = cl.nnode + ((long long)co.nb * co.B - cl.ndof);
+  band_assemble_kernel<D><<<dim3(grid1(threads), H), 256, 0, st>>>(
+      cl.st64, cl.fixed, cl.nnx, cl.nny, co.by_col, co.B, co.nb, co.blocks, h->status);
+  STT_TRY(check_launch("band assemble"));
+  const size_t smem = (size_t)3 * co.B * (co.B + 1) * sizeof(double);
+  STT_TRY(check_cuda(cudaFuncSetAttribute(band_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr"));
+  band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
+  return check_launch("band factor");
+}
+
+extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_bytes, int d, int nelx,
+                               int nely, int hrows, const double* rho, long long rho_rs,
+                               const double* reaction, long long r_rs, const uint8_t* fixed,
+                               const double* KE, int max_coarse_elements, int precision,
+                               stt_stream_t stream) {
+  if (!out || !workspace || !rho || !KE || (d != 1 && d != 2) || nelx <= 0 || nely <= 0 ||
+      hrows <= 0 || hrows > 65535 || (precision != STT_FP64 && precision != STT_FP32))
+    return set_error(STT_ERR_INVALID, "stt_hier_create: bad arguments");
+  if (((uintptr_t)workspace & 255) != 0)
+    return set_error(STT_ERR_INVALID, "stt_hier_create: workspace must be 256-byte aligned");
+  stt_hier* h = new stt_hier();
+  std::memset((void*)h, 0, sizeof(stt_hier));
+  h->d = d;
+  h->nelx = nelx;
+  h->nely = nely;
+  h->hrows = hrows;
+  h->precision = precision;
+  h->mce = max_coarse_elements;
+  for (int i = 0; i < 16 * d * d; ++i) h->KE[i] = KE[i];
+  const long long need = plan_hierarchy(*h, nullptr);
+  if (ws_bytes < need) {
+    delete h;
+    return set_error(STT_ERR_WORKSPACE, "stt_hier_create: workspace too small");
+  }
+  plan_hierarchy(*h, (char*)workspace);
+  h->status = (int*)((char*)workspace + need - 256);
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = check_cuda(cudaMemsetAsync(h->status, 0, 256, st), "memset status");
+  if (rc == STT_OK) rc = d == 2 ? build_levels<2>(h, rho, rho_rs, reaction, r_rs, fixed, st)
+                                : build_levels<1>(h, rho, rho_rs, reaction, r_rs, fixed, st);
+  if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, st) : build_coarse<1>(h, st);
+  if (rc == STT_OK) {
+    int s = 0;
+    rc = check_cuda(cudaMemcpyAsync(&s, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy");
+    if (rc == STT_OK) rc = check_cuda(cudaStreamSynchronize(st), "hierarchy build");
+    if (rc == STT_OK && (s & 1))
+      rc = set_error(STT_ERR_INVALID, "coarse operator is not positive definite (Cholesky pivot <= 0)");
+    if (rc == STT_OK && (s & 2))
+      rc = set_error(STT_ERR_INVALID, "coarse operator exceeds its planned band");
+  }
+  if (rc != STT_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return STT_OK;
+}
+
+extern "C" int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier** out) {
+  if (!h || !out) return set_error(STT_ERR_INVALID, "stt_hier_select: null");
+  stt_hier* v = new stt_hier(*h);
+  v->row_map = row_map;
+  *out = v;
+  return STT_OK;
+}
+
+extern "C" int stt_hier_destroy(stt_hier* h) {
+  delete h;
+  return STT_OK;
+}
+
+extern "C" int stt_hier_info(const stt_hier* h, int* nlevels, int* dims, int max_levels) {
+  if (!h || !nlevels) return set_error(STT_ERR_INVALID, "stt_hier_info: null");
+  *nlevels = h->nlevels;
+  if (dims)
+    for (int l = 0; l < h->nlevels && l < max_levels; ++l) {
+      dims[4 * l + 0] = h->lv[l].nelx;
+      dims[4 * l + 1] = h->lv[l].nely;
+      dims[4 * l + 2] = h->lv[l].kx;
+      dims[4 * l + 3] = h->lv[l].ky;
+    }
+  return STT_OK;
+}
+
+template <int D>
+__global__ void stencil_diag_kernel(const double* __restrict__ st, const uint8_t* __restrict__ fixed,
+                                    long long nnode, double* __restrict__ out) {
+  constexpr int NS = 5 * D * D;
+  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (n >= nnode) return;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double v = st[((size_t)h * NS + i * D + i) * nnode + n];
+    if ((fixed[n] >> i) & 1) v = 1.0;
+    out[((size_t)h * nnode + n) * D + i] = v;
+  }
+}
+
+extern "C" int stt_hier_level_diag(const stt_hier* h, int level, double* out, stt_stream_t stream) {
+  if (!h || !out || level < 0 || level >= h->nlevels) return set_error(STT_ERR_INVALID, "stt_hier_level_diag: bad level");
+  const LevelDesc& lv = h->lv[level];
+  cudaStream_t st = (cudaStream_t)stream;
+  if (level == 0)
+    return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.nel, lv.rdiag64, lv.ndof,
+                       lv.fixed, out, lv.ndof, h->KE, stream);
+  if (h->d == 2)
+    stencil_diag_kernel<2><<<dim3(grid1(lv.nnode), h->hrows), 256, 0, st>>>(lv.st64, lv.fixed, lv.nnode, out);
+  else
+    stencil_diag_kernel<1><<<dim3(grid1(lv.nnode), h->hrows), 256, 0, st>>>(lv.st64, lv.fixed, lv.nnode, out);
+  return check_launch("stencil diag");
+}
+
+extern "C" int stt_hier_level_fixed(const stt_hier* h, int level, uint8_t* out, stt_stream_t stream) {
+  if (!h || !out || level < 0 || level >= h->nlevels) return set_error(STT_ERR_INVALID, "stt_hier_level_fixed: bad level");
+  return check_cuda(cudaMemcpyAsync(out, h->lv[level].fixed, h->lv[level].nnode, cudaMemcpyDeviceToDevice,
+                                    (cudaStream_t)stream), "copy fixed");
+}

@@ -1,0 +1,329 @@
+// Element terms of the adjoint (FemSolve.backward, sttopt/torch_solve.py:144-152), the
+// element strain energy (compliance._element_strain_energy, sttopt/compliance.py:49-59),
+// the space-time stage glue with a hard stage threshold (compliance._gravity_load and
+// batched_whole_and_gravity_compliance, sttopt/compliance.py:137-161,198-253; gravity
+// load matrix sttopt/gravity.py:15-36), the virtual-heat element means
+// (sttopt/virtual_heat.py:162-166) and the PCG vector steps for arbitrary operators.
+#include <algorithm>
+
+#include "common.cuh"
+#include "errors.h"
+
+namespace stt {
+
+static int grid1(long long n, int bs = 256) {
+  long long g = (n + bs - 1) / bs;
+  if (g > (1 << 30)) g = 1 << 30;
+  return (int)(g < 1 ? 1 : g);
+}
+
+template <int D>
+struct KEd {
+  double v[16 * D * D];
+};
+
+// Element e's dofs in the reference's local order (BL, BR, TR, TL; d interleaved).
+template <int D>
+STT_DEV void element_dofs(int e, int nelx, long long (&dofs)[4 * D]) {
+  const int er = e / nelx, ec = e - er * nelx;
+  const int nnx = nelx + 1;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long node = (long long)(er + corner_dr(q)) * nnx + ec + corner_dc(q);
+#pragma unroll
+    for (int i = 0; i < D; ++i) dofs[q * D + i] = node * D + i;
+  }
+}
+
+template <int D>
+__global__ void element_sens_kernel(const double* __restrict__ U, long long U_rs,
+                                    const double* __restrict__ lam, long long lam_rs,
+                                    double* __restrict__ ce, double* __restrict__ gd,
+                                    double* __restrict__ gr, long long e_rs, int nelx, int nel,
+                                    KEd<D> ke) {
+  constexpr int NK = 4 * D;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (e >= nel) return;
+  long long dofs[NK];
+  element_dofs<D>(e, nelx, dofs);
+  double u[NK], l[NK];
+  const double* Us = U + (size_t)s * U_rs;
+#pragma unroll
+  for (int k = 0; k < NK; ++k) u[k] = __ldg(Us + dofs[k]);
+  if (lam) {
+    const double* ls = lam + (size_t)s * lam_rs;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) l[k] = __ldg(ls + dofs[k]);
+  }
+  // (Ue @ KE)[col] and (lam_e @ KE)[col]
+  double c = 0.0, g = 0.0, q = 0.0;
+#pragma unroll
+  for (int col = 0; col < NK; ++col) {
+    double uk = 0.0, lk = 0.0;
+#pragma unroll
+    for (int row = 0; row < NK; ++row) {
+      uk = fma(u[row], ke.v[row * NK + col], uk);
+      if (lam) lk = fma(l[row], ke.v[row * NK + col], lk);
+    }
+    c = fma(uk, u[col], c);
+    if (lam) {
+      g = fma(lk, u[col], g);
+      q = fma(l[col], u[col], q);
+    }
+  }
+  const size_t o = (size_t)s * e_rs + e;
+  if (ce) ce[o] = c;
+  if (gd) gd[o] = -g;
+  if (gr) gr[o] = -q / 4;
+}
+
+__global__ void stage_membership_kernel(const double* __restrict__ t, int nel, int n_stage,
+                                        uint8_t* __restrict__ member) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  const double te = t[e];
+  for (int s = 0; s < n_stage; ++s) member[(size_t)s * nel + e] = te <= (double)(s + 1) / n_stage ? 1 : 0;
+}
+
+STT_DEV double simp_pow(double x, double p) { return p == 3.0 ? x * x * x : pow(x, p); }
+
+// One thread per (node, stage): density rows of the elements handled by this node's
+// top-left role, and the y load of the node.
+__global__ void stage_rho_kernel(const double* __restrict__ x, const uint8_t* __restrict__ member,
+                                 int nel, int n_stage, double Emin, double Emax, double penal,
+                                 double* __restrict__ rho) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (e >= nel) return;
+  const double xt = x[e] * (double)member[(size_t)s * nel + e];
+  rho[(size_t)s * nel + e] = Emin + simp_pow(xt, penal) * (Emax - Emin);
+}
+
+__global__ void stage_load_kernel(const double* __restrict__ x, const uint8_t* __restrict__ member,
+                                  int nelx, int nely, const uint8_t* __restrict__ fixed,
+                                  double* __restrict__ F) {
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (n >= nnx * nny) return;
+  const int r = n / nnx, c = n - r * nnx;
+  const int nel = nelx * nely;
+  const double fe4 = (1.0 / ((double)nelx * nely)) / 4;
+  // elements around the node in ascending element index (the CSR column order)
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int er = r - 1 + a, ec = c - 1 + b;
+      if (er < 0 || er >= nely || ec < 0 || ec >= nelx) continue;
+      const int e = er * nelx + ec;
+      const double xt = x[e] * (double)member[(size_t)s * nel + e];
+      acc += fe4 * xt;
+    }
+  double* Fs = F + (size_t)s * 2 * nnx * nny;
+  const uint8_t fl = fixed ? fixed[n] : 0;
+  Fs[2 * (size_t)n] = 0.0;
+  Fs[2 * (size_t)n + 1] = (fl & 2) ? 0.0 : -acc;
+}
+
+__global__ void stage_gradient_kernel(const double* __restrict__ x, const uint8_t* __restrict__ member,
+                                      const double* __restrict__ ce, const double* __restrict__ gd,
+                                      const double* __restrict__ gF, int nelx, int nely, int n_stage,
+                                      double Emin, double Emax, double penal, double* __restrict__ grad) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nel = nelx * nely;
+  if (e >= nel) return;
+  const int er = e / nelx, ec = e - er * nelx, nnx = nelx + 1;
+  const long long nnode = (long long)nnx * (nely + 1);
+  const double fe4 = (1.0 / ((double)nelx * nely)) / 4;
+  double acc = 0.0;
+  for (int s = 0; s < n_stage; ++s) {
+    if (!member[(size_t)s * nel + e]) continue;
+    const double xt = x[e];
+    const double dsimp = penal * (penal == 3.0 ? xt * xt : pow(xt, penal - 1)) * (Emax - Emin);
+    const size_t o = (size_t)s * nel + e;
+    double load = 0.0;
+    const double* g = gF + (size_t)s * 2 * nnode;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long node = (long long)(er + corner_dr(q)) * nnx + ec + corner_dc(q);
+      load += g[2 * node + 1];
+    }
+    acc += (ce[o] + gd[o]) * dsimp - fe4 * load;
+  }
+  grad[e] += acc;
+}
+
+__global__ void heat_means_kernel(const double* __restrict__ T, int nelx, int nel, double* __restrict__ te) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  long long dofs[4];
+  element_dofs<1>(e, nelx, dofs);
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) s += 1.0 - T[dofs[q]];
+  te[e] = s / 4;
+}
+
+__global__ void heat_adjoint_load_kernel(const double* __restrict__ w, double scale, int nelx, int nely,
+                                         double* __restrict__ g) {
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nnx * nny) return;
+  const int r = n / nnx, c = n - r * nnx;
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int er = r - 1 + a, ec = c - 1 + b;
+      if (er < 0 || er >= nely || ec < 0 || ec >= nelx) continue;
+      acc += (w[er * nelx + ec] / scale) / 4;
+    }
+  g[n] = -acc;
+}
+
+// ---- PCG vector steps (arbitrary operator path) -----------------------------------
+
+__global__ void vec_dots_kernel(long long n, const double* __restrict__ a0, const double* __restrict__ b0,
+                                const double* __restrict__ a1, const double* __restrict__ b1,
+                                const double* __restrict__ a2, const double* __restrict__ b2,
+                                long long rs, int k, double* __restrict__ dots) {
+  // one block per row, deterministic
+  __shared__ double scratch[8];
+  const int s = blockIdx.x;
+  const double* A[3] = {a0, a1, a2};
+  const double* Bv[3] = {b0, b1, b2};
+  for (int j = 0; j < k; ++j) {
+    double acc = 0.0;
+    const double* a = A[j] + (size_t)s * rs;
+    const double* b = Bv[j] + (size_t)s * rs;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc = fma(a[i], b[i], acc);
+    acc = block_sum<256>(acc, scratch);
+    if (threadIdx.x == 0) dots[(size_t)s * k + j] = acc;
+  }
+}
+
+__global__ void vec_cg_update_kernel(long long n, const double* __restrict__ alpha, double* __restrict__ x,
+                                     double* __restrict__ r, const double* __restrict__ p,
+                                     const double* __restrict__ Ap, long long rs, double* __restrict__ rr) {
+  __shared__ double scratch[8];
+  const int s = blockIdx.x;
+  const double a = alpha[s];
+  double acc = 0.0;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    const size_t o = (size_t)s * rs + i;
+    x[o] = x[o] + a * p[o];
+    const double rv = r[o] - a * Ap[o];
+    r[o] = rv;
+    acc = fma(rv, rv, acc);
+  }
+  acc = block_sum<256>(acc, scratch);
+  if (threadIdx.x == 0) rr[s] = acc;
+}
+
+__global__ void vec_xpay_kernel(long long n, const double* __restrict__ z, const double* __restrict__ beta,
+                                double* __restrict__ p, long long rs) {
+  const int s = blockIdx.y;
+  const double b = beta[s];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const size_t o = (size_t)s * rs + i;
+    p[o] = p[o] * b + z[o];
+  }
+}
+
+}  // namespace stt
+
+using namespace stt;
+
+extern "C" int stt_element_sens(int d, int nelx, int nely, int nrows, const double* U, long long U_rs,
+                                const double* lam, long long lam_rs, const double* KE, double* ce,
+                                double* gdens, double* greac, long long e_rs, stt_stream_t stream) {
+  if (!U || !KE || nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || ((gdens || greac) && !lam))
+    return set_error(STT_ERR_INVALID, "stt_element_sens: bad arguments");
+  const int nel = nelx * nely;
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid(grid1(nel), nrows);
+  if (d == 2) {
+    KEd<2> k;
+    for (int i = 0; i < 64; ++i) k.v[i] = KE[i];
+    element_sens_kernel<2><<<grid, 256, 0, st>>>(U, U_rs, lam, lam_rs, ce, gdens, greac, e_rs, nelx, nel, k);
+  } else if (d == 1) {
+    KEd<1> k;
+    for (int i = 0; i < 16; ++i) k.v[i] = KE[i];
+    element_sens_kernel<1><<<grid, 256, 0, st>>>(U, U_rs, lam, lam_rs, ce, gdens, greac, e_rs, nelx, nel, k);
+  } else {
+    return set_error(STT_ERR_INVALID, "stt_element_sens: d must be 1 or 2");
+  }
+  return check_launch("element_sens");
+}
+
+extern "C" int stt_stage_membership(int nel, int n_stage, const double* tPhys, uint8_t* member,
+                                    stt_stream_t stream) {
+  if (nel <= 0 || n_stage <= 0 || !tPhys || !member) return set_error(STT_ERR_INVALID, "stt_stage_membership: bad arguments");
+  stage_membership_kernel<<<grid1(nel), 256, 0, (cudaStream_t)stream>>>(tPhys, nel, n_stage, member);
+  return check_launch("stage_membership");
+}
+
+extern "C" int stt_stage_rows(int nelx, int nely, int n_stage, const double* x, const uint8_t* member,
+                              double Emin, double Emax, double penal, const uint8_t* fixed, double* rho,
+                              double* F, stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || n_stage <= 0 || n_stage > 65535 || !x || !member)
+    return set_error(STT_ERR_INVALID, "stt_stage_rows: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nel = nelx * nely, nnode = (nelx + 1) * (nely + 1);
+  if (rho) stage_rho_kernel<<<dim3(grid1(nel), n_stage), 256, 0, st>>>(x, member, nel, n_stage, Emin, Emax, penal, rho);
+  if (F) stage_load_kernel<<<dim3(grid1(nnode), n_stage), 256, 0, st>>>(x, member, nelx, nely, fixed, F);
+  return check_launch("stage_rows");
+}
+
+extern "C" int stt_stage_gradient(int nelx, int nely, int n_stage, const double* x, const uint8_t* member,
+                                  const double* ce, const double* gdens, const double* gF, double Emin,
+                                  double Emax, double penal, double* grad, stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || n_stage <= 0 || !x || !member || !ce || !gdens || !gF || !grad)
+    return set_error(STT_ERR_INVALID, "stt_stage_gradient: bad arguments");
+  stage_gradient_kernel<<<grid1(nelx * nely), 256, 0, (cudaStream_t)stream>>>(
+      x, member, ce, gdens, gF, nelx, nely, n_stage, Emin, Emax, penal, grad);
+  return check_launch("stage_gradient");
+}
+
+extern "C" int stt_heat_element_means(int nelx, int nely, const double* T, double* t_e, stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || !T || !t_e) return set_error(STT_ERR_INVALID, "stt_heat_element_means: bad arguments");
+  heat_means_kernel<<<grid1(nelx * nely), 256, 0, (cudaStream_t)stream>>>(T, nelx, nelx * nely, t_e);
+  return check_launch("heat_means");
+}
+
+extern "C" int stt_heat_adjoint_load(int nelx, int nely, const double* w, double scale, double* g,
+                                     stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || !w || !g) return set_error(STT_ERR_INVALID, "stt_heat_adjoint_load: bad arguments");
+  heat_adjoint_load_kernel<<<grid1((nelx + 1) * (nely + 1)), 256, 0, (cudaStream_t)stream>>>(w, scale, nelx, nely, g);
+  return check_launch("heat_adjoint_load");
+}
+
+extern "C" int stt_vec_dots(int nrows, long long n, const double* a0, const double* b0, const double* a1,
+                            const double* b1, const double* a2, const double* b2, long long rs, double* dots,
+                            stt_stream_t stream) {
+  if (nrows <= 0 || n <= 0 || !a0 || !b0 || !dots) return set_error(STT_ERR_INVALID, "stt_vec_dots: bad arguments");
+  const int k = (a1 && b1) ? ((a2 && b2) ? 3 : 2) : 1;
+  vec_dots_kernel<<<nrows, 256, 0, (cudaStream_t)stream>>>(n, a0, b0, a1, b1, a2, b2, rs, k, dots);
+  return check_launch("vec_dots");
+}
+
+extern "C" int stt_vec_cg_update(int nrows, long long n, const double* alpha, double* x, double* r,
+                                 const double* p, const double* Ap, long long rs, double* rr,
+                                 stt_stream_t stream) {
+  if (nrows <= 0 || n <= 0 || !alpha || !x || !r || !p || !Ap || !rr)
+    return set_error(STT_ERR_INVALID, "stt_vec_cg_update: bad arguments");
+  vec_cg_update_kernel<<<nrows, 256, 0, (cudaStream_t)stream>>>(n, alpha, x, r, p, Ap, rs, rr);
+  return check_launch("vec_cg_update");
+}
+
+extern "C" int stt_vec_xpay(int nrows, long long n, const double* z, const double* beta, double* p,
+                            long long rs, stt_stream_t stream) {
+  if (nrows <= 0 || n <= 0 || !z || !beta || !p) return set_error(STT_ERR_INVALID, "stt_vec_xpay: bad arguments");
+  vec_xpay_kernel<<<dim3(std::min<long long>((n + 255) / 256, 1024), nrows), 256, 0, (cudaStream_t)stream>>>(n, z, beta, p, rs);
+  return check_launch("vec_xpay");
+}

@@ -1,0 +1,606 @@
+// V-cycle driver and the device-resident multigrid-preconditioned CG.
+//
+// The PCG recurrence is the reference's (torch_fem.pcg, sttopt/torch_fem.py:201-343):
+// per-row alpha/beta with safe_div, convergence on ||r|| / ||b|| checked before the
+// first iteration and after every update.  Converged rows stop (every kernel skips
+// rows whose device `active` flag is clear), which is the reference's row retirement
+// without the compaction copies; the host reads the row flags every few iterations
+// instead of syncing on every one.  Reductions are deterministic (block partials
+// summed in block order by the last block).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "errors.h"
+#include "hier.h"
+#include "mg.cuh"
+
+namespace stt {
+
+constexpr int kEwThreads = 256;
+
+static int grid1(long long n, int bs = 256) {
+  long long g = (n + bs - 1) / bs;
+  if (g > (1 << 30)) g = 1 << 30;
+  return (int)(g < 1 ? 1 : g);
+}
+
+static int ew_blocks(long long n) {
+  long long g = (n + kEwThreads * 4 - 1) / (kEwThreads * 4);
+  return (int)std::min<long long>(std::max<long long>(g, 1), 2048);
+}
+
+static dim3 tile_grid(int nelx, int nely, int rows) {
+  return dim3((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, rows);
+}
+
+// ---- workspace plan ---------------------------------------------------------------
+
+struct SolveWS {
+  RowState* rs;
+  double* partials;
+  unsigned* counters;
+  double *r, *p, *Ap;          // FP64 [nrows][ndof0]
+  void *z, *zold, *b0;         // cycle precision [nrows][ndof0]
+  void* x[kMaxLevels];         // per level [nrows][ndof_l]
+  void* t[kMaxLevels];
+  void* b[kMaxLevels];
+  void* acc[kMaxLevels];       // gamma > 1 only
+  void* rhs2[kMaxLevels];
+  double* cscratch;            // [nrows][nb * B]
+  int nblk_max;
+  long long bytes;
+};
+
+static char* carve(char* base, long long& used, long long bytes) {
+  const long long a = (bytes + 255) & ~255LL;
+  char* r = base ? base + used : nullptr;
+  used += a;
+  return r;
+}
+
+static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base, SolveWS& w) {
+  std::memset(&w, 0, sizeof(w));
+  long long used = 0;
+  const int es = h->precision == STT_FP32 ? 4 : 8;
+  const LevelDesc& l0 = h->lv[0];
+  const dim3 tg = tile_grid(h->nelx, h->nely, 1);
+  w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
+  w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
+  w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
+  w.counters = (unsigned*)carve(base, used, 4LL * nrows);
+  w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  w.Ap = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  w.z = carve(base, used, (long long)es * nrows * l0.ndof);
+  w.zold = carve(base, used, (long long)es * nrows * l0.ndof);
+  if (h->precision == STT_FP32) w.b0 = carve(base, used, 4LL * nrows * l0.ndof);
+  for (int l = 0; l < h->nlevels; ++l) {
+    const long long nd = h->lv[l].ndof;
+    w.x[l] = carve(base, used, (long long)es * nrows * nd);
+    w.t[l] = carve(base, used, (long long)es * nrows * nd);
+    if (l > 0) w.b[l] = carve(base, used, (long long)es * nrows * nd);
+    if (gamma > 1 && l > 0) {
+      w.acc[l] = carve(base, used, (long long)es * nrows * nd);
+      w.rhs2[l] = carve(base, used, (long long)es * nrows * nd);
+    }
+  }
+  w.cscratch = (double*)carve(base, used, 8LL * nrows * h->co.nb * h->co.B);
+  w.bytes = used;
+  return used;
+}
+
+// ---- V-cycle ---------------------------------------------------------------------
+
+template <int D, typename T>
+struct Cycle {
+  const stt_hier* h;
+  SolveWS& w;
+  int nrows;
+  T omega;
+  int n_smooth, gamma;
+  const RowState* rst;
+  cudaStream_t st;
+  KEq<D, T> ke;
+
+  T* X(int l) const { return (T*)w.x[l]; }
+  T* Tt(int l) const { return (T*)w.t[l]; }
+
+  const T* rho0() const {
+    if constexpr (sizeof(T) == 4) return (const T*)h->lv[0].rho32;
+    else return (const T*)h->lv[0].rho64;
+  }
+  const T* rdiag0() const {
+    if constexpr (sizeof(T) == 4) return (const T*)h->lv[0].rdiag32;
+    else return (const T*)h->lv[0].rdiag64;
+  }
+  const T* stl(int l) const {
+    if constexpr (sizeof(T) == 4) return (const T*)h->lv[l].st32;
+    else return (const T*)h->lv[l].st64;
+  }
+
+  // One smoother / residual / apply pass at level l: out = op(x, b).
+  template <int MODE>
+  void pass(int l, const T* x, long long x_rs, const T* b, long long b_rs, T* out, long long o_rs) {
+    const LevelDesc& lv = h->lv[l];
+    if (l == 0) {
+      l0_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
+          x, x_rs, b, b_rs, out, o_rs, rho0(), lv.nel, rdiag0(), lv.ndof, lv.fixed, h->row_map,
+          h->hrows, rst, lv.nelx, lv.nely, omega, ke);
+    } else {
+      st_sweep_kernel<D, T, MODE><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
+          x, b, out, lv.ndof, stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega);
+    }
+  }
+
+  void coarse(int l, const T* b, T* x) {
+    const LevelDesc& lv = h->lv[l];
+    const CoarseDesc& co = h->co;
+    coarse_solve_kernel<D, T><<<nrows, 256, 2 * co.B * sizeof(double), st>>>(
+        b, x, lv.ndof, co.blocks, co.B, co.nb, co.by_col, lv.nnx, lv.nny, lv.fixed, w.cscratch,
+        h->row_map, h->hrows, rst);
+  }
+
+  // Solves level l approximately for right-hand side b (row stride b_rs); returns the
+  // buffer holding the result (row stride ndof_l).
+  T* cycle(int l, const T* b, long long b_rs) {
+    const LevelDesc& lv = h->lv[l];
+    const long long nd = lv.ndof;
+    if (l == h->nlevels - 1) {
+      // the coarse solve reads b with the level's own row stride
+      const T* bb = b;
+      if (b_rs != nd) {
+        rows_convert_kernel<T, T><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(b, b_rs, Tt(l), nd, nd, rst);
+        bb = Tt(l);
+      }
+      coarse(l, bb, X(l));
+      return X(l);
+    }
+    T* xa = X(l);
+    T* xb = Tt(l);
+    pass<SW_FIRST>(l, nullptr, nd, b, b_rs, xa, nd);
+    for (int k = 1; k < n_smooth; ++k) {
+      pass<SW_SWEEP>(l, xa, nd, b, b_rs, xb, nd);
+      std::swap(xa, xb);
+    }
+    // residual into xb, restricted into b_{l+1}
+    pass<SW_RESID>(l, xa, nd, b, b_rs, xb, nd);
+    const LevelDesc& cl = h->lv[l + 1];
+    T* bc = (T*)w.b[l + 1];
+    restrict_kernel<D, T><<<dim3(grid1(cl.nnode), nrows), 256, 0, st>>>(
+        xb, nd, lv.nnx, bc, cl.ndof, cl.nnx, cl.nny, lv.kx, lv.ky, cl.fixed, rst);
+    T* ec = cycle(l + 1, bc, cl.ndof);
+    if (gamma > 1) {
+      T* acc = (T*)w.acc[l + 1];
+      T* rhs = (T*)w.rhs2[l + 1];
+      rows_convert_kernel<T, T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(ec, cl.ndof, acc, cl.ndof, cl.ndof, rst);
+      for (int g = 1; g < gamma; ++g) {
+        // rhs = b_c - A_c acc
+        pass<SW_RESID>(l + 1, acc, cl.ndof, bc, cl.ndof, rhs, cl.ndof);
+        T* e2 = cycle(l + 1, rhs, cl.ndof);
+        rows_axpy_kernel<T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(e2, acc, cl.ndof, cl.ndof, rst);
+      }
+      ec = acc;
+    }
+    prolong_add_kernel<D, T><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
+        ec, cl.ndof, cl.nnx, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
+    for (int k = 0; k < n_smooth; ++k) {
+      pass<SW_SWEEP>(l, xa, nd, b, b_rs, xb, nd);
+      std::swap(xa, xb);
+    }
+    return xa;
+  }
+};
+
+// ---- PCG kernels (FP64 outer iteration) -----------------------------------------
+
+struct PcgParams {
+  double rtol;
+  int it;
+  int flexible;
+};
+
+// r = b - A x (or r = b when x is null), reductions ||r||^2 and ||b||^2.
+// replace: keep bnorm and only re-test convergence (true-residual replacement).
+template <int D>
+__global__ void __launch_bounds__(kNT) pcg_init_kernel(
+    const double* __restrict__ b, long long b_rs, const double* __restrict__ x, long long x_rs,
+    double* __restrict__ r, long long r_rs, const double* __restrict__ rho, long long rho_rs,
+    const double* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
+    const int* __restrict__ row_map, int hrows, RowState* __restrict__ rst, GridRed red,
+    int nelx, int nely, KEq<D, double> ke, PcgParams pp, int replace) {
+  const int s = blockIdx.z;
+  if (replace && !rst[s].active) return;
+  __shared__ Q4Smem<D, double, double> sm;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
+  if (x) {
+    load_rho_tile<D, double, double>(sm, rho + (size_t)h * rho_rs, r0, c0, nelx, nely);
+    const double* xs = x + (size_t)s * x_rs;
+    load_u_tile<D, double, double>(sm, r0, c0, nnx, nny, [&](int node, double(&v)[D]) {
+      load_node<D, double>(xs, node, v);
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        if (is_fixed(fixed, node, j)) v[j] = 0.0;
+    });
+    __syncthreads();
+  }
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int rr = r0 + ty, cc = c0 + tx;
+  double vals[2] = {0.0, 0.0};
+  if (rr < nny && cc < nnx) {
+    const int node = rr * nnx + cc;
+    double bv[D], Ax[D], res[D];
+    load_node<D, double>(b + (size_t)s * b_rs, node, bv);
+#pragma unroll
+    for (int i = 0; i < D; ++i) Ax[i] = 0.0;
+    if (x) {
+      tile_Ku<D, double, double>(sm, ty, tx, ke, Ax);
+      const double* rd = rdiag + (size_t)h * rd_rs + (size_t)node * D;
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        Ax[i] = fma(__ldg(rd + i), sm.u[ty + 1][tx + 1][i], Ax[i]);
+        if (is_fixed(fixed, node, i)) Ax[i] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      res[i] = bv[i] - Ax[i];
+      vals[0] = fma(res[i], res[i], vals[0]);
+      vals[1] = fma(bv[i], bv[i], vals[1]);
+    }
+    store_node<D, double>(r + (size_t)s * r_rs, node, res);
+  }
+  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  grid_reduce<2, kNT>(red, s, bid, vals, [&](const double* t) {
+    RowState& S = rst[s];
+    if (!replace) {
+      const double bn = sqrt(t[1]);
+      S.bnorm_safe = bn > 0.0 ? bn : 1.0;
+      S.conv_iter = -1;
+      S.status = STT_OK;
+      S.active = 1;
+    }
+    S.rel = sqrt(t[0]) / S.bnorm_safe;
+    if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
+    if (S.rel <= pp.rtol) {
+      S.active = 0;
+      S.conv_iter = pp.it;
+    }
+  });
+}
+
+// Ap = A p (projected, + lumped reaction), pAp = p . Ap, alpha = safe_div(rz, pAp).
+template <int D>
+__global__ void __launch_bounds__(kNT) pcg_pap_kernel(
+    const double* __restrict__ p, double* __restrict__ Ap, long long rs,
+    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
+    long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map,
+    int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely, KEq<D, double> ke) {
+  const int s = blockIdx.z;
+  if (!rst[s].active) return;
+  __shared__ Q4Smem<D, double, double> sm;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
+  load_rho_tile<D, double, double>(sm, rho + (size_t)h * rho_rs, r0, c0, nelx, nely);
+  const double* ps = p + (size_t)s * rs;
+  load_u_tile<D, double, double>(sm, r0, c0, nnx, nny, [&](int node, double(&v)[D]) {
+    load_node<D, double>(ps, node, v);
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      if (is_fixed(fixed, node, j)) v[j] = 0.0;
+  });
+  __syncthreads();
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int rr = r0 + ty, cc = c0 + tx;
+  double vals[1] = {0.0};
+  if (rr < nny && cc < nnx) {
+    const int node = rr * nnx + cc;
+    double Ax[D];
+    tile_Ku<D, double, double>(sm, ty, tx, ke, Ax);
+    const double* rd = rdiag + (size_t)h * rd_rs + (size_t)node * D;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      Ax[i] = fma(__ldg(rd + i), sm.u[ty + 1][tx + 1][i], Ax[i]);
+      if (is_fixed(fixed, node, i)) Ax[i] = 0.0;
+      // p . Ap with p as stored (unprojected p is zero at fixed dofs by construction)
+      vals[0] = fma(ps[(size_t)node * D + i], Ax[i], vals[0]);
+    }
+    store_node<D, double>(Ap + (size_t)s * rs, node, Ax);
+  }
+  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  grid_reduce<1, kNT>(red, s, bid, vals, [&](const double* t) {
+    RowState& S = rst[s];
+    S.pAp = t[0];
+    S.alpha = safe_div(S.rz, t[0]);
+    if (!isfinite(S.alpha)) S.status = STT_ERR_BREAKDOWN;
+  });
+}
+
+// x += alpha p, r -= alpha Ap, ||r||^2, convergence.
+__global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
+    double* __restrict__ x, long long x_rs, double* __restrict__ r, const double* __restrict__ p,
+    const double* __restrict__ Ap, long long rs, long long n, RowState* __restrict__ rst,
+    GridRed red, PcgParams pp) {
+  const int s = blockIdx.y;
+  if (!rst[s].active) return;
+  const double alpha = rst[s].alpha;
+  double* xs = x + (size_t)s * x_rs;
+  double* rsv = r + (size_t)s * rs;
+  const double* ps = p + (size_t)s * rs;
+  const double* as = Ap + (size_t)s * rs;
+  double vals[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kEwThreads) {
+    xs[i] = xs[i] + alpha * ps[i];
+    const double rv = rsv[i] - alpha * as[i];
+    rsv[i] = rv;
+    vals[0] = fma(rv, rv, vals[0]);
+  }
+  grid_reduce<1, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
+    RowState& S = rst[s];
+    S.rel = sqrt(t[0]) / S.bnorm_safe;
+    if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
+    if (S.rel <= pp.rtol) {
+      S.active = 0;
+      S.conv_iter = pp.it;
+    }
+  });
+}
+
+// rz = r . z (and r . z_old for the flexible beta); first: p = z, rz_old = rz;
+// otherwise beta = safe_div(rz - rz_mix, rz_old), rz_old = rz.
+template <typename TZ>
+__global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
+    const double* __restrict__ r, const TZ* __restrict__ z, const TZ* __restrict__ zold,
+    double* __restrict__ p, long long rs, long long n, RowState* __restrict__ rst, GridRed red,
+    int first, int flexible) {
+  const int s = blockIdx.y;
+  if (!rst[s].active) return;
+  const double* rsv = r + (size_t)s * rs;
+  const TZ* zs = z + (size_t)s * rs;
+  const TZ* zo = zold + (size_t)s * rs;
+  double vals[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kEwThreads) {
+    const double zv = (double)zs[i];
+    vals[0] = fma(rsv[i], zv, vals[0]);
+    if (flexible && !first) vals[1] = fma(rsv[i], (double)zo[i], vals[1]);
+    if (first) p[(size_t)s * rs + i] = zv;
+  }
+  grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
+    RowState& S = rst[s];
+    if (first) {
+      S.rz = t[0];
+    } else {
+      const double num = flexible ? t[0] - t[1] : t[0];
+      S.beta = safe_div(num, S.rz);
+      S.rz = t[0];
+      if (!isfinite(S.beta)) S.status = STT_ERR_BREAKDOWN;
+    }
+  });
+}
+
+// p = p * beta + z
+template <typename TZ>
+__global__ void __launch_bounds__(kEwThreads) pcg_pupd_kernel(const TZ* __restrict__ z,
+                                                              double* __restrict__ p, long long rs,
+                                                              long long n, const RowState* __restrict__ rst) {
+  const int s = blockIdx.y;
+  if (!rst[s].active) return;
+  const double beta = rst[s].beta;
+  double* ps = p + (size_t)s * rs;
+  const TZ* zs = z + (size_t)s * rs;
+  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kEwThreads)
+    ps[i] = ps[i] * beta + (double)zs[i];
+}
+
+__global__ void rows_zero_kernel(double* __restrict__ x, long long rs, long long n) {
+  const int s = blockIdx.y;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[(size_t)s * rs + i] = 0.0;
+}
+
+// ---- drivers ----------------------------------------------------------------------
+
+template <int D, typename T>
+static KEq<D, T> ke_of(const stt_hier* h) {
+  KEq<D, T> k;
+  for (int i = 0; i < 16 * D * D; ++i) k.v[i] = T(h->KE[i]);
+  return k;
+}
+
+// z = M r over all rows (rst may gate rows).  r, z FP64 with row strides.
+template <int D, typename T>
+static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r, long long r_rs,
+                      T* zout /* cycle precision, row stride ndof0 */, double omega, int n_smooth,
+                      int gamma, const RowState* rst, cudaStream_t st) {
+  Cycle<D, T> cyc{h, w, nrows, T(omega), n_smooth, gamma, rst, st, ke_of<D, T>(h)};
+  const long long nd = h->lv[0].ndof;
+  const T* b0;
+  long long b_rs;
+  if constexpr (sizeof(T) == 4) {
+    rows_convert_kernel<double, float><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(
+        r, r_rs, (float*)w.b0, nd, nd, rst);
+    b0 = (const T*)w.b0;
+    b_rs = nd;
+  } else {
+    b0 = (const T*)r;
+    b_rs = r_rs;
+  }
+  T* res = cyc.cycle(0, b0, b_rs);
+  rows_convert_kernel<T, T><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(res, nd, zout, nd, nd, rst);
+  return check_launch("vcycle");
+}
+
+template <int D, typename T>
+static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, long long b_rs,
+                   double* x, long long x_rs, int has_x0, double rtol, int max_iter, double omega,
+                   int n_smooth, int gamma, int flexible, int replace_every, double* rel_out,
+                   int* conv_out, int* n_iter_out, cudaStream_t st) {
+  const LevelDesc& l0 = h->lv[0];
+  const long long nd = l0.ndof;
+  const dim3 tg = tile_grid(h->nelx, h->nely, nrows);
+  const int ewb = ew_blocks(nd);
+  GridRed red_tile{w.partials, w.counters, (int)(tg.x * tg.y)};
+  GridRed red_ew{w.partials, w.counters, ewb};
+  const KEq<D, double> ke = ke_of<D, double>(h);
+  STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4LL * nrows, st), "memset counters"));
+  STT_TRY(check_cuda(cudaMemsetAsync(w.rs, 0, sizeof(RowState) * nrows, st), "memset rows"));
+  if (!has_x0) rows_zero_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, nd);
+  PcgParams pp{rtol, 0, flexible};
+  pcg_init_kernel<D><<<tg, kNT, 0, st>>>(b, b_rs, has_x0 ? x : nullptr, x_rs, w.r, nd, l0.rho64, l0.nel,
+                                         l0.rdiag64, l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,
+                                         red_tile, h->nelx, h->nely, ke, pp, 0);
+  STT_TRY(check_launch("pcg init"));
+  std::vector<RowState> host(nrows);
+  auto pull = [&]() -> int {
+    STT_TRY(check_cuda(cudaMemcpyAsync(host.data(), w.rs, sizeof(RowState) * nrows, cudaMemcpyDeviceToHost, st), "row state"));
+    return check_cuda(cudaStreamSynchronize(st), "pcg sync");
+  };
+  auto n_active = [&]() {
+    int a = 0;
+    for (auto& s : host) a += s.active;
+    return a;
+  };
+  STT_TRY(pull());
+  int it = 0;
+  if (n_active() > 0) {
+    T* z = (T*)w.z;
+    T* zold = (T*)w.zold;
+    STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
+    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, nd, w.rs, red_ew, 1, flexible);
+    int check_every = 1;
+    for (it = 1; it <= max_iter; ++it) {
+      pp.it = it;
+      pcg_pap_kernel<D><<<tg, kNT, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.nel, l0.rdiag64, l0.ndof, l0.fixed,
+                                            h->row_map, h->hrows, w.rs, red_tile, h->nelx, h->nely, ke);
+      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, w.p, w.Ap, nd, nd, w.rs, red_ew, pp);
+      if (replace_every > 0 && it % replace_every == 0)
+        pcg_init_kernel<D><<<tg, kNT, 0, st>>>(b, b_rs, x, x_rs, w.r, nd, l0.rho64, l0.nel, l0.rdiag64,
+                                               l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs, red_tile,
+                                               h->nelx, h->nely, ke, pp, 1);
+      if (flexible) std::swap(z, zold);
+      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
+      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, nd, w.rs, red_ew, 0, flexible);
+      pcg_pupd_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(z, w.p, nd, nd, w.rs);
+      STT_TRY(check_launch("pcg iteration"));
+      if (it % check_every == 0 || it == max_iter) {
+        STT_TRY(pull());
+        if (n_active() == 0) break;
+        // a wider check interval once the solve is evidently long
+        if (it >= 8) check_every = 2;
+        if (it >= 32) check_every = 4;
+      }
+    }
+  }
+  STT_TRY(pull());
+  int worst = 0, status = STT_OK;
+  for (int s = 0; s < nrows; ++s) {
+    rel_out[s] = host[s].rel;
+    conv_out[s] = host[s].active ? -1 : host[s].conv_iter;
+    worst = std::max(worst, host[s].conv_iter);
+    if (host[s].active) status = STT_ERR_NOT_CONVERGED;
+  }
+  *n_iter_out = status == STT_OK ? worst : max_iter;
+  if (status != STT_OK)
+    return set_error(status, "CG did not converge within max_iter");
+  return STT_OK;
+}
+
+}  // namespace stt
+
+using namespace stt;
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+extern "C" long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int gamma) {
+  if (!h || nrows <= 0) return -1;
+  SolveWS w;
+  return plan_solve(h, nrows, gamma, nullptr, w);
+}
+
+extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
+                          long long z_rs, double omega, int n_smooth, int gamma, void* workspace,
+                          long long ws_bytes, stt_stream_t stream) {
+  if (!h || !r || !z || !workspace || nrows <= 0 || nrows > 65535 || n_smooth < 1 || gamma < 1)
+    return set_error(STT_ERR_INVALID, "stt_vcycle: bad arguments");
+  if (!aligned16(r) || !aligned16(z) || (r_rs % 2) || (z_rs % 2))
+    return set_error(STT_ERR_INVALID, "stt_vcycle: vectors must be 16-byte aligned with even row strides");
+  SolveWS w;
+  const long long need = plan_solve(h, nrows, gamma, nullptr, w);
+  if (ws_bytes < need) return set_error(STT_ERR_WORKSPACE, "stt_vcycle: workspace too small");
+  plan_solve(h, nrows, gamma, (char*)workspace, w);
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long nd = h->lv[0].ndof;
+  int rc;
+  if (h->precision == STT_FP32) {
+    rc = h->d == 2 ? run_vcycle<2, float>(h, w, nrows, r, r_rs, (float*)w.z, omega, n_smooth, gamma, nullptr, st)
+                   : run_vcycle<1, float>(h, w, nrows, r, r_rs, (float*)w.z, omega, n_smooth, gamma, nullptr, st);
+    if (rc == STT_OK)
+      rows_convert_kernel<float, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((float*)w.z, nd, z, z_rs, nd, nullptr);
+  } else {
+    rc = h->d == 2 ? run_vcycle<2, double>(h, w, nrows, r, r_rs, (double*)w.z, omega, n_smooth, gamma, nullptr, st)
+                   : run_vcycle<1, double>(h, w, nrows, r, r_rs, (double*)w.z, omega, n_smooth, gamma, nullptr, st);
+    if (rc == STT_OK)
+      rows_convert_kernel<double, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((double*)w.z, nd, z, z_rs, nd, nullptr);
+  }
+  if (rc != STT_OK) return rc;
+  return check_launch("stt_vcycle");
+}
+
+extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const double* v, long long v_rs,
+                               double* out, long long out_rs, stt_stream_t stream) {
+  if (!h || !v || !out || level < 0 || level >= h->nlevels || nrows <= 0 || nrows > 65535)
+    return set_error(STT_ERR_INVALID, "stt_level_apply: bad arguments");
+  if (!aligned16(v) || !aligned16(out) || (v_rs % 2) || (out_rs % 2))
+    return set_error(STT_ERR_INVALID, "stt_level_apply: vectors must be 16-byte aligned with even row strides");
+  cudaStream_t st = (cudaStream_t)stream;
+  const LevelDesc& lv = h->lv[level];
+  if (level == 0) {
+    if (h->d == 2)
+      l0_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.nel, lv.rdiag64, lv.ndof, lv.fixed, h->row_map,
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<2, double>(h));
+    else
+      l0_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.nel, lv.rdiag64, lv.ndof, lv.fixed, h->row_map,
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<1, double>(h));
+    return check_launch("level apply");
+  }
+  if (v_rs != lv.ndof || out_rs != lv.ndof)
+    return set_error(STT_ERR_INVALID, "stt_level_apply: coarse levels need contiguous rows");
+  if (h->d == 2)
+    st_sweep_kernel<2, double, SW_APPLY><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
+        v, nullptr, out, lv.ndof, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
+  else
+    st_sweep_kernel<1, double, SW_APPLY><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
+        v, nullptr, out, lv.ndof, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
+  return check_launch("level apply");
+}
+
+extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long long b_rs, double* x,
+                          long long x_rs, int has_x0, double rtol, int max_iter, double omega,
+                          int n_smooth, int gamma, int flexible, int replace_every, double* rel_resid,
+                          int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
+                          stt_stream_t stream) {
+  if (!h || !b || !x || !workspace || !rel_resid || !conv_iter || !n_iter || nrows <= 0 ||
+      nrows > 65535 || max_iter < 0 || n_smooth < 1 || gamma < 1)
+    return set_error(STT_ERR_INVALID, "stt_pcg_mg: bad arguments");
+  if (!aligned16(b) || !aligned16(x) || (b_rs % 2) || (x_rs % 2))
+    return set_error(STT_ERR_INVALID, "stt_pcg_mg: vectors must be 16-byte aligned with even row strides");
+  SolveWS w;
+  const long long need = plan_solve(h, nrows, gamma, nullptr, w);
+  if (ws_bytes < need) return set_error(STT_ERR_WORKSPACE, "stt_pcg_mg: workspace too small");
+  plan_solve(h, nrows, gamma, (char*)workspace, w);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (h->precision == STT_FP32)
+    return h->d == 2 ? run_pcg<2, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st)
+                     : run_pcg<1, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
+  return h->d == 2 ? run_pcg<2, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st)
+                   : run_pcg<1, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
+}

@@ -1,0 +1,339 @@
+"""Drop-in for ``sttopt.torch_mg``: the Galerkin geometric-multigrid V-cycle.
+
+``build_hierarchy`` builds every level on the device in one call (``stt_hier_create``):
+exact Galerkin element products ``sum_m S_m^T K_child S_m`` (sttopt/torch_mg.py:355-370),
+stored as symmetric 9-point block stencils, coarse masks sampled at collocated nodes
+(:376), and the coarsest level factorised by a block-banded FP64 Cholesky (:269-290).
+The hierarchy policy is the reference's: factors 2 or 3 per dimension
+(``coarsening_factors``), stop at ``max_coarse_elements``.
+
+``precision="mixed"`` keeps FP32 copies of the level operators and runs the V-cycle's
+smoothing, transfers and stencil applies in FP32 (the coarse Cholesky stays FP64);
+``"fp64"`` (the default) runs everything in FP64.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from . import _geom, _lib, fem, torch_fem
+
+MAX_COARSE_ELEMENTS = 700  # sttopt/torch_mg.py:50
+#: "fp64" or "mixed"; the precision ``build_hierarchy`` uses when none is given.
+DEFAULT_PRECISION = "fp64"
+
+
+def coarsening_factors(nelx: int, nely: int) -> tuple[int, int]:
+    """Smallest of 2, 3 dividing each dimension, else 1 (sttopt/torch_mg.py:53-72)."""
+
+    def factor(n: int) -> int:
+        return next((k for k in (2, 3) if n % k == 0), 1)
+
+    return factor(nelx), factor(nely)
+
+
+@functools.lru_cache(maxsize=None)
+def element_dof_map_tensor(nelx: int, nely: int, device, dofs_per_node: int = 2) -> Tensor:
+    """``fem.element_dof_map`` as a device tensor, memoised (sttopt/torch_mg.py:112-127)."""
+    return torch.tensor(fem.element_dof_map(nelx, nely, dofs_per_node), dtype=torch.int64,
+                        device=device)
+
+
+def _precision_code(precision: str | None) -> int:
+    p = DEFAULT_PRECISION if precision is None else precision
+    if p == "fp64":
+        return _lib.STT_FP64
+    if p in ("mixed", "fp32"):
+        return _lib.STT_FP32
+    raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+
+
+class _Hierarchy:
+    """Owner of one device hierarchy (C handle + workspace), or a row-selected view."""
+
+    def __init__(self, handle, ws, d, hrows, batch_shape, device, KE_host, parent=None,
+                 row_map: Tensor | None = None, nrows: int | None = None):
+        self.handle = handle
+        self.ws = ws
+        self.d = d
+        self.hrows = hrows
+        self.batch_shape = batch_shape  # leading batch shape of the density rows
+        self.device = device
+        self.KE_host = KE_host
+        self.parent = parent
+        self.row_map = row_map
+        # rows the view represents (hrows for the base, len(row_map) for views)
+        self.nrows = hrows if nrows is None else nrows
+        n = ctypes.c_int()
+        dims = (ctypes.c_int * 96)()
+        _lib.check(_lib.lib().stt_hier_info(handle, ctypes.byref(n), dims, 24))
+        self.nlevels = n.value
+        self.dims = [tuple(dims[4 * i: 4 * i + 4]) for i in range(self.nlevels)]
+        self.precision = None
+
+    @classmethod
+    def build(cls, density: Tensor, mask: Tensor, KE: Tensor, nelx: int, nely: int,
+              reaction: Tensor | None, max_coarse_elements: int, precision: str | None):
+        _lib.require_cuda(density, mask, reaction)
+        d = KE.shape[-1] // 4
+        nel = nelx * nely
+        prec = _precision_code(precision)
+        batch_shape = density.shape[:-1]
+        rho = density.detach().to(torch.float64).reshape(-1, nel).contiguous()
+        hrows = rho.shape[0]
+        reac = None
+        if reaction is not None:
+            reac = reaction.detach().to(torch.float64).expand(*batch_shape, nel).reshape(-1, nel).contiguous()
+        fixed = _geom.fixed_flags(mask, (nelx + 1) * (nely + 1), d)
+        nbytes = _lib.lib().stt_hier_workspace_bytes(d, nelx, nely, hrows, max_coarse_elements, prec)
+        if nbytes < 0:
+            raise ValueError("bad hierarchy shape")
+        ws = _lib.workspace(nbytes, density.device)
+        ke_host = _geom.host_KE(KE)
+        handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().stt_hier_create(
+            ctypes.byref(handle), _lib.ptr(ws), ws.numel(), d, nelx, nely, hrows, _lib.ptr(rho),
+            nel, _lib.ptr(reac), nel, _lib.ptr(fixed), _lib.dbl_array(ke_host),
+            max_coarse_elements, prec, _lib.stream()))
+        h = cls(handle, ws, d, hrows, batch_shape, density.device, ke_host)
+        h.precision = "fp64" if prec == _lib.STT_FP64 else "mixed"
+        return h
+
+    def select(self, rows: Tensor) -> "_Hierarchy":
+        """The same operators restricted to batch rows ``rows``."""
+        if self.hrows == 1 and self.row_map is None:
+            return self  # one shared density field: nothing to select
+        rows = rows.to(device=self.device, dtype=torch.int64)
+        base = self.row_map if self.row_map is not None else torch.arange(
+            self.hrows, device=self.device, dtype=torch.int32)
+        rm = base[rows].to(torch.int32).contiguous()
+        handle = ctypes.c_void_p()
+        _lib.check(_lib.lib().stt_hier_select(self.handle, _lib.ptr(rm), ctypes.byref(handle)))
+        v = _Hierarchy(handle, None, self.d, self.hrows, self.batch_shape, self.device,
+                       self.KE_host, parent=self, row_map=rm, nrows=rm.numel())
+        v.precision = self.precision
+        return v
+
+    def __del__(self):
+        try:
+            if self.handle:
+                _lib.lib().stt_hier_destroy(self.handle)
+                self.handle = None
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def _rows_for(h: _Hierarchy, v: Tensor) -> tuple[Tensor, int, tuple]:
+    """``v`` as ``(rows, n)``: one row per view row (broadcast against a shared field)."""
+    n = v.shape[-1]
+    if h.hrows == 1 and h.row_map is None:
+        flat = v.reshape(-1, n)
+        return flat.contiguous(), flat.shape[0], v.shape[:-1]
+    batch = torch.broadcast_shapes(v.shape[:-1], (h.nrows,) if h.row_map is not None else h.batch_shape)
+    flat = v.expand(*batch, n).reshape(-1, n).contiguous()
+    if flat.shape[0] != h.nrows:
+        raise ValueError(f"{flat.shape[0]} vector rows for a hierarchy of {h.nrows} rows")
+    return flat, flat.shape[0], batch
+
+
+class _Level:
+    """One grid of the hierarchy; calling it applies ``P(K P v)`` at this level
+    (sttopt/torch_mg.py:211-266).  ``diag`` and ``mask`` are read back from the
+    device on first access."""
+
+    def __init__(self, hier: _Hierarchy, index: int, *, edofMat=None, KE=None, density=None,
+                 reaction_diag=None):
+        self._hier = hier
+        self._index = index
+        nelx, nely, kx, ky = hier.dims[index]
+        self.nelx, self.nely, self.kx, self.ky = nelx, nely, kx, ky
+        self.ndof = hier.d * (nelx + 1) * (nely + 1)
+        self.KE = KE
+        self.density = density
+        self.reaction_diag = reaction_diag
+        self.keff = None  # coarse operators live on the device as stencils
+        self.chol = None  # the coarse factor lives on the device in band blocks
+        self._edofMat = edofMat
+        self._diag = None
+        self._mask = None
+
+    @property
+    def edofMat(self) -> Tensor:
+        if self._edofMat is None:
+            self._edofMat = element_dof_map_tensor(self.nelx, self.nely, self._hier.device, self._hier.d)
+        return self._edofMat
+
+    @property
+    def mask(self) -> Tensor:
+        if self._mask is None:
+            h = self._hier
+            nnode = (self.nelx + 1) * (self.nely + 1)
+            flags = torch.empty(nnode, dtype=torch.uint8, device=h.device)
+            _lib.check(_lib.lib().stt_hier_level_fixed(h.handle, self._index, _lib.ptr(flags), _lib.stream()))
+            bits = torch.stack([(flags >> i) & 1 for i in range(h.d)], dim=-1).reshape(-1)
+            self._mask = bits == 0
+        return self._mask
+
+    @property
+    def diag(self) -> Tensor:
+        if self._diag is None:
+            h = self._hier
+            full = torch.empty(h.hrows, self.ndof, dtype=torch.float64, device=h.device)
+            _lib.check(_lib.lib().stt_hier_level_diag(h.handle, self._index, _lib.ptr(full), _lib.stream()))
+            if h.row_map is not None:
+                full = full[h.row_map.to(torch.int64)]
+            elif h.hrows == 1 and len(h.batch_shape) == 0:
+                full = full[0]
+            else:
+                full = full.reshape(*h.batch_shape, self.ndof)
+            self._diag = full
+        return self._diag
+
+    def __call__(self, v: Tensor) -> Tensor:
+        _lib.require_cuda(v)
+        h = self._hier
+        flat, rows, batch = _rows_for(h, v.to(torch.float64))
+        out = torch.empty_like(flat)
+        _lib.check(_lib.lib().stt_level_apply(h.handle, self._index, rows, _lib.ptr(flat), self.ndof,
+                                              _lib.ptr(out), self.ndof, _lib.stream()))
+        return out.reshape(*batch, self.ndof)
+
+    def select(self, rows: Tensor) -> "_Level":
+        lv = _Level(self._hier.select(rows), self._index, edofMat=self._edofMat, KE=self.KE,
+                    density=None if self.density is None or self.density.ndim == 1 else self.density[rows],
+                    reaction_diag=self.reaction_diag)
+        lv._mask = self._mask
+        return lv
+
+    def _native_pcg(self, b: Tensor, M: "VCycle", *, rtol, max_iter, x0, info):
+        """The whole MG-PCG solve on the device when ``M`` cycles this hierarchy."""
+        h = self._hier
+        if self._index != 0 or M._is_vcycle_of is not h or b.ndim > 2:
+            return None
+        _lib.require_cuda(b, x0)
+        flat, rows, batch = _rows_for(h, b.detach().to(torch.float64))
+        n = self.ndof
+        x = torch.empty_like(flat)
+        if x0 is not None:
+            x.copy_(x0.detach().to(torch.float64).expand(*batch, n).reshape(-1, n))
+        nbytes = _lib.lib().stt_solve_workspace_bytes(h.handle, rows, M.gamma)
+        ws = _lib.workspace(nbytes, flat.device)
+        rel = (ctypes.c_double * rows)()
+        conv = (ctypes.c_int * rows)()
+        n_iter = ctypes.c_int()
+        mixed = h.precision == "mixed"
+        rc = _lib.lib().stt_pcg_mg(
+            h.handle, rows, _lib.ptr(flat), n, _lib.ptr(x), n, 1 if x0 is not None else 0, rtol, max_iter,
+            M.omega, M.n_smooth, M.gamma, 1 if mixed else 0, 0, rel, conv, ctypes.byref(n_iter),
+            _lib.ptr(ws), ws.numel(), _lib.stream())
+        conv_list = list(conv)
+        n_rows_ref = b.shape[0] if b.ndim == 2 else 1
+        if info is not None:
+            info["row_iters"] = torch_fem.row_iters_from_schedule(conv_list, n_rows_ref, max_iter) \
+                if b.ndim == 2 else (max(conv_list) if min(conv_list) >= 0 else max_iter)
+        if rc == _lib.STT_ERR_NOT_CONVERGED:
+            resid = torch.tensor(list(rel), dtype=torch.float64, device=b.device)
+            raise torch_fem.CGConvergenceError(resid.reshape(batch) if b.ndim == 2 else resid[0], max_iter, rtol)
+        _lib.check(rc)
+        return x.reshape(*batch, n), n_iter.value
+
+
+def build_hierarchy(density: Tensor, edofMat: Tensor, KE: Tensor, mask: Tensor, nelx: int,
+                    nely: int, *, reaction: Tensor | None = None,
+                    max_coarse_elements: int = MAX_COARSE_ELEMENTS,
+                    precision: str | None = None) -> list[_Level]:
+    """Levels from finest to coarsest (sttopt/torch_mg.py:293-400), built on the device."""
+    ndof = mask.shape[-1]
+    d = KE.shape[-1] // 4
+    if d * (nelx + 1) * (nely + 1) != ndof:
+        raise ValueError("mask does not match the grid")
+    h = _Hierarchy.build(density, mask, KE, nelx, nely, reaction, max_coarse_elements, precision)
+    reaction_diag = None
+    if reaction is not None:
+        reaction_diag = torch_fem.lumped_reaction(reaction.detach(), edofMat, ndof)
+    levels = [_Level(h, 0, edofMat=edofMat, KE=KE, density=density, reaction_diag=reaction_diag)]
+    for i in range(1, h.nlevels):
+        levels.append(_Level(h, i))
+    levels[0]._mask = mask.to(torch.bool)
+    return levels
+
+
+class VCycle:
+    """Damped-Jacobi V-cycle with an exact coarse solve, as an SPD preconditioner
+    (sttopt/torch_mg.py:403-476); one ``stt_vcycle`` call per application."""
+
+    def __init__(self, levels: list[_Level], *, omega: float = 0.6, n_smooth: int = 2,
+                 gamma: int = 1) -> None:
+        if not levels or not isinstance(levels[0], _Level):
+            raise TypeError("VCycle needs levels from sttopt_b200.torch_mg.build_hierarchy")
+        self.levels = levels
+        self.omega = omega
+        self.n_smooth = n_smooth
+        self.gamma = gamma
+        self._is_vcycle_of = levels[0]._hier
+
+    def select(self, rows: Tensor) -> "VCycle":
+        return VCycle([lv.select(rows) for lv in self.levels], omega=self.omega,
+                      n_smooth=self.n_smooth, gamma=self.gamma)
+
+    def __call__(self, r: Tensor) -> Tensor:
+        _lib.require_cuda(r)
+        h = self._is_vcycle_of
+        n = self.levels[0].ndof
+        flat, rows, batch = _rows_for(h, r.to(torch.float64))
+        z = torch.empty_like(flat)
+        nbytes = _lib.lib().stt_solve_workspace_bytes(h.handle, rows, self.gamma)
+        ws = _lib.workspace(nbytes, flat.device)
+        _lib.check(_lib.lib().stt_vcycle(h.handle, rows, _lib.ptr(flat), n, _lib.ptr(z), n, self.omega,
+                                         self.n_smooth, self.gamma, _lib.ptr(ws), ws.numel(), _lib.stream()))
+        return z.reshape(*batch, n)
+
+
+def solve(F: Tensor, xPhys: Tensor, edofMat: Tensor, KE: Tensor, Emin: float, Emax: float,
+          penal: float, mask: Tensor, nelx: int, nely: int, *, rtol: float = 1e-8,
+          max_iter: int = 500, x0: Tensor | None = None, omega: float = 0.6, n_smooth: int = 2,
+          gamma: int = 1, max_coarse_elements: int = MAX_COARSE_ELEMENTS,
+          info: dict | None = None, precision: str | None = None) -> tuple[Tensor, int]:
+    """MG-preconditioned CG for ``K U = F`` (sttopt/torch_mg.py:479-535)."""
+    density = torch_fem.simp_density(xPhys, Emin, Emax, penal)
+    levels = build_hierarchy(density, edofMat, KE, mask, nelx, nely,
+                             max_coarse_elements=max_coarse_elements, precision=precision)
+    precond = VCycle(levels, omega=omega, n_smooth=n_smooth, gamma=gamma)
+    U, n_iter = torch_fem.pcg(levels[0], torch_fem.project(F, mask), precond, rtol=rtol,
+                              max_iter=max_iter, x0=x0, info=info)
+    return torch_fem.project(U, mask), n_iter
+
+
+# ---- host-side transfer utilities (API parity; the cycle uses device kernels) ------
+
+
+def child_interpolation_matrices(kx: int, ky: int, device=None, dtype=torch.float64,
+                                 dofs_per_node: int = 2) -> Tensor:
+    """``S[m]``: coarse element dofs -> child ``m``'s dofs (sttopt/torch_mg.py:140-165)."""
+    d = dofs_per_node
+    nk = 4 * d
+    S = np.zeros((kx * ky, nk, nk))
+    corner = [(1, 0), (1, 1), (0, 1), (0, 0)]  # BL, BR, TR, TL (row, col)
+
+    def interp1(a, b, j, k):
+        if j == k:
+            return b
+        w = j / k
+        return a * (1 - w) + b * w
+
+    for qc, (cr, cc) in enumerate(corner):
+        for my in range(ky):
+            for mx in range(kx):
+                for qf, (fr0, fc0) in enumerate(corner):
+                    fr, fc = my + fr0, mx + fc0
+                    g = [interp1(1.0 if (R == cr and cc == 0) else 0.0,
+                                 1.0 if (R == cr and cc == 1) else 0.0, fc, kx) for R in (0, 1)]
+                    v = interp1(g[0], g[1], fr, ky)
+                    for i in range(d):
+                        S[my * kx + mx, qf * d + i, qc * d + i] = v
+    return torch.tensor(S, dtype=dtype, device=device)

@@ -1,0 +1,108 @@
+"""CPU-only checks of the boundary: the C-ABI library loads and exports every entry
+point ``include/sttb200.h`` declares, the Python binding covers them all, and the host
+logic (hierarchy planning, row accounting) matches the reference's policies.  No
+compute is launched here."""
+
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden
+from oracle import sttopt_oracle as O
+
+HEADER = ROOT / "include" / "sttb200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(stt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert sorted(_lib.exported_symbols()) == declared_symbols()
+
+
+def test_workspace_planning_follows_the_reference_policy(pkg):
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    # sizes are positive and grow with rows; invalid shapes are rejected
+    a = lib.stt_hier_workspace_bytes(2, 120, 40, 1, 700, 0)
+    b = lib.stt_hier_workspace_bytes(2, 120, 40, 4, 700, 0)
+    c = lib.stt_hier_workspace_bytes(2, 120, 40, 4, 700, 1)
+    assert 0 < a < b < c
+    assert lib.stt_hier_workspace_bytes(3, 120, 40, 1, 700, 0) < 0
+    assert lib.stt_hier_workspace_bytes(2, 0, 40, 1, 700, 0) < 0
+
+
+def test_invalid_arguments_fail_without_a_device(pkg):
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    rc = lib.stt_q4_apply(0, 3, 4, 4, 1, None, 0, None, 0, None, 0, None, 0, None, 0, None, None)
+    assert rc == _lib.STT_ERR_INVALID
+    assert b"stt_q4_apply" in lib.stt_last_error()
+    out = ctypes.c_void_p()
+    rc = lib.stt_hier_create(ctypes.byref(out), None, 0, 2, 4, 4, 1, None, 0, None, 0, None, None,
+                             700, 0, None)
+    assert rc == _lib.STT_ERR_INVALID
+
+
+@pytest.mark.parametrize("sizes", [(2048, 1024), (1024, 512), (512, 256), (120, 40), (768, 384),
+                                   (1536, 768), (256, 128), (30, 10), (97, 89)])
+def test_coarsening_policy_matches_oracle(pkg, sizes):
+    from sttopt_b200 import torch_mg
+
+    nelx, nely = sizes
+    assert torch_mg.coarsening_factors(nelx, nely) == O.coarsening_factors(nelx, nely)
+
+
+def test_child_interpolation_matches_golden_bitwise(pkg):
+    from sttopt_b200 import torch_mg
+
+    g = golden("transfers")
+    for kx, ky in [(2, 2), (3, 3), (3, 1), (2, 3), (1, 2)]:
+        for d in (1, 2):
+            S = torch_mg.child_interpolation_matrices(kx, ky, dofs_per_node=d).numpy()
+            np.testing.assert_array_equal(S, g[f"S_k{kx}{ky}_d{d}"])
+
+
+def test_row_iters_schedule_matches_reference(pkg):
+    from sttopt_b200 import torch_fem
+
+    g = golden("pcg_cases")
+    # per-row convergence iterations of the oracle run that the reference recorded
+    nelx, nely = 18, 12
+    edof = O.element_dof_map(nelx, nely)
+    KE = O.plane_stress_KE(0.3)
+    conv = []
+    for s in range(3):
+        if not np.any(g["F"][s]):
+            conv.append(0)
+            continue
+        _, n = O.mg_solve(g["F"][s], g["x"][s], edof, KE, 1e-9, 1.0, 3.0, g["mask"], nelx, nely,
+                          rtol=1e-11, max_coarse_elements=24)
+        conv.append(n)
+    assert torch_fem.row_iters_from_schedule(conv, 3, 500) == int(g["row_iters"])
+    assert torch_fem.row_iters_from_schedule([0, 0], 2, 500) == 0
+    assert torch_fem.row_iters_from_schedule([5], 1, 500) == 5
+
+
+def test_package_refuses_cpu_tensors(pkg):
+    import torch
+
+    from sttopt_b200 import torch_fem
+
+    KE = torch.tensor(O.plane_stress_KE(0.3))
+    edof = torch.tensor(O.element_dof_map(4, 3))
+    with pytest.raises(ValueError, match="CUDA"):
+        torch_fem.matvec(torch.zeros(40, dtype=torch.float64), torch.ones(12, dtype=torch.float64),
+                         edof, KE, 40)
