@@ -529,8 +529,8 @@ extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long lo
                           long long ws_bytes, stt_stream_t stream) {
   if (!h || !r || !z || !workspace || nrows <= 0 || nrows > 65535 || n_smooth < 1 || gamma < 1)
     return set_error(STT_ERR_INVALID, "stt_vcycle: bad arguments");
-  if (!aligned16(r) || !aligned16(z) || (r_rs % 2) || (z_rs % 2))
-    return set_error(STT_ERR_INVALID, "stt_vcycle: vectors must be 16-byte aligned with even row strides");
+  if (h->d == 2 && (!aligned16(r) || !aligned16(z) || (r_rs % 2) || (z_rs % 2)))
+    return set_error(STT_ERR_INVALID, "stt_vcycle: 2-dof vectors must be 16-byte aligned with even row strides");
   SolveWS w;
   const long long need = plan_solve(h, nrows, gamma, nullptr, w);
   if (ws_bytes < need) return set_error(STT_ERR_WORKSPACE, "stt_vcycle: workspace too small");
@@ -557,8 +557,8 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
                                double* out, long long out_rs, stt_stream_t stream) {
   if (!h || !v || !out || level < 0 || level >= h->nlevels || nrows <= 0 || nrows > 65535)
     return set_error(STT_ERR_INVALID, "stt_level_apply: bad arguments");
-  if (!aligned16(v) || !aligned16(out) || (v_rs % 2) || (out_rs % 2))
-    return set_error(STT_ERR_INVALID, "stt_level_apply: vectors must be 16-byte aligned with even row strides");
+  if (h->d == 2 && (!aligned16(v) || !aligned16(out) || (v_rs % 2) || (out_rs % 2)))
+    return set_error(STT_ERR_INVALID, "stt_level_apply: 2-dof vectors must be 16-byte aligned with even row strides");
   cudaStream_t st = (cudaStream_t)stream;
   const LevelDesc& lv = h->lv[level];
   if (level == 0) {
@@ -591,8 +591,8 @@ extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long lo
   if (!h || !b || !x || !workspace || !rel_resid || !conv_iter || !n_iter || nrows <= 0 ||
       nrows > 65535 || max_iter < 0 || n_smooth < 1 || gamma < 1)
     return set_error(STT_ERR_INVALID, "stt_pcg_mg: bad arguments");
-  if (!aligned16(b) || !aligned16(x) || (b_rs % 2) || (x_rs % 2))
-    return set_error(STT_ERR_INVALID, "stt_pcg_mg: vectors must be 16-byte aligned with even row strides");
+  if (h->d == 2 && (!aligned16(b) || !aligned16(x) || (b_rs % 2) || (x_rs % 2)))
+    return set_error(STT_ERR_INVALID, "stt_pcg_mg: 2-dof vectors must be 16-byte aligned with even row strides");
   SolveWS w;
   const long long need = plan_solve(h, nrows, gamma, nullptr, w);
   if (ws_bytes < need) return set_error(STT_ERR_WORKSPACE, "stt_pcg_mg: workspace too small");
