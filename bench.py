@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the space-time full gradient on B200.
+
+One step = one evaluation of the full 16-stage space-time objective and its gradient
+on a 2048 x 1024 Q4 grid: the virtual-heat time-field solve, stage membership
+``t <= s/16``, 16 self-weight stage solves (one batched device PCG, rtol 1e-8, FP32
+V-cycle inside FP64 PCG), the stage adjoints, the heat adjoint and the sensitivity
+field.  Metric: converged stage solves per second (16 per step, summed over ranks);
+the JSON line also carries the time per full gradient.
+
+``--impl reference`` times the CPU restatement of the reference algorithm (the
+oracle; the reference itself is Python and is not installed on the GPU box) on a
+bounded sample of the same workload, scaled to the same metric.
+
+Multi-GPU: the path has no exchange step, so N ranks run N independent replicas
+(weak scaling); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NELX, NELY, N_STAGE = 2048, 1024, 16
+SEED = 3
+METRIC = "stage solves/s (space-time objective + full gradient, 2048x1024 Q4, 16 stages, rtol 1e-8)"
+UNIT = "stage solves/s"
+# Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the roofline
+# kernel from the ncu capture summarised in profiles/ (None until captured).
+NCU_TRAFFIC = {"l0_apply_fp32_16rows": None}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-profile", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---- CPU baseline: the oracle on a bounded sample ------------------------------------
+
+def cpu_sample(steps: int, warmup: int):
+    """Times the oracle's full objective + gradient on a smaller grid of the same
+    workload (16 stages) and scales by the element count (MG iterations are
+    mesh-independent here: 20 stage / 9 heat iterations at 256x128 and 512x256)."""
+    import numpy as np
+
+    from oracle import sttopt_oracle as O
+
+    nx, ny = (256, 128) if steps + warmup <= 8 else (128, 64)
+    x = O.smoothed_density(nx, ny, SEED)
+    w = np.random.default_rng(SEED).uniform(-1, 1, (ny, nx))
+    t0 = time.perf_counter()
+    out = O.spacetime_objective(x, w, n_stage=N_STAGE)
+    dt = time.perf_counter() - t0
+    scale = (NELX * NELY) / (nx * ny)
+    full_s = dt * scale
+    return dict(value=N_STAGE / full_s, full_gradient_ms=full_s * 1e3, sample=(
+        f"oracle full objective+gradient at {nx}x{ny}, 16 stages ({dt:.2f} s, "
+        f"{out['forward_n_iter']} stage / {out['heat_n_iter']} heat iterations), scaled x{scale:.0f} "
+        "by element count"), seconds=dt)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ.setdefault(k, str(threads))
+    vals, ms, last = [], [], None
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(args.steps, args.warmup)
+        if i >= args.warmup:
+            vals.append(s["value"])
+            ms.append(s["full_gradient_ms"])
+        last = s
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(ms),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded smoothed density, seeded time weights)",
+        "config": {"workload": "space-time full gradient 2048x1024x16 stages, CPU oracle sample",
+                   "nelx": NELX, "nely": NELY, "n_stage": N_STAGE},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": last["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- clocks -----------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- the GPU arm --------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from __graft_entry__ import load_package
+
+    load_package()
+    from sttopt_b200 import _lib, spacetime, synthetic
+
+    x = synthetic.smoothed_density(NELX, NELY, SEED, device=dev)
+    w = synthetic.time_weights(NELX, NELY, SEED, device=dev)
+    problem = spacetime.SpaceTimeProblem(NELX, NELY, dev)
+    info: dict = {}
+
+    def step(xx, ww, precision=args.precision, batched=True):
+        return spacetime.objective_and_gradient(xx, ww, n_stage=N_STAGE, precision=precision,
+                                                problem=problem, info=info, batched=batched)
+
+    for _ in range(max(args.warmup, 0)):
+        out = step(x, w)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # timed region: inputs resident in HBM
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            out = step(x, w)
+        end.record()
+        torch.cuda.synchronize()
+        barrier()
+    elapsed_ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = N_STAGE * args.steps * world / (elapsed_ms / 1e3)
+    iters = dict(info)
+
+    # end to end through the public call with host buffers
+    xh = x.detach().cpu().pin_memory()
+    wh = w.detach().cpu().pin_memory()
+    gh = torch.empty(NELY, NELX, dtype=torch.float64).pin_memory()
+    oh = torch.empty(1, dtype=torch.float64).pin_memory()
+    xd, wd = torch.empty_like(x), torch.empty_like(w)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        xd.copy_(xh, non_blocking=True)
+        wd.copy_(wh, non_blocking=True)
+        o = step(xd, wd)
+        gh.copy_(o["gradient"], non_blocking=True)
+        oh.copy_(o["objective"].reshape(1), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = N_STAGE * args.steps * world / (e2e_ms / 1e3)
+    h2d = xh.numel() * 8 + wh.numel() * 8
+    d2h = gh.numel() * 8 + 8
+
+    extra = {}
+    if rank == 0:
+        extra["roofline"], extra["roofline_detail"] = roofline(_lib, problem, out, dev)
+        # the plain FP64 GPU form: unbatched stages, FP64 V-cycle
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        step(x, w, precision="fp64", batched=False)
+        p0.record()
+        ref = step(x, w, precision="fp64", batched=False)
+        p1.record()
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+        c_err = float(((out["c_s"] - ref["c_s"]).abs() / ref["c_s"].abs()).max())
+        g_err = float((out["gradient"] - ref["gradient"]).norm() / ref["gradient"].norm())
+        extra["plain_fp64_form"] = {"full_gradient_ms": plain_ms, "speedup_batched_mixed": plain_ms / ms_per_step,
+                                    "max_rel_err_stage_compliance": c_err, "rel_err_gradient_l2": g_err}
+        if not args.no_profile:
+            extra["gpu_launches_per_step"], extra["top_kernels"] = profile_step(step, x, w)
+        if world == 1 and not args.no_cpu_baseline:
+            s = cpu_sample(1, 0)
+            extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": 1, "kind": "port",
+                                     "sample": s["sample"], "full_gradient_ms": s["full_gradient_ms"]}
+    if rank == 0:
+        launches = extra.pop("gpu_launches_per_step", None)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 outer PCG + f32 V-cycle" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded N(0,1) noise, radius-4 cone filter, mapped to [1e-3, 1]; seeded U(-1,1) time weights)",
+            "config": {"workload": "space-time objective + full gradient: heat time field, 16 hard-threshold "
+                                   "gravity stages, batched MG-PCG rtol 1e-8, stage + heat adjoints",
+                       "nelx": NELX, "nely": NELY, "n_stage": N_STAGE, "precision": args.precision,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "working set (16 stage rows x 4.2M dofs, hierarchy) far above the 126 MB L2; no flush"},
+            "full_gradient_ms": ms_per_step,
+            "iterations": iters,
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "full_gradient_ms": e2e_ms / args.steps},
+            "gpu_launches": None if launches is None else launches * args.steps,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def roofline(_lib, P, out, dev):
+    """Live CUDA-event timing of the level-0 operator apply over the 16 stage rows:
+    FP32 (the V-cycle's fine-level kernel) and FP64 (the outer PCG's)."""
+    import torch
+
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    L = _lib.lib()
+    st = _lib.stream()
+    ndof, nel = 2 * P.nnode, P.nel
+    rows = N_STAGE
+    detail = {}
+    for name, dt, prec, es in [("l0_apply_fp32_16rows", torch.float32, _lib.STT_FP32, 4),
+                               ("l0_apply_fp64_16rows", torch.float64, _lib.STT_FP64, 8)]:
+        u = out["U"].to(dt).contiguous()
+        rho = torch.rand(rows, nel, device=dev, dtype=torch.float64).to(dt)
+        o = torch.empty_like(u)
+        for _ in range(3):
+            _lib.check(L.stt_q4_apply(prec, 2, NELX, NELY, rows, _lib.ptr(u), ndof, _lib.ptr(o), ndof,
+                                      _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2), 3, P.ke, st))
+        n = 20
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            _lib.check(L.stt_q4_apply(prec, 2, NELX, NELY, rows, _lib.ptr(u), ndof, _lib.ptr(o), ndof,
+                                      _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2), 3, P.ke, st))
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / n
+        alg = rows * (2 * ndof * es + nel * es)  # read u, write Ku, read rho (flags: 1 B/node not counted)
+        gbs = alg / (ms * 1e-3) / 1e9
+        detail[name] = {"achieved": gbs, "ms_per_launch": ms, "algorithmic_bytes": alg, "frac": gbs / peak}
+    main_k = detail["l0_apply_fp32_16rows"]
+    roof = {"bound": "hbm", "achieved": main_k["achieved"], "peak": peak, "unit": "GB/s",
+            "frac": main_k["frac"], "peak_source": peak_src, "kernel": "l0 Q4 apply, FP32, 16 stage rows",
+            "traffic": NCU_TRAFFIC["l0_apply_fp32_16rows"]}
+    return roof, detail
+
+
+def profile_step(step, x, w):
+    """Kernel launches of one step (CUPTI through torch.profiler) and the top kernels."""
+    import torch
+
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            step(x, w)
+            torch.cuda.synchronize()
+        totals: dict = {}
+        count = 0
+        for ev in prof.events():
+            if ev.device_type.name != "CUDA":
+                continue
+            name = ev.name
+            if "stt::" not in name:
+                continue
+            count += 1
+            key = name.split("(")[0].replace("void ", "")
+            t = totals.setdefault(key, [0, 0.0])
+            t[0] += 1
+            t[1] += ev.device_time_total if hasattr(ev, "device_time_total") else ev.cuda_time_total
+        total = sum(v[1] for v in totals.values()) or 1.0
+        top = sorted(totals.items(), key=lambda kv: -kv[1][1])[:8]
+        return count, [{"kernel": k, "launches": v[0], "us": round(v[1], 1), "share": round(v[1] / total, 3)}
+                       for k, v in top]
+    except Exception as exc:  # profiler unavailable: report, do not fail the bench
+        return None, [{"error": str(exc)[:200]}]
+
+
+if __name__ == "__main__":
+    sys.exit(main())
