@@ -116,6 +116,20 @@ int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, do
                long long z_rs, double omega, int n_smooth, int gamma, void* workspace,
                long long ws_bytes, stt_stream_t stream);
 
+/* stt_vcycle without a caller workspace.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory: plugins inside a host application that owns
+ * the device memory pool and forbids outside cudaMalloc, multi-stream pipelines that
+ * cannot afford cudaMalloc's implicit device synchronisation mid-run, and bindings that
+ * can pass input and output buffers but cannot size and own scratch.
+ * Its scratch is a fixed 32 MiB array inside this library, held by every GPU that loads
+ * the library until exit; calls needing more (stt_solve_workspace_bytes) return
+ * STT_ERR_WORKSPACE without launching.  All calls on a device share that array: calls
+ * that overlap on the GPU race, so order them on one stream.  The first call on each
+ * device looks up the array's device address and should come before any stream capture.
+ * Results equal stt_vcycle's for the same arguments. */
+int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
+                       long long z_rs, double omega, int n_smooth, int gamma, stt_stream_t stream);
+
 /* MG-preconditioned CG on all batch rows, entirely on the device.  x holds the warm
  * start when has_x0, else is zeroed; b must already be projected.  Outputs: rel_resid
  * [nrows] (host), conv_iter [nrows] (host, -1 = not converged), *n_iter (host).

@@ -50,6 +50,7 @@ _SIGS = {
     "stt_level_apply": (_c_int, [_p, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
     "stt_solve_workspace_bytes": (_c_ll, [_p, _c_int, _c_int]),
     "stt_vcycle": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p, _c_ll, _p]),
+    "stt_vcycle_noalloc": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p]),
     "stt_pcg_mg": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_int, _c_double, _c_int, _c_double, _c_int,
                             _c_int, _c_int, _c_int, _pd, _pi, _pi, _p, _c_ll, _p]),
     "stt_vec_dots": (_c_int, [_c_int, _c_ll, _p, _p, _p, _p, _p, _p, _c_ll, _p, _p]),

@@ -9,6 +9,7 @@
 // summed in block order by the last block).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "errors.h"
@@ -603,4 +604,67 @@ extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long lo
                      : run_pcg<1, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
   return h->d == 2 ? run_pcg<2, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st)
                    : run_pcg<1, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
+}
+
+// ---- V-cycle without a caller workspace ---------------------------------------------
+//
+// Some callers cannot allocate device memory: plugins inside a host application that
+// owns the device memory pool and forbids outside cudaMalloc, multi-stream pipelines
+// that cannot afford cudaMalloc's implicit device synchronisation mid-run, or
+// foreign-language bindings that can hand over input and output buffers but not size
+// and own a scratch buffer.  stt_vcycle_noalloc serves
+// them: it runs exactly stt_vcycle, with its scratch taken from a fixed-size array
+// compiled into this library instead of a caller workspace.
+//
+// Limits and rules:
+//  * the scratch is kVCycleScratchBytes (32 MiB) per device; every GPU that loads the
+//    library holds it until the process exits.  A call whose V-cycle scratch
+//    (stt_solve_workspace_bytes for the same hierarchy, rows and gamma) exceeds it is
+//    rejected with STT_ERR_WORKSPACE before anything is launched;
+//  * all calls on a device share the one array and it keeps the last call's
+//    contents; the V-cycle writes every scratch word before reading it, so nothing has
+//    to start at zero.  Calls that overlap on the GPU (different streams, or threads
+//    without ordering) race on the array: order them on one stream;
+//  * the first call on each device looks up the array's device address
+//    (cudaGetSymbolAddress) with that device current; make that first call before
+//    any stream capture begins.
+
+namespace {
+
+constexpr long long kVCycleScratchBytes = 32LL << 20;
+
+__device__ __align__(256) unsigned char g_vcycle_scratch[kVCycleScratchBytes];
+
+std::mutex g_vcycle_scratch_mu;
+void* g_vcycle_scratch_ptr[256] = {};
+
+int vcycle_scratch_address(void** out) {
+  int dev = 0;
+  STT_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+  if (dev < 0 || dev >= 256) return set_error(STT_ERR_INVALID, "stt_vcycle_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_vcycle_scratch_mu);
+  if (!g_vcycle_scratch_ptr[dev]) {
+    void* p = nullptr;
+    STT_TRY(check_cuda(cudaGetSymbolAddress(&p, g_vcycle_scratch), "cudaGetSymbolAddress(g_vcycle_scratch)"));
+    g_vcycle_scratch_ptr[dev] = p;
+  }
+  *out = g_vcycle_scratch_ptr[dev];
+  return STT_OK;
+}
+
+}  // namespace
+
+extern "C" int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r, long long r_rs,
+                                  double* z, long long z_rs, double omega, int n_smooth, int gamma,
+                                  stt_stream_t stream) {
+  if (!h || nrows <= 0 || nrows > 65535 || gamma < 1)
+    return set_error(STT_ERR_INVALID, "stt_vcycle_noalloc: bad arguments");
+  const long long need = stt_solve_workspace_bytes(h, nrows, gamma);
+  if (need < 0 || need > kVCycleScratchBytes)
+    return set_error(STT_ERR_WORKSPACE,
+                     "stt_vcycle_noalloc: this V-cycle needs more scratch than the library's fixed 32 MiB; "
+                     "use stt_vcycle with a caller workspace");
+  void* scratch = nullptr;
+  STT_TRY(vcycle_scratch_address(&scratch));
+  return stt_vcycle(h, nrows, r, r_rs, z, z_rs, omega, n_smooth, gamma, scratch, kVCycleScratchBytes, stream);
 }
