@@ -130,4 +130,15 @@ STT_DEV void grid_reduce(const GridRed& g, int row, int bid, const double (&v)[K
 
 STT_DEV double safe_div(double num, double den) { return den != 0.0 ? num / den : 0.0; }
 
+// n / k and n % k for the coarsening factors k in {1, 2, 3} and 0 <= n < 2^30, without
+// an integer division (0x55555556 = ceil(2^32 / 3) gives floor(n / 3) exactly there).
+STT_DEV int div_k(int n, int k) {
+  return k == 2 ? (n >> 1) : (k == 3 ? (int)__umulhi((unsigned)n, 0x55555556u) : n);
+}
+
+// The sweep update x0 + (omega * res) / diag: exact division in FP64 (the reference's
+// arithmetic), the fast division in the FP32 V-cycle (a preconditioner, no reference).
+STT_DEV double sweep_div(double num, double den) { return num / den; }
+STT_DEV float sweep_div(float num, float den) { return __fdividef(num, den); }
+
 }  // namespace stt

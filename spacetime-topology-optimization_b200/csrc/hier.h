@@ -25,6 +25,7 @@ struct LevelDesc {
   int kx, ky;      // coarsening factors to the next level (1, 1 at the coarsest)
   int nnx, nny;
   long long nnode, ndof, nel;
+  long long rs_rho;  // row stride of rho64 / rho32: nel rounded up to 4 (16-byte aligned rows)
   uint8_t* fixed;  // [nnode] bit i = dof i fixed
   // level 0 only
   double* rho64;    // [hrows][nel]
@@ -53,6 +54,7 @@ struct stt_hier_impl {
   double* keffA;     // build temporaries
   double* keffB;
   const int* row_map;  // batch row -> hierarchy row (device), or null
+  int has_reaction;    // level 0 carries a lumped reaction (drain) term
   int* status;         // device status word of the build (bit 0: pivot <= 0, bit 1: band)
   long long ws_bytes;
 };

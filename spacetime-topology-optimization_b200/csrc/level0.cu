@@ -8,68 +8,66 @@
 namespace stt {
 
 template <int D, typename T>
-__global__ void __launch_bounds__(kNT) q4_apply_kernel(
+__global__ void __launch_bounds__(kQThreads) q4_apply_kernel(
     const T* __restrict__ u, long long u_rs, T* __restrict__ out, long long out_rs,
     const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag, long long rdiag_rs,
     const uint8_t* __restrict__ fixed, int proj_in, int proj_out, int nelx, int nely,
     KEq<D, T> ke) {
-  __shared__ Q4Smem<D, T, T> s;
   const int nnx = nelx + 1, nny = nely + 1;
   const int row = blockIdx.z;
-  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
   const T* ur = u + (size_t)row * u_rs;
-  load_rho_tile<D, T, T>(s, rho + (size_t)row * rho_rs, r0, c0, nelx, nely);
-  load_u_tile<D, T, T>(s, r0, c0, nnx, nny, [&](int node, T(&v)[D]) {
-    load_node<D, T>(ur, node, v);
-    if (proj_in) {
+  const T* rr = rho + (size_t)row * rho_rs;
+  const T* rdr = rdiag ? rdiag + (size_t)row * rdiag_rs : nullptr;
+  T* outr = out + (size_t)row * out_rs;
+  const uint8_t* pin = proj_in ? fixed : nullptr;
+  march<D, T, true, false, FlagX>(
+      ke, nnx, nny,
+      [&](int r, int c, T(&v)[D]) {
+        const int node = r * nnx + c;
+        load_node<D, T>(ur, node, v);
+        if (pin) {
+          const uint8_t fl = __ldg(pin + node);
 #pragma unroll
-      for (int j = 0; j < D; ++j)
-        if (is_fixed(fixed, node, j)) v[j] = T(0);
-    }
-  });
-  __syncthreads();
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int r = r0 + ty, c = c0 + tx;
-  if (r >= nny || c >= nnx) return;
-  const int node = r * nnx + c;
-  T acc[D];
-  tile_Ku<D, T, T>(s, ty, tx, ke, acc);
-  if (rdiag) {
-    const T* rd = rdiag + (size_t)row * rdiag_rs + (size_t)node * D;
+          for (int d = 0; d < D; ++d)
+            if ((fl >> d) & 1) v[d] = T(0);
+        }
+      },
+      [&](int r, int c) { return __ldg(rr + (size_t)r * nelx + c); },
+      [&](int r, int c) { return FlagX{proj_out ? __ldg(fixed + r * nnx + c) : (uint8_t)0}; },
+      [&](int r, int c, T(&acc)[D], T(&)[D], const T(&uc)[D], const FlagX& ex) {
+        const int node = r * nnx + c;
+        if (rdr) {
 #pragma unroll
-    for (int i = 0; i < D; ++i) acc[i] = fma(__ldg(rd + i), s.u[ty + 1][tx + 1][i], acc[i]);
-  }
-  if (proj_out) {
+          for (int i = 0; i < D; ++i) acc[i] = fma(__ldg(rdr + node * D + i), uc[i], acc[i]);
+        }
 #pragma unroll
-    for (int i = 0; i < D; ++i)
-      if (is_fixed(fixed, node, i)) acc[i] = T(0);
-  }
-  store_node<D, T>(out + (size_t)row * out_rs, node, acc);
+        for (int i = 0; i < D; ++i)
+          if ((ex.fl >> i) & 1) acc[i] = T(0);
+        store_node<D, T>(outr, node, acc);
+      });
 }
 
 template <int D>
-__global__ void __launch_bounds__(kNT) q4_diag_kernel(
+__global__ void __launch_bounds__(kQThreads) q4_diag_kernel(
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
     long long rdiag_rs, const uint8_t* __restrict__ fixed, double* __restrict__ out,
     long long out_rs, int nelx, int nely, KEq<D, double> ke) {
-  __shared__ Q4Smem<D, double, double> s;
   const int nnx = nelx + 1, nny = nely + 1;
   const int row = blockIdx.z;
-  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
-  load_rho_tile<D, double, double>(s, rho + (size_t)row * rho_rs, r0, c0, nelx, nely);
-  __syncthreads();
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int r = r0 + ty, c = c0 + tx;
-  if (r >= nny || c >= nnx) return;
-  const int node = r * nnx + c;
-  double dg[D];
-  tile_diag<D, double, double>(s, ty, tx, ke, dg);
+  const double* rr = rho + (size_t)row * rho_rs;
+  march<D, double, false, true>(
+      ke, nnx, nny, [&](int, int, double(&)[D]) {},
+      [&](int r, int c) { return __ldg(rr + (size_t)r * nelx + c); },
+      [&](int, int) { return NoExtra{}; },
+      [&](int r, int c, double(&)[D], double(&dg)[D], const double(&)[D], const NoExtra&) {
+        const int node = r * nnx + c;
 #pragma unroll
-  for (int i = 0; i < D; ++i) {
-    if (rdiag) dg[i] += __ldg(rdiag + (size_t)row * rdiag_rs + (size_t)node * D + i);
-    if (is_fixed(fixed, node, i)) dg[i] = 1.0;
-  }
-  store_node<D, double>(out + (size_t)row * out_rs, node, dg);
+        for (int i = 0; i < D; ++i) {
+          if (rdiag) dg[i] += __ldg(rdiag + (size_t)row * rdiag_rs + (size_t)node * D + i);
+          if (is_fixed(fixed, node, i)) dg[i] = 1.0;
+        }
+        store_node<D, double>(out + (size_t)row * out_rs, node, dg);
+      });
 }
 
 // rdiag[node * D + i] = sum of reaction[e] / 4 over the elements around the node.
@@ -107,8 +105,8 @@ int launch_apply(int nelx, int nely, int nrows, const void* u, long long u_rs, v
                  long long out_rs, const void* rho, long long rho_rs, const void* rdiag,
                  long long rdiag_rs, const uint8_t* fixed, int flags, const double* KE,
                  cudaStream_t st) {
-  dim3 grid((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, nrows);
-  q4_apply_kernel<D, T><<<grid, kNT, 0, st>>>(
+  const dim3 grid = q4_grid(nelx, nely, nrows);
+  q4_apply_kernel<D, T><<<grid, kQThreads, 0, st>>>(
       (const T*)u, u_rs, (T*)out, out_rs, (const T*)rho, rho_rs, (const T*)rdiag, rdiag_rs,
       fixed, (flags & STT_PROJECT_IN) ? 1 : 0, (flags & STT_PROJECT_OUT) ? 1 : 0, nelx, nely,
       make_ke<D, T>(KE));
@@ -146,11 +144,11 @@ extern "C" int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* r
   if (nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || !rho || !out || !KE)
     return set_error(STT_ERR_INVALID, "stt_q4_diag: bad sizes or null pointer");
   cudaStream_t st = (cudaStream_t)stream;
-  dim3 grid((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, nrows);
+  const dim3 grid = q4_grid(nelx, nely, nrows);
   if (d == 2)
-    q4_diag_kernel<2><<<grid, kNT, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<2, double>(KE));
+    q4_diag_kernel<2><<<grid, kQThreads, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<2, double>(KE));
   else if (d == 1)
-    q4_diag_kernel<1><<<grid, kNT, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<1, double>(KE));
+    q4_diag_kernel<1><<<grid, kQThreads, 0, st>>>(rho, rho_rs, rdiag, rdiag_rs, fixed, out, out_rs, nelx, nely, make_ke<1, double>(KE));
   else
     return set_error(STT_ERR_INVALID, "stt_q4_diag: d must be 1 or 2");
   return check_launch("q4_diag");

@@ -11,222 +11,21 @@
 
 namespace stt {
 
-enum SweepMode { SW_FIRST = 0, SW_SWEEP = 1, SW_RESID = 2, SW_APPLY = 3 };
+enum SweepMode { SW_FIRST = 0, SW_SWEEP = 1, SW_RESID = 2, SW_APPLY = 3, SW_POST = 4 };
 
-// ---- level 0: density-scaled Q4 tiles ------------------------------------------
-//   SW_FIRST: out = (omega * b) / diag               (sweep from x = 0)
-//   SW_SWEEP: out = x + (omega * (b - A x)) / diag
-//   SW_RESID: out = b - A x
-//   SW_APPLY: out = A x
-// A is the projected operator P(K P .) (+ lumped reaction); x is read projected.
-template <int D, typename T, int MODE>
-__global__ void __launch_bounds__(kNT) l0_sweep_kernel(
-    const T* __restrict__ x, long long x_rs, const T* __restrict__ b, long long b_rs,
-    T* __restrict__ out, long long o_rs, const T* __restrict__ rho, long long rho_rs,
-    const T* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
-    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, int nelx,
-    int nely, T omega, KEq<D, T> ke) {
-  const int s = blockIdx.z;
-  if (rst && !rst[s].active) return;
-  __shared__ Q4Smem<D, T, T> sm;
-  const int nnx = nelx + 1, nny = nely + 1;
-  const int h = hier_row(row_map, hrows, s);
-  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
-  load_rho_tile<D, T, T>(sm, rho + (size_t)h * rho_rs, r0, c0, nelx, nely);
-  const T* xs = x + (size_t)s * x_rs;
-  if (MODE != SW_FIRST) {
-    load_u_tile<D, T, T>(sm, r0, c0, nnx, nny, [&](int node, T(&v)[D]) {
-      load_node<D, T>(xs, node, v);
-#pragma unroll
-      for (int j = 0; j < D; ++j)
-        if (is_fixed(fixed, node, j)) v[j] = T(0);
-    });
-  }
-  __syncthreads();
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int r = r0 + ty, c = c0 + tx;
-  if (r >= nny || c >= nnx) return;
-  const int node = r * nnx + c;
-  const T* rd = rdiag + (size_t)h * rd_rs + (size_t)node * D;
-  const uint8_t fl = fixed[node];
-  T Ax[D], bv[D], res[D];
-  if (MODE != SW_FIRST) {
-    tile_Ku<D, T, T>(sm, ty, tx, ke, Ax);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      Ax[i] = fma(__ldg(rd + i), sm.u[ty + 1][tx + 1][i], Ax[i]);
-      if ((fl >> i) & 1) Ax[i] = T(0);
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < D; ++i) Ax[i] = T(0);
-  }
-  if (MODE != SW_APPLY) load_node<D, T>(b + (size_t)s * b_rs, node, bv);
-  if (MODE == SW_FIRST || MODE == SW_SWEEP) {
-    T dg[D];
-    tile_diag<D, T, T>(sm, ty, tx, ke, dg);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      dg[i] += __ldg(rd + i);
-      if ((fl >> i) & 1) dg[i] = T(1);
-      const T xo = MODE == SW_FIRST ? T(0) : sm.u[ty + 1][tx + 1][i];
-      res[i] = xo + (omega * (bv[i] - Ax[i])) / dg[i];
-    }
-  } else if (MODE == SW_RESID) {
-#pragma unroll
-    for (int i = 0; i < D; ++i) res[i] = bv[i] - Ax[i];
-  } else {
-#pragma unroll
-    for (int i = 0; i < D; ++i) res[i] = Ax[i];
-  }
-  store_node<D, T>(out + (size_t)s * o_rs, node, res);
-}
+// Coarse-grid correction folded into a sweep's input (SW_POST): the sweep reads
+// x + P_f(P e_c), bilinear interpolation x pass then y pass (torch_mg._interp_axis,
+// sttopt/torch_mg.py:75-81), so the prolongation needs no pass of its own.
+template <typename T>
+struct ProlongSrc {
+  const T* ec;  // coarse correction of this batch row (set per row in the kernel)
+  long long rs;
+  int cnnx, kx, ky;
+};
 
-// ---- stencil levels -------------------------------------------------------------
-
-// (A x) at node (r, c) from the symmetric half stencil (centre, E, S, SE, SW blocks of
-// this node; W, N, NW, NE couplings are the transposed E, S, SE, SW blocks of the
-// neighbours).  st is this hierarchy row's [NS][nnode] array, x this row's vector.
 template <int D, typename T>
-STT_DEV void stencil_Ax(const T* __restrict__ st, long long nnode, int nnx, int nny, int r, int c,
-                        const T* __restrict__ x, T (&acc)[D]) {
-  constexpr int DD = D * D;
-#pragma unroll
-  for (int i = 0; i < D; ++i) acc[i] = T(0);
-  const long long n = (long long)r * nnx + c;
-  const int odr[5] = {0, 0, 1, 1, 1}, odc[5] = {0, 1, 0, 1, -1};
-#pragma unroll
-  for (int blk = 0; blk < 5; ++blk) {
-    const int mr = r + odr[blk], mc = c + odc[blk];
-    if (mr >= nny || mc < 0 || mc >= nnx) continue;
-    const long long m = (long long)mr * nnx + mc;
-    T xm[D];
-    load_node<D, T>(x, (int)m, xm);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int j = 0; j < D; ++j)
-        acc[i] = fma(__ldg(st + (size_t)(blk * DD + i * D + j) * nnode + n), xm[j], acc[i]);
-  }
-  // transposed couplings held by the neighbours: W (E block), N (S), NW (SE), NE (SW)
-  const int tdr[4] = {0, -1, -1, -1}, tdc[4] = {-1, 0, -1, 1}, tblk[4] = {1, 2, 3, 4};
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const int mr = r + tdr[t], mc = c + tdc[t];
-    if (mr < 0 || mc < 0 || mc >= nnx) continue;
-    const long long m = (long long)mr * nnx + mc;
-    T xm[D];
-    load_node<D, T>(x, (int)m, xm);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int j = 0; j < D; ++j)
-        acc[i] = fma(__ldg(st + (size_t)(tblk[t] * DD + j * D + i) * nnode + m), xm[j], acc[i]);
-  }
-}
-
-template <int D, typename T, int MODE>
-__global__ void __launch_bounds__(256) st_sweep_kernel(
-    const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
-    const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
-    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega) {
-  constexpr int NS = 5 * D * D;
-  const int s = blockIdx.y;
-  if (rst && !rst[s].active) return;
-  const long long nnode = (long long)nnx * nny;
-  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= nnode) return;
-  const int h = hier_row(row_map, hrows, s);
-  const T* sth = st + (size_t)h * NS * nnode;
-  const int r = (int)(n / nnx), c = (int)(n - (long long)r * nnx);
-  const uint8_t fl = fixed[n];
-  T Ax[D], bv[D], res[D];
-  if (MODE != SW_FIRST) {
-    stencil_Ax<D, T>(sth, nnode, nnx, nny, r, c, x + (size_t)s * vec_rs, Ax);
-  } else {
-#pragma unroll
-    for (int i = 0; i < D; ++i) Ax[i] = T(0);
-  }
-  if (MODE != SW_APPLY) load_node<D, T>(b + (size_t)s * vec_rs, (int)n, bv);
-  if (MODE == SW_FIRST || MODE == SW_SWEEP) {
-    T xo[D];
-    if (MODE == SW_SWEEP) load_node<D, T>(x + (size_t)s * vec_rs, (int)n, xo);
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      T dg = __ldg(sth + (size_t)(i * D + i) * nnode + n);
-      if ((fl >> i) & 1) dg = T(1);
-      const T x0 = MODE == SW_FIRST ? T(0) : xo[i];
-      res[i] = x0 + (omega * (bv[i] - Ax[i])) / dg;
-    }
-  } else if (MODE == SW_RESID) {
-#pragma unroll
-    for (int i = 0; i < D; ++i) res[i] = bv[i] - Ax[i];
-  } else {
-#pragma unroll
-    for (int i = 0; i < D; ++i) res[i] = Ax[i];
-  }
-  store_node<D, T>(out + (size_t)s * vec_rs, (int)n, res);
-}
-
-// ---- transfers -------------------------------------------------------------------
-
-// One axis of full weighting at coarse index I (nc coarse intervals), in the
-// reference's order: (block I weighted 1 - j/k) + (block I-1 weighted j/k), plus the
-// last fine value on the last coarse node.
-template <typename T, typename F>
-STT_DEV T restrict1(F fetch, int I, int k, int nc) {
-  if (k == 1) return fetch(I);
-  T lo = T(0), hi = T(0);
-  if (I < nc) {
-    for (int j = 0; j < k; ++j) lo += fetch(k * I + j) * T(1.0 - (double)j / k);
-  }
-  if (I >= 1) {
-    for (int j = 1; j < k; ++j) hi += fetch(k * (I - 1) + j) * T((double)j / k);
-  }
-  T out = lo + hi;
-  if (I == nc) out += fetch(k * nc);
-  return out;
-}
-
-// rc = P_c (R r_f): x pass then y pass (torch_mg._on_node_grid with _restrict_axis).
-template <int D, typename T>
-__global__ void restrict_kernel(const T* __restrict__ rf, long long f_rs, int fnnx, T* __restrict__ rc,
-                                long long c_rs, int cnnx, int cnny, int kx, int ky,
-                                const uint8_t* __restrict__ cfixed, const RowState* __restrict__ rst) {
-  const int s = blockIdx.y;
-  if (rst && !rst[s].active) return;
-  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= (long long)cnnx * cnny) return;
-  const int R = (int)(n / cnnx), C = (int)(n - (long long)R * cnnx);
-  const T* f = rf + (size_t)s * f_rs;
-  const uint8_t fl = cfixed[n];
-  T out[D];
-#pragma unroll
-  for (int i = 0; i < D; ++i) {
-    auto xpass = [&](int fr) -> T {
-      return restrict1<T>([&](int fc) -> T { return __ldg(f + ((size_t)fr * fnnx + fc) * D + i); },
-                          C, kx, cnnx - 1);
-    };
-    out[i] = ((fl >> i) & 1) ? T(0) : restrict1<T>(xpass, R, ky, cnny - 1);
-  }
-  store_node<D, T>(rc + (size_t)s * c_rs, (int)n, out);
-}
-
-// x_f += P_f (P e_c): bilinear interpolation, x pass then y pass (_interp_axis).
-template <int D, typename T>
-__global__ void prolong_add_kernel(const T* __restrict__ ec, long long c_rs, int cnnx,
-                                   T* __restrict__ xf, long long f_rs, int fnnx, int fnny, int kx,
-                                   int ky, const uint8_t* __restrict__ ffixed,
-                                   const RowState* __restrict__ rst) {
-  const int s = blockIdx.y;
-  if (rst && !rst[s].active) return;
-  const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= (long long)fnnx * fnny) return;
-  const int r = (int)(n / fnnx), c = (int)(n - (long long)r * fnnx);
-  const int R = r / ky, jy = r - R * ky, C = c / kx, jx = c - C * kx;
-  const T* e = ec + (size_t)s * c_rs;
-  const uint8_t fl = ffixed[n];
-  T* xs = xf + (size_t)s * f_rs;
+STT_DEV void prolong_at(const T* __restrict__ e, int cnnx, int kx, int ky, int r, int c, T (&v)[D]) {
+  const int R = div_k(r, ky), jy = r - R * ky, C = div_k(c, kx), jx = c - C * kx;
   const T wx = T((double)jx / kx), wy = T((double)jy / ky);
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -236,34 +35,450 @@ __global__ void prolong_add_kernel(const T* __restrict__ ec, long long c_rs, int
       const T b = __ldg(e + ((size_t)RR * cnnx + C + 1) * D + i);
       return a * (T(1) - wx) + b * wx;
     };
-    T v = g(R);
-    if (jy != 0) v = v * (T(1) - wy) + g(R + 1) * wy;
-    if ((fl >> i) & 1) v = T(0);
-    xs[(size_t)n * D + i] += v;
+    T t = g(R);
+    if (jy != 0) t = t * (T(1) - wy) + g(R + 1) * wy;
+    v[i] = t;
   }
 }
 
-// ---- coarsest level: block-banded Cholesky solve (one CTA per batch row) ----------
+// ---- level 0: density-scaled Q4 tiles ------------------------------------------
+//   SW_FIRST: out = (omega * b) / diag               (sweep from x = 0)
+//   SW_SWEEP: out = x + (omega * (b - A x)) / diag
+//   SW_RESID: out = b - A x
+//   SW_APPLY: out = A x
+// A is the projected operator P(K P .) (+ lumped reaction); x is read projected.
+template <int D, typename T, int MODE>
+__global__ void __launch_bounds__(kQThreads) l0_sweep_kernel(
+    const T* __restrict__ x, long long x_rs, const T* __restrict__ b, long long b_rs,
+    T* __restrict__ out, long long o_rs, const T* __restrict__ rho, long long rho_rs,
+    const T* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, int nelx,
+    int nely, T omega, KEq<D, T> ke, int proj_in, ProlongSrc<T> pro) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const T* xs = x + (size_t)s * x_rs;
+  const T* es = MODE == SW_POST ? pro.ec + (size_t)s * pro.rs : nullptr;
+  const T* rh = rho + (size_t)h * rho_rs;
+  const T* rdh = rdiag ? rdiag + (size_t)h * rd_rs : nullptr;
+  const T* bs = b + (size_t)s * b_rs;
+  T* os = out + (size_t)s * o_rs;
+  const uint8_t* pin = proj_in ? fixed : nullptr;
+  constexpr bool KU = MODE != SW_FIRST;
+  constexpr bool DG = MODE == SW_FIRST || MODE == SW_SWEEP || MODE == SW_POST;
+  march<D, T, KU, DG, RhsX<D, T>>(
+      ke, nnx, nny,
+      [&](int r, int c, T(&v)[D]) {
+        const int node = r * nnx + c;
+        load_node<D, T>(xs, node, v);
+        if (MODE == SW_POST) {
+          T pv[D];
+          prolong_at<D, T>(es, pro.cnnx, pro.kx, pro.ky, r, c, pv);
+          const uint8_t fl = __ldg(fixed + node);
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            if (!((fl >> d) & 1)) v[d] += pv[d];
+        }
+        if (pin) {
+          const uint8_t fl = __ldg(pin + node);
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            if ((fl >> d) & 1) v[d] = T(0);
+        }
+      },
+      [&](int r, int c) { return __ldg(rh + (size_t)r * nelx + c); },
+      [&](int r, int c) {
+        RhsX<D, T> x;
+        const int node = r * nnx + c;
+        if (MODE != SW_APPLY) load_node<D, T>(bs, node, x.b);
+        x.fl = __ldg(fixed + node);
+        return x;
+      },
+      [&](int r, int c, T(&Ax)[D], T(&dg)[D], const T(&xo)[D], const RhsX<D, T>& ex) {
+        const int node = r * nnx + c;
+        const uint8_t fl = ex.fl;
+        T bv[D], res[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) bv[i] = ex.b[i];
+        if (KU) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            if (rdh) Ax[i] = fma(__ldg(rdh + node * D + i), xo[i], Ax[i]);
+            if ((fl >> i) & 1) Ax[i] = T(0);
+          }
+        }
+        if (DG) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) {
+            if (rdh) dg[i] += __ldg(rdh + node * D + i);
+            if ((fl >> i) & 1) dg[i] = T(1);
+            const T x0 = MODE == SW_FIRST ? T(0) : xo[i];
+            res[i] = x0 + sweep_div(omega * (bv[i] - (KU ? Ax[i] : T(0))), dg[i]);
+          }
+        } else if (MODE == SW_RESID) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) res[i] = bv[i] - Ax[i];
+        } else {
+#pragma unroll
+          for (int i = 0; i < D; ++i) res[i] = Ax[i];
+        }
+        store_node<D, T>(os, node, res);
+      });
+}
+
+// ---- stencil levels: column-marching sweeps -----------------------------------------
+//
+// The symmetric half stencil stores, per node, the centre, E, S, SE, SW blocks; the W,
+// N, NW, NE couplings are the transposed E block of the left neighbour (a shuffle), S of
+// the node above (this lane's previous row) and SE / SW of the nodes above-left /
+// above-right (the neighbours' previous rows, shuffles).  Marching a warp down a strip
+// of columns, every coefficient and every vector value is loaded once, coalesced.
+//   SW_FIRST / SW_SWEEP / SW_POST / SW_RESID / SW_APPLY as on level 0; x is projected.
+template <int D, typename T, int MODE>
+__global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
+    const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
+    const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega,
+    ProlongSrc<T> pro) {
+  constexpr int DD = D * D, NS = 5 * DD;
+  constexpr bool KU = MODE != SW_FIRST;
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const long long nnode = (long long)nnx * nny;
+  const int h = hier_row(row_map, hrows, s);
+  const T* sth = st + (size_t)h * NS * nnode;
+  const T* xs = x + (size_t)s * vec_rs;
+  const T* bs = b + (size_t)s * vec_rs;
+  T* os = out + (size_t)s * vec_rs;
+  const T* es = MODE == SW_POST ? pro.ec + (size_t)s * pro.rs : nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kQCols - 1 + lane;
+  const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  auto X = [&](int r, T(&v)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    if (!KU || !col_ok || r < 0 || r >= nny) return;
+    const int node = r * nnx + c;
+    load_node<D, T>(xs, node, v);
+    if (MODE == SW_POST) {
+      T pv[D];
+      prolong_at<D, T>(es, pro.cnnx, pro.kx, pro.ky, r, c, pv);
+      const uint8_t fl = __ldg(fixed + node);
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        if (!((fl >> d) & 1)) v[d] += pv[d];
+    }
+  };
+  auto CO = [&](int r, int k) -> T {
+    return (col_ok && r >= 0 && r < nny) ? __ldg(sth + (size_t)k * nnode + (size_t)r * nnx + c) : T(0);
+  };
+  auto up = [](T v) { return __shfl_up_sync(0xffffffffu, v, 1); };
+  auto dn = [](T v) { return __shfl_down_sync(0xffffffffu, v, 1); };
+  T xa[D], xb[D], xal[D], xar[D], xbl[D], xbr[D];
+  T pS[DD], pSE[DD], pSW[DD];  // this lane's S, SE, SW blocks of the previous row
+  X(r0 - 1, xa);
+  X(r0, xb);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    xal[d] = up(xa[d]);
+    xar[d] = dn(xa[d]);
+    xbl[d] = up(xb[d]);
+    xbr[d] = dn(xb[d]);
+  }
+#pragma unroll
+  for (int q = 0; q < DD; ++q) {
+    pS[q] = KU ? CO(r0 - 1, 2 * DD + q) : T(0);
+    pSE[q] = KU ? CO(r0 - 1, 3 * DD + q) : T(0);
+    pSW[q] = KU ? CO(r0 - 1, 4 * DD + q) : T(0);
+  }
+  // one-row lookahead: coefficients, rhs and flags of row r, input of row r + 1
+  auto load_row = [&](int r, T(&Cc)[DD], T(&E)[DD], T(&S)[DD], T(&SE)[DD], T(&SW)[DD], T(&xc)[D], T(&bv)[D],
+                      uint8_t& fl) {
+    X(r + 1, xc);
+#pragma unroll
+    for (int q = 0; q < DD; ++q) {
+      Cc[q] = CO(r, q);
+      E[q] = KU ? CO(r, DD + q) : T(0);
+      S[q] = KU ? CO(r, 2 * DD + q) : T(0);
+      SE[q] = KU ? CO(r, 3 * DD + q) : T(0);
+      SW[q] = KU ? CO(r, 4 * DD + q) : T(0);
+    }
+    const bool ok = out_lane && r < r1;
+    if (MODE != SW_APPLY && ok) {
+      load_node<D, T>(bs, (long long)r * nnx + c, bv);
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d) bv[d] = T(0);
+    }
+    fl = ok ? __ldg(fixed + (size_t)r * nnx + c) : (uint8_t)0;
+  };
+  T Cc[DD], E[DD], S[DD], SE[DD], SW[DD], xc[D], bv[D];
+  uint8_t fl;
+  load_row(r0, Cc, E, S, SE, SW, xc, bv, fl);
+  for (int r = r0; r < r1; ++r) {
+    T nC[DD], nE[DD], nS[DD], nSE[DD], nSW[DD], nxc[D], nbv[D];
+    uint8_t nfl;
+    load_row(r + 1, nC, nE, nS, nSE, nSW, nxc, nbv, nfl);
+    T xcl[D], xcr[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      xcl[d] = up(xc[d]);
+      xcr[d] = dn(xc[d]);
+    }
+    T Ax[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) Ax[i] = T(0);
+    if (KU) {
+#pragma unroll
+      for (int q = 0; q < DD; ++q) {
+        const T Ew = up(E[q]), SEnw = up(pSE[q]), SWne = dn(pSW[q]);
+        const int i = q / D, j = q % D;  // block (i, j); transposed blocks contribute (j, i)
+        Ax[i] = fma(Cc[q], xb[j], Ax[i]);
+        Ax[i] = fma(E[q], xbr[j], Ax[i]);
+        Ax[i] = fma(S[q], xc[j], Ax[i]);
+        Ax[i] = fma(SE[q], xcr[j], Ax[i]);
+        Ax[i] = fma(SW[q], xcl[j], Ax[i]);
+        Ax[j] = fma(Ew, xbl[i], Ax[j]);
+        Ax[j] = fma(pS[q], xa[i], Ax[j]);
+        Ax[j] = fma(SEnw, xal[i], Ax[j]);
+        Ax[j] = fma(SWne, xar[i], Ax[j]);
+      }
+    }
+    if (out_lane) {
+      const int node = r * nnx + c;
+      T res[D];
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        if (MODE == SW_FIRST || MODE == SW_SWEEP || MODE == SW_POST) {
+          const T dg = ((fl >> i) & 1) ? T(1) : Cc[i * D + i];
+          const T x0 = MODE == SW_FIRST ? T(0) : xb[i];
+          res[i] = x0 + sweep_div(omega * (bv[i] - Ax[i]), dg);
+        } else if (MODE == SW_RESID) {
+          res[i] = bv[i] - Ax[i];
+        } else {
+          res[i] = Ax[i];
+        }
+      }
+      store_node<D, T>(os, node, res);
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      xa[d] = xb[d];
+      xal[d] = xbl[d];
+      xar[d] = xbr[d];
+      xb[d] = xc[d];
+      xbl[d] = xcl[d];
+      xbr[d] = xcr[d];
+      xc[d] = nxc[d];
+      bv[d] = nbv[d];
+    }
+#pragma unroll
+    for (int q = 0; q < DD; ++q) {
+      pS[q] = S[q];
+      pSE[q] = SE[q];
+      pSW[q] = SW[q];
+      Cc[q] = nC[q];
+      E[q] = nE[q];
+      S[q] = nS[q];
+      SE[q] = nSE[q];
+      SW[q] = nSW[q];
+    }
+    fl = nfl;
+  }
+}
+
+// ---- restriction: column-marching full weighting ---------------------------------
+//
+// rc = P_c (R r_f), the x pass then the y pass of torch_mg._restrict_axis
+// (sttopt/torch_mg.py:84-93): per axis, (block I weighted 1 - j/k) + (block I-1 weighted
+// j/k), the last fine value landing on the last coarse node.  A warp marches down a
+// strip of coarse columns; each lane loads its coarse column's own kx fine columns and
+// takes the left neighbour's from the lane beside it, so every fine value is loaded
+// once.  The x-pass values of the fine rows shared by consecutive coarse rows are kept.
+template <int D, typename T>
+__global__ void __launch_bounds__(kQThreads) restrict_kernel(
+    const T* __restrict__ rf, long long f_rs, int fnnx, int fnny, T* __restrict__ rc, long long c_rs,
+    int cnnx, int cnny, int kx, int ky, const uint8_t* __restrict__ cfixed,
+    const RowState* __restrict__ rst) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const T* f = rf + (size_t)s * f_rs;
+  T* o = rc + (size_t)s * c_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int C = strip * kQCols - 1 + lane;
+  const bool out_lane = lane >= 1 && lane <= kQCols && C < cnnx;
+  const bool col_ok = C >= 0 && C < cnnx;
+  const int R0 = blockIdx.y * kQRows;
+  const int R1 = min(R0 + kQRows, cnny);
+  // x pass of fine row fr at this lane's coarse column
+  auto xpass = [&](int fr, T(&g)[D]) {
+    T own[3][D], left[3][D];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int fc = kx * C + j;
+      const bool ok = j < kx && col_ok && fr >= 0 && fr < fnny && fc < fnnx;
+      T v[D];
+      if (ok) {
+        load_node<D, T>(f, (long long)fr * fnnx + fc, v);
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[d] = T(0);
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        own[j][d] = v[d];
+        left[j][d] = __shfl_up_sync(0xffffffffu, v[d], 1);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      if (kx == 1) {
+        g[d] = own[0][d];
+        continue;
+      }
+      T lo = T(0), hi = T(0);
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        if (j < kx) lo += own[j][d] * T(1.0 - (double)j / kx);
+#pragma unroll
+      for (int j = 1; j < 3; ++j)
+        if (j < kx) hi += left[j][d] * T((double)j / kx);
+      g[d] = lo + hi;
+    }
+  };
+  T gprev[3][D];  // x-pass values of fine rows ky (R-1) + j, j = 1 .. ky-1
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    if (j >= 1 && j < ky && R0 >= 1) {
+      xpass(ky * (R0 - 1) + j, gprev[j]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d) gprev[j][d] = T(0);
+    }
+  }
+  for (int R = R0; R < R1; ++R) {
+    T gcur[3][D];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if (j < ky) {
+        xpass(ky * R + j, gcur[j]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) gcur[j][d] = T(0);
+      }
+    }
+    if (out_lane) {
+      const uint8_t fl = __ldg(cfixed + (size_t)R * cnnx + C);
+      T v[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        if (ky == 1) {
+          v[d] = gcur[0][d];
+        } else {
+          T lo = T(0), hi = T(0);
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            if (j < ky) lo += gcur[j][d] * T(1.0 - (double)j / ky);
+#pragma unroll
+          for (int j = 1; j < 3; ++j)
+            if (j < ky) hi += gprev[j][d] * T((double)j / ky);
+          v[d] = lo + hi;
+        }
+        if ((fl >> d) & 1) v[d] = T(0);
+      }
+      store_node<D, T>(o, (long long)R * cnnx + C, v);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int d = 0; d < D; ++d) gprev[j][d] = gcur[j][d];
+  }
+}
+
+// ---- prolongation -----------------------------------------------------------------
+//
+// x_f += P_f (P e_c), the x pass then the y pass of torch_mg._interp_axis
+// (sttopt/torch_mg.py:75-81).  One thread per fine node on a 2-D grid (x = columns,
+// y = fine rows), so the coarse values a warp reads are contiguous and L1-resident.
+constexpr int kProlongThreads = 128;
 
 template <int D, typename T>
-__global__ void __launch_bounds__(256) coarse_solve_kernel(
+__global__ void __launch_bounds__(kProlongThreads) prolong_kernel(
+    const T* __restrict__ ec, long long c_rs, int cnnx, int cnny, T* __restrict__ xf, long long f_rs,
+    int fnnx, int fnny, int kx, int ky, const uint8_t* __restrict__ ffixed,
+    const RowState* __restrict__ rst) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const int r = blockIdx.y;
+  const int c = blockIdx.x * kProlongThreads + threadIdx.x;
+  if (c >= fnnx) return;
+  const T* e = ec + (size_t)s * c_rs;
+  T* x = xf + (size_t)s * f_rs;
+  const long long node = (long long)r * fnnx + c;
+  T v[D], pv[D];
+  load_node<D, T>(x, node, v);
+  prolong_at<D, T>(e, cnnx, kx, ky, r, c, pv);
+  const uint8_t fl = __ldg(ffixed + node);
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    if (!((fl >> d) & 1)) v[d] += pv[d];
+  store_node<D, T>(x, node, v);
+}
+
+// ---- coarsest level: block-banded Cholesky solve (one CTA per batch row) ----------
+//
+// Forward  y_k = Dinv_k (b_k - E_k y_{k-1}),  backward x_k = Dinv_k^T (y_k - E_{k+1}^T x_{k+1}):
+// 2 nb sequential steps of two B x B GEMVs.  The steps are latency-bound, so each GEMV
+// row is split over 4 threads (a quad: NC = B / 4 columns each, 128-bit loads, two
+// shuffles), and the matrices of step j+1 are loaded into registers while step j
+// computes.  blockDim = 4 B.
+
+template <int NC>
+STT_DEV void load_quad_row(const double* __restrict__ M, int B, int i, int q, double (&reg)[NC]) {
+  const double2* src = reinterpret_cast<const double2*>(M + (size_t)i * B + q * NC);
+#pragma unroll
+  for (int c = 0; c < NC / 2; ++c) {
+    const double2 t = __ldg(src + c);
+    reg[2 * c] = t.x;
+    reg[2 * c + 1] = t.y;
+  }
+}
+
+template <int NC>
+STT_DEV double quad_dot(const double (&reg)[NC], const double* __restrict__ v, int q) {
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc = fma(reg[c], v[q * NC + c], acc);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+  return acc;
+}
+
+template <int D, typename T, int NC>
+__global__ void __launch_bounds__(4 * 4 * NC) coarse_solve_kernel(
     const T* __restrict__ b, T* __restrict__ x, long long rs, const double* __restrict__ blocks,
-    int B, int nb, int by_col, int nnx, int nny, const uint8_t* __restrict__ fixed,
+    int nb, int by_col, int nnx, int nny, const uint8_t* __restrict__ fixed,
     double* __restrict__ scratch, const int* __restrict__ row_map, int hrows,
     const RowState* __restrict__ rst) {
-  extern __shared__ double csm[];
-  double* vp = csm;      // previous block's solution
-  double* tv = csm + B;  // right-hand side of the current block
+  constexpr int B = 4 * NC;
+  __shared__ double vp[B];  // previous step's block solution
+  __shared__ double tv[B];  // current step's right-hand side
   const int s = blockIdx.x;
   if (rst && !rst[s].active) return;
   const int h = hier_row(row_map, hrows, s);
   const double* bh = blocks + (size_t)h * nb * 4 * B * B;
   const long long nnode = (long long)nnx * nny, n = nnode * D, np = (long long)nb * B;
   double* y = scratch + (size_t)s * np;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  auto node_of = [&](long long P, int& r, int& c, int& i) {
+  const int tid = threadIdx.x, i = tid >> 2, q = tid & 3;
+  auto node_of = [&](long long P, int& r, int& c, int& d) {
     const long long nd = P / D;
-    i = (int)(P - nd * D);
+    d = (int)(P - nd * D);
     if (by_col) {
       c = (int)(nd / nny);
       r = (int)(nd - (long long)c * nny);
@@ -276,57 +491,66 @@ __global__ void __launch_bounds__(256) coarse_solve_kernel(
   for (long long P = tid; P < np; P += blockDim.x) {
     double v = 0.0;
     if (P < n) {
-      int r, c, i;
-      node_of(P, r, c, i);
-      v = (double)bs[((size_t)r * nnx + c) * D + i];
+      int r, c, d;
+      node_of(P, r, c, d);
+      v = (double)bs[((size_t)r * nnx + c) * D + d];
     }
     y[P] = v;
   }
-  __syncthreads();
-  auto gemv = [&](const double* M, const double* v, double* o, bool sub, const double* base) {
-    // o[i] = (sub ? base[i] - (M v)[i] : (M v)[i]), M row-major B x B; warp per row
-    for (int i = warp; i < B; i += nw) {
-      double acc = 0.0;
-      for (int l = lane; l < B; l += 32) acc = fma(M[(size_t)i * B + l], v[l], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) o[i] = sub ? base[i] - acc : acc;
+  // step j < nb: forward block k = j, matrices (E_k | none, Dinv_k);
+  // step j >= nb: backward block k = 2 nb - 1 - j, matrices (E_{k+1}^T | none, Dinv_k^T)
+  auto mats = [&](int j, const double*& A, const double*& M) {
+    if (j < nb) {
+      const double* blk = bh + (size_t)j * 4 * B * B;
+      A = j > 0 ? blk + 2 * (size_t)B * B : nullptr;
+      M = blk;
+    } else {
+      const int k = 2 * nb - 1 - j;
+      A = k < nb - 1 ? bh + (size_t)(k + 1) * 4 * B * B + 3 * (size_t)B * B : nullptr;
+      M = bh + (size_t)k * 4 * B * B + (size_t)B * B;
     }
   };
-  // forward: y_k = Dinv_k (b_k - E_k y_{k-1})
-  for (int k = 0; k < nb; ++k) {
-    const double* blk = bh + (size_t)k * 4 * B * B;
-    if (k == 0) {
-      for (int i = tid; i < B; i += blockDim.x) tv[i] = y[i];
-    } else {
-      gemv(blk + 2 * (size_t)B * B, vp, tv, true, y + (size_t)k * B);
+  double ra[NC], rm[NC], na[NC], nm[NC];
+  const double *A, *M;
+  mats(0, A, M);
+  if (A) load_quad_row<NC>(A, B, i, q, ra);
+  load_quad_row<NC>(M, B, i, q, rm);
+  __syncthreads();
+  for (int j = 0; j < 2 * nb; ++j) {
+    const int k = j < nb ? j : 2 * nb - 1 - j;
+    const bool hasA = A != nullptr;
+    // prefetch the next step's matrices
+    const double *A2 = nullptr, *M2 = nullptr;
+    if (j + 1 < 2 * nb) {
+      mats(j + 1, A2, M2);
+      if (A2) load_quad_row<NC>(A2, B, i, q, na);
+      load_quad_row<NC>(M2, B, i, q, nm);
+    }
+    double rhs = y[(size_t)k * B + i];
+    if (hasA) rhs -= quad_dot<NC>(ra, vp, q);
+    if (q == 0) tv[i] = rhs;
+    __syncthreads();
+    const double v = quad_dot<NC>(rm, tv, q);
+    __syncthreads();  // every quad has read vp and tv
+    if (q == 0) {
+      vp[i] = v;
+      y[(size_t)k * B + i] = v;
     }
     __syncthreads();
-    gemv(blk, tv, vp, false, nullptr);
-    __syncthreads();
-    for (int i = tid; i < B; i += blockDim.x) y[(size_t)k * B + i] = vp[i];
-    __syncthreads();
-  }
-  // backward: x_k = Dinv_k^T (y_k - E_{k+1}^T x_{k+1}); vp holds x_{k+1}
-  for (int k = nb - 1; k >= 0; --k) {
-    const double* blk = bh + (size_t)k * 4 * B * B;
-    if (k == nb - 1) {
-      for (int i = tid; i < B; i += blockDim.x) tv[i] = y[(size_t)k * B + i];
-    } else {
-      const double* nxt = bh + (size_t)(k + 1) * 4 * B * B;
-      gemv(nxt + 3 * (size_t)B * B, vp, tv, true, y + (size_t)k * B);
+    A = A2;
+    M = M2;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      ra[c] = na[c];
+      rm[c] = nm[c];
     }
-    __syncthreads();
-    gemv(blk + (size_t)B * B, tv, vp, false, nullptr);
-    __syncthreads();
-    for (int i = tid; i < B; i += blockDim.x) y[(size_t)k * B + i] = vp[i];
-    __syncthreads();
   }
   T* xs = x + (size_t)s * rs;
   for (long long P = tid; P < n; P += blockDim.x) {
-    int r, c, i;
-    node_of(P, r, c, i);
+    int r, c, d;
+    node_of(P, r, c, d);
     const long long node = (long long)r * nnx + c;
-    xs[node * D + i] = ((fixed[node] >> i) & 1) ? T(0) : T(y[P]);
+    xs[node * D + d] = ((fixed[node] >> d) & 1) ? T(0) : T(y[P]);
   }
 }
 

@@ -95,6 +95,7 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     lv.nnode = (long long)lv.nnx * lv.nny;
     lv.ndof = lv.nnode * d;
     lv.nel = (long long)nx * ny;
+    lv.rs_rho = (lv.nel + 3) & ~3LL;
     lv.kx = lv.ky = 1;
     ++L;
     if ((long long)nx * ny <= h.mce) break;
@@ -112,8 +113,8 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     LevelDesc& lv = h.lv[l];
     lv.fixed = (uint8_t*)carve(p, used, lv.nnode);
     if (l == 0) {
-      lv.rho64 = (double*)carve(p, used, 8LL * h.hrows * lv.nel);
-      if (f32) lv.rho32 = (float*)carve(p, used, 4LL * h.hrows * lv.nel);
+      lv.rho64 = (double*)carve(p, used, 8LL * h.hrows * lv.rs_rho);
+      if (f32) lv.rho32 = (float*)carve(p, used, 4LL * h.hrows * lv.rs_rho);
       lv.rdiag64 = (double*)carve(p, used, 8LL * h.hrows * lv.ndof);
       if (f32) lv.rdiag32 = (float*)carve(p, used, 4LL * h.hrows * lv.ndof);
     }
@@ -155,11 +156,11 @@ __global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, 
 }
 
 __global__ void copy_rows_kernel(const double* __restrict__ in, long long in_rs,
-                                 double* __restrict__ out, long long n) {
+                                 double* __restrict__ out, long long out_rs, long long n) {
   const int row = blockIdx.y;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    out[(size_t)row * n + i] = in[(size_t)row * in_rs + i];
+    out[(size_t)row * out_rs + i] = in[(size_t)row * in_rs + i];
 }
 
 // Coarse fixed flags: the fine flags at the collocated nodes (torch_mg.py:376).
@@ -526,7 +527,7 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   const int H = h->hrows;
   LevelDesc& l0 = h->lv[0];
   // level 0: copies of the densities, the lumped reaction diagonal, the flags
-  copy_rows_kernel<<<dim3(grid1(l0.nel), H), 256, 0, st>>>(rho, rho_rs, l0.rho64, l0.nel);
+  copy_rows_kernel<<<dim3(grid1(l0.nel), H), 256, 0, st>>>(rho, rho_rs, l0.rho64, l0.rs_rho, l0.nel);
   if (reaction) {
     STT_TRY(stt_lumped_reaction(D, h->nelx, h->nely, H, reaction, r_rs, l0.rdiag64, l0.ndof,
                                 (stt_stream_t)st));
@@ -538,7 +539,7 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   else
     STT_TRY(check_cuda(cudaMemsetAsync(l0.fixed, 0, l0.nnode, st), "memset"));
   if (h->precision == STT_FP32) {
-    convert_kernel<double, float><<<grid1(H * l0.nel), 256, 0, st>>>(l0.rho64, l0.rho32, H * l0.nel);
+    convert_kernel<double, float><<<grid1(H * l0.rs_rho), 256, 0, st>>>(l0.rho64, l0.rho32, H * l0.rs_rho);
     convert_kernel<double, float><<<grid1(H * l0.ndof), 256, 0, st>>>(l0.rdiag64, l0.rdiag32, H * l0.ndof);
   }
   STT_TRY(check_launch("level0 copies"));
@@ -565,7 +566,7 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     double* kc = (l % 2 == 1) ? h->keffA : h->keffB;
     const dim3 g(grid1(c.nel * NK), H);
     if (l == 1)
-      keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.nel, reaction, r_rs, S + kTableStride,
+      keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride,
                                                      S + 2 * kTableStride, f.nelx, f.kx, f.ky, c.nelx,
                                                      (int)c.nel, kc);
     else
@@ -584,7 +585,7 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     KEq<D, double> ke;
     for (int i = 0; i < NK * NK; ++i) ke.v[i] = h->KE[i];
     stencil_kernel<D, DensitySource<D>><<<dim3(grid1(cl.nnode), H), 256, 0, st>>>(
-        DensitySource<D>{l0.rho64, l0.nel, reaction, r_rs, ke}, cl.fixed, cl.nelx, cl.nely, cl.st64);
+        DensitySource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, ke}, cl.fixed, cl.nelx, cl.nely, cl.st64);
   }
   return STT_OK;
 }
@@ -624,6 +625,7 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   h->hrows = hrows;
   h->precision = precision;
   h->mce = max_coarse_elements;
+  h->has_reaction = reaction != nullptr;
   for (int i = 0; i < 16 * d * d; ++i) h->KE[i] = KE[i];
   const long long need = plan_hierarchy(*h, nullptr);
   if (ws_bytes < need) {
@@ -700,7 +702,7 @@ extern "C" int stt_hier_level_diag(const stt_hier* h, int level, double* out, st
   const LevelDesc& lv = h->lv[level];
   cudaStream_t st = (cudaStream_t)stream;
   if (level == 0)
-    return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.nel, lv.rdiag64, lv.ndof,
+    return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.rs_rho, lv.rdiag64, lv.ndof,
                        lv.fixed, out, lv.ndof, h->KE, stream);
   if (h->d == 2)
     stencil_diag_kernel<2><<<dim3(grid1(lv.nnode), h->hrows), 256, 0, st>>>(lv.st64, lv.fixed, lv.nnode, out);

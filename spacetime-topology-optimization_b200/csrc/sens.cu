@@ -6,8 +6,12 @@
 // (sttopt/virtual_heat.py:162-166) and the PCG vector steps for arbitrary operators.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "errors.h"
+
+namespace cg = cooperative_groups;
 
 namespace stt {
 
@@ -187,23 +191,46 @@ __global__ void heat_adjoint_load_kernel(const double* __restrict__ w, double sc
 
 // ---- PCG vector steps (arbitrary operator path) -----------------------------------
 
-__global__ void vec_dots_kernel(long long n, const double* __restrict__ a0, const double* __restrict__ b0,
-                                const double* __restrict__ a1, const double* __restrict__ b1,
-                                const double* __restrict__ a2, const double* __restrict__ b2,
-                                long long rs, int k, double* __restrict__ dots) {
-  // one block per row, deterministic
-  __shared__ double scratch[8];
-  const int s = blockIdx.x;
+// Dot products of up to three vector pairs per row.  One thread-block cluster of
+// kDotCluster CTAs per row: each CTA reduces a fixed contiguous chunk in a fixed order,
+// and CTA 0 of the cluster sums the CTAs' partials in rank order through distributed
+// shared memory -- deterministic, and no global scratch.
+constexpr int kDotCluster = 8;
+constexpr int kDotThreads = 512;
+
+__global__ void __cluster_dims__(kDotCluster, 1, 1) __launch_bounds__(kDotThreads)
+    vec_dots_kernel(long long n, const double* __restrict__ a0, const double* __restrict__ b0,
+                    const double* __restrict__ a1, const double* __restrict__ b1,
+                    const double* __restrict__ a2, const double* __restrict__ b2, long long rs, int k,
+                    double* __restrict__ dots) {
+  __shared__ double scratch[kDotThreads / 32];
+  __shared__ double part[3];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int s = blockIdx.y;
+  const long long lo = n * rank / kDotCluster, hi = n * (rank + 1) / kDotCluster;
   const double* A[3] = {a0, a1, a2};
   const double* Bv[3] = {b0, b1, b2};
   for (int j = 0; j < k; ++j) {
-    double acc = 0.0;
     const double* a = A[j] + (size_t)s * rs;
     const double* b = Bv[j] + (size_t)s * rs;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) acc = fma(a[i], b[i], acc);
-    acc = block_sum<256>(acc, scratch);
-    if (threadIdx.x == 0) dots[(size_t)s * k + j] = acc;
+    double acc0 = 0.0, acc1 = 0.0;
+    long long i = lo + threadIdx.x;
+    for (; i + kDotThreads < hi; i += 2 * kDotThreads) {
+      acc0 = fma(__ldg(a + i), __ldg(b + i), acc0);
+      acc1 = fma(__ldg(a + i + kDotThreads), __ldg(b + i + kDotThreads), acc1);
+    }
+    if (i < hi) acc0 = fma(__ldg(a + i), __ldg(b + i), acc0);
+    const double t = block_sum<kDotThreads>(acc0 + acc1, scratch);
+    if (threadIdx.x == 0) part[j] = t;
   }
+  cluster.sync();
+  if (rank == 0 && threadIdx.x < k) {
+    double t = 0.0;
+    for (int r = 0; r < kDotCluster; ++r) t += cluster.map_shared_rank(part, r)[threadIdx.x];
+    dots[(size_t)s * k + threadIdx.x] = t;
+  }
+  cluster.sync();
 }
 
 __global__ void vec_cg_update_kernel(long long n, const double* __restrict__ alpha, double* __restrict__ x,
@@ -307,8 +334,10 @@ extern "C" int stt_vec_dots(int nrows, long long n, const double* a0, const doub
                             const double* b1, const double* a2, const double* b2, long long rs, double* dots,
                             stt_stream_t stream) {
   if (nrows <= 0 || n <= 0 || !a0 || !b0 || !dots) return set_error(STT_ERR_INVALID, "stt_vec_dots: bad arguments");
+  if (nrows > 65535) return set_error(STT_ERR_INVALID, "stt_vec_dots: too many rows");
   const int k = (a1 && b1) ? ((a2 && b2) ? 3 : 2) : 1;
-  vec_dots_kernel<<<nrows, 256, 0, (cudaStream_t)stream>>>(n, a0, b0, a1, b1, a2, b2, rs, k, dots);
+  vec_dots_kernel<<<dim3(kDotCluster, nrows), kDotThreads, 0, (cudaStream_t)stream>>>(n, a0, b0, a1, b1, a2,
+                                                                                       b2, rs, k, dots);
   return check_launch("vec_dots");
 }
 

@@ -31,11 +31,18 @@ static int ew_blocks(long long n) {
   return (int)std::min<long long>(std::max<long long>(g, 1), 2048);
 }
 
-static dim3 tile_grid(int nelx, int nely, int rows) {
-  return dim3((nelx + 1 + kTX - 1) / kTX, (nely + 1 + kTY - 1) / kTY, rows);
+static dim3 tile_grid(int nelx, int nely, int rows) { return q4_grid(nelx, nely, rows); }
+
+// prolong_kernel: one thread per fine node, x = fine columns, y = fine rows.
+static dim3 prolong_grid(int fnnx, int fnny, int rows) {
+  return dim3((fnnx + kProlongThreads - 1) / kProlongThreads, fnny, rows);
 }
 
 // ---- workspace plan ---------------------------------------------------------------
+
+// Row stride of the cycle's own per-level vectors: ndof rounded up to 4 words, so every
+// batch row starts 16-byte aligned (the tile kernels' 128-bit staging needs it).
+static long long vstride(long long ndof) { return (ndof + 3) & ~3LL; }
 
 struct SolveWS {
   RowState* rs;
@@ -73,11 +80,11 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
   w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
   w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
   w.Ap = (double*)carve(base, used, 8LL * nrows * l0.ndof);
-  w.z = carve(base, used, (long long)es * nrows * l0.ndof);
-  w.zold = carve(base, used, (long long)es * nrows * l0.ndof);
-  if (h->precision == STT_FP32) w.b0 = carve(base, used, 4LL * nrows * l0.ndof);
+  w.z = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
+  w.zold = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
+  if (h->precision == STT_FP32) w.b0 = carve(base, used, 4LL * nrows * vstride(l0.ndof));
   for (int l = 0; l < h->nlevels; ++l) {
-    const long long nd = h->lv[l].ndof;
+    const long long nd = vstride(h->lv[l].ndof);
     w.x[l] = carve(base, used, (long long)es * nrows * nd);
     w.t[l] = carve(base, used, (long long)es * nrows * nd);
     if (l > 0) w.b[l] = carve(base, used, (long long)es * nrows * nd);
@@ -103,6 +110,7 @@ struct Cycle {
   const RowState* rst;
   cudaStream_t st;
   KEq<D, T> ke;
+  T* final_out = nullptr;  // where level 0's last sweep writes (row stride vstride(ndof0))
 
   T* X(int l) const { return (T*)w.x[l]; }
   T* Tt(int l) const { return (T*)w.t[l]; }
@@ -112,6 +120,7 @@ struct Cycle {
     else return (const T*)h->lv[0].rho64;
   }
   const T* rdiag0() const {
+    if (!h->has_reaction) return nullptr;
     if constexpr (sizeof(T) == 4) return (const T*)h->lv[0].rdiag32;
     else return (const T*)h->lv[0].rdiag64;
   }
@@ -120,38 +129,50 @@ struct Cycle {
     else return (const T*)h->lv[l].st64;
   }
 
-  // One smoother / residual / apply pass at level l: out = op(x, b).
+  // One smoother / residual / apply pass at level l: out = op(x, b); SW_POST reads
+  // x + P(pro.ec) (the coarse correction) in place of x.
   template <int MODE>
-  void pass(int l, const T* x, long long x_rs, const T* b, long long b_rs, T* out, long long o_rs) {
+  void pass(int l, const T* x, long long x_rs, const T* b, long long b_rs, T* out, long long o_rs,
+            ProlongSrc<T> pro = ProlongSrc<T>{nullptr, 0, 1, 1, 1}) {
     const LevelDesc& lv = h->lv[l];
     if (l == 0) {
-      l0_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
-          x, x_rs, b, b_rs, out, o_rs, rho0(), lv.nel, rdiag0(), lv.ndof, lv.fixed, h->row_map,
-          h->hrows, rst, lv.nelx, lv.nely, omega, ke);
+      l0_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+          x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
+          h->hrows, rst, lv.nelx, lv.nely, omega, ke, 0, pro);
     } else {
-      st_sweep_kernel<D, T, MODE><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
-          x, b, out, lv.ndof, stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega);
+      st_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+          x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
+          pro);
     }
   }
 
   void coarse(int l, const T* b, T* x) {
     const LevelDesc& lv = h->lv[l];
     const CoarseDesc& co = h->co;
-    coarse_solve_kernel<D, T><<<nrows, 256, 2 * co.B * sizeof(double), st>>>(
-        b, x, lv.ndof, co.blocks, co.B, co.nb, co.by_col, lv.nnx, lv.nny, lv.fixed, w.cscratch,
-        h->row_map, h->hrows, rst);
+#define STT_COARSE(NC)                                                                          \
+  coarse_solve_kernel<D, T, NC><<<nrows, 16 * NC, 0, st>>>(b, x, vstride(lv.ndof), co.blocks, co.nb, co.by_col, \
+                                                          lv.nnx, lv.nny, lv.fixed, w.cscratch,       \
+                                                          h->row_map, h->hrows, rst)
+    switch (co.B) {
+      case 32: STT_COARSE(8); break;
+      case 64: STT_COARSE(16); break;
+      case 96: STT_COARSE(24); break;
+      case 128: STT_COARSE(32); break;
+      default: set_error(STT_ERR_INVALID, "coarse band block size above 128 is not supported");
+    }
+#undef STT_COARSE
   }
 
   // Solves level l approximately for right-hand side b (row stride b_rs); returns the
   // buffer holding the result (row stride ndof_l).
   T* cycle(int l, const T* b, long long b_rs) {
     const LevelDesc& lv = h->lv[l];
-    const long long nd = lv.ndof;
+    const long long nd = vstride(lv.ndof);
     if (l == h->nlevels - 1) {
       // the coarse solve reads b with the level's own row stride
       const T* bb = b;
       if (b_rs != nd) {
-        rows_convert_kernel<T, T><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(b, b_rs, Tt(l), nd, nd, rst);
+        rows_convert_kernel<T, T><<<dim3(ew_blocks(lv.ndof), nrows), kEwThreads, 0, st>>>(b, b_rs, Tt(l), nd, lv.ndof, rst);
         bb = Tt(l);
       }
       coarse(l, bb, X(l));
@@ -167,27 +188,30 @@ struct Cycle {
     // residual into xb, restricted into b_{l+1}
     pass<SW_RESID>(l, xa, nd, b, b_rs, xb, nd);
     const LevelDesc& cl = h->lv[l + 1];
+    const long long cnd = vstride(cl.ndof);
     T* bc = (T*)w.b[l + 1];
-    restrict_kernel<D, T><<<dim3(grid1(cl.nnode), nrows), 256, 0, st>>>(
-        xb, nd, lv.nnx, bc, cl.ndof, cl.nnx, cl.nny, lv.kx, lv.ky, cl.fixed, rst);
-    T* ec = cycle(l + 1, bc, cl.ndof);
+    restrict_kernel<D, T><<<tile_grid(cl.nelx, cl.nely, nrows), kQThreads, 0, st>>>(
+        xb, nd, lv.nnx, lv.nny, bc, cnd, cl.nnx, cl.nny, lv.kx, lv.ky, cl.fixed, rst);
+    T* ec = cycle(l + 1, bc, cnd);
     if (gamma > 1) {
       T* acc = (T*)w.acc[l + 1];
       T* rhs = (T*)w.rhs2[l + 1];
-      rows_convert_kernel<T, T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(ec, cl.ndof, acc, cl.ndof, cl.ndof, rst);
+      rows_convert_kernel<T, T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(ec, cnd, acc, cnd, cl.ndof, rst);
       for (int g = 1; g < gamma; ++g) {
         // rhs = b_c - A_c acc
-        pass<SW_RESID>(l + 1, acc, cl.ndof, bc, cl.ndof, rhs, cl.ndof);
-        T* e2 = cycle(l + 1, rhs, cl.ndof);
-        rows_axpy_kernel<T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(e2, acc, cl.ndof, cl.ndof, rst);
+        pass<SW_RESID>(l + 1, acc, cnd, bc, cnd, rhs, cnd);
+        T* e2 = cycle(l + 1, rhs, cnd);
+        rows_axpy_kernel<T><<<dim3(ew_blocks(cl.ndof), nrows), kEwThreads, 0, st>>>(e2, acc, cnd, cl.ndof, rst);
       }
       ec = acc;
     }
-    prolong_add_kernel<D, T><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
-        ec, cl.ndof, cl.nnx, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
+    prolong_kernel<D, T><<<prolong_grid(lv.nnx, lv.nny, nrows), kProlongThreads, 0, st>>>(
+        ec, cnd, cl.nnx, cl.nny, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
+    // post-smoothing; level 0's last sweep writes straight into final_out when given
     for (int k = 0; k < n_smooth; ++k) {
-      pass<SW_SWEEP>(l, xa, nd, b, b_rs, xb, nd);
-      std::swap(xa, xb);
+      T* dst = (l == 0 && final_out && k == n_smooth - 1) ? final_out : xb;
+      pass<SW_SWEEP>(l, xa, nd, b, b_rs, dst, nd);
+      if (dst == xb) std::swap(xa, xb); else xa = dst;
     }
     return xa;
   }
@@ -204,7 +228,7 @@ struct PcgParams {
 // r = b - A x (or r = b when x is null), reductions ||r||^2 and ||b||^2.
 // replace: keep bnorm and only re-test convergence (true-residual replacement).
 template <int D>
-__global__ void __launch_bounds__(kNT) pcg_init_kernel(
+__global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
     const double* __restrict__ b, long long b_rs, const double* __restrict__ x, long long x_rs,
     double* __restrict__ r, long long r_rs, const double* __restrict__ rho, long long rho_rs,
     const double* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
@@ -212,49 +236,55 @@ __global__ void __launch_bounds__(kNT) pcg_init_kernel(
     int nelx, int nely, KEq<D, double> ke, PcgParams pp, int replace) {
   const int s = blockIdx.z;
   if (replace && !rst[s].active) return;
-  __shared__ Q4Smem<D, double, double> sm;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
-  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
-  if (x) {
-    load_rho_tile<D, double, double>(sm, rho + (size_t)h * rho_rs, r0, c0, nelx, nely);
-    const double* xs = x + (size_t)s * x_rs;
-    load_u_tile<D, double, double>(sm, r0, c0, nnx, nny, [&](int node, double(&v)[D]) {
-      load_node<D, double>(xs, node, v);
-#pragma unroll
-      for (int j = 0; j < D; ++j)
-        if (is_fixed(fixed, node, j)) v[j] = 0.0;
-    });
-    __syncthreads();
-  }
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int rr = r0 + ty, cc = c0 + tx;
+  const double* xs = x ? x + (size_t)s * x_rs : nullptr;
+  const double* rh = rho + (size_t)h * rho_rs;
+  const double* rdh = rdiag ? rdiag + (size_t)h * rd_rs : nullptr;
+  const double* bs = b + (size_t)s * b_rs;
+  double* rs_ = r + (size_t)s * r_rs;
   double vals[2] = {0.0, 0.0};
-  if (rr < nny && cc < nnx) {
+  auto loadu = [&](int rr, int cc, double(&v)[D]) {
     const int node = rr * nnx + cc;
-    double bv[D], Ax[D], res[D];
-    load_node<D, double>(b + (size_t)s * b_rs, node, bv);
+    load_node<D, double>(xs, node, v);
+    const uint8_t fl = __ldg(fixed + node);
 #pragma unroll
-    for (int i = 0; i < D; ++i) Ax[i] = 0.0;
-    if (x) {
-      tile_Ku<D, double, double>(sm, ty, tx, ke, Ax);
-      const double* rd = rdiag + (size_t)h * rd_rs + (size_t)node * D;
-#pragma unroll
-      for (int i = 0; i < D; ++i) {
-        Ax[i] = fma(__ldg(rd + i), sm.u[ty + 1][tx + 1][i], Ax[i]);
-        if (is_fixed(fixed, node, i)) Ax[i] = 0.0;
-      }
-    }
+    for (int d = 0; d < D; ++d)
+      if ((fl >> d) & 1) v[d] = 0.0;
+  };
+  auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
+  auto loadx = [&](int rr, int cc) {
+    RhsX<D, double> e;
+    const int node = rr * nnx + cc;
+    load_node<D, double>(bs, node, e.b);
+    e.fl = __ldg(fixed + node);
+    return e;
+  };
+  auto emit = [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const RhsX<D, double>& ex) {
+    const int node = rr * nnx + cc;
+    double res[D];
+    const double* bv = ex.b;
+    const uint8_t fl = ex.fl;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      res[i] = bv[i] - Ax[i];
+      double a = 0.0;
+      if (xs) {
+        a = Ax[i];
+        if (rdh) a = fma(__ldg(rdh + node * D + i), uc[i], a);
+        if ((fl >> i) & 1) a = 0.0;
+      }
+      res[i] = bv[i] - a;
       vals[0] = fma(res[i], res[i], vals[0]);
       vals[1] = fma(bv[i], bv[i], vals[1]);
     }
-    store_node<D, double>(r + (size_t)s * r_rs, node, res);
-  }
+    store_node<D, double>(rs_, node, res);
+  };
+  if (xs)
+    march<D, double, true, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+  else
+    march<D, double, false, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-  grid_reduce<2, kNT>(red, s, bid, vals, [&](const double* t) {
+  grid_reduce<2, kQThreads>(red, s, bid, vals, [&](const double* t) {
     RowState& S = rst[s];
     if (!replace) {
       const double bn = sqrt(t[1]);
@@ -273,46 +303,39 @@ __global__ void __launch_bounds__(kNT) pcg_init_kernel(
 }
 
 // Ap = A p (projected, + lumped reaction), pAp = p . Ap, alpha = safe_div(rz, pAp).
+// p is zero at fixed dofs by construction (it is built from the projected z).
 template <int D>
-__global__ void __launch_bounds__(kNT) pcg_pap_kernel(
+__global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
     const double* __restrict__ p, double* __restrict__ Ap, long long rs,
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
     long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map,
     int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely, KEq<D, double> ke) {
   const int s = blockIdx.z;
   if (!rst[s].active) return;
-  __shared__ Q4Smem<D, double, double> sm;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
-  const int r0 = blockIdx.y * kTY, c0 = blockIdx.x * kTX;
-  load_rho_tile<D, double, double>(sm, rho + (size_t)h * rho_rs, r0, c0, nelx, nely);
   const double* ps = p + (size_t)s * rs;
-  load_u_tile<D, double, double>(sm, r0, c0, nnx, nny, [&](int node, double(&v)[D]) {
-    load_node<D, double>(ps, node, v);
-#pragma unroll
-    for (int j = 0; j < D; ++j)
-      if (is_fixed(fixed, node, j)) v[j] = 0.0;
-  });
-  __syncthreads();
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int rr = r0 + ty, cc = c0 + tx;
+  const double* rh = rho + (size_t)h * rho_rs;
+  const double* rdh = rdiag ? rdiag + (size_t)h * rd_rs : nullptr;
+  double* As = Ap + (size_t)s * rs;
   double vals[1] = {0.0};
-  if (rr < nny && cc < nnx) {
-    const int node = rr * nnx + cc;
-    double Ax[D];
-    tile_Ku<D, double, double>(sm, ty, tx, ke, Ax);
-    const double* rd = rdiag + (size_t)h * rd_rs + (size_t)node * D;
+  march<D, double, true, false, FlagX>(
+      ke, nnx, nny, [&](int rr, int cc, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); },
+      [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); },
+      [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
+      [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const FlagX& ex) {
+        const int node = rr * nnx + cc;
+        const uint8_t fl = ex.fl;
 #pragma unroll
-    for (int i = 0; i < D; ++i) {
-      Ax[i] = fma(__ldg(rd + i), sm.u[ty + 1][tx + 1][i], Ax[i]);
-      if (is_fixed(fixed, node, i)) Ax[i] = 0.0;
-      // p . Ap with p as stored (unprojected p is zero at fixed dofs by construction)
-      vals[0] = fma(ps[(size_t)node * D + i], Ax[i], vals[0]);
-    }
-    store_node<D, double>(Ap + (size_t)s * rs, node, Ax);
-  }
+        for (int i = 0; i < D; ++i) {
+          if (rdh) Ax[i] = fma(__ldg(rdh + node * D + i), uc[i], Ax[i]);
+          if ((fl >> i) & 1) Ax[i] = 0.0;
+          vals[0] = fma(uc[i], Ax[i], vals[0]);
+        }
+        store_node<D, double>(As, node, Ax);
+      });
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-  grid_reduce<1, kNT>(red, s, bid, vals, [&](const double* t) {
+  grid_reduce<1, kQThreads>(red, s, bid, vals, [&](const double* t) {
     RowState& S = rst[s];
     S.pAp = t[0];
     S.alpha = safe_div(S.rz, t[0]);
@@ -324,7 +347,7 @@ __global__ void __launch_bounds__(kNT) pcg_pap_kernel(
 __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
     double* __restrict__ x, long long x_rs, double* __restrict__ r, const double* __restrict__ p,
     const double* __restrict__ Ap, long long rs, long long n, RowState* __restrict__ rst,
-    GridRed red, PcgParams pp) {
+    GridRed red, PcgParams pp, float* __restrict__ r32, long long r32_rs) {
   const int s = blockIdx.y;
   if (!rst[s].active) return;
   const double alpha = rst[s].alpha;
@@ -332,12 +355,14 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
   double* rsv = r + (size_t)s * rs;
   const double* ps = p + (size_t)s * rs;
   const double* as = Ap + (size_t)s * rs;
+  float* r32s = r32 ? r32 + (size_t)s * r32_rs : nullptr;
   double vals[1] = {0.0};
   for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kEwThreads) {
     xs[i] = xs[i] + alpha * ps[i];
     const double rv = rsv[i] - alpha * as[i];
     rsv[i] = rv;
+    if (r32s) r32s[i] = (float)rv;  // the FP32 V-cycle's right-hand side
     vals[0] = fma(rv, rv, vals[0]);
   }
   grid_reduce<1, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
@@ -356,13 +381,13 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
 template <typename TZ>
 __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
     const double* __restrict__ r, const TZ* __restrict__ z, const TZ* __restrict__ zold,
-    double* __restrict__ p, long long rs, long long n, RowState* __restrict__ rst, GridRed red,
-    int first, int flexible) {
+    double* __restrict__ p, long long rs, long long z_rs, long long n, RowState* __restrict__ rst,
+    GridRed red, int first, int flexible) {
   const int s = blockIdx.y;
   if (!rst[s].active) return;
   const double* rsv = r + (size_t)s * rs;
-  const TZ* zs = z + (size_t)s * rs;
-  const TZ* zo = zold + (size_t)s * rs;
+  const TZ* zs = z + (size_t)s * z_rs;
+  const TZ* zo = zold + (size_t)s * z_rs;
   double vals[2] = {0.0, 0.0};
   for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kEwThreads) {
@@ -388,12 +413,13 @@ __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
 template <typename TZ>
 __global__ void __launch_bounds__(kEwThreads) pcg_pupd_kernel(const TZ* __restrict__ z,
                                                               double* __restrict__ p, long long rs,
-                                                              long long n, const RowState* __restrict__ rst) {
+                                                              long long z_rs, long long n,
+                                                              const RowState* __restrict__ rst) {
   const int s = blockIdx.y;
   if (!rst[s].active) return;
   const double beta = rst[s].beta;
   double* ps = p + (size_t)s * rs;
-  const TZ* zs = z + (size_t)s * rs;
+  const TZ* zs = z + (size_t)s * z_rs;
   for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kEwThreads)
     ps[i] = ps[i] * beta + (double)zs[i];
@@ -415,26 +441,31 @@ static KEq<D, T> ke_of(const stt_hier* h) {
   return k;
 }
 
-// z = M r over all rows (rst may gate rows).  r, z FP64 with row strides.
+// z = M r over all rows (rst may gate rows).  r FP64 with row stride r_rs; zout in the
+// cycle precision with the padded stride vstride(ndof0).
 template <int D, typename T>
 static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r, long long r_rs,
-                      T* zout /* cycle precision, row stride ndof0 */, double omega, int n_smooth,
-                      int gamma, const RowState* rst, cudaStream_t st) {
+                      T* zout, double omega, int n_smooth,
+                      int gamma, const RowState* rst, cudaStream_t st, bool b0_ready = false) {
   Cycle<D, T> cyc{h, w, nrows, T(omega), n_smooth, gamma, rst, st, ke_of<D, T>(h)};
-  const long long nd = h->lv[0].ndof;
+  const long long n = h->lv[0].ndof, vs = vstride(n);
   const T* b0;
   long long b_rs;
   if constexpr (sizeof(T) == 4) {
-    rows_convert_kernel<double, float><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(
-        r, r_rs, (float*)w.b0, nd, nd, rst);
+    // the PCG update may have written the FP32 copy of r already
+    if (!b0_ready)
+      rows_convert_kernel<double, float><<<dim3(ew_blocks(n), nrows), kEwThreads, 0, st>>>(
+          r, r_rs, (float*)w.b0, vs, n, rst);
     b0 = (const T*)w.b0;
-    b_rs = nd;
+    b_rs = vs;
   } else {
     b0 = (const T*)r;
     b_rs = r_rs;
   }
+  cyc.final_out = zout;
   T* res = cyc.cycle(0, b0, b_rs);
-  rows_convert_kernel<T, T><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>(res, nd, zout, nd, nd, rst);
+  if (res != zout)
+    rows_convert_kernel<T, T><<<dim3(ew_blocks(n), nrows), kEwThreads, 0, st>>>(res, vs, zout, vs, n, rst);
   return check_launch("vcycle");
 }
 
@@ -450,12 +481,13 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   GridRed red_tile{w.partials, w.counters, (int)(tg.x * tg.y)};
   GridRed red_ew{w.partials, w.counters, ewb};
   const KEq<D, double> ke = ke_of<D, double>(h);
+  const double* rd0 = h->has_reaction ? l0.rdiag64 : nullptr;
   STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4LL * nrows, st), "memset counters"));
   STT_TRY(check_cuda(cudaMemsetAsync(w.rs, 0, sizeof(RowState) * nrows, st), "memset rows"));
   if (!has_x0) rows_zero_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, nd);
   PcgParams pp{rtol, 0, flexible};
-  pcg_init_kernel<D><<<tg, kNT, 0, st>>>(b, b_rs, has_x0 ? x : nullptr, x_rs, w.r, nd, l0.rho64, l0.nel,
-                                         l0.rdiag64, l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,
+  pcg_init_kernel<D><<<tg, kQThreads, 0, st>>>(b, b_rs, has_x0 ? x : nullptr, x_rs, w.r, nd, l0.rho64, l0.rs_rho,
+                                         rd0, l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,
                                          red_tile, h->nelx, h->nely, ke, pp, 0);
   STT_TRY(check_launch("pcg init"));
   std::vector<RowState> host(nrows);
@@ -474,21 +506,24 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     T* z = (T*)w.z;
     T* zold = (T*)w.zold;
     STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
-    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, nd, w.rs, red_ew, 1, flexible);
+    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, vstride(nd), nd, w.rs, red_ew, 1, flexible);
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
-      pcg_pap_kernel<D><<<tg, kNT, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.nel, l0.rdiag64, l0.ndof, l0.fixed,
+      pcg_pap_kernel<D><<<tg, kQThreads, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.rs_rho, rd0, l0.ndof, l0.fixed,
                                             h->row_map, h->hrows, w.rs, red_tile, h->nelx, h->nely, ke);
-      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, w.p, w.Ap, nd, nd, w.rs, red_ew, pp);
-      if (replace_every > 0 && it % replace_every == 0)
-        pcg_init_kernel<D><<<tg, kNT, 0, st>>>(b, b_rs, x, x_rs, w.r, nd, l0.rho64, l0.nel, l0.rdiag64,
+      float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
+      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, w.p, w.Ap, nd, nd, w.rs, red_ew, pp,
+                                                                  r32, vstride(nd));
+      const bool replaced = replace_every > 0 && it % replace_every == 0;
+      if (replaced)
+        pcg_init_kernel<D><<<tg, kQThreads, 0, st>>>(b, b_rs, x, x_rs, w.r, nd, l0.rho64, l0.rs_rho, rd0,
                                                l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs, red_tile,
                                                h->nelx, h->nely, ke, pp, 1);
       if (flexible) std::swap(z, zold);
-      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
-      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, nd, w.rs, red_ew, 0, flexible);
-      pcg_pupd_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(z, w.p, nd, nd, w.rs);
+      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
+      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
+      pcg_pupd_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(z, w.p, nd, vstride(nd), nd, w.rs);
       STT_TRY(check_launch("pcg iteration"));
       if (it % check_every == 0 || it == max_iter) {
         STT_TRY(pull());
@@ -543,12 +578,12 @@ extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long lo
     rc = h->d == 2 ? run_vcycle<2, float>(h, w, nrows, r, r_rs, (float*)w.z, omega, n_smooth, gamma, nullptr, st)
                    : run_vcycle<1, float>(h, w, nrows, r, r_rs, (float*)w.z, omega, n_smooth, gamma, nullptr, st);
     if (rc == STT_OK)
-      rows_convert_kernel<float, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((float*)w.z, nd, z, z_rs, nd, nullptr);
+      rows_convert_kernel<float, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((float*)w.z, vstride(nd), z, z_rs, nd, nullptr);
   } else {
     rc = h->d == 2 ? run_vcycle<2, double>(h, w, nrows, r, r_rs, (double*)w.z, omega, n_smooth, gamma, nullptr, st)
                    : run_vcycle<1, double>(h, w, nrows, r, r_rs, (double*)w.z, omega, n_smooth, gamma, nullptr, st);
     if (rc == STT_OK)
-      rows_convert_kernel<double, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((double*)w.z, nd, z, z_rs, nd, nullptr);
+      rows_convert_kernel<double, double><<<dim3(ew_blocks(nd), nrows), kEwThreads, 0, st>>>((double*)w.z, vstride(nd), z, z_rs, nd, nullptr);
   }
   if (rc != STT_OK) return rc;
   return check_launch("stt_vcycle");
@@ -564,23 +599,25 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
   const LevelDesc& lv = h->lv[level];
   if (level == 0) {
     if (h->d == 2)
-      l0_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
-          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.nel, lv.rdiag64, lv.ndof, lv.fixed, h->row_map,
-          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<2, double>(h));
+      l0_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof, lv.fixed, h->row_map,
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<2, double>(h), 1, ProlongSrc<double>{nullptr, 0, 1, 1, 1});
     else
-      l0_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kNT, 0, st>>>(
-          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.nel, lv.rdiag64, lv.ndof, lv.fixed, h->row_map,
-          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<1, double>(h));
+      l0_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof, lv.fixed, h->row_map,
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<1, double>(h), 1, ProlongSrc<double>{nullptr, 0, 1, 1, 1});
     return check_launch("level apply");
   }
-  if (v_rs != lv.ndof || out_rs != lv.ndof)
-    return set_error(STT_ERR_INVALID, "stt_level_apply: coarse levels need contiguous rows");
+  if (v_rs != out_rs)
+    return set_error(STT_ERR_INVALID, "stt_level_apply: coarse levels need equal row strides");
   if (h->d == 2)
-    st_sweep_kernel<2, double, SW_APPLY><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
-        v, nullptr, out, lv.ndof, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
+    st_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0,
+        ProlongSrc<double>{nullptr, 0, 1, 1, 1});
   else
-    st_sweep_kernel<1, double, SW_APPLY><<<dim3(grid1(lv.nnode), nrows), 256, 0, st>>>(
-        v, nullptr, out, lv.ndof, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
+    st_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0,
+        ProlongSrc<double>{nullptr, 0, 1, 1, 1});
   return check_launch("level apply");
 }
 
