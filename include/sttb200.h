@@ -16,6 +16,7 @@
  *   stt_q4_apply        sttopt/torch_fem.py:62-83 (matvec), :135-159 (operator)
  *   stt_q4_diag         sttopt/torch_fem.py:86-98 (matvec_diagonal), :162-181 (jacobi diag)
  *   stt_lumped_reaction sttopt/torch_fem.py:117-132
+ *   stt_ke_modal        sttopt/fem.py:17-30, :98-111 (the element matrices it recognises)
  *   stt_hier_*          sttopt/torch_mg.py:293-400 (build_hierarchy), :257-266 (select)
  *   stt_level_apply     sttopt/torch_mg.py:239-255 (_Level.__call__), :179-193 (keff_matvec)
  *   stt_vcycle          sttopt/torch_mg.py:403-476 (VCycle.__call__)
@@ -72,6 +73,13 @@ int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho, long lo
 /* rdiag[n * d + i] = sum over elements e touching node n of reaction[e] / 4.  FP64. */
 int stt_lumped_reaction(int d, int nelx, int nely, int nrows, const double* reaction,
                         long long r_rs, double* out, long long out_rs, stt_stream_t stream);
+
+/* Host only (no device work).  Returns 1 and writes m[8] when KE ((4d)^2 doubles) has
+ * the modal form KE = T^T M T of the unit-square bilinear element (the reference's
+ * plane-stress KE for any nu, and its diffusion KE), which the level-0 kernels then
+ * apply through the element's edge modes; returns 0 for any other KE (those take the
+ * generic 8 x 8 product).  m = {m00, m01, m11, m22, m44, m55, kd0, kd1}. */
+int stt_ke_modal(int d, const double* KE, double* m);
 
 /* ---- multigrid hierarchy ------------------------------------------------------- */
 

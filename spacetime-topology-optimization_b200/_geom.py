@@ -3,8 +3,9 @@ host copies of element matrices, and per-node "fixed" flags from a free-dof mask
 
 The reference's functions take ``edofMat``/``KE``/``mask`` tensors; the kernels need
 the grid shape, the element matrix as a small host array and a byte of flags per
-node.  Each conversion is cached per tensor (keyed on its storage and version), so a
-solve loop pays the device-to-host read once.
+node.  Each conversion is memoised on the tensor object itself (keyed on its version
+counter), so a solve loop pays the device-to-host read once, and a new tensor that
+reuses a freed tensor's memory never sees the old tensor's result.
 """
 
 from __future__ import annotations
@@ -14,20 +15,33 @@ import torch
 
 from . import fem
 
-_grid_cache: dict = {}
-_ke_cache: dict = {}
-_flags_cache: dict = {}
+_MEMO = "_sttb200_memo"
 
 
-def _key(t: torch.Tensor):
-    return (t.data_ptr(), t._version, tuple(t.shape), t.dtype, str(t.device))
+def _memo_get(t: torch.Tensor, key):
+    store = getattr(t, _MEMO, None)
+    return None if store is None else store.get((t._version,) + key)
+
+
+def _memo_put(t: torch.Tensor, key, value):
+    store = getattr(t, _MEMO, None)
+    if store is None:
+        store = {}
+        try:
+            setattr(t, _MEMO, store)
+        except (AttributeError, TypeError):  # a tensor subclass without a __dict__: no memo
+            return value
+    if len(store) > 8:
+        store.clear()
+    store[(t._version,) + key] = value
+    return value
 
 
 def grid_shape(edofMat: torch.Tensor, ndof: int, dofs_per_node: int) -> tuple[int, int]:
     """``(nelx, nely)`` of the structured grid ``edofMat`` maps; checks it is the
     reference's map (sttopt/fem.py:72-95) -- the kernels handle no other."""
-    key = _key(edofMat) + (ndof, dofs_per_node)
-    hit = _grid_cache.get(key)
+    key = ("grid", ndof, dofs_per_node)
+    hit = _memo_get(edofMat, key)
     if hit is not None:
         return hit
     d = dofs_per_node
@@ -41,16 +55,13 @@ def grid_shape(edofMat: torch.Tensor, ndof: int, dofs_per_node: int) -> tuple[in
     expect = torch.as_tensor(fem.element_dof_map(nelx, nely, d), device=edofMat.device)
     if not torch.equal(edofMat.to(expect.dtype), expect):
         raise ValueError("edofMat is not the reference's element dof map of a structured grid")
-    if len(_grid_cache) > 256:
-        _grid_cache.clear()
-    _grid_cache[key] = (nelx, nely)
-    return nelx, nely
+    return _memo_put(edofMat, key, (nelx, nely))
 
 
 def host_KE(KE: torch.Tensor) -> tuple[float, ...]:
     """Element matrix as a flat tuple of doubles (row-major); must be symmetric."""
-    key = _key(KE)
-    hit = _ke_cache.get(key)
+    key = ("KE",)
+    hit = _memo_get(KE, key)
     if hit is not None:
         return hit
     k = KE.detach().to("cpu", torch.float64).numpy()
@@ -58,30 +69,22 @@ def host_KE(KE: torch.Tensor) -> tuple[float, ...]:
         raise ValueError("KE must be 4x4 (scalar) or 8x8 (plane stress)")
     if not np.array_equal(k, k.T):
         raise ValueError("KE must be exactly symmetric")
-    vals = tuple(float(v) for v in k.ravel())
-    if len(_ke_cache) > 64:
-        _ke_cache.clear()
-    _ke_cache[key] = vals
-    return vals
+    return _memo_put(KE, key, tuple(float(v) for v in k.ravel()))
 
 
 def fixed_flags(mask: torch.Tensor | None, nnode: int, d: int) -> torch.Tensor | None:
     """One byte per node, bit ``i`` set when dof ``i`` is fixed (``mask`` False)."""
     if mask is None:
         return None
-    key = _key(mask) + (nnode, d)
-    hit = _flags_cache.get(key)
+    key = ("flags", nnode, d)
+    hit = _memo_get(mask, key)
     if hit is not None:
         return hit
     fixed = (~mask.to(torch.bool)).reshape(nnode, d).to(torch.uint8)
     flags = fixed[:, 0].clone()
     for i in range(1, d):
         flags |= fixed[:, i] << i
-    flags = flags.contiguous()
-    if len(_flags_cache) > 64:
-        _flags_cache.clear()
-    _flags_cache[key] = flags
-    return flags
+    return _memo_put(mask, key, flags.contiguous())
 
 
 def rows2d(t: torch.Tensor, n: int) -> tuple[torch.Tensor, int]:

@@ -39,6 +39,7 @@ _SIGS = {
                               _p, _c_ll, _p, _c_int, _pd, _p]),
     "stt_q4_diag": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _p, _c_ll, _pd, _p]),
     "stt_lumped_reaction": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_ke_modal": (_c_int, [_c_int, _pd, _pd]),
     "stt_hier_workspace_bytes": (_c_ll, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int]),
     "stt_hier_create": (_c_int, [ctypes.POINTER(_p), _p, _c_ll, _c_int, _c_int, _c_int, _c_int, _p, _c_ll,
                                  _p, _c_ll, _p, _pd, _c_int, _c_int, _p]),

@@ -50,6 +50,8 @@ struct stt_hier_impl {
   LevelDesc lv[kMaxLevels];
   CoarseDesc co;
   double KE[64];
+  int modal;         // KE has the modal form (march_modal); mq holds its constants
+  double mq[8];
   double* tables;    // device: per transition S[9][64], G[9][64], GM[9][64]
   double* keffA;     // build temporaries
   double* keffB;

@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "errors.h"
+#include "modal.h"
 #include "q4.cuh"
 
 namespace stt {
@@ -43,6 +44,41 @@ __global__ void __launch_bounds__(kQThreads) q4_apply_kernel(
 #pragma unroll
         for (int i = 0; i < D; ++i)
           if ((ex.fl >> i) & 1) acc[i] = T(0);
+        store_node<D, T>(outr, node, acc);
+      });
+}
+
+// The same operator with KE in modal form; FL selects the options at compile time:
+// bit 0 projects the input, bit 1 the output, bit 2 adds the reaction term.
+template <int D, typename T, int FL>
+__global__ void __launch_bounds__(kQThreads) q4_apply_modal_kernel(
+    const T* __restrict__ u, long long u_rs, T* __restrict__ out, long long out_rs,
+    const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag, long long rdiag_rs,
+    const uint8_t* __restrict__ fixed, int nelx, int nely, MQ<T> mq) {
+  constexpr bool PIN = FL & 1, POUT = FL & 2, RD = FL & 4;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int row = blockIdx.z;
+  const T* ur = u + (size_t)row * u_rs;
+  const T* rr = rho + (size_t)row * rho_rs;
+  const T* rdr = RD ? rdiag + (size_t)row * rdiag_rs : nullptr;
+  T* outr = out + (size_t)row * out_rs;
+  march_modal<D, T, true, false, PIN>(
+      mq, nnx, nny,
+      [&](int r, int c) -> uint8_t { return (PIN || POUT) ? __ldg(fixed + r * nnx + c) : (uint8_t)0; },
+      [&](int r, int c, uint8_t, T(&v)[D]) { load_node<D, T>(ur, r * nnx + c, v); },
+      [&](int r, int c) { return __ldg(rr + (size_t)r * nelx + c); },
+      [&](int, int) { return NoExtra{}; },
+      [&](int r, int c, T(&acc)[D], T(&)[D], const T(&uc)[D], uint8_t fl, const NoExtra&) {
+        const int node = r * nnx + c;
+        if constexpr (RD) {
+#pragma unroll
+          for (int i = 0; i < D; ++i) acc[i] = fma(__ldg(rdr + node * D + i), uc[i], acc[i]);
+        }
+        if constexpr (POUT) {
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+            if ((fl >> i) & 1) acc[i] = T(0);
+        }
         store_node<D, T>(outr, node, acc);
       });
 }
@@ -105,11 +141,32 @@ int launch_apply(int nelx, int nely, int nrows, const void* u, long long u_rs, v
                  long long out_rs, const void* rho, long long rho_rs, const void* rdiag,
                  long long rdiag_rs, const uint8_t* fixed, int flags, const double* KE,
                  cudaStream_t st) {
+  double m[8];
+  const int pin = (flags & STT_PROJECT_IN) ? 1 : 0, pout = (flags & STT_PROJECT_OUT) ? 1 : 0;
   const dim3 grid = q4_grid(nelx, nely, nrows);
-  q4_apply_kernel<D, T><<<grid, kQThreads, 0, st>>>(
-      (const T*)u, u_rs, (T*)out, out_rs, (const T*)rho, rho_rs, (const T*)rdiag, rdiag_rs,
-      fixed, (flags & STT_PROJECT_IN) ? 1 : 0, (flags & STT_PROJECT_OUT) ? 1 : 0, nelx, nely,
-      make_ke<D, T>(KE));
+  if (modal_from_ke(D, KE, m)) {
+    const MQ<T> mq = mq_cast<T>(m);
+    const int fl = pin | (pout << 1) | (rdiag ? 4 : 0);
+#define STT_MODAL_APPLY(FL)                                                                          \
+  q4_apply_modal_kernel<D, T, FL><<<grid, kQThreads, 0, st>>>((const T*)u, u_rs, (T*)out, out_rs,    \
+                                                              (const T*)rho, rho_rs, (const T*)rdiag, \
+                                                              rdiag_rs, fixed, nelx, nely, mq)
+    switch (fl) {
+      case 0: STT_MODAL_APPLY(0); break;
+      case 1: STT_MODAL_APPLY(1); break;
+      case 2: STT_MODAL_APPLY(2); break;
+      case 3: STT_MODAL_APPLY(3); break;
+      case 4: STT_MODAL_APPLY(4); break;
+      case 5: STT_MODAL_APPLY(5); break;
+      case 6: STT_MODAL_APPLY(6); break;
+      default: STT_MODAL_APPLY(7); break;
+    }
+#undef STT_MODAL_APPLY
+  } else {
+    q4_apply_kernel<D, T><<<grid, kQThreads, 0, st>>>(
+        (const T*)u, u_rs, (T*)out, out_rs, (const T*)rho, rho_rs, (const T*)rdiag, rdiag_rs,
+        fixed, pin, pout, nelx, nely, make_ke<D, T>(KE));
+  }
   return check_launch("q4_apply");
 }
 
@@ -135,6 +192,14 @@ extern "C" int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
     if (d == 1) return launch_apply<1, float>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
   }
   return set_error(STT_ERR_INVALID, "stt_q4_apply: d must be 1 or 2, precision FP64 or FP32");
+}
+
+extern "C" int stt_ke_modal(int d, const double* KE, double* m) {
+  if (!KE || !m || (d != 1 && d != 2)) return 0;
+  double t[8];
+  if (!modal_from_ke(d, KE, t)) return 0;
+  for (int i = 0; i < 8; ++i) m[i] = t[i];
+  return 1;
 }
 
 extern "C" int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho,

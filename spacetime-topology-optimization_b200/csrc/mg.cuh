@@ -47,6 +47,38 @@ STT_DEV void prolong_at(const T* __restrict__ e, int cnnx, int kx, int ky, int r
 //   SW_RESID: out = b - A x
 //   SW_APPLY: out = A x
 // A is the projected operator P(K P .) (+ lumped reaction); x is read projected.
+
+// The per-node result of a level-0 pass from A x (unprojected, without reaction), the
+// diagonal of K, the node's x and b, its fixed flags and its reaction value.
+template <int D, typename T, int MODE>
+STT_DEV void l0_result(T (&Ax)[D], T (&dg)[D], const T (&xo)[D], const T (&bv)[D], uint8_t fl,
+                       const T (&rd)[D], T omega, T (&res)[D]) {
+  constexpr bool KU = MODE != SW_FIRST;
+  constexpr bool DG = MODE == SW_FIRST || MODE == SW_SWEEP || MODE == SW_POST;
+  if (KU) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      Ax[i] = fma(rd[i], xo[i], Ax[i]);
+      if ((fl >> i) & 1) Ax[i] = T(0);
+    }
+  }
+  if (DG) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      dg[i] += rd[i];
+      if ((fl >> i) & 1) dg[i] = T(1);
+      const T x0 = MODE == SW_FIRST ? T(0) : xo[i];
+      res[i] = x0 + sweep_div(omega * (bv[i] - (KU ? Ax[i] : T(0))), dg[i]);
+    }
+  } else if (MODE == SW_RESID) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = bv[i] - Ax[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < D; ++i) res[i] = Ax[i];
+  }
+}
+
 template <int D, typename T, int MODE>
 __global__ void __launch_bounds__(kQThreads) l0_sweep_kernel(
     const T* __restrict__ x, long long x_rs, const T* __restrict__ b, long long b_rs,
@@ -97,32 +129,70 @@ __global__ void __launch_bounds__(kQThreads) l0_sweep_kernel(
       },
       [&](int r, int c, T(&Ax)[D], T(&dg)[D], const T(&xo)[D], const RhsX<D, T>& ex) {
         const int node = r * nnx + c;
-        const uint8_t fl = ex.fl;
-        T bv[D], res[D];
+        T rd[D], res[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) bv[i] = ex.b[i];
-        if (KU) {
+        for (int i = 0; i < D; ++i) rd[i] = rdh ? __ldg(rdh + node * D + i) : T(0);
+        l0_result<D, T, MODE>(Ax, dg, xo, ex.b, ex.fl, rd, omega, res);
+        store_node<D, T>(os, node, res);
+      });
+}
+
+// Right-hand side of an output node (the modal kernels take the flags separately).
+template <int D, typename T>
+struct RhsB {
+  T b[D];
+};
+
+// The same passes with KE in modal form (march_modal); RD adds the reaction term.  The
+// input is projected in SW_APPLY only (the cycle's vectors are projected already).
+template <int D, typename T, int MODE, bool RD>
+__global__ void __launch_bounds__(kQThreads) l0_sweep_modal_kernel(
+    const T* __restrict__ x, long long x_rs, const T* __restrict__ b, long long b_rs,
+    T* __restrict__ out, long long o_rs, const T* __restrict__ rho, long long rho_rs,
+    const T* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, int nelx,
+    int nely, T omega, MQ<T> mq, ProlongSrc<T> pro) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const T* xs = x + (size_t)s * x_rs;
+  const T* es = MODE == SW_POST ? pro.ec + (size_t)s * pro.rs : nullptr;
+  const T* rh = rho + (size_t)h * rho_rs;
+  const T* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
+  const T* bs = b + (size_t)s * b_rs;
+  T* os = out + (size_t)s * o_rs;
+  constexpr bool KU = MODE != SW_FIRST;
+  constexpr bool DG = MODE == SW_FIRST || MODE == SW_SWEEP || MODE == SW_POST;
+  march_modal<D, T, KU, DG, MODE == SW_APPLY, RhsB<D, T>>(
+      mq, nnx, nny, [&](int r, int c) { return __ldg(fixed + r * nnx + c); },
+      [&](int r, int c, uint8_t fl, T(&v)[D]) {
+        load_node<D, T>(xs, r * nnx + c, v);
+        if constexpr (MODE == SW_POST) {
+          T pv[D];
+          prolong_at<D, T>(es, pro.cnnx, pro.kx, pro.ky, r, c, pv);
 #pragma unroll
-          for (int i = 0; i < D; ++i) {
-            if (rdh) Ax[i] = fma(__ldg(rdh + node * D + i), xo[i], Ax[i]);
-            if ((fl >> i) & 1) Ax[i] = T(0);
-          }
+          for (int d = 0; d < D; ++d)
+            if (!((fl >> d) & 1)) v[d] += pv[d];
         }
-        if (DG) {
-#pragma unroll
-          for (int i = 0; i < D; ++i) {
-            if (rdh) dg[i] += __ldg(rdh + node * D + i);
-            if ((fl >> i) & 1) dg[i] = T(1);
-            const T x0 = MODE == SW_FIRST ? T(0) : xo[i];
-            res[i] = x0 + sweep_div(omega * (bv[i] - (KU ? Ax[i] : T(0))), dg[i]);
-          }
-        } else if (MODE == SW_RESID) {
-#pragma unroll
-          for (int i = 0; i < D; ++i) res[i] = bv[i] - Ax[i];
+      },
+      [&](int r, int c) { return __ldg(rh + (size_t)r * nelx + c); },
+      [&](int r, int c) {
+        RhsB<D, T> e;
+        if constexpr (MODE != SW_APPLY) {
+          load_node<D, T>(bs, r * nnx + c, e.b);
         } else {
 #pragma unroll
-          for (int i = 0; i < D; ++i) res[i] = Ax[i];
+          for (int d = 0; d < D; ++d) e.b[d] = T(0);
         }
+        return e;
+      },
+      [&](int r, int c, T(&Ax)[D], T(&dg)[D], const T(&xo)[D], uint8_t fl, const RhsB<D, T>& ex) {
+        const int node = r * nnx + c;
+        T rd[D], res[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) rd[i] = RD ? __ldg(rdh + node * D + i) : T(0);
+        l0_result<D, T, MODE>(Ax, dg, xo, ex.b, fl, rd, omega, res);
         store_node<D, T>(os, node, res);
       });
 }

@@ -7,6 +7,7 @@
 
 #include "errors.h"
 #include "hier.h"
+#include "modal.h"
 #include "q4.cuh"
 
 namespace stt {
@@ -627,6 +628,7 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   h->mce = max_coarse_elements;
   h->has_reaction = reaction != nullptr;
   for (int i = 0; i < 16 * d * d; ++i) h->KE[i] = KE[i];
+  h->modal = modal_from_ke(d, KE, h->mq) ? 1 : 0;
   const long long need = plan_hierarchy(*h, nullptr);
   if (ws_bytes < need) {
     delete h;

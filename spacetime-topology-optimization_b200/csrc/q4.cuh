@@ -202,4 +202,209 @@ STT_DEV void march(const KEq<D, T>& ke, int nnx, int nny, LoadU loadu, LoadR loa
   }
 }
 
+// ---- modal form of the element operator ----------------------------------------------
+//
+// On the unit-square bilinear element every element matrix of the reference (the
+// plane-stress KE of sttopt/fem.py:17-30 for any nu, the diffusion KE of :98-111)
+// factors exactly as KE = T^T M T.  T maps the element's corner values (per
+// displacement component) to three edge modes, all with +-1 weights:
+//   Gx = (u_BR - u_BL) + (u_TR - u_TL),  Gy = (u_TL + u_TR) - (u_BL + u_BR),
+//   H  = (u_TR - u_TL) - (u_BR - u_BL)   (x derivative, y derivative, hourglass),
+// and M is sparse: plane stress couples Gx(ux) with Gy(uy) (normal stresses), shares
+// one coefficient for the shear strain Gy(ux) + Gx(uy), and keeps the two hourglass
+// modes diagonal; diffusion is diagonal.  K(rho) u per element then costs ~35 flops
+// instead of the 8 x 8 product's 72, and the edge sums/differences of a grid row are
+// shared by the element rows above and below it.  The host recognises the form from
+// the KE it is given (modal_from_ke); any other KE takes the generic march above.
+template <typename T>
+struct MQ {
+  T m00, m01, m11, m22, m44, m55;  // D = 2: normal (00, 01, 11), shear (22), hourglass (44, 55)
+                                   // D = 1: Gx (00), Gy (11), hourglass (22)
+  T kd0, kd1;                      // diagonal of KE per component (equal at every corner)
+};
+
+template <typename T>
+MQ<T> mq_cast(const double (&m)[8]) {
+  return MQ<T>{T(m[0]), T(m[1]), T(m[2]), T(m[3]), T(m[4]), T(m[5]), T(m[6]), T(m[7])};
+}
+
+// Corner forces of one component from its mode coefficients (alpha on Gx, beta on Gy,
+// gamma on H): TR = a + b + g, BL = -a - b + g, BR = a - b - g, TL = -a + b - g.
+// `own` gets TL (+ the carry to this node), `send` TR (+ the carry to the right node);
+// the carries become BL and BR, which land on the next grid row.
+template <typename T>
+STT_DEV void modal_corners(T al, T be, T ga, T& co, T& cr, T& own, T& send) {
+  const T s = al + be, t = al - be;
+  own = co - (t + ga);
+  send = cr + (s + ga);
+  co = ga - s;
+  cr = t - ga;
+}
+
+// The level-0 operator with KE in modal form.  The warp marches element rows: lane c
+// owns element (er, c) and its top-left node.  For element row er it loads the bottom
+// grid row er + 1, takes the right neighbour's value by a shuffle, forms the element's
+// modes, and splits its forces: TL to its own node (er, c), TR to the right lane (one
+// shuffle), BL and BR carried to grid row er + 1.  Node row er is then complete and is
+// emitted.
+//
+// Loaders (called for in-grid positions only; zero outside):
+//   loadf(r, c) -> uint8_t   the node's fixed flags (0 when the operator has none); read
+//                            once per node and used for the input projection (PIN) and
+//                            handed to emit;
+//   loadu(r, c, fl, v)       the node's input value (fl: its flags); loads only, no
+//                            arithmetic on loaded values (it would stall the lookahead);
+//   loadr(r, c) -> T         element density;
+//   loadx(r, c) -> Extra     per-output-node values (right-hand side ...).
+// emit(r, c, Ku, dg, uc, fl, ex) gets K u (KU), diag(K) (DG), the node's (projected)
+// input, flags and Extra.  Every option is a template parameter or a loader that
+// returns a constant: a runtime-uniform branch around a load in this loop cost the FP32
+// apply 2x on B200 (measured), as it keeps the loads from being issued ahead.
+// AHEAD rows of loads stay in flight; at ~46 registers a thread the SM holds 11 blocks,
+// and on B200 that beat deeper lookahead (4 rows: -20 %, 8 rows: -50 % for the FP32
+// apply at 2048x1024 x 16 rows) and two grid columns per lane (-12 %), all measured.
+template <int D, typename T, bool KU, bool DG, bool PIN, typename Extra = NoExtra, int AHEAD = 2,
+          int BAND = kQRows, typename LoadF, typename LoadU, typename LoadR, typename LoadX, typename Emit>
+STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU loadu, LoadR loadr, LoadX loadx,
+                         Emit emit) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kQCols - 1 + lane;  // this lane's column
+  const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
+  const int r0 = blockIdx.y * BAND;
+  const int r1 = min(r0 + BAND, nny);
+  const int nelx = nnx - 1, nely = nny - 1;
+  const bool col_ok = c >= 0 && c < nnx;
+  const bool ecol_ok = c >= 0 && c < nelx;
+  // loads only: anything computed from a loaded value here would wait for the load and
+  // expose its latency, so the input projection is applied when the row is consumed
+  auto U = [&](int r, T(&v)[D], uint8_t& fl) {
+    fl = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    if (col_ok && r >= 0 && r < nny) {
+      fl = loadf(r, c);
+      if constexpr (KU) loadu(r, c, fl, v);
+    }
+  };
+  auto project = [&](T(&v)[D], uint8_t fl) {
+    if constexpr (PIN) {
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        if ((fl >> d) & 1) v[d] = T(0);
+    }
+  };
+  auto Rho = [&](int r) -> T { return (ecol_ok && r >= 0 && r < nely) ? loadr(r, c) : T(0); };
+  auto X = [&](int r) -> Extra { return (out_lane && r < r1) ? loadx(r, c) : Extra{}; };
+  T ut[D];          // this lane's node on the top edge of the element row
+  uint8_t ft;       // its flags
+  T sT[D], dT[D];   // top edge: u(c) + u(c + 1), u(c + 1) - u(c)
+  T co[D], cr[D];   // forces from the element row above: to this node, to the right node
+  T rp = T(0);      // density of the element above (for the diagonal)
+  auto edge = [&](const T(&v)[D], T(&s)[D], T(&dd)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const T vr = __shfl_down_sync(0xffffffffu, v[d], 1);
+      s[d] = v[d] + vr;
+      dd[d] = vr - v[d];
+    }
+  };
+  // element row with bottom edge ub and density rho; own / send as in modal_corners
+  auto step = [&](const T(&ub)[D], T rho, T(&own)[D], T(&send)[D]) {
+    T sB[D], dB[D];
+    edge(ub, sB, dB);
+    if constexpr (KU) {
+      T Gx[D], Gy[D], H[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        Gx[d] = dB[d] + dT[d];
+        Gy[d] = sT[d] - sB[d];
+        H[d] = dT[d] - dB[d];
+      }
+      if constexpr (D == 2) {
+        const T p = rho * Gx[0], pq = rho * Gy[1];
+        const T a = fma(q.m01, pq, q.m00 * p);
+        const T cc = fma(q.m01, p, q.m11 * pq);
+        const T b = (rho * q.m22) * (Gy[0] + Gx[1]);
+        modal_corners(a, b, (rho * q.m44) * H[0], co[0], cr[0], own[0], send[0]);
+        modal_corners(b, cc, (rho * q.m55) * H[1], co[1], cr[1], own[1], send[1]);
+      } else {
+        modal_corners((rho * q.m00) * Gx[0], (rho * q.m11) * Gy[0], (rho * q.m22) * H[0], co[0], cr[0],
+                      own[0], send[0]);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      sT[d] = sB[d];
+      dT[d] = dB[d];
+    }
+  };
+  // element row r0 - 1 (zero density above the grid) fills the carries of grid row r0
+  {
+    T u0[D], own[D], send[D];
+    uint8_t f0;
+    U(r0 - 1, u0, f0);
+    project(u0, f0);
+    edge(u0, sT, dT);
+#pragma unroll
+    for (int d = 0; d < D; ++d) co[d] = cr[d] = T(0);
+    U(r0, ut, ft);
+    project(ut, ft);
+    const T rho = Rho(r0 - 1);
+    step(ut, rho, own, send);
+    rp = rho;
+  }
+  // prefetch queue: bottom edges (and flags) r+1 .. r+AHEAD, density and extra rows
+  // r .. r+AHEAD-1
+  T qu[AHEAD][D], qr[AHEAD];
+  uint8_t qf[AHEAD];
+  Extra qx[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) {
+    U(r0 + 1 + k, qu[k], qf[k]);
+    qr[k] = Rho(r0 + k);
+    qx[k] = X(r0 + k);
+  }
+  for (int rb0 = r0; rb0 < r1; rb0 += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int r = rb0 + k;
+      T ub[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) ub[d] = qu[k][d];
+      const uint8_t fb = qf[k];
+      project(ub, fb);
+      const T rho = qr[k];
+      const Extra ex = qx[k];
+      U(r + 1 + AHEAD, qu[k], qf[k]);  // refill the slot
+      qr[k] = Rho(r + AHEAD);
+      qx[k] = X(r + AHEAD);
+      T own[D], send[D], Ku[D], dg[D];
+      step(ub, rho, own, send);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        Ku[d] = KU ? own[d] + __shfl_up_sync(0xffffffffu, send[d], 1) : T(0);
+        dg[d] = T(0);
+      }
+      if constexpr (DG) {
+        const T rs = rho + rp;
+        const T rsum = rs + __shfl_up_sync(0xffffffffu, rs, 1);
+        dg[0] = q.kd0 * rsum;
+        if constexpr (D == 2) dg[1] = q.kd1 * rsum;
+      }
+      rp = rho;
+      if (out_lane && r < r1) emit(r, c, Ku, dg, ut, ft, ex);
+#pragma unroll
+      for (int d = 0; d < D; ++d) ut[d] = ub[d];
+      ft = fb;
+    }
+  }
+}
+
+// Launch grid of the marching kernels (generic and modal share it).
+template <bool MODAL, typename T>
+inline dim3 march_grid(int nelx, int nely, int rows) {
+  return q4_grid(nelx, nely, rows);
+}
+
 }  // namespace stt

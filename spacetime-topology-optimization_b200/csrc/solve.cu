@@ -110,6 +110,7 @@ struct Cycle {
   const RowState* rst;
   cudaStream_t st;
   KEq<D, T> ke;
+  MQ<T> mq;
   T* final_out = nullptr;  // where level 0's last sweep writes (row stride vstride(ndof0))
 
   T* X(int l) const { return (T*)w.x[l]; }
@@ -136,9 +137,19 @@ struct Cycle {
             ProlongSrc<T> pro = ProlongSrc<T>{nullptr, 0, 1, 1, 1}) {
     const LevelDesc& lv = h->lv[l];
     if (l == 0) {
-      l0_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-          x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
-          h->hrows, rst, lv.nelx, lv.nely, omega, ke, 0, pro);
+      const dim3 g = march_grid<true, T>(lv.nelx, lv.nely, nrows);
+      if (h->modal && h->has_reaction)
+        l0_sweep_modal_kernel<D, T, MODE, true><<<g, kQThreads, 0, st>>>(
+            x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
+            h->hrows, rst, lv.nelx, lv.nely, omega, mq, pro);
+      else if (h->modal)
+        l0_sweep_modal_kernel<D, T, MODE, false><<<g, kQThreads, 0, st>>>(
+            x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
+            h->hrows, rst, lv.nelx, lv.nely, omega, mq, pro);
+      else
+        l0_sweep_kernel<D, T, MODE><<<g, kQThreads, 0, st>>>(
+            x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
+            h->hrows, rst, lv.nelx, lv.nely, omega, ke, 0, pro);
     } else {
       st_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
           x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
@@ -227,50 +238,35 @@ struct PcgParams {
 
 // r = b - A x (or r = b when x is null), reductions ||r||^2 and ||b||^2.
 // replace: keep bnorm and only re-test convergence (true-residual replacement).
-template <int D>
+template <int D, bool MODAL, bool RD>
 __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
     const double* __restrict__ b, long long b_rs, const double* __restrict__ x, long long x_rs,
     double* __restrict__ r, long long r_rs, const double* __restrict__ rho, long long rho_rs,
     const double* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
     const int* __restrict__ row_map, int hrows, RowState* __restrict__ rst, GridRed red,
-    int nelx, int nely, KEq<D, double> ke, PcgParams pp, int replace) {
+    int nelx, int nely, KEq<D, double> ke, MQ<double> mq, PcgParams pp, int replace) {
   const int s = blockIdx.z;
   if (replace && !rst[s].active) return;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
   const double* xs = x ? x + (size_t)s * x_rs : nullptr;
   const double* rh = rho + (size_t)h * rho_rs;
-  const double* rdh = rdiag ? rdiag + (size_t)h * rd_rs : nullptr;
+  const double* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
   const double* bs = b + (size_t)s * b_rs;
   double* rs_ = r + (size_t)s * r_rs;
   double vals[2] = {0.0, 0.0};
-  auto loadu = [&](int rr, int cc, double(&v)[D]) {
-    const int node = rr * nnx + cc;
-    load_node<D, double>(xs, node, v);
-    const uint8_t fl = __ldg(fixed + node);
-#pragma unroll
-    for (int d = 0; d < D; ++d)
-      if ((fl >> d) & 1) v[d] = 0.0;
-  };
   auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
-  auto loadx = [&](int rr, int cc) {
-    RhsX<D, double> e;
-    const int node = rr * nnx + cc;
-    load_node<D, double>(bs, node, e.b);
-    e.fl = __ldg(fixed + node);
-    return e;
-  };
-  auto emit = [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const RhsX<D, double>& ex) {
+  // the residual of one node from A x (unprojected) and b
+  auto finish = [&](int rr, int cc, const double(&Ax)[D], const double(&uc)[D], const double(&bv)[D],
+                    uint8_t fl, bool has_x) {
     const int node = rr * nnx + cc;
     double res[D];
-    const double* bv = ex.b;
-    const uint8_t fl = ex.fl;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
       double a = 0.0;
-      if (xs) {
+      if (has_x) {
         a = Ax[i];
-        if (rdh) a = fma(__ldg(rdh + node * D + i), uc[i], a);
+        if (RD) a = fma(__ldg(rdh + node * D + i), uc[i], a);
         if ((fl >> i) & 1) a = 0.0;
       }
       res[i] = bv[i] - a;
@@ -279,10 +275,47 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
     }
     store_node<D, double>(rs_, node, res);
   };
-  if (xs)
-    march<D, double, true, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
-  else
-    march<D, double, false, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+  if constexpr (MODAL) {
+    auto loadf = [&](int rr, int cc) { return __ldg(fixed + rr * nnx + cc); };
+    auto loadu = [&](int rr, int cc, uint8_t, double(&v)[D]) { load_node<D, double>(xs, rr * nnx + cc, v); };
+    auto loadx = [&](int rr, int cc) {
+      RhsB<D, double> e;
+      load_node<D, double>(bs, rr * nnx + cc, e.b);
+      return e;
+    };
+    if (xs)
+      march_modal<D, double, true, false, true, RhsB<D, double>>(
+          mq, nnx, nny, loadf, loadu, loadr, loadx,
+          [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl,
+              const RhsB<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, fl, true); });
+    else
+      march_modal<D, double, false, false, false, RhsB<D, double>>(
+          mq, nnx, nny, loadf, loadu, loadr, loadx,
+          [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl,
+              const RhsB<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, fl, false); });
+  } else {
+    auto loadu = [&](int rr, int cc, double(&v)[D]) {
+      const int node = rr * nnx + cc;
+      load_node<D, double>(xs, node, v);
+      const uint8_t fl = __ldg(fixed + node);
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        if ((fl >> d) & 1) v[d] = 0.0;
+    };
+    auto loadx = [&](int rr, int cc) {
+      RhsX<D, double> e;
+      const int node = rr * nnx + cc;
+      load_node<D, double>(bs, node, e.b);
+      e.fl = __ldg(fixed + node);
+      return e;
+    };
+    auto emit = [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D],
+                    const RhsX<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, ex.fl, xs != nullptr); };
+    if (xs)
+      march<D, double, true, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+    else
+      march<D, double, false, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+  }
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
   grid_reduce<2, kQThreads>(red, s, bid, vals, [&](const double* t) {
     RowState& S = rst[s];
@@ -304,36 +337,49 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
 
 // Ap = A p (projected, + lumped reaction), pAp = p . Ap, alpha = safe_div(rz, pAp).
 // p is zero at fixed dofs by construction (it is built from the projected z).
-template <int D>
+template <int D, bool MODAL, bool RD>
 __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
     const double* __restrict__ p, double* __restrict__ Ap, long long rs,
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
     long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map,
-    int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely, KEq<D, double> ke) {
+    int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely, KEq<D, double> ke,
+    MQ<double> mq) {
   const int s = blockIdx.z;
   if (!rst[s].active) return;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
   const double* ps = p + (size_t)s * rs;
   const double* rh = rho + (size_t)h * rho_rs;
-  const double* rdh = rdiag ? rdiag + (size_t)h * rd_rs : nullptr;
+  const double* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
   double* As = Ap + (size_t)s * rs;
   double vals[1] = {0.0};
-  march<D, double, true, false, FlagX>(
-      ke, nnx, nny, [&](int rr, int cc, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); },
-      [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); },
-      [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
-      [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const FlagX& ex) {
-        const int node = rr * nnx + cc;
-        const uint8_t fl = ex.fl;
+  auto finish = [&](int rr, int cc, double(&Ax)[D], const double(&uc)[D], uint8_t fl) {
+    const int node = rr * nnx + cc;
 #pragma unroll
-        for (int i = 0; i < D; ++i) {
-          if (rdh) Ax[i] = fma(__ldg(rdh + node * D + i), uc[i], Ax[i]);
-          if ((fl >> i) & 1) Ax[i] = 0.0;
-          vals[0] = fma(uc[i], Ax[i], vals[0]);
-        }
-        store_node<D, double>(As, node, Ax);
-      });
+    for (int i = 0; i < D; ++i) {
+      if (RD) Ax[i] = fma(__ldg(rdh + node * D + i), uc[i], Ax[i]);
+      if ((fl >> i) & 1) Ax[i] = 0.0;
+      vals[0] = fma(uc[i], Ax[i], vals[0]);
+    }
+    store_node<D, double>(As, node, Ax);
+  };
+  auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
+  if constexpr (MODAL) {
+    march_modal<D, double, true, false, false>(
+        mq, nnx, nny, [&](int rr, int cc) { return __ldg(fixed + rr * nnx + cc); },
+        [&](int rr, int cc, uint8_t, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); }, loadr,
+        [&](int, int) { return NoExtra{}; },
+        [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl, const NoExtra&) {
+          finish(rr, cc, Ax, uc, fl);
+        });
+  } else {
+    march<D, double, true, false, FlagX>(
+        ke, nnx, nny, [&](int rr, int cc, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); }, loadr,
+        [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
+        [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const FlagX& ex) {
+          finish(rr, cc, Ax, uc, ex.fl);
+        });
+  }
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
   grid_reduce<1, kQThreads>(red, s, bid, vals, [&](const double* t) {
     RowState& S = rst[s];
@@ -447,7 +493,7 @@ template <int D, typename T>
 static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r, long long r_rs,
                       T* zout, double omega, int n_smooth,
                       int gamma, const RowState* rst, cudaStream_t st, bool b0_ready = false) {
-  Cycle<D, T> cyc{h, w, nrows, T(omega), n_smooth, gamma, rst, st, ke_of<D, T>(h)};
+  Cycle<D, T> cyc{h, w, nrows, T(omega), n_smooth, gamma, rst, st, ke_of<D, T>(h), mq_cast<T>(h->mq)};
   const long long n = h->lv[0].ndof, vs = vstride(n);
   const T* b0;
   long long b_rs;
@@ -485,10 +531,24 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4LL * nrows, st), "memset counters"));
   STT_TRY(check_cuda(cudaMemsetAsync(w.rs, 0, sizeof(RowState) * nrows, st), "memset rows"));
   if (!has_x0) rows_zero_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, nd);
+  const MQ<double> mq = mq_cast<double>(h->mq);
+  // r = b - A x (x may be null: r = b); replace = 1 keeps ||b|| (true-residual replacement)
+  auto init = [&](const double* xx, const PcgParams& pq, int replace) {
+#define STT_INIT(MODAL, RD)                                                                              \
+  pcg_init_kernel<D, MODAL, RD><<<tg, kQThreads, 0, st>>>(b, b_rs, xx, x_rs, w.r, nd, l0.rho64, l0.rs_rho, rd0, \
+                                                          l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,        \
+                                                          red_tile, h->nelx, h->nely, ke, mq, pq, replace)
+    if (h->modal) {
+      if (rd0) STT_INIT(true, true);
+      else STT_INIT(true, false);
+    } else {
+      if (rd0) STT_INIT(false, true);
+      else STT_INIT(false, false);
+    }
+#undef STT_INIT
+  };
   PcgParams pp{rtol, 0, flexible};
-  pcg_init_kernel<D><<<tg, kQThreads, 0, st>>>(b, b_rs, has_x0 ? x : nullptr, x_rs, w.r, nd, l0.rho64, l0.rs_rho,
-                                         rd0, l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,
-                                         red_tile, h->nelx, h->nely, ke, pp, 0);
+  init(has_x0 ? x : nullptr, pp, 0);
   STT_TRY(check_launch("pcg init"));
   std::vector<RowState> host(nrows);
   auto pull = [&]() -> int {
@@ -510,16 +570,23 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
-      pcg_pap_kernel<D><<<tg, kQThreads, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.rs_rho, rd0, l0.ndof, l0.fixed,
-                                            h->row_map, h->hrows, w.rs, red_tile, h->nelx, h->nely, ke);
+#define STT_PAP(MODAL, RD)                                                                                \
+  pcg_pap_kernel<D, MODAL, RD><<<tg, kQThreads, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.rs_rho, rd0, l0.ndof,     \
+                                                         l0.fixed, h->row_map, h->hrows, w.rs, red_tile,         \
+                                                         h->nelx, h->nely, ke, mq)
+      if (h->modal) {
+        if (rd0) STT_PAP(true, true);
+        else STT_PAP(true, false);
+      } else {
+        if (rd0) STT_PAP(false, true);
+        else STT_PAP(false, false);
+      }
+#undef STT_PAP
       float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
       pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, w.p, w.Ap, nd, nd, w.rs, red_ew, pp,
                                                                   r32, vstride(nd));
       const bool replaced = replace_every > 0 && it % replace_every == 0;
-      if (replaced)
-        pcg_init_kernel<D><<<tg, kQThreads, 0, st>>>(b, b_rs, x, x_rs, w.r, nd, l0.rho64, l0.rs_rho, rd0,
-                                               l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs, red_tile,
-                                               h->nelx, h->nely, ke, pp, 1);
+      if (replaced) init(x, pp, 1);
       if (flexible) std::swap(z, zold);
       STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
       pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
@@ -598,14 +665,28 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
   cudaStream_t st = (cudaStream_t)stream;
   const LevelDesc& lv = h->lv[level];
   if (level == 0) {
-    if (h->d == 2)
-      l0_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof, lv.fixed, h->row_map,
-          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<2, double>(h), 1, ProlongSrc<double>{nullptr, 0, 1, 1, 1});
-    else
-      l0_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof, lv.fixed, h->row_map,
-          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<1, double>(h), 1, ProlongSrc<double>{nullptr, 0, 1, 1, 1});
+    const dim3 g = tile_grid(lv.nelx, lv.nely, nrows);
+    const double* rd = h->has_reaction ? lv.rdiag64 : nullptr;
+    const MQ<double> mq = mq_cast<double>(h->mq);
+    const ProlongSrc<double> none{nullptr, 0, 1, 1, 1};
+#define STT_L0_APPLY(D)                                                                                  \
+  do {                                                                                                   \
+    if (h->modal && rd)                                                                                  \
+      l0_sweep_modal_kernel<D, double, SW_APPLY, true><<<g, kQThreads, 0, st>>>(                        \
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, rd, lv.ndof, lv.fixed, h->row_map,      \
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, mq, none);                                          \
+    else if (h->modal)                                                                                   \
+      l0_sweep_modal_kernel<D, double, SW_APPLY, false><<<g, kQThreads, 0, st>>>(                       \
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, rd, lv.ndof, lv.fixed, h->row_map,      \
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, mq, none);                                          \
+    else                                                                                                 \
+      l0_sweep_kernel<D, double, SW_APPLY><<<g, kQThreads, 0, st>>>(                                    \
+          v, v_rs, nullptr, 0, out, out_rs, lv.rho64, lv.rs_rho, rd, lv.ndof, lv.fixed, h->row_map,      \
+          h->hrows, nullptr, lv.nelx, lv.nely, 1.0, ke_of<D, double>(h), 1, none);                      \
+  } while (0)
+    if (h->d == 2) STT_L0_APPLY(2);
+    else STT_L0_APPLY(1);
+#undef STT_L0_APPLY
     return check_launch("level apply");
   }
   if (v_rs != out_rs)

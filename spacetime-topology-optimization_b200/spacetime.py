@@ -164,3 +164,29 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
     out["gradient"] = grad.reshape(nely, nelx)
     out["lam"] = lam
     return out
+
+
+class SpaceTimeObjective(torch.autograd.Function):
+    """``objective(xPhys)`` as an autograd node: the forward pass runs the batched solves
+    and the hand-written adjoints at once (``objective_and_gradient``); the backward
+    pass scales the stored gradient, so ``torch.autograd.grad`` and
+    ``sensitivity.jacobian_rows`` see the space-time objective like any torch function
+    (the reference reaches it through autograd over compliance.py and
+    virtual_heat.py)."""
+
+    @staticmethod
+    def forward(ctx, xPhys, w, kw):
+        out = objective_and_gradient(xPhys, w, gradient=ctx.needs_input_grad[0], **kw)
+        ctx.save_for_backward(out.get("gradient", torch.zeros_like(xPhys)))
+        return out["objective"].clone()
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return g * grad.to(g.dtype), None, None
+
+
+def objective(xPhys: Tensor, w: Tensor, **kw) -> Tensor:
+    """Differentiable space-time objective ``sum_s c_s + sum(w tPhys)`` (a 0-d tensor);
+    keyword arguments as ``objective_and_gradient``."""
+    return SpaceTimeObjective.apply(xPhys, w, kw)

@@ -354,6 +354,22 @@ def gen_spacetime():
     save("spacetime", **out)
 
 
+def gen_spacetime_512():
+    """The differentiation configuration: the space-time objective at 512x256, 16 stages.
+
+    Inputs are regenerated from the seed by the tests (``smoothed_density`` and
+    ``default_rng(seed).uniform``); only their checksums are stored, with the reference's
+    outputs (stage membership bit-packed)."""
+    nelx, nely, n_stage, seed = 512, 256, 16, 4
+    rng = np.random.default_rng(seed)
+    x = smoothed_density(nelx, nely, seed)
+    w = rng.uniform(-1, 1, (nely, nelx))
+    res = spacetime_reference(x, w, n_stage)
+    save("spacetime512", x_sum=x.sum(), w_sum=w.sum(), tPhys=res["tPhys"], c_s=res["c_s"],
+         J_t=res["J_t"], L=res["L"], grad=res["grad"], member_bits=np.packbits(res["member"], axis=-1),
+         fwd_iter=res["fwd_iter"], bwd_iter=res["bwd_iter"])
+
+
 def gen_pcg_cases():
     """Retirement, zero rows, warm starts and non-convergence, as the reference does them."""
     nelx, nely = 18, 12
@@ -390,3 +406,5 @@ if __name__ == "__main__":
     gen_cantilever()
     gen_heat()
     gen_spacetime()
+    if "--with-512" in sys.argv:
+        gen_spacetime_512()

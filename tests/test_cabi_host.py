@@ -106,3 +106,63 @@ def test_package_refuses_cpu_tensors(pkg):
     with pytest.raises(ValueError, match="CUDA"):
         torch_fem.matvec(torch.zeros(40, dtype=torch.float64), torch.ones(12, dtype=torch.float64),
                          edof, KE, 40)
+
+
+def test_modal_form_recognises_the_reference_element_matrices(pkg):
+    """stt_ke_modal accepts the plane-stress KE for any nu and the diffusion KE, and
+    rebuilds them exactly from the modal constants; a general SPD KE is rejected."""
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    pat = np.array([[-1, 1, 1, -1], [-1, -1, 1, 1], [1, -1, 1, -1]], dtype=np.float64)
+
+    def modal(d, KE):
+        m = (ctypes.c_double * 8)()
+        ok = lib.stt_ke_modal(d, _lib.dbl_array(np.ascontiguousarray(KE).ravel().tolist()), m)
+        return ok, np.array(m[:])
+
+    for nu in (0.0, 0.25, 0.3, 0.45):
+        KE = O.plane_stress_KE(nu)
+        ok, m = modal(2, KE)
+        assert ok == 1, nu
+        T = np.zeros((6, 8))
+        T[0, 0::2], T[1, 1::2], T[2, 0::2], T[3, 1::2], T[4, 0::2], T[5, 1::2] = pat[0], pat[1], pat[1], pat[0], pat[2], pat[2]
+        M = np.zeros((6, 6))
+        M[0, 0], M[0, 1], M[1, 0], M[1, 1] = m[0], m[1], m[1], m[2]
+        M[2:4, 2:4] = m[3]
+        M[4, 4], M[5, 5] = m[4], m[5]
+        assert np.abs(T.T @ M @ T - KE).max() < 1e-15
+        assert m[6] == m[7] == KE[0, 0]
+    ok, m = modal(1, O.diffusion_KE())
+    assert ok == 1
+    assert np.abs(pat.T @ np.diag([m[0], m[2], m[3]]) @ pat - O.diffusion_KE()).max() < 1e-15
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((8, 8))
+    assert modal(2, A @ A.T)[0] == 0
+    KE = O.plane_stress_KE(0.3).copy()
+    KE[0, 3] += 1e-9
+    KE[3, 0] += 1e-9
+    assert modal(2, KE)[0] == 0
+
+
+def test_host_conversions_are_memoised_per_tensor_object(pkg):
+    """Element-matrix and grid conversions are cached on the tensor object and follow
+    in-place edits; a new tensor never inherits another tensor's cached result (torch's
+    allocator reuses freed addresses, so an address-keyed cache would)."""
+    import torch
+
+    from sttopt_b200 import _geom
+
+    a = torch.tensor(O.plane_stress_KE(0.3))
+    va = _geom.host_KE(a)
+    assert va == tuple(O.plane_stress_KE(0.3).ravel())
+    a.mul_(2.0)
+    assert _geom.host_KE(a) == tuple((2.0 * O.plane_stress_KE(0.3)).ravel())
+    for nu in (0.1, 0.2, 0.3):
+        b = torch.tensor(O.plane_stress_KE(nu))
+        assert _geom.host_KE(b) == tuple(O.plane_stress_KE(nu).ravel())
+        del b
+    e1 = torch.as_tensor(O.element_dof_map(6, 4))
+    assert _geom.grid_shape(e1, 2 * 7 * 5, 2) == (6, 4)
+    e2 = torch.as_tensor(O.element_dof_map(4, 6))
+    assert _geom.grid_shape(e2, 2 * 5 * 7, 2) == (4, 6)

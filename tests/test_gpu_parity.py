@@ -74,6 +74,47 @@ def test_operator_fp32_and_large_grid(m):
     assert rel_err(got32, ref) < 1e-5
 
 
+def _generic_KE():
+    """A symmetric positive semi-definite element matrix outside the modal form (the
+    library's generic path): plane stress plus a small seeded rank-one term."""
+    v = np.random.default_rng(21).standard_normal(8)
+    return O.plane_stress_KE(0.3) + 1e-3 * np.outer(v, v)
+
+
+def test_generic_element_matrix_path(m, pkg):
+    """A KE that stt_ke_modal rejects runs the generic 8 x 8 product: applies and a
+    V-cycle still match the oracle at the plane-stress tolerances."""
+    import ctypes
+
+    from sttopt_b200 import _lib
+
+    KE_np = _generic_KE()
+    mm = (ctypes.c_double * 8)()
+    assert _lib.lib().stt_ke_modal(2, _lib.dbl_array(KE_np.ravel().tolist()), mm) == 0
+    rng = np.random.default_rng(11)
+    nelx, nely = 67, 45
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    edof_np = O.element_dof_map(nelx, nely)
+    dens = O.simp_density(rng.uniform(1e-3, 1, nelx * nely), EMIN, EMAX, PENAL)
+    U = rng.standard_normal((3, ndof))
+    ref = O.matvec(U, dens, edof_np, KE_np, ndof)
+    KE, edof = T(KE_np), T(edof_np, torch.int64)
+    assert rel_err(m.fem.matvec(T(U), T(dens), edof, KE, ndof).cpu(), ref) < 1e-13
+    got32 = m.fem.matvec(T(U, torch.float32), T(dens, torch.float32), edof, KE, ndof).cpu().numpy()
+    assert rel_err(got32, ref) < 1e-5
+    nelx, nely = 48, 36
+    x = rng.uniform(1e-3, 1.0, nelx * nely)
+    F, mask = O.cantilever_point_load(nelx, nely)
+    dens = O.simp_density(x, EMIN, EMAX, PENAL)
+    levels = m.mg.build_hierarchy(T(dens), T(O.element_dof_map(nelx, nely), torch.int64), KE,
+                                  T(mask, torch.bool), nelx, nely, max_coarse_elements=20)
+    ol = O.build_hierarchy(dens, O.element_dof_map(nelx, nely), KE_np, mask, nelx, nely,
+                           max_coarse_elements=20)
+    u = O.project(rng.standard_normal(len(F)), mask)
+    assert rel_err(levels[0](T(u)).cpu(), ol[0](u)) < 1e-13
+    assert rel_err(m.mg.VCycle(levels)(T(u)).cpu(), O.VCycle(ol)(u)) < 1e-10
+
+
 def _levels(m, nelx, nely, x, mask, mce, precision="fp64"):
     dens = O.simp_density(x, EMIN, EMAX, PENAL)
     KE, edof = T(O.plane_stress_KE(0.3)), T(O.element_dof_map(nelx, nely), torch.int64)
