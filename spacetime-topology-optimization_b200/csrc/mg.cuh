@@ -27,17 +27,23 @@ template <int D, typename T>
 STT_DEV void prolong_at(const T* __restrict__ e, int cnnx, int kx, int ky, int r, int c, T (&v)[D]) {
   const int R = div_k(r, ky), jy = r - R * ky, C = div_k(c, kx), jx = c - C * kx;
   const T wx = T((double)jx / kx), wy = T((double)jy / ky);
+  const long long n0 = (long long)R * cnnx + C;
+  // one vector load per coarse corner
+  T e00[D], e01[D], e10[D], e11[D];
+  load_node<D, T>(e, n0, e00);
+  if (jx) load_node<D, T>(e, n0 + 1, e01);
+  if (jy) {
+    load_node<D, T>(e, n0 + cnnx, e10);
+    if (jx) load_node<D, T>(e, n0 + cnnx + 1, e11);
+  }
 #pragma unroll
   for (int i = 0; i < D; ++i) {
-    auto g = [&](int RR) -> T {
-      const T a = __ldg(e + ((size_t)RR * cnnx + C) * D + i);
-      if (jx == 0) return a;
-      const T b = __ldg(e + ((size_t)RR * cnnx + C + 1) * D + i);
-      return a * (T(1) - wx) + b * wx;
-    };
-    T t = g(R);
-    if (jy != 0) t = t * (T(1) - wy) + g(R + 1) * wy;
-    v[i] = t;
+    T t0 = e00[i], t1 = jy ? e10[i] : T(0);
+    if (jx) {
+      t0 = e00[i] * (T(1) - wx) + e01[i] * wx;
+      if (jy) t1 = e10[i] * (T(1) - wx) + e11[i] * wx;
+    }
+    v[i] = jy ? t0 * (T(1) - wy) + t1 * wy : t0;
   }
 }
 
@@ -143,6 +149,7 @@ struct RhsB {
   T b[D];
 };
 
+
 // The same passes with KE in modal form (march_modal); RD adds the reaction term.  The
 // input is projected in SW_APPLY only (the cycle's vectors are projected already).
 template <int D, typename T, int MODE, bool RD>
@@ -157,44 +164,261 @@ __global__ void __launch_bounds__(kQThreads) l0_sweep_modal_kernel(
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
   const T* xs = x + (size_t)s * x_rs;
-  const T* es = MODE == SW_POST ? pro.ec + (size_t)s * pro.rs : nullptr;
   const T* rh = rho + (size_t)h * rho_rs;
   const T* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
   const T* bs = b + (size_t)s * b_rs;
   T* os = out + (size_t)s * o_rs;
   constexpr bool KU = MODE != SW_FIRST;
-  constexpr bool DG = MODE == SW_FIRST || MODE == SW_SWEEP || MODE == SW_POST;
+  constexpr bool DG = MODE == SW_FIRST || MODE == SW_SWEEP;
+  auto loadf = [&](int r, int c) { return __ldg(fixed + r * nnx + c); };
+  auto loadr = [&](int r, int c) { return __ldg(rh + (size_t)r * nelx + c); };
+  auto loadx = [&](int r, int c) {
+    RhsB<D, T> e;
+    if constexpr (MODE != SW_APPLY) {
+      load_node<D, T>(bs, r * nnx + c, e.b);
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d) e.b[d] = T(0);
+    }
+    return e;
+  };
+  auto emit = [&](int r, int c, T(&Ax)[D], T(&dg)[D], const T(&xo)[D], uint8_t fl, const RhsB<D, T>& ex) {
+    const int node = r * nnx + c;
+    T rd[D], res[D];
+#pragma unroll
+    for (int i = 0; i < D; ++i) rd[i] = RD ? __ldg(rdh + node * D + i) : T(0);
+    l0_result<D, T, MODE>(Ax, dg, xo, ex.b, fl, rd, omega, res);
+    store_node<D, T>(os, node, res);
+  };
+  static_assert(MODE != SW_POST, "the cycle prolongs with prolong_kernel");
   march_modal<D, T, KU, DG, MODE == SW_APPLY, RhsB<D, T>>(
-      mq, nnx, nny, [&](int r, int c) { return __ldg(fixed + r * nnx + c); },
-      [&](int r, int c, uint8_t fl, T(&v)[D]) {
-        load_node<D, T>(xs, r * nnx + c, v);
-        if constexpr (MODE == SW_POST) {
-          T pv[D];
-          prolong_at<D, T>(es, pro.cnnx, pro.kx, pro.ky, r, c, pv);
+      mq, nnx, nny, loadf, [&](int r, int c, uint8_t, T(&v)[D]) { load_node<D, T>(xs, r * nnx + c, v); },
+      loadr, loadx, emit);
+}
+
+// ---- level 0: pre-smoothing in one pass (modal form, n_smooth = 2) --------------------
+//
+// The two pre-smoothing sweeps and the residual as one streaming pass: the passes of
+// the unfused cycle (torch_mg.VCycle._smooth, sttopt/torch_mg.py:440-476) chained inside
+// a warp, each one grid row behind the one before, so b and the densities cross HBM
+// once instead of three times.  Per node the arithmetic is the unfused kernels' (same
+// operations in the same order), so results agree with the unfused passes to rounding.
+//
+//   x1 = omega b / D;  x2 = x1 + omega (b - A x1) / D;  r = b - A x2.  Writes x2 and r.
+//
+// Each chained stage needs its input on the neighbouring lanes, so a stage's valid
+// lanes shrink by one on each side (and lane 0 has no left neighbour for the diagonal):
+// lanes 3..29 are output (27 columns a warp).  The front row f feeds stage A at element
+// row f - 1 and stage B at f - 2; a band [r0, r1) runs f = r0 - 2 .. r1 + 1 so both
+// stages are exact on the band.  (A post-smoothing twin, prolongation + two sweeps in one
+// pass, measured slower on B200 than prolong_kernel + two sweeps: at 128 registers its
+// 4 blocks an SM could not keep the loads in flight.)
+
+// One modal element-row stage: the top edge, the carries and the top node's value.
+template <int D, typename T>
+struct ModalStage {
+  T sT[D], dT[D], co[D], cr[D], ut[D];
+
+  STT_DEV void reset() {
 #pragma unroll
-          for (int d = 0; d < D; ++d)
-            if (!((fl >> d) & 1)) v[d] += pv[d];
+    for (int d = 0; d < D; ++d) sT[d] = dT[d] = co[d] = cr[d] = ut[d] = T(0);
+  }
+  // element row with bottom edge ub and density rho: Ku of the top node row; then the
+  // bottom row becomes the top (ut = ub)
+  STT_DEV void step(const MQ<T>& q, const T (&ub)[D], T rho, T (&Ku)[D]) {
+    T sB[D], dB[D], own[D], send[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const T vr = __shfl_down_sync(0xffffffffu, ub[d], 1);
+      sB[d] = ub[d] + vr;
+      dB[d] = vr - ub[d];
+    }
+    T Gx[D], Gy[D], H[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      Gx[d] = dB[d] + dT[d];
+      Gy[d] = sT[d] - sB[d];
+      H[d] = dT[d] - dB[d];
+    }
+    if constexpr (D == 2) {
+      const T p = rho * Gx[0], pq = rho * Gy[1];
+      const T a = fma(q.m01, pq, q.m00 * p);
+      const T cc = fma(q.m01, p, q.m11 * pq);
+      const T b = (rho * q.m22) * (Gy[0] + Gx[1]);
+      modal_corners(a, b, (rho * q.m44) * H[0], co[0], cr[0], own[0], send[0]);
+      modal_corners(b, cc, (rho * q.m55) * H[1], co[1], cr[1], own[1], send[1]);
+    } else {
+      modal_corners((rho * q.m00) * Gx[0], (rho * q.m11) * Gy[0], (rho * q.m22) * H[0], co[0], cr[0], own[0],
+                    send[0]);
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      Ku[d] = own[d] + __shfl_up_sync(0xffffffffu, send[d], 1);
+      sT[d] = sB[d];
+      dT[d] = dB[d];
+      ut[d] = ub[d];
+    }
+  }
+};
+
+// Raw loads of one front row (no arithmetic, so they stay in flight).
+template <int D, typename T, bool RD>
+struct FrontRow {
+  T b[D];
+  T rd[RD ? D : 1];
+  T rho;
+  uint8_t fl;
+};
+
+// Per-row values a stage reads one or two rows after the front.
+template <int D, typename T, bool RD>
+struct DelayRow {
+  T b[D], dg[D];
+  T rd[RD ? D : 1];
+  T rho;
+  uint8_t fl;
+};
+
+constexpr int kPreCols = 27;  // output columns per warp strip of l0_presmooth_kernel
+
+inline dim3 presmooth_grid(int nelx, int nely, int rows) {
+  const int strips = (nelx + 1 + kPreCols - 1) / kPreCols;
+  return dim3((strips + kQWarps - 1) / kQWarps, (nely + 1 + kQRows - 1) / kQRows, rows);
+}
+
+// FP32: 6 blocks of 128 threads an SM (<= 80 registers), measured fastest on B200 at
+// 2048x1024 x 16 rows (333 us against 351 us at the compiler's 80-95 registers with
+// fewer blocks).  FP64 needs twice the registers for the same state: 3 blocks.
+template <int D, typename T, bool RD, int AHEAD = 2>
+__global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmooth_kernel(
+    const T* __restrict__ b, long long b_rs, T* __restrict__ out_x, long long ox_rs, T* __restrict__ out_r,
+    long long or_rs, const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag,
+    long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows,
+    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q) {
+  constexpr int LO = 3, HI = 29;
+  static_assert(HI - LO + 1 == kPreCols, "strip width");
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const T* rh = rho + (size_t)h * rho_rs;
+  const T* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
+  const T* bs = b + (size_t)s * b_rs;
+  T* ox = out_x + (size_t)s * ox_rs;
+  T* orr = out_r + (size_t)s * or_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kPreCols - LO + lane;
+  const bool out_lane = lane >= LO && lane <= HI && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const bool ecol_ok = c >= 0 && c < nelx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  auto load_front = [&](int f, FrontRow<D, T, RD>& F) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) F.b[d] = T(0);
+    if constexpr (RD) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) F.rd[d] = T(0);
+    }
+    F.fl = 0;
+    F.rho = (ecol_ok && f >= 0 && f < nely) ? __ldg(rh + (size_t)f * nelx + c) : T(0);
+    if (!col_ok || f < 0 || f >= nny) return;
+    const long long node = (long long)f * nnx + c;
+    F.fl = __ldg(fixed + node);
+    load_node<D, T>(bs, node, F.b);
+    if constexpr (RD) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) F.rd[d] = __ldg(rdh + node * D + d);
+    }
+  };
+  ModalStage<D, T> A, B;
+  A.reset();
+  B.reset();
+  DelayRow<D, T, RD> d1{}, d2{};  // rows f - 1 and f - 2
+  const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
+  T rho_prev = (ecol_ok && f0 - 1 >= 0 && f0 - 1 < nely) ? __ldg(rh + (size_t)(f0 - 1) * nelx + c) : T(0);
+  FrontRow<D, T, RD> qf[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) load_front(f0 + k, qf[k]);
+  for (int fb = f0; fb <= f1; fb += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int f = fb + k;
+      const FrontRow<D, T, RD> F = qf[k];
+      load_front(f + AHEAD, qf[k]);
+      // diagonal of K at row f (kd times the densities around the node)
+      DelayRow<D, T, RD> cur;
+      {
+        const T rs = F.rho + rho_prev;
+        const T dsum = rs + __shfl_up_sync(0xffffffffu, rs, 1);
+        cur.dg[0] = q.kd0 * dsum;
+        if constexpr (D == 2) cur.dg[1] = q.kd1 * dsum;
+      }
+      rho_prev = F.rho;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        cur.b[d] = F.b[d];
+        if constexpr (RD) cur.rd[d] = F.rd[d];
+      }
+      cur.rho = F.rho;
+      cur.fl = F.fl;
+      // x1 at row f (the first sweep from zero)
+      T x1[D];
+      {
+        T zero[D], Ax[D], dg[D], rdv[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          zero[d] = Ax[d] = T(0);
+          dg[d] = cur.dg[d];
+          rdv[d] = RD ? F.rd[d] : T(0);
         }
-      },
-      [&](int r, int c) { return __ldg(rh + (size_t)r * nelx + c); },
-      [&](int r, int c) {
-        RhsB<D, T> e;
-        if constexpr (MODE != SW_APPLY) {
-          load_node<D, T>(bs, r * nnx + c, e.b);
-        } else {
+        l0_result<D, T, SW_FIRST>(Ax, dg, zero, F.b, F.fl, rdv, omega, x1);
+        if (!(col_ok && f >= 0 && f < nny)) {
 #pragma unroll
-          for (int d = 0; d < D; ++d) e.b[d] = T(0);
+          for (int d = 0; d < D; ++d) x1[d] = T(0);
         }
-        return e;
-      },
-      [&](int r, int c, T(&Ax)[D], T(&dg)[D], const T(&xo)[D], uint8_t fl, const RhsB<D, T>& ex) {
-        const int node = r * nnx + c;
-        T rd[D], res[D];
+      }
+      // stage A: element row f - 1 -> second sweep at node row f - 1
+      T KA[D], xa[D], xo_a[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) rd[i] = RD ? __ldg(rdh + node * D + i) : T(0);
-        l0_result<D, T, MODE>(Ax, dg, xo, ex.b, fl, rd, omega, res);
-        store_node<D, T>(os, node, res);
-      });
+      for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
+      A.step(q, x1, d1.rho, KA);
+      {
+        T rd1[D], dg[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          rd1[d] = RD ? d1.rd[d] : T(0);
+          dg[d] = d1.dg[d];
+        }
+        l0_result<D, T, SW_SWEEP>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
+        if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
+#pragma unroll
+          for (int d = 0; d < D; ++d) xa[d] = T(0);
+        }
+      }
+      // stage B: element row f - 2 -> residual at node row f - 2
+      T KB[D], rb[D], xo_b[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
+      B.step(q, xa, d2.rho, KB);
+      {
+        T rd2[D], dg[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          rd2[d] = RD ? d2.rd[d] : T(0);
+          dg[d] = d2.dg[d];
+        }
+        l0_result<D, T, SW_RESID>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, rb);
+      }
+      if (out_lane) {
+        if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);
+        if (f - 2 >= r0 && f - 2 < r1) store_node<D, T>(orr, (long long)(f - 2) * nnx + c, rb);
+      }
+      d2 = d1;
+      d1 = cur;
+    }
+  }
 }
 
 // ---- stencil levels: column-marching sweeps -----------------------------------------

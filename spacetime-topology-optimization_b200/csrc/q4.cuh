@@ -241,6 +241,17 @@ STT_DEV void modal_corners(T al, T be, T ga, T& co, T& cr, T& own, T& send) {
   cr = t - ga;
 }
 
+// The default input record of march_modal: the node's values, used as loaded.
+struct CopyIn {
+  template <typename In, typename V>
+  STT_DEV void operator()(int, int, uint8_t, const In& in, V& v) const {
+#pragma unroll
+    for (int d = 0; d < (int)(sizeof(V) / sizeof(v[0])); ++d) v[d] = in[d];
+  }
+};
+
+constexpr uint8_t kInGrid = 0x80;  // march_modal's flag bit: the row was in the grid
+
 // The level-0 operator with KE in modal form.  The warp marches element rows: lane c
 // owns element (er, c) and its top-left node.  For element row er it loads the bottom
 // grid row er + 1, takes the right neighbour's value by a shuffle, forms the element's
@@ -248,25 +259,29 @@ STT_DEV void modal_corners(T al, T be, T ga, T& co, T& cr, T& own, T& send) {
 // shuffle), BL and BR carried to grid row er + 1.  Node row er is then complete and is
 // emitted.
 //
-// Loaders (called for in-grid positions only; zero outside):
+// Loaders (called for in-grid positions only):
 //   loadf(r, c) -> uint8_t   the node's fixed flags (0 when the operator has none); read
 //                            once per node and used for the input projection (PIN) and
 //                            handed to emit;
-//   loadu(r, c, fl, v)       the node's input value (fl: its flags); loads only, no
-//                            arithmetic on loaded values (it would stall the lookahead);
+//   loadu(r, c, fl, In& in)  raw loads of the node's input record (In = T[D] by default);
+//                            no arithmetic on loaded values, which would wait for the
+//                            load and expose its latency;
+//   value(r, c, fl, in, v)   the node's input value from its record, evaluated when the
+//                            row is consumed (default: the loaded values);
 //   loadr(r, c) -> T         element density;
 //   loadx(r, c) -> Extra     per-output-node values (right-hand side ...).
-// emit(r, c, Ku, dg, uc, fl, ex) gets K u (KU), diag(K) (DG), the node's (projected)
-// input, flags and Extra.  Every option is a template parameter or a loader that
-// returns a constant: a runtime-uniform branch around a load in this loop cost the FP32
-// apply 2x on B200 (measured), as it keeps the loads from being issued ahead.
-// AHEAD rows of loads stay in flight; at ~46 registers a thread the SM holds 11 blocks,
-// and on B200 that beat deeper lookahead (4 rows: -20 %, 8 rows: -50 % for the FP32
-// apply at 2048x1024 x 16 rows) and two grid columns per lane (-12 %), all measured.
-template <int D, typename T, bool KU, bool DG, bool PIN, typename Extra = NoExtra, int AHEAD = 2,
-          int BAND = kQRows, typename LoadF, typename LoadU, typename LoadR, typename LoadX, typename Emit>
+// Positions outside the grid read as zero.  emit(r, c, Ku, dg, uc, fl, ex) gets K u
+// (KU), diag(K) (DG), the node's (projected) input, flags and Extra.  Every option is a
+// template parameter or a loader that returns a constant: a runtime-uniform branch
+// around a load in this loop cost the FP32 apply 2x on B200 (measured).  AHEAD rows of
+// loads stay in flight; at ~46 registers a thread the SM holds 11 blocks, and on B200
+// that beat deeper lookahead (4 rows: -20 %, 8 rows: -50 % for the FP32 apply at
+// 2048x1024 x 16 rows) and two grid columns per lane (-12 %), all measured.
+template <int D, typename T, bool KU, bool DG, bool PIN, typename Extra = NoExtra, typename In = T[D],
+          int AHEAD = 2, int BAND = kQRows, typename LoadF, typename LoadU, typename LoadR, typename LoadX,
+          typename Emit, typename Value = CopyIn>
 STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU loadu, LoadR loadr, LoadX loadx,
-                         Emit emit) {
+                         Emit emit, Value value = Value{}) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int strip = blockIdx.x * kQWarps + warp;
   const int c = strip * kQCols - 1 + lane;  // this lane's column
@@ -276,22 +291,24 @@ STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU lo
   const int nelx = nnx - 1, nely = nny - 1;
   const bool col_ok = c >= 0 && c < nnx;
   const bool ecol_ok = c >= 0 && c < nelx;
-  // loads only: anything computed from a loaded value here would wait for the load and
-  // expose its latency, so the input projection is applied when the row is consumed
-  auto U = [&](int r, T(&v)[D], uint8_t& fl) {
+  auto U = [&](int r, In& in, uint8_t& fl) {
     fl = 0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) v[d] = T(0);
     if (col_ok && r >= 0 && r < nny) {
-      fl = loadf(r, c);
-      if constexpr (KU) loadu(r, c, fl, v);
+      fl = loadf(r, c) | kInGrid;
+      if constexpr (KU) loadu(r, c, fl, in);
     }
   };
-  auto project = [&](T(&v)[D], uint8_t fl) {
-    if constexpr (PIN) {
+  // the consumed row's value: evaluated from its record, projected (PIN)
+  auto V = [&](int r, const In& in, uint8_t fl, T(&v)[D]) {
 #pragma unroll
-      for (int d = 0; d < D; ++d)
-        if ((fl >> d) & 1) v[d] = T(0);
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    if (KU && (fl & kInGrid)) {
+      value(r, c, fl, in, v);
+      if constexpr (PIN) {
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+          if ((fl >> d) & 1) v[d] = T(0);
+      }
     }
   };
   auto Rho = [&](int r) -> T { return (ecol_ok && r >= 0 && r < nely) ? loadr(r, c) : T(0); };
@@ -341,22 +358,24 @@ STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU lo
   };
   // element row r0 - 1 (zero density above the grid) fills the carries of grid row r0
   {
+    In i0, i1;
     T u0[D], own[D], send[D];
     uint8_t f0;
-    U(r0 - 1, u0, f0);
-    project(u0, f0);
+    U(r0 - 1, i0, f0);
+    U(r0, i1, ft);
+    V(r0 - 1, i0, f0, u0);
     edge(u0, sT, dT);
 #pragma unroll
     for (int d = 0; d < D; ++d) co[d] = cr[d] = T(0);
-    U(r0, ut, ft);
-    project(ut, ft);
+    V(r0, i1, ft, ut);
     const T rho = Rho(r0 - 1);
     step(ut, rho, own, send);
     rp = rho;
   }
   // prefetch queue: bottom edges (and flags) r+1 .. r+AHEAD, density and extra rows
   // r .. r+AHEAD-1
-  T qu[AHEAD][D], qr[AHEAD];
+  In qu[AHEAD];
+  T qr[AHEAD];
   uint8_t qf[AHEAD];
   Extra qx[AHEAD];
 #pragma unroll
@@ -370,10 +389,8 @@ STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU lo
     for (int k = 0; k < AHEAD; ++k) {
       const int r = rb0 + k;
       T ub[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) ub[d] = qu[k][d];
       const uint8_t fb = qf[k];
-      project(ub, fb);
+      V(r + 1, qu[k], fb, ub);
       const T rho = qr[k];
       const Extra ex = qx[k];
       U(r + 1 + AHEAD, qu[k], qf[k]);  // refill the slot
@@ -393,7 +410,7 @@ STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU lo
         if constexpr (D == 2) dg[1] = q.kd1 * rsum;
       }
       rp = rho;
-      if (out_lane && r < r1) emit(r, c, Ku, dg, ut, ft, ex);
+      if (out_lane && r < r1) emit(r, c, Ku, dg, ut, (uint8_t)(ft & ~kInGrid), ex);
 #pragma unroll
       for (int d = 0; d < D; ++d) ut[d] = ub[d];
       ft = fb;
