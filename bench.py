@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the roofline kernel's timing (the small case for an ncu capture)")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the batched uneven multi-problem measurement")
+    ap.add_argument("--uneven-only", action="store_true",
+                    help="run only the batched uneven multi-problem measurement")
     return ap.parse_args()
 
 
@@ -111,6 +115,67 @@ def run_reference(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ---- batched uneven problems ---------------------------------------------------------
+
+UNEVEN_SIZES = [(256, 128), (512, 256), (768, 384), (1024, 512), (1536, 768)]
+UNEVEN_PROBLEMS = 64
+
+
+def uneven_workload(dev, seed=SEED):
+    """64 independent space-time problems: seeded grid sizes from UNEVEN_SIZES, 4-16
+    stages each, seeded smoothed densities and time weights."""
+    import numpy as np
+
+    from sttopt_b200 import synthetic
+
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, len(UNEVEN_SIZES), UNEVEN_PROBLEMS)
+    stages = rng.integers(4, 17, UNEVEN_PROBLEMS)
+    xs, ws = [], []
+    for k, i in enumerate(picks):
+        nx, ny = UNEVEN_SIZES[i]
+        xs.append(synthetic.smoothed_density(nx, ny, 1000 * seed + k, device=dev))
+        ws.append(synthetic.time_weights(nx, ny, 1000 * seed + k, device=dev))
+    return xs, ws, [int(n) for n in stages]
+
+
+def run_uneven(dev, steps=2, warmup=1):
+    """Stage solves per second over the 64 uneven problems (objective + full gradient of
+    each), grouped per grid size into batched solves on concurrent streams."""
+    import torch
+
+    from sttopt_b200 import spacetime
+
+    xs, ws, ns = uneven_workload(dev)
+    cache: dict = {}
+    info: dict = {}
+    for _ in range(warmup):
+        spacetime.objective_and_gradient_many(xs, ws, ns, problems=cache, info=info)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        spacetime.objective_and_gradient_many(xs, ws, ns, problems=cache, info=info)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    counts: dict = {}
+    for x, n in zip(xs, ns):
+        key = f"{x.shape[1]}x{x.shape[0]}"
+        c = counts.setdefault(key, {"problems": 0, "stages": 0})
+        c["problems"] += 1
+        c["stages"] += n
+    del cache
+    torch.cuda.empty_cache()
+    return {"metric": "stage solves/s (64 uneven space-time problems, objective + full gradient, rtol 1e-8)",
+            "value": sum(ns) / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "problems": len(xs), "stage_rows": sum(ns), "groups": counts,
+            "peak_device_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1),
+            "iterations": {f"{k[0]}x{k[1]}": v for k, v in info.items()},
+            "batching": "one batched device PCG per grid size (heat, stages, adjoints), the size groups "
+                        "on concurrent CUDA streams"}
 
 
 # ---- clocks -----------------------------------------------------------------------
@@ -191,6 +256,10 @@ def main():
         u = torch.randn(N_STAGE, 2 * problem.nnode, device=dev, dtype=torch.float64)
         roof, detail = roofline(_lib, problem, {"U": u}, dev)
         print(json.dumps({"roofline": roof, "roofline_detail": detail}), flush=True)
+        return 0
+    if args.uneven_only:
+        print(json.dumps({"batched_uneven": run_uneven(dev, steps=max(args.steps, 1), warmup=max(args.warmup, 1))}),
+              flush=True)
         return 0
     info: dict = {}
 
@@ -274,6 +343,10 @@ def main():
                                     "max_rel_err_stage_compliance": c_err, "rel_err_gradient_l2": g_err}
         if not args.no_profile:
             extra["gpu_launches_per_step"], extra["top_kernels"] = profile_step(step, x, w)
+        if not args.no_uneven:
+            del ref
+            torch.cuda.empty_cache()
+            extra["batched_uneven"] = run_uneven(dev)
         if world == 1 and not args.no_cpu_baseline:
             s = cpu_sample(1, 0)
             extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": 1, "kind": "port",

@@ -73,41 +73,136 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
     """Objective, stage compliances, ``tPhys`` and (optionally) ``d objective / d xPhys``."""
     _lib.require_cuda(xPhys, w)
     nely, nelx = xPhys.shape
-    dev = xPhys.device
     P = problem if problem is not None and (problem.nelx, problem.nely) == (nelx, nely) else \
-        SpaceTimeProblem(nelx, nely, dev)
+        SpaceTimeProblem(nelx, nely, xPhys.device)
+    opts = dict(precision=precision, rtol=rtol, max_iter=max_iter, drain_beta=drain_beta,
+                conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
+                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched)
+    return _solve_group(P, [xPhys], [w], [n_stage], info=info, **opts)[0]
+
+
+def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
+                                precision: str = "mixed", rtol: float = 1e-8, max_iter: int = 500,
+                                drain_beta: float = 25.0, conduction_penal: float = 3.0,
+                                Emin: float = EMIN, Emax: float = EMAX, penal: float = PENAL,
+                                max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS,
+                                gradient: bool = True, concurrent: bool = True,
+                                problems: dict | None = None, info: dict | None = None) -> list[dict]:
+    """Many independent space-time problems of uneven grid sizes and stage counts.
+
+    Problems of one grid size form one group: their heat solves are one batched device
+    PCG (a row per problem), and all their stage solves and stage adjoints are one
+    batched device PCG each (a row per stage, hierarchy rows per stage density).  With
+    ``concurrent`` the groups run on their own CUDA streams from host threads, so the
+    GPU overlaps them.  Results come back in input order, each as
+    ``objective_and_gradient`` returns it.  ``problems`` caches ``SpaceTimeProblem`` per
+    shape; ``info`` receives per-group iteration counts under ``(nelx, nely)``.
+    """
+    if not (len(xs) == len(ws) == len(n_stages)):
+        raise ValueError("xs, ws and n_stages must have the same length")
+    _lib.require_cuda(*xs, *ws)
+    opts = dict(precision=precision, rtol=rtol, max_iter=max_iter, drain_beta=drain_beta,
+                conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
+                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=True)
+    groups: dict = {}
+    for k, x in enumerate(xs):
+        groups.setdefault(tuple(x.shape), []).append(k)
+    cache = problems if problems is not None else {}
+    dev = xs[0].device
+    for (nely, nelx) in groups:
+        if (nelx, nely) not in cache:
+            cache[(nelx, nely)] = SpaceTimeProblem(nelx, nely, dev)
+    results: list = [None] * len(xs)
+
+    def run(shape, idx):
+        nely, nelx = shape
+        sub = {} if info is not None else None
+        out = _solve_group(cache[(nelx, nely)], [xs[k] for k in idx], [ws[k] for k in idx],
+                           [n_stages[k] for k in idx], info=sub, **opts)
+        if info is not None:
+            info[(nelx, nely)] = sub
+        for k, o in zip(idx, out):
+            results[k] = o
+
+    if not concurrent or len(groups) == 1:
+        for shape, idx in groups.items():
+            run(shape, idx)
+        return results
+    import concurrent.futures
+
+    main = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(main)
+    streams = {shape: torch.cuda.Stream(device=dev) for shape in groups}
+
+    def on_stream(shape, idx):
+        torch.cuda.set_device(dev)
+        s = streams[shape]
+        s.wait_event(ready)
+        with torch.cuda.stream(s):
+            run(shape, idx)
+        return s
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(groups)) as ex:
+        futs = [ex.submit(on_stream, shape, idx) for shape, idx in groups.items()]
+        done = [f.result() for f in futs]
+    for s in done:  # the results were made on the side streams
+        main.wait_stream(s)
+    for o in results:
+        for v in o.values():
+            if isinstance(v, torch.Tensor) and v.is_cuda:
+                v.record_stream(main)
+    return results
+
+
+def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
+                 precision: str, rtol: float, max_iter: int, drain_beta: float, conduction_penal: float,
+                 Emin: float, Emax: float, penal: float, max_coarse_elements: int, gradient: bool,
+                 batched: bool, info: dict | None) -> list[dict]:
+    """G problems on one grid: batched heat solve, all stage rows in one batched solve."""
     L = _lib.lib()
     st = _lib.stream()
-    x = xPhys.detach().to(torch.float64).reshape(-1).contiguous()
-    nel, nnode = P.nel, P.nnode
+    nelx, nely, nel, nnode = P.nelx, P.nely, P.nel, P.nnode
+    dev = P.device
+    G = len(xs)
+    X = torch.stack([x.detach().to(torch.float64).reshape(-1) for x in xs]).contiguous()  # (G, nel)
+    W = torch.stack([w.detach().to(torch.float64).reshape(-1) for w in ws]).contiguous()
 
-    # 1. heat time field
-    chi = torch.clamp(x ** conduction_penal, min=1e-6).contiguous()
+    # 1. heat time fields (a row per problem)
+    chi = torch.clamp(X ** conduction_penal, min=1e-6).contiguous()
     alpha = drain_beta / (nelx * nely)
     reac = torch.full_like(chi, alpha)
     hl = torch_mg.build_hierarchy(chi, P.edof1, P.KEh, P.heat_mask, nelx, nely, reaction=reac,
                                   max_coarse_elements=max_coarse_elements, precision=precision)
-    rdiag = hl[0].reaction_diag
-    Klift = torch.empty(nnode, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 1, nelx, nely, 1, _lib.ptr(P.lift), nnode, _lib.ptr(Klift),
+    rdiag = hl[0].reaction_diag.reshape(G, nnode).contiguous()
+    Klift = torch.empty(G, nnode, dtype=torch.float64, device=dev)
+    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 1, nelx, nely, G, _lib.ptr(P.lift), 0, _lib.ptr(Klift),
                               nnode, _lib.ptr(chi), nel, _lib.ptr(rdiag), nnode, _lib.ptr(P.fixed1),
                               _lib.STT_PROJECT_OUT, P.keh, st))
     heat_rhs = (-Klift).contiguous()  # F - K_lift, projected (F = 0)
-    T_free = _pcg(hl, heat_rhs, None, rtol, max_iter, "heat_n_iter", info)
-    T = T_free + P.lift
-    t_e = torch.empty(nel, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_heat_element_means(nelx, nely, _lib.ptr(T), _lib.ptr(t_e), st))
-    part = x >= x.max() / 2
-    scale = torch.where(part, t_e, torch.full_like(t_e, -torch.inf)).max()
+    T_free = _pcg(hl, heat_rhs, None, rtol, max_iter, "heat_n_iter", info).reshape(G, nnode)
+    T = (T_free + P.lift).contiguous()
+    t_e = torch.empty(G, nel, dtype=torch.float64, device=dev)
+    for g in range(G):
+        _lib.check(L.stt_heat_element_means(nelx, nely, _lib.ptr(T[g]), _lib.ptr(t_e[g]), st))
+    part = X >= X.max(dim=1, keepdim=True).values / 2
+    scale = torch.where(part, t_e, torch.full_like(t_e, -torch.inf)).max(dim=1, keepdim=True).values
     tPhys = (t_e / scale).contiguous()
 
-    # 2.-3. stage rows and the batched stage solves
-    member = torch.empty(n_stage, nel, dtype=torch.uint8, device=dev)
-    _lib.check(L.stt_stage_membership(nel, n_stage, _lib.ptr(tPhys), _lib.ptr(member), st))
-    rho = torch.empty(n_stage, nel, dtype=torch.float64, device=dev)
-    F = torch.empty(n_stage, 2 * nnode, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_stage_rows(nelx, nely, n_stage, _lib.ptr(x), _lib.ptr(member), Emin, Emax, penal,
-                                _lib.ptr(P.fixed2), _lib.ptr(rho), _lib.ptr(F), st))
+    # 2.-3. stage rows of every problem, then the batched stage solves
+    offs = [0]
+    for n in n_stages:
+        offs.append(offs[-1] + n)
+    S = offs[-1]
+    members = []
+    rho = torch.empty(S, nel, dtype=torch.float64, device=dev)
+    F = torch.empty(S, 2 * nnode, dtype=torch.float64, device=dev)
+    for g, n in enumerate(n_stages):
+        m = torch.empty(n, nel, dtype=torch.uint8, device=dev)
+        _lib.check(L.stt_stage_membership(nel, n, _lib.ptr(tPhys[g]), _lib.ptr(m), st))
+        _lib.check(L.stt_stage_rows(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(m), Emin, Emax, penal,
+                                    _lib.ptr(P.fixed2), _lib.ptr(rho[offs[g]]), _lib.ptr(F[offs[g]]), st))
+        members.append(m)
     if batched:
         sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
                                       max_coarse_elements=max_coarse_elements, precision=precision)
@@ -115,55 +210,62 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
         stage_levels = [sl]
     else:
         Us, stage_levels = [], []
-        for s in range(n_stage):
+        for s in range(S):
             sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
                                           max_coarse_elements=max_coarse_elements, precision=precision)
             Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
             stage_levels.append(sl)
         U = torch.stack(Us)
-    terms = torch_fem.element_terms(U, P.edof, P.KE)
-    ce = terms["ce"]
+    ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
     c_s = (rho * ce).sum(-1)
-    J_t = (w.reshape(-1).to(torch.float64) * tPhys).sum()
-    out = dict(objective=c_s.sum() + J_t, c_s=c_s, J_t=J_t, tPhys=tPhys.reshape(nely, nelx), U=U,
-               T=T, member=member)
+    J_t = (W * tPhys).sum(-1)
+    outs = []
+    for g in range(G):
+        a, b = offs[g], offs[g + 1]
+        outs.append(dict(objective=c_s[a:b].sum() + J_t[g], c_s=c_s[a:b], J_t=J_t[g],
+                         tPhys=tPhys[g].reshape(nely, nelx), U=U[a:b], T=T[g], member=members[g]))
     if not gradient:
-        return out
+        return outs
 
     # 5a. stage adjoints: dL/dU = 2 K U; warm start alpha U (exact for compliance)
-    g = torch.empty_like(U)
-    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, n_stage, _lib.ptr(U), 2 * nnode, _lib.ptr(g),
+    gK = torch.empty_like(U)
+    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
                               2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
                               _lib.STT_PROJECT_OUT, P.ke, st))
-    g = 2 * g
-    a = torch_fem.safe_div(torch_fem._dots(U, g), torch_fem._dots(U, F))
-    x0 = (a[:, None] * U).contiguous()
+    gK = 2 * gK
+    a_ = torch_fem.safe_div(torch_fem._dots(U, gK), torch_fem._dots(U, F))
+    x0 = (a_[:, None] * U).contiguous()
     if batched:
-        lam = _pcg(stage_levels[0], g, x0, rtol, max_iter, "adjoint_n_iter", info)
+        lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
     else:
-        lam = torch.stack([_pcg(stage_levels[s], g[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
-                           for s in range(n_stage)])
+        lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
+                           for s in range(S)])
+    lam = lam.contiguous()
     gd = torch_fem.element_terms(U, P.edof, P.KE, lam=lam)["gdens"]
-    grad = torch.zeros(nel, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_stage_gradient(nelx, nely, n_stage, _lib.ptr(x), _lib.ptr(member), _lib.ptr(ce),
-                                    _lib.ptr(gd), _lib.ptr(lam.contiguous()), Emin, Emax, penal,
-                                    _lib.ptr(grad), st))
+    grads = torch.zeros(G, nel, dtype=torch.float64, device=dev)
+    for g, n in enumerate(n_stages):
+        a = offs[g]
+        _lib.check(L.stt_stage_gradient(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(members[g]), _lib.ptr(ce[a]),
+                                        _lib.ptr(gd[a]), _lib.ptr(lam[a]), Emin, Emax, penal,
+                                        _lib.ptr(grads[g]), st))
 
-    # 5b. heat adjoint: d(sum w tPhys)/dT = -(w / scale) / 4 per corner
-    ws = (w.reshape(-1).to(torch.float64) / scale).contiguous()
-    gT = torch.empty(nnode, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_heat_adjoint_load(nelx, nely, _lib.ptr(ws), 1.0, _lib.ptr(gT), st))
+    # 5b. heat adjoints: d(sum w tPhys)/dT = -(w / scale) / 4 per corner
+    Ws = (W / scale).contiguous()
+    gT = torch.empty(G, nnode, dtype=torch.float64, device=dev)
+    for g in range(G):
+        _lib.check(L.stt_heat_adjoint_load(nelx, nely, _lib.ptr(Ws[g]), 1.0, _lib.ptr(gT[g]), st))
     gT = torch_fem.project(gT, P.heat_mask).contiguous()
     ah = torch_fem.safe_div(torch_fem._dots(T_free, gT), torch_fem._dots(T_free, heat_rhs))
-    lam_h = _pcg(hl, gT, (ah * T_free).contiguous(), rtol, max_iter, "heat_adjoint_n_iter", info)
+    lam_h = _pcg(hl, gT, (ah[:, None] * T_free).contiguous(), rtol, max_iter, "heat_adjoint_n_iter", info)
     # -lam_e^T KE_h T_e covers both femsolve's density term and the lift term
-    g_chi = torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h)["gdens"]
+    g_chi = torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h.reshape(G, nnode))["gdens"]
     q = conduction_penal
-    dpen = torch.where(x ** q >= 1e-6, q * x ** (q - 1), torch.zeros_like(x))
-    grad = grad + g_chi * dpen
-    out["gradient"] = grad.reshape(nely, nelx)
-    out["lam"] = lam
-    return out
+    dpen = torch.where(X ** q >= 1e-6, q * X ** (q - 1), torch.zeros_like(X))
+    grads = grads + g_chi * dpen
+    for g in range(G):
+        outs[g]["gradient"] = grads[g].reshape(nely, nelx)
+        outs[g]["lam"] = lam[offs[g]:offs[g + 1]]
+    return outs
 
 
 class SpaceTimeObjective(torch.autograd.Function):

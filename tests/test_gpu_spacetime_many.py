@@ -1,0 +1,68 @@
+"""Many space-time problems of uneven sizes and stage counts in one call (the batched
+uneven configuration): grouped by grid size into batched device solves on concurrent
+streams.  Each problem's result must equal the one-problem call on the same inputs, and
+the oracle's, in FP64 and in mixed precision.
+
+Tolerances: grouped against one-problem calls 1e-12 (same arithmetic per row, only the
+batching differs); against the oracle 1e-9 on the objective and 5e-9 on the gradient
+(two FP64 solves at rtol 1e-8); mixed precision 1e-6 against the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from oracle import sttopt_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(48, 24), (32, 16), (48, 24), (64, 32), (32, 16), (40, 20)]
+STAGES = [3, 5, 4, 2, 6, 1]
+
+
+def _inputs():
+    xs, ws = [], []
+    for k, (nx, ny) in enumerate(SIZES):
+        xs.append(O.smoothed_density(nx, ny, 100 + k))
+        ws.append(np.random.default_rng(100 + k).uniform(-1, 1, (ny, nx)))
+    return xs, ws
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_many_equals_one_at_a_time_and_the_oracle(pkg, precision):
+    from sttopt_b200 import spacetime
+
+    xs, ws = _inputs()
+    X = [torch.tensor(x, device="cuda") for x in xs]
+    W = [torch.tensor(w, device="cuda") for w in ws]
+    info = {}
+    many = spacetime.objective_and_gradient_many(X, W, STAGES, precision=precision, info=info)
+    assert set(info) == {(nx, ny) for nx, ny in SIZES}
+    for k, (x, w, n) in enumerate(zip(X, W, STAGES)):
+        one = spacetime.objective_and_gradient(x, w, n_stage=n, precision=precision)
+        got = many[k]
+        assert got["c_s"].shape == (n,)
+        assert got["gradient"].shape == x.shape
+        assert torch.equal(got["member"], one["member"])
+        assert rel_err(got["c_s"].cpu(), one["c_s"].cpu()) < 1e-12
+        assert rel_err(got["gradient"].cpu(), one["gradient"].cpu()) < 1e-12
+        assert abs(float(got["objective"] - one["objective"])) <= 1e-12 * abs(float(one["objective"]))
+    tol_c, tol_g = (1e-9, 5e-9) if precision == "fp64" else (1e-6, 1e-6)
+    for k in (0, 3, 5):
+        ref = O.spacetime_objective(xs[k], ws[k], n_stage=STAGES[k])
+        got = many[k]
+        assert abs(float(got["objective"]) - ref["objective"]) <= tol_c * abs(ref["objective"])
+        assert rel_err(got["gradient"].cpu(), ref["gradient"]) < tol_g
+
+
+def test_many_sequential_matches_concurrent(pkg):
+    from sttopt_b200 import spacetime
+
+    xs, ws = _inputs()
+    X = [torch.tensor(x, device="cuda") for x in xs]
+    W = [torch.tensor(w, device="cuda") for w in ws]
+    a = spacetime.objective_and_gradient_many(X, W, STAGES, precision="mixed", concurrent=True)
+    b = spacetime.objective_and_gradient_many(X, W, STAGES, precision="mixed", concurrent=False)
+    for p, q in zip(a, b):
+        assert torch.equal(p["gradient"], q["gradient"])
+        assert torch.equal(p["c_s"], q["c_s"])
