@@ -36,7 +36,7 @@ METRIC = "stage solves/s (space-time objective + full gradient, 2048x1024 Q4, 16
 UNIT = "stage solves/s"
 # Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the roofline
 # kernel from the ncu capture summarised in profiles/q4_apply_fp32_2048x1024_16rows.md.
-NCU_TRAFFIC = {"l0_apply_fp32_16rows": 654672896}
+NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576}
 
 
 def parse():
