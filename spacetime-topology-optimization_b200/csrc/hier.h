@@ -52,6 +52,8 @@ struct stt_hier_impl {
   double KE[64];
   int modal;         // KE has the modal form (march_modal); mq holds its constants
   double mq[8];
+  int l1;            // level 1 is applied from the level-0 densities (l1_sweep_kernel)
+  double l1m[9][21]; // per child m of a level-1 element: T G_m T^T / 16, packed upper triangle
   double* tables;    // device: per transition S[9][64], G[9][64], GM[9][64]
   double* keffA;     // build temporaries
   double* keffB;

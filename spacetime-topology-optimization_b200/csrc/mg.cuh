@@ -586,6 +586,353 @@ __global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
   }
 }
 
+// ---- stencil levels: column-marching sweeps, coupling products shuffled -------------
+//
+// st_sweep_kernel's operator with the four transposed couplings (W, N, NW, NE) formed by
+// the lane that owns the block and shuffled as products: lane c - 1 sends E^T x (the W
+// term of node c), the node above keeps S^T x for the row below, lane c - 1 sends SE^T x
+// to c (NW of the row below) and lane c + 1 sends SW^T x to c (NE).  Per node that is
+// 2 shuffles of x plus 3 of products per component (10 for D = 2) instead of a shuffle
+// per coefficient (16), and only the coefficients of the row being emitted are held.
+// AHEAD rows of raw loads (coefficients, rhs, flags, and x one row further) stay in
+// flight.  Modes as st_sweep_kernel, SW_POST excepted.
+template <int D, typename T, int MODE, int AHEAD = 1>
+__global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
+    const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
+    const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega) {
+  static_assert(MODE != SW_POST, "no folded prolongation on stencil levels");
+  constexpr int DD = D * D, NS = 5 * DD;
+  constexpr bool KU = MODE != SW_FIRST;
+  constexpr int NC = KU ? NS : DD;  // coefficients read per node
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const long long nnode = (long long)nnx * nny;
+  const int h = hier_row(row_map, hrows, s);
+  const T* sth = st + (size_t)h * NS * nnode;
+  const T* xs = x + (size_t)s * vec_rs;
+  const T* bs = b + (size_t)s * vec_rs;
+  T* os = out + (size_t)s * vec_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kQCols - 1 + lane;
+  const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  struct Row {
+    T co[NC];   // Cc, E, S, SE, SW of node (r, c)
+    T xn[D];    // x(r + 1, c)
+    T b[D];
+    uint8_t fl;
+  };
+  auto load_x = [&](int r, T(&v)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    if (KU && col_ok && r >= 0 && r < nny) load_node<D, T>(xs, (long long)r * nnx + c, v);
+  };
+  auto load_row = [&](int r, Row& R) {
+#pragma unroll
+    for (int k = 0; k < NC; ++k) R.co[k] = T(0);
+#pragma unroll
+    for (int d = 0; d < D; ++d) R.b[d] = T(0);
+    R.fl = 0;
+    load_x(r + 1, R.xn);
+    if (!col_ok || r < 0 || r >= nny) return;
+    const long long node = (long long)r * nnx + c;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) R.co[k] = __ldg(sth + (size_t)k * nnode + node);
+    if (MODE != SW_APPLY) load_node<D, T>(bs, node, R.b);
+    R.fl = __ldg(fixed + node);
+  };
+  // (B v)_i and (B^T v)_j of a D x D block stored row-major
+  auto bx = [](const T* B, const T(&v)[D], T(&acc)[D]) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc[i] = fma(B[i * D + j], v[j], acc[i]);
+  };
+  auto btx = [](const T* B, const T(&v)[D], T(&acc)[D]) {
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+#pragma unroll
+      for (int i = 0; i < D; ++i) acc[j] = fma(B[i * D + j], v[i], acc[j]);
+  };
+  // state: x(r, c), x(r, c + 1), and the N / NW / NE products from row r - 1
+  T xr[D], xrr[D], nN[D], nNW[D], nNE[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) nN[d] = nNW[d] = nNE[d] = T(0);
+  {
+    // row r0 - 1 seeds the products for row r0
+    T xp[D];
+    load_x(r0 - 1, xp);
+    load_x(r0, xr);
+#pragma unroll
+    for (int d = 0; d < D; ++d) xrr[d] = __shfl_down_sync(0xffffffffu, xr[d], 1);
+    if constexpr (KU) {
+      T Sp[DD], SEp[DD], SWp[DD];
+      const bool ok = col_ok && r0 - 1 >= 0;
+      const long long node = (long long)(r0 - 1) * nnx + c;
+#pragma unroll
+      for (int q = 0; q < DD; ++q) {
+        Sp[q] = ok ? __ldg(sth + (size_t)(2 * DD + q) * nnode + node) : T(0);
+        SEp[q] = ok ? __ldg(sth + (size_t)(3 * DD + q) * nnode + node) : T(0);
+        SWp[q] = ok ? __ldg(sth + (size_t)(4 * DD + q) * nnode + node) : T(0);
+      }
+      T pse[D], psw[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) pse[d] = psw[d] = T(0);
+      btx(Sp, xp, nN);
+      btx(SEp, xp, pse);
+      btx(SWp, xp, psw);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        nNW[d] = __shfl_up_sync(0xffffffffu, pse[d], 1);
+        nNE[d] = __shfl_down_sync(0xffffffffu, psw[d], 1);
+      }
+    }
+  }
+  Row q[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) load_row(r0 + k, q[k]);
+  for (int rb0 = r0; rb0 < r1; rb0 += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int r = rb0 + k;
+      const Row R = q[k];
+      load_row(r + AHEAD, q[k]);
+      T Ax[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) Ax[d] = T(0);
+      T xnl[D], xnr[D];
+      if constexpr (KU) {
+        const T* Cc = R.co;
+        const T* E = R.co + DD;
+        const T* S = R.co + 2 * DD;
+        const T* SE = R.co + 3 * DD;
+        const T* SW = R.co + 4 * DD;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          xnl[d] = __shfl_up_sync(0xffffffffu, R.xn[d], 1);
+          xnr[d] = __shfl_down_sync(0xffffffffu, R.xn[d], 1);
+        }
+        T wp[D], pse[D], psw[D], pn[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) wp[d] = pse[d] = psw[d] = pn[d] = T(0);
+        btx(E, xr, wp);    // W term of the right neighbour
+        btx(S, xr, pn);    // N term of the node below
+        btx(SE, xr, pse);  // NW term of the node below-right
+        btx(SW, xr, psw);  // NE term of the node below-left
+        bx(Cc, xr, Ax);
+        bx(E, xrr, Ax);
+        bx(S, R.xn, Ax);
+        bx(SE, xnr, Ax);
+        bx(SW, xnl, Ax);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          Ax[d] += __shfl_up_sync(0xffffffffu, wp[d], 1);
+          Ax[d] += nN[d] + nNW[d] + nNE[d];
+          nN[d] = pn[d];
+          nNW[d] = __shfl_up_sync(0xffffffffu, pse[d], 1);
+          nNE[d] = __shfl_down_sync(0xffffffffu, psw[d], 1);
+        }
+      }
+      if (out_lane && r < r1) {
+        T res[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          if (MODE == SW_FIRST || MODE == SW_SWEEP) {
+            const T dg = ((R.fl >> i) & 1) ? T(1) : R.co[i * D + i];
+            const T x0 = MODE == SW_FIRST ? T(0) : xr[i];
+            res[i] = x0 + sweep_div(omega * (R.b[i] - Ax[i]), dg);
+          } else if (MODE == SW_RESID) {
+            res[i] = R.b[i] - Ax[i];
+          } else {
+            res[i] = Ax[i];
+          }
+        }
+        store_node<D, T>(os, (long long)r * nnx + c, res);
+      }
+      if constexpr (KU) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          xr[d] = R.xn[d];
+          xrr[d] = xnr[d];
+        }
+      }
+    }
+  }
+}
+
+// ---- level 1 from the level-0 densities (plane stress) --------------------------------
+//
+// The Galerkin element matrices of level 1 are keff[E] = sum over E's KX x KY children
+// m of rho_m S_m^T KE S_m (torch_mg.build_hierarchy, sttopt/torch_mg.py:355-370, on the
+// level-0 element matrices rho KE).  Each S_m^T KE S_m annihilates the coarse
+// translations, so it is T^T M_m T in the element's edge modes (march_modal), with M_m a
+// symmetric 6 x 6 computed on the host.  A level-1 sweep therefore reads KX*KY densities
+// per element (16 B for 2 x 2, FP32) instead of 20 stencil coefficients per node (80 B):
+// per element M = sum_m rho_m M_m, q = M (Gx, Gy, H modes), corner forces as
+// march_modal.  The Jacobi diagonal comes from the stored stencil's centre block (the
+// projected operator's diagonal).  Sweep and residual modes; the first sweep from zero
+// needs only the diagonal and stays on the stencil kernel.
+template <typename T, int NM>
+struct L1Mat {
+  T m[NM][21];  // packed upper triangle, row-major
+};
+
+template <typename T, int MODE, int KX, int KY, int AHEAD = 2>
+__global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
+    const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
+    const T* __restrict__ rho0, long long rho_rs, int fnelx, const T* __restrict__ st,
+    const uint8_t* __restrict__ fixed, int nnx, int nny, const int* __restrict__ row_map, int hrows,
+    const RowState* __restrict__ rst, T omega, L1Mat<T, KX * KY> M) {
+  static_assert(MODE == SW_SWEEP || MODE == SW_RESID, "sweep and residual only");
+  constexpr int D = 2, NM = KX * KY;
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const long long nnode = (long long)nnx * nny;
+  const int h = hier_row(row_map, hrows, s);
+  const T* rh = rho0 + (size_t)h * rho_rs;
+  const T* dgh = st + (size_t)h * 5 * D * D * nnode;  // centre block: coefficients 0 and 3
+  const T* xs = x + (size_t)s * vec_rs;
+  const T* bs = b + (size_t)s * vec_rs;
+  T* os = out + (size_t)s * vec_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kQCols - 1 + lane;
+  const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const int nelx = nnx - 1, nely = nny - 1;
+  const bool ecol_ok = c >= 0 && c < nelx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  struct Ex {
+    T b[D], dg[D];
+    uint8_t fl;
+  };
+  auto X = [&](int r, T(&v)[D]) {
+    v[0] = v[1] = T(0);
+    if (col_ok && r >= 0 && r < nny) load_node<D, T>(xs, (long long)r * nnx + c, v);
+  };
+  auto Rho = [&](int r, T(&rm)[NM]) {
+    const bool ok = ecol_ok && r >= 0 && r < nely;
+#pragma unroll
+    for (int my = 0; my < KY; ++my)
+#pragma unroll
+      for (int mx = 0; mx < KX; ++mx)
+        rm[my * KX + mx] = ok ? __ldg(rh + (size_t)(KY * r + my) * fnelx + KX * c + mx) : T(0);
+  };
+  auto Ext = [&](int r, Ex& e) {
+    e.b[0] = e.b[1] = e.dg[0] = e.dg[1] = T(0);
+    e.fl = 0;
+    if (!(out_lane && r < r1)) return;
+    const long long node = (long long)r * nnx + c;
+    load_node<D, T>(bs, node, e.b);
+    e.dg[0] = __ldg(dgh + node);
+    e.dg[1] = __ldg(dgh + 3 * nnode + node);
+    e.fl = __ldg(fixed + node);
+  };
+  T ut[D], sT[D], dT[D], co[D], cr[D];
+  auto edge = [&](const T(&v)[D], T(&sv)[D], T(&dv)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const T vr = __shfl_down_sync(0xffffffffu, v[d], 1);
+      sv[d] = v[d] + vr;
+      dv[d] = vr - v[d];
+    }
+  };
+  auto step = [&](const T(&ub)[D], const T(&rm)[NM], T(&own)[D], T(&send)[D]) {
+    T sB[D], dB[D];
+    edge(ub, sB, dB);
+    T md[6];
+    md[0] = dB[0] + dT[0];  // Gx(ux)
+    md[1] = sT[1] - sB[1];  // Gy(uy)
+    md[2] = sT[0] - sB[0];  // Gy(ux)
+    md[3] = dB[1] + dT[1];  // Gx(uy)
+    md[4] = dT[0] - dB[0];  // H(ux)
+    md[5] = dT[1] - dB[1];  // H(uy)
+    T Me[21];
+#pragma unroll
+    for (int e = 0; e < 21; ++e) {
+      T a = rm[0] * M.m[0][e];
+#pragma unroll
+      for (int m = 1; m < NM; ++m) a = fma(rm[m], M.m[m][e], a);
+      Me[e] = a;
+    }
+    T q[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) q[i] = T(0);
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j, ++e) {
+        q[i] = fma(Me[e], md[j], q[i]);
+        if (j != i) q[j] = fma(Me[e], md[i], q[j]);
+      }
+    modal_corners(q[0], q[2], q[4], co[0], cr[0], own[0], send[0]);
+    modal_corners(q[3], q[1], q[5], co[1], cr[1], own[1], send[1]);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      sT[d] = sB[d];
+      dT[d] = dB[d];
+    }
+  };
+  {
+    T u0[D], own[D], send[D], rm[NM];
+    X(r0 - 1, u0);
+    edge(u0, sT, dT);
+    co[0] = co[1] = cr[0] = cr[1] = T(0);
+    X(r0, ut);
+    Rho(r0 - 1, rm);
+    step(ut, rm, own, send);
+  }
+  T qx[AHEAD][D], qr[AHEAD][NM];
+  Ex qe[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) {
+    X(r0 + 1 + k, qx[k]);
+    Rho(r0 + k, qr[k]);
+    Ext(r0 + k, qe[k]);
+  }
+  for (int rb0 = r0; rb0 < r1; rb0 += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int r = rb0 + k;
+      T ub[D], rm[NM];
+#pragma unroll
+      for (int d = 0; d < D; ++d) ub[d] = qx[k][d];
+#pragma unroll
+      for (int m = 0; m < NM; ++m) rm[m] = qr[k][m];
+      const Ex ex = qe[k];
+      X(r + 1 + AHEAD, qx[k]);
+      Rho(r + AHEAD, qr[k]);
+      Ext(r + AHEAD, qe[k]);
+      T own[D], send[D], Ax[D];
+      step(ub, rm, own, send);
+#pragma unroll
+      for (int d = 0; d < D; ++d) Ax[d] = own[d] + __shfl_up_sync(0xffffffffu, send[d], 1);
+      if (out_lane && r < r1) {
+        T res[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          if ((ex.fl >> i) & 1) Ax[i] = T(0);
+          if constexpr (MODE == SW_SWEEP) {
+            const T dg = ((ex.fl >> i) & 1) ? T(1) : ex.dg[i];
+            res[i] = ut[i] + sweep_div(omega * (ex.b[i] - Ax[i]), dg);
+          } else {
+            res[i] = ex.b[i] - Ax[i];
+          }
+        }
+        store_node<D, T>(os, (long long)r * nnx + c, res);
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d) ut[d] = ub[d];
+    }
+  }
+}
+
 // ---- restriction: column-marching full weighting ---------------------------------
 //
 // rc = P_c (R r_f), the x pass then the y pass of torch_mg._restrict_axis

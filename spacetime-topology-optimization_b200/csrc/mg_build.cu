@@ -74,6 +74,46 @@ static void galerkin_table(const double* S, const double* K, int nm, int nk, dou
 
 constexpr int kTableStride = 9 * 64;  // doubles per table (max 9 children x 8 x 8)
 
+// M_m = T G_m T^T / 16 for the nm plane-stress child matrices G (8 x 8 each), packed as
+// the upper triangle of the symmetric 6 x 6 (row-major, i <= j); mode order Gx(ux),
+// Gy(uy), Gy(ux), Gx(uy), H(ux), H(uy) as modal_from_ke.  False unless T^T M_m T
+// reproduces every G_m to 1e-12 of its largest entry.
+static bool l1_tables(const double* G, int nm, double (*out)[21]) {
+  static const double pat[3][4] = {{-1, 1, 1, -1}, {-1, -1, 1, 1}, {1, -1, 1, -1}};
+  double T[6][8] = {};
+  for (int k = 0; k < 4; ++k) {
+    T[0][2 * k] = pat[0][k];
+    T[1][2 * k + 1] = pat[1][k];
+    T[2][2 * k] = pat[1][k];
+    T[3][2 * k + 1] = pat[0][k];
+    T[4][2 * k] = pat[2][k];
+    T[5][2 * k + 1] = pat[2][k];
+  }
+  for (int m = 0; m < nm; ++m) {
+    const double* Gm = G + (size_t)m * 64;
+    double M[6][6], gmax = 0.0;
+    for (int i = 0; i < 64; ++i) gmax = std::fmax(gmax, std::fabs(Gm[i]));
+    for (int a = 0; a < 6; ++a)
+      for (int b = 0; b < 6; ++b) {
+        double s = 0.0;
+        for (int i = 0; i < 8; ++i)
+          for (int j = 0; j < 8; ++j) s += T[a][i] * Gm[i * 8 + j] * T[b][j];
+        M[a][b] = s / 16.0;
+      }
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 8; ++j) {
+        double s = 0.0;
+        for (int a = 0; a < 6; ++a)
+          for (int b = 0; b < 6; ++b) s += T[a][i] * 0.5 * (M[a][b] + M[b][a]) * T[b][j];
+        if (!(std::fabs(s - Gm[i * 8 + j]) <= 1e-12 * gmax)) return false;
+      }
+    int e = 0;
+    for (int a = 0; a < 6; ++a)
+      for (int b = a; b < 6; ++b) out[m][e++] = 0.5 * (M[a][b] + M[b][a]);
+  }
+  return true;
+}
+
 static inline char* carve(char*& p, long long& used, long long bytes) {
   const long long a = (bytes + 255) & ~255LL;
   char* r = p ? p + used : nullptr;
@@ -558,6 +598,13 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     }
   }
   STT_TRY(check_cuda(cudaMemcpyAsync(h->tables, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st), "tables"));
+  // level 1 from the level-0 densities: its element matrices are sum_m rho_m G_m, and each
+  // G_m = S_m^T KE S_m annihilates the coarse translations, so G_m = T^T M_m T in the
+  // bilinear edge modes (q4.cuh); kept when M_m rebuilds G_m to 1e-12 (plane stress, no
+  // reaction, 2 or 3 children a direction, level 1 not the coarsest)
+  h->l1 = 0;
+  if (D == 2 && h->modal && !reaction && h->nlevels > 2 && h->lv[0].kx >= 2 && h->lv[0].ky >= 2)
+    h->l1 = l1_tables(&tab[kTableStride], h->lv[0].kx * h->lv[0].ky, h->l1m) ? 1 : 0;
 
   const double* kprev = nullptr;
   for (int l = 1; l < h->nlevels; ++l) {

@@ -130,6 +130,37 @@ struct Cycle {
     else return (const T*)h->lv[l].st64;
   }
 
+  // Level 1's sweep or residual from the level-0 densities (l1_sweep_kernel) when the
+  // hierarchy allows it; false when the stencil kernel must run.
+  template <int MODE>
+  bool l1_pass(int l, const T* x, const T* b, T* out) {
+    if constexpr (D != 2 || !(MODE == SW_SWEEP || MODE == SW_RESID)) {
+      return false;
+    } else {
+      if (l != 1 || !h->l1) return false;
+      const LevelDesc& f = h->lv[0];
+      const LevelDesc& lv = h->lv[1];
+      const dim3 g = tile_grid(lv.nelx, lv.nely, nrows);
+      const T* r0 = rho0();
+#define STT_L1(KX, KY)                                                                               \
+  do {                                                                                               \
+    L1Mat<T, KX * KY> M;                                                                             \
+    for (int m = 0; m < KX * KY; ++m)                                                                \
+      for (int e = 0; e < 21; ++e) M.m[m][e] = T(h->l1m[m][e]);                                      \
+    l1_sweep_kernel<T, MODE, KX, KY><<<g, kQThreads, 0, st>>>(x, b, out, vstride(lv.ndof), r0, f.rs_rho, \
+                                                              f.nelx, stl(1), lv.fixed, lv.nnx, lv.nny,  \
+                                                              h->row_map, h->hrows, rst, omega, M);      \
+  } while (0)
+      if (f.kx == 2 && f.ky == 2) STT_L1(2, 2);
+      else if (f.kx == 2 && f.ky == 3) STT_L1(2, 3);
+      else if (f.kx == 3 && f.ky == 2) STT_L1(3, 2);
+      else if (f.kx == 3 && f.ky == 3) STT_L1(3, 3);
+      else return false;
+#undef STT_L1
+      return true;
+    }
+  }
+
   // One smoother / residual / apply pass at level l: out = op(x, b); SW_POST reads
   // x + P(pro.ec) (the coarse correction) in place of x.
   template <int MODE>
@@ -150,10 +181,16 @@ struct Cycle {
         l0_sweep_kernel<D, T, MODE><<<g, kQThreads, 0, st>>>(
             x, x_rs, b, b_rs, out, o_rs, rho0(), lv.rs_rho, rdiag0(), lv.ndof, lv.fixed, h->row_map,
             h->hrows, rst, lv.nelx, lv.nely, omega, ke, 0, pro);
+    } else if (l1_pass<MODE>(l, x, b, out)) {
+      // level 1 applied from the level-0 densities
     } else {
-      st_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-          x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
-          pro);
+      if constexpr (MODE == SW_POST)
+        st_sweep_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+            x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
+            pro);
+      else
+        st_sweep2_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+            x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega);
     }
   }
 
@@ -724,13 +761,11 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
   if (v_rs != out_rs)
     return set_error(STT_ERR_INVALID, "stt_level_apply: coarse levels need equal row strides");
   if (h->d == 2)
-    st_sweep_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0,
-        ProlongSrc<double>{nullptr, 0, 1, 1, 1});
+    st_sweep2_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
   else
-    st_sweep_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0,
-        ProlongSrc<double>{nullptr, 0, 1, 1, 1});
+    st_sweep2_kernel<1, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+        v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);
   return check_launch("level apply");
 }
 
