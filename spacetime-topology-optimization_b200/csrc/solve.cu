@@ -48,7 +48,7 @@ struct SolveWS {
   RowState* rs;
   double* partials;
   unsigned* counters;
-  double *r, *p, *Ap;          // FP64 [nrows][ndof0]
+  double *r, *p, *p2, *Ap;     // FP64 [nrows][ndof0]; p and p2 alternate
   void *z, *zold, *b0;         // cycle precision [nrows][ndof0]
   void* x[kMaxLevels];         // per level [nrows][ndof_l]
   void* t[kMaxLevels];
@@ -79,6 +79,7 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
   w.counters = (unsigned*)carve(base, used, 4LL * nrows);
   w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
   w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  w.p2 = (double*)carve(base, used, 8LL * nrows * l0.ndof);
   w.Ap = (double*)carve(base, used, 8LL * nrows * l0.ndof);
   w.z = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
   w.zold = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
@@ -404,20 +405,35 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
   });
 }
 
-// Ap = A p (projected, + lumped reaction), pAp = p . Ap, alpha = safe_div(rz, pAp).
-// p is zero at fixed dofs by construction (it is built from the projected z).
-template <int D, bool MODAL, bool RD>
+// The search direction and its operator product in one pass:
+//   PMODE 1 (first iteration): p = z;   PMODE 2: p = beta p_old + z   (p written to pout)
+//   Ap = A p (projected, + lumped reaction), pAp = p . Ap, alpha = safe_div(rz, pAp).
+// The reference's p update (torch_fem.py:325-331) folded into the p.Ap pass, so p and z
+// cross HBM once per iteration instead of twice.  p_old and pout are different buffers:
+// the halo columns and rows of a strip belong to its neighbours, which may already have
+// written their p.  p is zero at fixed dofs by construction (z is projected).
+template <typename TZ, int D>
+struct PZIn {
+  double p[D];
+  TZ z[D];
+};
+
+template <int D, bool MODAL, bool RD, typename TZ, int PMODE>
 __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
-    const double* __restrict__ p, double* __restrict__ Ap, long long rs,
-    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag,
-    long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map,
-    int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely, KEq<D, double> ke,
-    MQ<double> mq) {
+    const double* __restrict__ pold, double* __restrict__ pout, const TZ* __restrict__ z, long long z_rs,
+    double* __restrict__ Ap, long long rs, const double* __restrict__ rho, long long rho_rs,
+    const double* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
+    const int* __restrict__ row_map, int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely,
+    KEq<D, double> ke, MQ<double> mq) {
+  static_assert(PMODE == 1 || PMODE == 2, "p = z or p = beta p + z");
   const int s = blockIdx.z;
   if (!rst[s].active) return;
+  const double beta = PMODE == 2 ? rst[s].beta : 0.0;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
-  const double* ps = p + (size_t)s * rs;
+  const double* ps = PMODE == 2 ? pold + (size_t)s * rs : nullptr;
+  double* po = pout + (size_t)s * rs;
+  const TZ* zs = z + (size_t)s * z_rs;
   const double* rh = rho + (size_t)h * rho_rs;
   const double* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
   double* As = Ap + (size_t)s * rs;
@@ -431,20 +447,38 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
       vals[0] = fma(uc[i], Ax[i], vals[0]);
     }
     store_node<D, double>(As, node, Ax);
+    store_node<D, double>(po, node, uc);
   };
   auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
   if constexpr (MODAL) {
-    march_modal<D, double, true, false, false>(
+    march_modal<D, double, true, false, false, NoExtra, PZIn<TZ, D>>(
         mq, nnx, nny, [&](int rr, int cc) { return __ldg(fixed + rr * nnx + cc); },
-        [&](int rr, int cc, uint8_t, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); }, loadr,
-        [&](int, int) { return NoExtra{}; },
+        [&](int rr, int cc, uint8_t, PZIn<TZ, D>& in) {
+          const long long node = (long long)rr * nnx + cc;
+          if (PMODE == 2) load_node<D, double>(ps, node, in.p);
+          load_node<D, TZ>(zs, node, in.z);
+        },
+        loadr, [&](int, int) { return NoExtra{}; },
         [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl, const NoExtra&) {
           finish(rr, cc, Ax, uc, fl);
+        },
+        [&](int, int, uint8_t, const PZIn<TZ, D>& in, double(&v)[D]) {
+#pragma unroll
+          for (int d = 0; d < D; ++d) v[d] = PMODE == 2 ? fma(in.p[d], beta, (double)in.z[d]) : (double)in.z[d];
         });
   } else {
     march<D, double, true, false, FlagX>(
-        ke, nnx, nny, [&](int rr, int cc, double(&v)[D]) { load_node<D, double>(ps, rr * nnx + cc, v); }, loadr,
-        [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
+        ke, nnx, nny,
+        [&](int rr, int cc, double(&v)[D]) {
+          const long long node = (long long)rr * nnx + cc;
+          TZ zv[D];
+          load_node<D, TZ>(zs, node, zv);
+          double pv[D];
+          if (PMODE == 2) load_node<D, double>(ps, node, pv);
+#pragma unroll
+          for (int d = 0; d < D; ++d) v[d] = PMODE == 2 ? fma(pv[d], beta, (double)zv[d]) : (double)zv[d];
+        },
+        loadr, [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
         [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const FlagX& ex) {
           finish(rr, cc, Ax, uc, ex.fl);
         });
@@ -509,7 +543,7 @@ __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
     const double zv = (double)zs[i];
     vals[0] = fma(rsv[i], zv, vals[0]);
     if (flexible && !first) vals[1] = fma(rsv[i], (double)zo[i], vals[1]);
-    if (first) p[(size_t)s * rs + i] = zv;
+    if (first && p) p[(size_t)s * rs + i] = zv;
   }
   grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
     RowState& S = rst[s];
@@ -524,21 +558,6 @@ __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
   });
 }
 
-// p = p * beta + z
-template <typename TZ>
-__global__ void __launch_bounds__(kEwThreads) pcg_pupd_kernel(const TZ* __restrict__ z,
-                                                              double* __restrict__ p, long long rs,
-                                                              long long z_rs, long long n,
-                                                              const RowState* __restrict__ rst) {
-  const int s = blockIdx.y;
-  if (!rst[s].active) return;
-  const double beta = rst[s].beta;
-  double* ps = p + (size_t)s * rs;
-  const TZ* zs = z + (size_t)s * z_rs;
-  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kEwThreads)
-    ps[i] = ps[i] * beta + (double)zs[i];
-}
 
 __global__ void rows_zero_kernel(double* __restrict__ x, long long rs, long long n) {
   const int s = blockIdx.y;
@@ -634,32 +653,40 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   if (n_active() > 0) {
     T* z = (T*)w.z;
     T* zold = (T*)w.zold;
+    double* pcur = w.p;    // p of the previous iteration
+    double* pnext = w.p2;  // where this iteration's p goes
     STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
-    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, vstride(nd), nd, w.rs, red_ew, 1, flexible);
+    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 1, flexible);
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
-#define STT_PAP(MODAL, RD)                                                                                \
-  pcg_pap_kernel<D, MODAL, RD><<<tg, kQThreads, 0, st>>>(w.p, w.Ap, nd, l0.rho64, l0.rs_rho, rd0, l0.ndof,     \
-                                                         l0.fixed, h->row_map, h->hrows, w.rs, red_tile,         \
-                                                         h->nelx, h->nely, ke, mq)
-      if (h->modal) {
-        if (rd0) STT_PAP(true, true);
-        else STT_PAP(true, false);
-      } else {
-        if (rd0) STT_PAP(false, true);
-        else STT_PAP(false, false);
-      }
+#define STT_PAP(MODAL, RD, PM)                                                                            \
+  pcg_pap_kernel<D, MODAL, RD, T, PM><<<tg, kQThreads, 0, st>>>(pcur, pnext, z, vstride(nd), w.Ap, nd, l0.rho64,  \
+                                                                l0.rs_rho, rd0, l0.ndof, l0.fixed, h->row_map,    \
+                                                                h->hrows, w.rs, red_tile, h->nelx, h->nely, ke, mq)
+#define STT_PAP2(PM)                 \
+  do {                               \
+    if (h->modal) {                  \
+      if (rd0) STT_PAP(true, true, PM);   \
+      else STT_PAP(true, false, PM);      \
+    } else {                         \
+      if (rd0) STT_PAP(false, true, PM);  \
+      else STT_PAP(false, false, PM);     \
+    }                                \
+  } while (0)
+      if (it == 1) STT_PAP2(1);
+      else STT_PAP2(2);
+#undef STT_PAP2
 #undef STT_PAP
       float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
-      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, w.p, w.Ap, nd, nd, w.rs, red_ew, pp,
+      std::swap(pcur, pnext);
+      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, pcur, w.Ap, nd, nd, w.rs, red_ew, pp,
                                                                   r32, vstride(nd));
       const bool replaced = replace_every > 0 && it % replace_every == 0;
       if (replaced) init(x, pp, 1);
       if (flexible) std::swap(z, zold);
       STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
-      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, w.p, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
-      pcg_pupd_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(z, w.p, nd, vstride(nd), nd, w.rs);
+      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
       STT_TRY(check_launch("pcg iteration"));
       if (it % check_every == 0 || it == max_iter) {
         STT_TRY(pull());

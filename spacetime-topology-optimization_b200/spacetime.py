@@ -130,13 +130,14 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
         return results
     import concurrent.futures
 
-    main = torch.cuda.current_stream(dev)
+    dev_i = _device_index(dev)
+    main = torch.cuda.current_stream(dev_i)
     ready = torch.cuda.Event()
     ready.record(main)
-    streams = {shape: torch.cuda.Stream(device=dev) for shape in groups}
+    streams = {shape: torch.cuda.Stream(device=dev_i) for shape in groups}
 
     def on_stream(shape, idx):
-        torch.cuda.set_device(dev)
+        torch.cuda.set_device(dev_i)
         s = streams[shape]
         s.wait_event(ready)
         with torch.cuda.stream(s):
@@ -153,6 +154,59 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
             if isinstance(v, torch.Tensor) and v.is_cuda:
                 v.record_stream(main)
     return results
+
+
+def _device_index(dev) -> int:
+    """The CUDA device index of ``dev`` (an index-less "cuda" means the caller's current
+    device), for host threads, whose current device is their own."""
+    dev = torch.device(dev)
+    return dev.index if dev.index is not None else torch.cuda.current_device()
+
+
+class _HeatAdjoint:
+    """The heat adjoint solves of a group on a side stream, driven by a host thread.
+
+    d(sum w tPhys)/dT = -(w / scale) / 4 per corner; the adjoint is warm-started at the
+    exact multiple of T_free (compliance-like), and -lam_e^T KE_h T_e gives both the
+    density term of the solve and the lift term.  ``result()`` joins the thread and
+    orders the caller's stream after the side stream."""
+
+    def __init__(self, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info):
+        import concurrent.futures
+
+        self.dev = _device_index(P.device)
+        self.main = torch.cuda.current_stream(self.dev)
+        self.side = torch.cuda.Stream(device=self.dev)
+        self.side.wait_stream(self.main)
+        self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+        self.fut = self.pool.submit(self._run, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info)
+
+    def _run(self, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info):
+        torch.cuda.set_device(self.dev)
+        with torch.cuda.stream(self.side):
+            L, st = _lib.lib(), _lib.stream()
+            G, nnode = T.shape
+            gT = torch.empty(G, nnode, dtype=torch.float64, device=P.device)
+            for g in range(G):
+                _lib.check(L.stt_heat_adjoint_load(P.nelx, P.nely, _lib.ptr(Ws[g]), 1.0, _lib.ptr(gT[g]), st))
+            gT = torch_fem.project(gT, P.heat_mask).contiguous()
+            ah = torch_fem.safe_div(torch_fem._dots(T_free, gT), torch_fem._dots(T_free, heat_rhs))
+            lam_h = _pcg(hl, gT, (ah[:, None] * T_free).contiguous(), rtol, max_iter, "heat_adjoint_n_iter", info)
+            return torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h.reshape(G, nnode))["gdens"]
+
+    def result(self):
+        try:
+            g_chi = self.fut.result()
+        finally:
+            self.pool.shutdown(wait=True)
+        self.main.wait_stream(self.side)
+        g_chi.record_stream(self.main)
+        return g_chi
+
+    def abandon(self):
+        """Wait for the side work and drop it (the caller is unwinding an error)."""
+        self.pool.shutdown(wait=True)
+        self.main.wait_stream(self.side)
 
 
 def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
@@ -189,83 +243,88 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
     scale = torch.where(part, t_e, torch.full_like(t_e, -torch.inf)).max(dim=1, keepdim=True).values
     tPhys = (t_e / scale).contiguous()
 
-    # 2.-3. stage rows of every problem, then the batched stage solves
-    offs = [0]
-    for n in n_stages:
-        offs.append(offs[-1] + n)
-    S = offs[-1]
-    members = []
-    rho = torch.empty(S, nel, dtype=torch.float64, device=dev)
-    F = torch.empty(S, 2 * nnode, dtype=torch.float64, device=dev)
-    for g, n in enumerate(n_stages):
-        m = torch.empty(n, nel, dtype=torch.uint8, device=dev)
-        _lib.check(L.stt_stage_membership(nel, n, _lib.ptr(tPhys[g]), _lib.ptr(m), st))
-        _lib.check(L.stt_stage_rows(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(m), Emin, Emax, penal,
-                                    _lib.ptr(P.fixed2), _lib.ptr(rho[offs[g]]), _lib.ptr(F[offs[g]]), st))
-        members.append(m)
-    if batched:
-        sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
-                                      max_coarse_elements=max_coarse_elements, precision=precision)
-        U = _pcg(sl, F, None, rtol, max_iter, "stage_n_iter", info)
-        stage_levels = [sl]
-    else:
-        Us, stage_levels = [], []
-        for s in range(S):
-            sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
+    # 5b (overlapped). The heat adjoints need only T, tPhys's scale and w, not the stage
+    # solves: they run from a host thread on a side stream while this thread launches the
+    # stage work, so the heat solve's small, latency-bound kernels fill gaps in the
+    # bandwidth-bound stage kernels instead of adding to the step.
+    heat_adj = None
+    if gradient:
+        heat_adj = _HeatAdjoint(P, hl, T, T_free, heat_rhs, (W / scale).contiguous(), rtol, max_iter, info)
+
+    try:
+        # 2.-3. stage rows of every problem, then the batched stage solves
+        offs = [0]
+        for n in n_stages:
+            offs.append(offs[-1] + n)
+        S = offs[-1]
+        members = []
+        rho = torch.empty(S, nel, dtype=torch.float64, device=dev)
+        F = torch.empty(S, 2 * nnode, dtype=torch.float64, device=dev)
+        for g, n in enumerate(n_stages):
+            m = torch.empty(n, nel, dtype=torch.uint8, device=dev)
+            _lib.check(L.stt_stage_membership(nel, n, _lib.ptr(tPhys[g]), _lib.ptr(m), st))
+            _lib.check(L.stt_stage_rows(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(m), Emin, Emax, penal,
+                                        _lib.ptr(P.fixed2), _lib.ptr(rho[offs[g]]), _lib.ptr(F[offs[g]]), st))
+            members.append(m)
+        if batched:
+            sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
                                           max_coarse_elements=max_coarse_elements, precision=precision)
-            Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
-            stage_levels.append(sl)
-        U = torch.stack(Us)
-    ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
-    c_s = (rho * ce).sum(-1)
-    J_t = (W * tPhys).sum(-1)
-    outs = []
-    for g in range(G):
-        a, b = offs[g], offs[g + 1]
-        outs.append(dict(objective=c_s[a:b].sum() + J_t[g], c_s=c_s[a:b], J_t=J_t[g],
-                         tPhys=tPhys[g].reshape(nely, nelx), U=U[a:b], T=T[g], member=members[g]))
-    if not gradient:
+            U = _pcg(sl, F, None, rtol, max_iter, "stage_n_iter", info)
+            stage_levels = [sl]
+        else:
+            Us, stage_levels = [], []
+            for s in range(S):
+                sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
+                                              max_coarse_elements=max_coarse_elements, precision=precision)
+                Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
+                stage_levels.append(sl)
+            U = torch.stack(Us)
+        ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
+        c_s = (rho * ce).sum(-1)
+        J_t = (W * tPhys).sum(-1)
+        outs = []
+        for g in range(G):
+            a, b = offs[g], offs[g + 1]
+            outs.append(dict(objective=c_s[a:b].sum() + J_t[g], c_s=c_s[a:b], J_t=J_t[g],
+                             tPhys=tPhys[g].reshape(nely, nelx), U=U[a:b], T=T[g], member=members[g]))
+        if not gradient:
+            return outs
+
+        # 5a. stage adjoints: dL/dU = 2 K U; warm start alpha U (exact for compliance)
+        gK = torch.empty_like(U)
+        _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
+                                  2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
+                                  _lib.STT_PROJECT_OUT, P.ke, st))
+        gK = 2 * gK
+        a_ = torch_fem.safe_div(torch_fem._dots(U, gK), torch_fem._dots(U, F))
+        x0 = (a_[:, None] * U).contiguous()
+        if batched:
+            lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
+        else:
+            lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
+                               for s in range(S)])
+        lam = lam.contiguous()
+        gd = torch_fem.element_terms(U, P.edof, P.KE, lam=lam)["gdens"]
+        grads = torch.zeros(G, nel, dtype=torch.float64, device=dev)
+        for g, n in enumerate(n_stages):
+            a = offs[g]
+            _lib.check(L.stt_stage_gradient(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(members[g]), _lib.ptr(ce[a]),
+                                            _lib.ptr(gd[a]), _lib.ptr(lam[a]), Emin, Emax, penal,
+                                            _lib.ptr(grads[g]), st))
+
+        # 5b. the heat adjoints' share of the gradient
+        g_chi = heat_adj.result()
+        q = conduction_penal
+        dpen = torch.where(X ** q >= 1e-6, q * X ** (q - 1), torch.zeros_like(X))
+        grads = grads + g_chi * dpen
+        for g in range(G):
+            outs[g]["gradient"] = grads[g].reshape(nely, nelx)
+            outs[g]["lam"] = lam[offs[g]:offs[g + 1]]
         return outs
-
-    # 5a. stage adjoints: dL/dU = 2 K U; warm start alpha U (exact for compliance)
-    gK = torch.empty_like(U)
-    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
-                              2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
-                              _lib.STT_PROJECT_OUT, P.ke, st))
-    gK = 2 * gK
-    a_ = torch_fem.safe_div(torch_fem._dots(U, gK), torch_fem._dots(U, F))
-    x0 = (a_[:, None] * U).contiguous()
-    if batched:
-        lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
-    else:
-        lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
-                           for s in range(S)])
-    lam = lam.contiguous()
-    gd = torch_fem.element_terms(U, P.edof, P.KE, lam=lam)["gdens"]
-    grads = torch.zeros(G, nel, dtype=torch.float64, device=dev)
-    for g, n in enumerate(n_stages):
-        a = offs[g]
-        _lib.check(L.stt_stage_gradient(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(members[g]), _lib.ptr(ce[a]),
-                                        _lib.ptr(gd[a]), _lib.ptr(lam[a]), Emin, Emax, penal,
-                                        _lib.ptr(grads[g]), st))
-
-    # 5b. heat adjoints: d(sum w tPhys)/dT = -(w / scale) / 4 per corner
-    Ws = (W / scale).contiguous()
-    gT = torch.empty(G, nnode, dtype=torch.float64, device=dev)
-    for g in range(G):
-        _lib.check(L.stt_heat_adjoint_load(nelx, nely, _lib.ptr(Ws[g]), 1.0, _lib.ptr(gT[g]), st))
-    gT = torch_fem.project(gT, P.heat_mask).contiguous()
-    ah = torch_fem.safe_div(torch_fem._dots(T_free, gT), torch_fem._dots(T_free, heat_rhs))
-    lam_h = _pcg(hl, gT, (ah[:, None] * T_free).contiguous(), rtol, max_iter, "heat_adjoint_n_iter", info)
-    # -lam_e^T KE_h T_e covers both femsolve's density term and the lift term
-    g_chi = torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h.reshape(G, nnode))["gdens"]
-    q = conduction_penal
-    dpen = torch.where(X ** q >= 1e-6, q * X ** (q - 1), torch.zeros_like(X))
-    grads = grads + g_chi * dpen
-    for g in range(G):
-        outs[g]["gradient"] = grads[g].reshape(nely, nelx)
-        outs[g]["lam"] = lam[offs[g]:offs[g + 1]]
-    return outs
+    except BaseException:
+        if heat_adj is not None:
+            heat_adj.abandon()
+        raise
 
 
 class SpaceTimeObjective(torch.autograd.Function):
