@@ -41,7 +41,8 @@ struct RowState {
   int active;         // 1 while the row iterates
   int conv_iter;      // iteration at which the row converged (-1 while active)
   int status;         // STT_OK, or STT_ERR_BREAKDOWN on a non-finite scalar
-  int pad;
+  int xpend;          // alpha p of the last update is not yet added to x
+  int pbuf;           // which p buffer holds this row's last p (0 or 1)
 };
 
 STT_DEV int hier_row(const int* row_map, int hrows, int s) {

@@ -418,17 +418,28 @@ struct PZIn {
   TZ z[D];
 };
 
-template <int D, bool MODAL, bool RD, typename TZ, int PMODE>
+// XP: also add the previous update's alpha p_old to x at each output node (the row's
+// pending x update, RowState::xpend), so x is not streamed by the update kernel.
+template <int D>
+struct XPExtra {
+  double x[D], p[D];
+};
+
+template <int D, bool MODAL, bool RD, typename TZ, int PMODE, bool XP>
 __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
-    const double* __restrict__ pold, double* __restrict__ pout, const TZ* __restrict__ z, long long z_rs,
-    double* __restrict__ Ap, long long rs, const double* __restrict__ rho, long long rho_rs,
-    const double* __restrict__ rdiag, long long rd_rs, const uint8_t* __restrict__ fixed,
-    const int* __restrict__ row_map, int hrows, RowState* __restrict__ rst, GridRed red, int nelx, int nely,
-    KEq<D, double> ke, MQ<double> mq) {
+    const double* __restrict__ pold, double* __restrict__ pout, int pout_buf, const TZ* __restrict__ z,
+    long long z_rs, double* __restrict__ x, long long x_rs, double* __restrict__ Ap, long long rs,
+    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ rdiag, long long rd_rs,
+    const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows, RowState* __restrict__ rst,
+    GridRed red, int nelx, int nely, KEq<D, double> ke, MQ<double> mq) {
   static_assert(PMODE == 1 || PMODE == 2, "p = z or p = beta p + z");
+  static_assert(!XP || PMODE == 2, "a pending x update follows an earlier p");
   const int s = blockIdx.z;
   if (!rst[s].active) return;
   const double beta = PMODE == 2 ? rst[s].beta : 0.0;
+  const bool xp = XP && rst[s].xpend;
+  const double alpha_prev = XP ? rst[s].alpha : 0.0;
+  double* xsr = XP ? x + (size_t)s * x_rs : nullptr;
   const int nnx = nelx + 1, nny = nely + 1;
   const int h = hier_row(row_map, hrows, s);
   const double* ps = PMODE == 2 ? pold + (size_t)s * rs : nullptr;
@@ -438,7 +449,7 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
   const double* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
   double* As = Ap + (size_t)s * rs;
   double vals[1] = {0.0};
-  auto finish = [&](int rr, int cc, double(&Ax)[D], const double(&uc)[D], uint8_t fl) {
+  auto finish = [&](int rr, int cc, double(&Ax)[D], const double(&uc)[D], uint8_t fl, const XPExtra<D>& ex) {
     const int node = rr * nnx + cc;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -448,20 +459,34 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
     }
     store_node<D, double>(As, node, Ax);
     store_node<D, double>(po, node, uc);
+    if (XP && xp) {
+      double xn[D];
+#pragma unroll
+      for (int i = 0; i < D; ++i) xn[i] = ex.x[i] + alpha_prev * ex.p[i];
+      store_node<D, double>(xsr, node, xn);
+    }
+  };
+  auto loadxp = [&](int rr, int cc) {
+    XPExtra<D> e{};
+    if (XP && xp) {
+      const long long node = (long long)rr * nnx + cc;
+      load_node<D, double>(xsr, node, e.x);
+      load_node<D, double>(ps, node, e.p);
+    }
+    return e;
   };
   auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
   if constexpr (MODAL) {
-    march_modal<D, double, true, false, false, NoExtra, PZIn<TZ, D>>(
+    march_modal<D, double, true, false, false, XPExtra<D>, PZIn<TZ, D>>(
         mq, nnx, nny, [&](int rr, int cc) { return __ldg(fixed + rr * nnx + cc); },
         [&](int rr, int cc, uint8_t, PZIn<TZ, D>& in) {
           const long long node = (long long)rr * nnx + cc;
           if (PMODE == 2) load_node<D, double>(ps, node, in.p);
           load_node<D, TZ>(zs, node, in.z);
         },
-        loadr, [&](int, int) { return NoExtra{}; },
-        [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl, const NoExtra&) {
-          finish(rr, cc, Ax, uc, fl);
-        },
+        loadr, loadxp,
+        [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl,
+            const XPExtra<D>& ex) { finish(rr, cc, Ax, uc, fl, ex); },
         [&](int, int, uint8_t, const PZIn<TZ, D>& in, double(&v)[D]) {
 #pragma unroll
           for (int d = 0; d < D; ++d) v[d] = PMODE == 2 ? fma(in.p[d], beta, (double)in.z[d]) : (double)in.z[d];
@@ -480,7 +505,7 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
         },
         loadr, [&](int rr, int cc) { return FlagX{__ldg(fixed + rr * nnx + cc)}; },
         [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], const FlagX& ex) {
-          finish(rr, cc, Ax, uc, ex.fl);
+          finish(rr, cc, Ax, uc, ex.fl, loadxp(rr, cc));
         });
   }
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
@@ -488,27 +513,27 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
     RowState& S = rst[s];
     S.pAp = t[0];
     S.alpha = safe_div(S.rz, t[0]);
+    S.pbuf = pout_buf;
+    if (XP) S.xpend = 0;
     if (!isfinite(S.alpha)) S.status = STT_ERR_BREAKDOWN;
   });
 }
 
 // x += alpha p, r -= alpha Ap, ||r||^2, convergence.
+// r -= alpha Ap, ||r||^2, convergence.  x += alpha p is deferred: the next p.Ap pass
+// (which reads this p anyway) or the final flush adds it (RowState::xpend).
 __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
-    double* __restrict__ x, long long x_rs, double* __restrict__ r, const double* __restrict__ p,
-    const double* __restrict__ Ap, long long rs, long long n, RowState* __restrict__ rst,
-    GridRed red, PcgParams pp, float* __restrict__ r32, long long r32_rs) {
+    double* __restrict__ r, const double* __restrict__ Ap, long long rs, long long n,
+    RowState* __restrict__ rst, GridRed red, PcgParams pp, float* __restrict__ r32, long long r32_rs) {
   const int s = blockIdx.y;
   if (!rst[s].active) return;
   const double alpha = rst[s].alpha;
-  double* xs = x + (size_t)s * x_rs;
   double* rsv = r + (size_t)s * rs;
-  const double* ps = p + (size_t)s * rs;
   const double* as = Ap + (size_t)s * rs;
   float* r32s = r32 ? r32 + (size_t)s * r32_rs : nullptr;
   double vals[1] = {0.0};
   for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kEwThreads) {
-    xs[i] = xs[i] + alpha * ps[i];
     const double rv = rsv[i] - alpha * as[i];
     rsv[i] = rv;
     if (r32s) r32s[i] = (float)rv;  // the FP32 V-cycle's right-hand side
@@ -516,6 +541,7 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
   }
   grid_reduce<1, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
     RowState& S = rst[s];
+    S.xpend = 1;
     S.rel = sqrt(t[0]) / S.bnorm_safe;
     if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
     if (S.rel <= pp.rtol) {
@@ -523,6 +549,27 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
       S.conv_iter = pp.it;
     }
   });
+}
+
+// x += alpha p for every row whose last update is still pending (p from the buffer its
+// last p.Ap pass wrote); then pcg_xclear_kernel clears the flags.
+__global__ void __launch_bounds__(kEwThreads) pcg_xflush_kernel(double* __restrict__ x, long long x_rs,
+                                                                const double* __restrict__ p0,
+                                                                const double* __restrict__ p1, long long rs,
+                                                                long long n, const RowState* __restrict__ rst) {
+  const int s = blockIdx.y;
+  if (!rst[s].xpend) return;
+  const double alpha = rst[s].alpha;
+  double* xs = x + (size_t)s * x_rs;
+  const double* ps = (rst[s].pbuf ? p1 : p0) + (size_t)s * rs;
+  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kEwThreads)
+    xs[i] = xs[i] + alpha * ps[i];
+}
+
+__global__ void pcg_xclear_kernel(RowState* __restrict__ rst, int nrows) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nrows) rst[s].xpend = 0;
 }
 
 // rz = r . z (and r . z_old for the flexible beta); first: p = z, rz_old = rz;
@@ -655,35 +702,50 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     T* zold = (T*)w.zold;
     double* pcur = w.p;    // p of the previous iteration
     double* pnext = w.p2;  // where this iteration's p goes
+    int pnext_buf = 1;     // index of pnext: 0 = w.p, 1 = w.p2
+    // adds every row's pending alpha p to x (before a true-residual replacement and at
+    // the end); the p.Ap pass of the next iteration does it for rows still iterating
+    auto flush_x = [&]() {
+      pcg_xflush_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.p, w.p2, nd, nd, w.rs);
+      pcg_xclear_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(w.rs, nrows);
+    };
+    bool pending = false;  // the rows still iterating have an x update pending
     STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
     pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 1, flexible);
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
-#define STT_PAP(MODAL, RD, PM)                                                                            \
-  pcg_pap_kernel<D, MODAL, RD, T, PM><<<tg, kQThreads, 0, st>>>(pcur, pnext, z, vstride(nd), w.Ap, nd, l0.rho64,  \
-                                                                l0.rs_rho, rd0, l0.ndof, l0.fixed, h->row_map,    \
-                                                                h->hrows, w.rs, red_tile, h->nelx, h->nely, ke, mq)
-#define STT_PAP2(PM)                 \
-  do {                               \
-    if (h->modal) {                  \
-      if (rd0) STT_PAP(true, true, PM);   \
-      else STT_PAP(true, false, PM);      \
-    } else {                         \
-      if (rd0) STT_PAP(false, true, PM);  \
-      else STT_PAP(false, false, PM);     \
-    }                                \
+#define STT_PAP(MODAL, RD, PM, XP)                                                                         \
+  pcg_pap_kernel<D, MODAL, RD, T, PM, XP><<<tg, kQThreads, 0, st>>>(                                       \
+      pcur, pnext, pnext_buf, z, vstride(nd), x, x_rs, w.Ap, nd, l0.rho64, l0.rs_rho, rd0, l0.ndof, l0.fixed, \
+      h->row_map, h->hrows, w.rs, red_tile, h->nelx, h->nely, ke, mq)
+#define STT_PAP2(PM, XP)                    \
+  do {                                      \
+    if (h->modal) {                         \
+      if (rd0) STT_PAP(true, true, PM, XP);   \
+      else STT_PAP(true, false, PM, XP);      \
+    } else {                                \
+      if (rd0) STT_PAP(false, true, PM, XP);  \
+      else STT_PAP(false, false, PM, XP);     \
+    }                                       \
   } while (0)
-      if (it == 1) STT_PAP2(1);
-      else STT_PAP2(2);
+      if (it == 1) STT_PAP2(1, false);
+      else if (pending) STT_PAP2(2, true);
+      else STT_PAP2(2, false);
 #undef STT_PAP2
 #undef STT_PAP
       float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
       std::swap(pcur, pnext);
-      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, w.r, pcur, w.Ap, nd, nd, w.rs, red_ew, pp,
-                                                                  r32, vstride(nd));
+      pnext_buf ^= 1;
+      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, w.Ap, nd, nd, w.rs, red_ew, pp, r32,
+                                                                  vstride(nd));
+      pending = true;
       const bool replaced = replace_every > 0 && it % replace_every == 0;
-      if (replaced) init(x, pp, 1);
+      if (replaced) {
+        flush_x();
+        pending = false;
+        init(x, pp, 1);
+      }
       if (flexible) std::swap(z, zold);
       STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
       pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
@@ -696,6 +758,8 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
         if (it >= 32) check_every = 4;
       }
     }
+    flush_x();
+    STT_TRY(check_launch("pcg flush"));
   }
   STT_TRY(pull());
   int worst = 0, status = STT_OK;
