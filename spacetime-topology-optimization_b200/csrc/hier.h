@@ -55,8 +55,9 @@ struct stt_hier_impl {
   int l1;            // level 1 is applied from the level-0 densities (l1_sweep_kernel)
   double l1m[9][21]; // per child m of a level-1 element: T G_m T^T / 16, packed upper triangle
   double* tables;    // device: per transition S[9][64], G[9][64], GM[9][64]
-  double* keffA;     // build temporaries
-  double* keffB;
+  double* gtables;   // device: level-0 grandchildren of a level-2 element, H[81][64], HM[81][64]
+  double* keffA;     // build temporaries: element matrices of levels 3, 5, ...
+  double* keffB;     // ... and of levels 2, 4, ...
   const int* row_map;  // batch row -> hierarchy row (device), or null
   int has_reaction;    // level 0 carries a lumped reaction (drain) term
   int* status;         // device status word of the build (bit 0: pivot <= 0, bit 1: band)

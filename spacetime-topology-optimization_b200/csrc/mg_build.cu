@@ -72,7 +72,28 @@ static void galerkin_table(const double* S, const double* K, int nm, int nk, dou
   }
 }
 
-constexpr int kTableStride = 9 * 64;  // doubles per table (max 9 children x 8 x 8)
+constexpr int kTableStride = 9 * 64;   // doubles per table (max 9 children x 8 x 8)
+constexpr int kGrandStride = 81 * 64;  // doubles per grandchild table (max 81 x 8 x 8)
+
+// H[g] = S1_{m1}^T G[m0] S1_{m1} for the level-0 grandchild g = (m1, m0) of a level-2
+// element, with G the level-0 -> 1 child tables (S0^T K S0) and S1 the level-1 -> 2
+// interpolations; g is numbered as a child of a (kx0 kx1) x (ky0 ky1) coarsening, row
+// my1 ky0 + my0 and column mx1 kx0 + mx0, so keff_from_density_kernel applies it.
+static void grand_table(const double* S1, const double* G, int kx0, int ky0, int kx1, int ky1, int nk,
+                        double* H) {
+  const int KX = kx0 * kx1;
+  std::vector<double> t(nk * nk);
+  for (int my1 = 0; my1 < ky1; ++my1)
+    for (int mx1 = 0; mx1 < kx1; ++mx1) {
+      const double* Sm = S1 + (size_t)(my1 * kx1 + mx1) * nk * nk;
+      for (int my0 = 0; my0 < ky0; ++my0)
+        for (int mx0 = 0; mx0 < kx0; ++mx0) {
+          const double* Gm = G + (size_t)(my0 * kx0 + mx0) * nk * nk;
+          const int g = (my1 * ky0 + my0) * KX + (mx1 * kx0 + mx0);
+          galerkin_table(Sm, Gm, 1, nk, H + (size_t)g * nk * nk);
+        }
+    }
+}
 
 // M_m = T G_m T^T / 16 for the nm plane-stress child matrices G (8 x 8 each), packed as
 // the upper triangle of the symmetric 6 x 6 (row-major, i <= j); mode order Gx(ux),
@@ -178,10 +199,12 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     co.blocks = (double*)carve(p, used, 8LL * h.hrows * co.nb * 4 * co.B * co.B);
   }
   h.tables = (double*)carve(p, used, 8LL * kMaxLevels * 3 * kTableStride);
-  if (L > 1) {
-    h.keffA = (double*)carve(p, used, 8LL * h.hrows * h.lv[1].nel * NK * NK);
-    if (L > 2) h.keffB = (double*)carve(p, used, 8LL * h.hrows * h.lv[2].nel * NK * NK);
-  }
+  h.gtables = (double*)carve(p, used, 8LL * 2 * kGrandStride);
+  // level 1 is assembled straight from the level-0 densities and level 2's element
+  // matrices from its level-0 grandchildren, so the element-matrix buffers start at
+  // level 2 (keffB: even levels, keffA: odd levels >= 3)
+  if (L > 2) h.keffB = (double*)carve(p, used, 8LL * h.hrows * h.lv[2].nel * NK * NK);
+  if (L > 3) h.keffA = (double*)carve(p, used, 8LL * h.hrows * h.lv[3].nel * NK * NK);
   carve(p, used, 256);  // status word
   h.ws_bytes = used;
   return used;
@@ -304,6 +327,31 @@ struct KeffSource {  // explicit element matrices
     return __ldg(keff + (((size_t)h * nel + e) * (4 * D) + p) * (4 * D) + q);
   }
 };
+template <int D>
+struct ChildSource {  // level 1: sum over the level-0 children m of rho_m G_m (+ reaction_m GM_m)
+  const double* rho;
+  long long rho_rs;
+  const double* reac;
+  long long r_rs;
+  const double* G;   // [kx ky][4D][4D]
+  const double* GM;
+  int fnelx, kx, ky, cnelx;
+  STT_DEV double operator()(int h, int e, int p, int q) const {
+    constexpr int NK = 4 * D;
+    const int R = e / cnelx, C = e - R * cnelx;
+    const double* rr = rho + (size_t)h * rho_rs;
+    double v = 0.0;
+    for (int my = 0; my < ky; ++my)
+      for (int mx = 0; mx < kx; ++mx) {
+        const int m = my * kx + mx;
+        const size_t fe = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
+        v = fma(__ldg(rr + fe), __ldg(G + ((size_t)m * NK + p) * NK + q), v);
+        if (reac) v = fma(__ldg(reac + (size_t)h * r_rs + fe), __ldg(GM + ((size_t)m * NK + p) * NK + q), v);
+      }
+    return v;
+  }
+};
+
 template <int D>
 struct DensitySource {  // rho_e KE (+ reaction_e I / 4), level 0 used as the coarsest
   const double* rho;
@@ -606,27 +654,48 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   if (D == 2 && h->modal && !reaction && h->nlevels > 2 && h->lv[0].kx >= 2 && h->lv[0].ky >= 2)
     h->l1 = l1_tables(&tab[kTableStride], h->lv[0].kx * h->lv[0].ky, h->l1m) ? 1 : 0;
 
+  // level 2's element matrices from the level-0 grandchildren
+  if (h->nlevels > 2) {
+    const LevelDesc& f0 = h->lv[0];
+    const LevelDesc& f1 = h->lv[1];
+    std::vector<double> gt((size_t)2 * kGrandStride, 0.0);
+    const double* S1 = &tab[(size_t)1 * 3 * kTableStride];
+    grand_table(S1, &tab[kTableStride], f0.kx, f0.ky, f1.kx, f1.ky, NK, gt.data());
+    grand_table(S1, &tab[2 * kTableStride], f0.kx, f0.ky, f1.kx, f1.ky, NK, gt.data() + kGrandStride);
+    STT_TRY(check_cuda(cudaMemcpyAsync(h->gtables, gt.data(), gt.size() * 8, cudaMemcpyHostToDevice, st),
+                       "grandchild tables"));
+  }
   const double* kprev = nullptr;
   for (int l = 1; l < h->nlevels; ++l) {
     const LevelDesc& f = h->lv[l - 1];
     LevelDesc& c = h->lv[l];
     const double* S = h->tables + (size_t)(l - 1) * 3 * kTableStride;
-    double* kc = (l % 2 == 1) ? h->keffA : h->keffB;
-    const dim3 g(grid1(c.nel * NK), H);
-    if (l == 1)
-      keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride,
-                                                     S + 2 * kTableStride, f.nelx, f.kx, f.ky, c.nelx,
-                                                     (int)c.nel, kc);
-    else
-      keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
-                                                 (int)c.nel, kc);
     coarse_fixed_kernel<<<grid1(c.nnode), 256, 0, st>>>(f.fixed, f.nnx, f.kx, f.ky, c.fixed, c.nnx, c.nny);
-    stencil_kernel<D, KeffSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
-        KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64);
+    if (l == 1) {
+      // level 1: keff[E] = sum_m rho_m G_m (+ reaction) evaluated inside the assembly
+      stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
+          ChildSource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
+                         f.kx, f.ky, c.nelx},
+          c.fixed, c.nelx, c.nely, c.st64);
+    } else {
+      double* kc = (l % 2 == 0) ? h->keffB : h->keffA;
+      const dim3 g(grid1(c.nel * NK), H);
+      if (l == 2) {
+        const LevelDesc& f0 = h->lv[0];
+        keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables,
+                                                       h->gtables + kGrandStride, f0.nelx, f0.kx * f.kx,
+                                                       f0.ky * f.ky, c.nelx, (int)c.nel, kc);
+      } else {
+        keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
+                                                   (int)c.nel, kc);
+      }
+      stencil_kernel<D, KeffSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
+          KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64);
+      kprev = kc;
+    }
     if (h->precision == STT_FP32)
       convert_kernel<double, float><<<grid1(H * NS * c.nnode), 256, 0, st>>>(c.st64, c.st32, H * NS * c.nnode);
     STT_TRY(check_launch("galerkin level"));
-    kprev = kc;
   }
   LevelDesc& cl = h->lv[h->nlevels - 1];
   if (h->nlevels == 1) {
