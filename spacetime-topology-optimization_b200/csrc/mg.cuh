@@ -421,6 +421,24 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
   }
 }
 
+// Rows a block marches on the coarse levels: 32 where the grid then fills the GPU,
+// shorter bands on small grids (the heat solve's single row, the coarse levels), whose
+// launches are otherwise latency-bound by the sequential march down 32 rows.  The
+// kernels derive their band from gridDim.y, so any grid.y covers the rows.
+inline int band_rows(int xblocks, int nny, int rows) {
+  constexpr int kTarget = 4 * 148;  // blocks: four waves of one block per B200 SM
+  for (int band = 32; band > 4; band /= 2)
+    if ((long long)xblocks * ((nny + band - 1) / band) * rows >= kTarget) return band;
+  return 4;
+}
+
+inline dim3 coarse_grid(int nelx, int nely, int rows) {
+  const int strips = (nelx + 1 + kQCols - 1) / kQCols;
+  const int xb = (strips + kQWarps - 1) / kQWarps;
+  const int band = band_rows(xb, nely + 1, rows);
+  return dim3(xb, (nely + 1 + band - 1) / band, rows);
+}
+
 // ---- stencil levels: column-marching sweeps -----------------------------------------
 //
 // The symmetric half stencil stores, per node, the centre, E, S, SE, SW blocks; the W,
@@ -451,8 +469,9 @@ __global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
   const int c = strip * kQCols - 1 + lane;
   const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
   const bool col_ok = c >= 0 && c < nnx;
-  const int r0 = blockIdx.y * kQRows;
-  const int r1 = min(r0 + kQRows, nny);
+  const int band = (nny + gridDim.y - 1) / gridDim.y;  // rows per block (any grid.y)
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
   auto X = [&](int r, T(&v)[D]) {
 #pragma unroll
     for (int d = 0; d < D; ++d) v[d] = T(0);
@@ -618,8 +637,9 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
   const int c = strip * kQCols - 1 + lane;
   const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
   const bool col_ok = c >= 0 && c < nnx;
-  const int r0 = blockIdx.y * kQRows;
-  const int r1 = min(r0 + kQRows, nny);
+  const int band = (nny + gridDim.y - 1) / gridDim.y;  // rows per block (any grid.y)
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
   struct Row {
     T co[NC];   // Cc, E, S, SE, SW of node (r, c)
     T xn[D];    // x(r + 1, c)
@@ -805,8 +825,9 @@ __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
   const bool col_ok = c >= 0 && c < nnx;
   const int nelx = nnx - 1, nely = nny - 1;
   const bool ecol_ok = c >= 0 && c < nelx;
-  const int r0 = blockIdx.y * kQRows;
-  const int r1 = min(r0 + kQRows, nny);
+  const int band = (nny + gridDim.y - 1) / gridDim.y;  // rows per block (any grid.y)
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
   struct Ex {
     T b[D], dg[D];
     uint8_t fl;
@@ -955,8 +976,9 @@ __global__ void __launch_bounds__(kQThreads) restrict_kernel(
   const int C = strip * kQCols - 1 + lane;
   const bool out_lane = lane >= 1 && lane <= kQCols && C < cnnx;
   const bool col_ok = C >= 0 && C < cnnx;
-  const int R0 = blockIdx.y * kQRows;
-  const int R1 = min(R0 + kQRows, cnny);
+  const int band = (cnny + gridDim.y - 1) / gridDim.y;  // coarse rows per block (any grid.y)
+  const int R0 = blockIdx.y * band;
+  const int R1 = min(R0 + band, cnny);
   // x pass of fine row fr at this lane's coarse column
   auto xpass = [&](int fr, T(&g)[D]) {
     T own[3][D], left[3][D];
@@ -1070,6 +1092,81 @@ __global__ void __launch_bounds__(kProlongThreads) prolong_kernel(
   for (int d = 0; d < D; ++d)
     if (!((fl >> d) & 1)) v[d] += pv[d];
   store_node<D, T>(x, node, v);
+}
+
+// Column-marching prolongation: a warp owns 32 fine columns and marches down a band of
+// fine rows; every lane is an output column (no halo: a fine node needs only coarse
+// values).  The coarse rows R and R + 1 around the current fine row are held in
+// registers for the lane's coarse columns C and C + 1 and shifted when R advances, so a
+// coarse value is loaded once per coarse row (with the next coarse row in flight) instead
+// of up to four times per fine node.  Arithmetic as prolong_at.
+inline dim3 prolong2_grid(int fnnx, int fnny, int rows) {
+  const int xb = ((fnnx + 31) / 32 + kQWarps - 1) / kQWarps;
+  return dim3(xb, (fnny + band_rows(xb, fnny, rows) - 1) / band_rows(xb, fnny, rows), rows);
+}
+
+template <int D, typename T>
+__global__ void __launch_bounds__(kQThreads) prolong2_kernel(
+    const T* __restrict__ ec, long long c_rs, int cnnx, int cnny, T* __restrict__ xf, long long f_rs, int fnnx,
+    int fnny, int kx, int ky, const uint8_t* __restrict__ ffixed, const RowState* __restrict__ rst) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const T* e = ec + (size_t)s * c_rs;
+  T* x = xf + (size_t)s * f_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = (blockIdx.x * kQWarps + warp) * 32 + lane;
+  const bool col_ok = c < fnnx;
+  const int C = col_ok ? div_k(c, kx) : 0, jx = c - C * kx;
+  const T wx = T((double)jx / kx);
+  const bool c1 = col_ok && jx != 0;  // needs coarse column C + 1
+  const int band = (fnny + gridDim.y - 1) / gridDim.y;  // fine rows per block (any grid.y)
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, fnny);
+  // coarse row RR at columns C (v0) and C + 1 (v1); zero outside
+  auto crow = [&](int RR, T(&v0)[D], T(&v1)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v0[d] = v1[d] = T(0);
+    if (!col_ok || RR < 0 || RR >= cnny) return;
+    const long long n0 = (long long)RR * cnnx + C;
+    load_node<D, T>(e, n0, v0);
+    if (c1) load_node<D, T>(e, n0 + 1, v1);
+  };
+  int R = div_k(r0, ky);
+  T a0[D], a1[D], b0[D], b1[D], n0[D], n1[D];  // rows R, R + 1, and R + 2 in flight
+  crow(R, a0, a1);
+  crow(R + 1, b0, b1);
+  crow(R + 2, n0, n1);
+  for (int r = r0; r < r1; ++r) {
+    const int Rr = div_k(r, ky), jy = r - Rr * ky;
+    if (Rr != R) {  // advance one coarse row (the band steps rows one at a time)
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        a0[d] = b0[d];
+        a1[d] = b1[d];
+        b0[d] = n0[d];
+        b1[d] = n1[d];
+      }
+      R = Rr;
+      crow(R + 2, n0, n1);
+    }
+    if (!col_ok) continue;
+    const long long node = (long long)r * fnnx + c;
+    T v[D];
+    load_node<D, T>(x, node, v);
+    const uint8_t fl = __ldg(ffixed + node);
+    const T wy = T((double)jy / ky);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      T t0 = a0[d], t1 = b0[d];
+      if (jx) {
+        t0 = a0[d] * (T(1) - wx) + a1[d] * wx;
+        t1 = b0[d] * (T(1) - wx) + b1[d] * wx;
+      }
+      const T pv = jy ? t0 * (T(1) - wy) + t1 * wy : t0;
+      if (!((fl >> d) & 1)) v[d] += pv;
+    }
+    store_node<D, T>(x, node, v);
+  }
 }
 
 // ---- coarsest level: block-banded Cholesky solve (one CTA per batch row) ----------

@@ -141,7 +141,7 @@ struct Cycle {
       if (l != 1 || !h->l1) return false;
       const LevelDesc& f = h->lv[0];
       const LevelDesc& lv = h->lv[1];
-      const dim3 g = tile_grid(lv.nelx, lv.nely, nrows);
+      const dim3 g = coarse_grid(lv.nelx, lv.nely, nrows);
       const T* r0 = rho0();
 #define STT_L1(KX, KY)                                                                               \
   do {                                                                                               \
@@ -190,7 +190,7 @@ struct Cycle {
             x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
             pro);
       else
-        st_sweep2_kernel<D, T, MODE><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
+        st_sweep2_kernel<D, T, MODE><<<coarse_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
             x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega);
     }
   }
@@ -283,11 +283,11 @@ struct Cycle {
     const LevelDesc& cl = h->lv[l + 1];
     const long long cnd = vstride(cl.ndof);
     T* bc = (T*)w.b[l + 1];
-    restrict_kernel<D, T><<<tile_grid(cl.nelx, cl.nely, nrows), kQThreads, 0, st>>>(
+    restrict_kernel<D, T><<<coarse_grid(cl.nelx, cl.nely, nrows), kQThreads, 0, st>>>(
         xb, nd, lv.nnx, lv.nny, bc, cnd, cl.nnx, cl.nny, lv.kx, lv.ky, cl.fixed, rst);
     T* ec = coarse_correction(l, bc);
-    prolong_kernel<D, T><<<prolong_grid(lv.nnx, lv.nny, nrows), kProlongThreads, 0, st>>>(
-          ec, cnd, cl.nnx, cl.nny, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
+    prolong2_kernel<D, T><<<prolong2_grid(lv.nnx, lv.nny, nrows), kQThreads, 0, st>>>(
+        ec, cnd, cl.nnx, cl.nny, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
     // post-smoothing; level 0's last sweep writes straight into final_out when given
     for (int k = 0; k < n_smooth; ++k) {
       T* dst = (l == 0 && final_out && k == n_smooth - 1) ? final_out : xb;

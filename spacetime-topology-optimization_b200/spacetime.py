@@ -53,6 +53,16 @@ class SpaceTimeProblem:
         self.lift = plate.to(torch.float64)
         self.ke = _lib.dbl_array(_geom.host_KE(self.KE))
         self.keh = _lib.dbl_array(_geom.host_KE(self.KEh))
+        self._streams: dict = {}
+
+    def stream(self, name: str) -> torch.cuda.Stream:
+        """A CUDA stream kept for this problem's lifetime.  Side work reuses one stream
+        per role across evaluations: torch's caching allocator pools memory per stream,
+        so a fresh stream per evaluation would cudaMalloc (and stall) every time."""
+        s = self._streams.get(name)
+        if s is None:
+            s = self._streams[name] = torch.cuda.Stream(device=_device_index(self.device))
+        return s
 
 
 def _pcg(levels, b, x0, rtol, max_iter, info_key, info):
@@ -69,15 +79,17 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
                            conduction_penal: float = 3.0, Emin: float = EMIN, Emax: float = EMAX,
                            penal: float = PENAL, max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS,
                            gradient: bool = True, batched: bool = True,
-                           problem: SpaceTimeProblem | None = None, info: dict | None = None) -> dict:
-    """Objective, stage compliances, ``tPhys`` and (optionally) ``d objective / d xPhys``."""
+                           problem: SpaceTimeProblem | None = None, info: dict | None = None,
+                           overlap: bool = True) -> dict:
+    """Objective, stage compliances, ``tPhys`` and (optionally) ``d objective / d xPhys``.
+    ``overlap`` runs the heat adjoint on a side stream concurrently with the stage work."""
     _lib.require_cuda(xPhys, w)
     nely, nelx = xPhys.shape
     P = problem if problem is not None and (problem.nelx, problem.nely) == (nelx, nely) else \
         SpaceTimeProblem(nelx, nely, xPhys.device)
     opts = dict(precision=precision, rtol=rtol, max_iter=max_iter, drain_beta=drain_beta,
                 conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
-                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched)
+                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched, overlap=overlap)
     return _solve_group(P, [xPhys], [w], [n_stage], info=info, **opts)[0]
 
 
@@ -103,7 +115,7 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
     _lib.require_cuda(*xs, *ws)
     opts = dict(precision=precision, rtol=rtol, max_iter=max_iter, drain_beta=drain_beta,
                 conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
-                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=True)
+                max_coarse_elements=max_coarse_elements, gradient=gradient, batched=True, overlap=True)
     groups: dict = {}
     for k, x in enumerate(xs):
         groups.setdefault(tuple(x.shape), []).append(k)
@@ -134,7 +146,7 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
     main = torch.cuda.current_stream(dev_i)
     ready = torch.cuda.Event()
     ready.record(main)
-    streams = {shape: torch.cuda.Stream(device=dev_i) for shape in groups}
+    streams = {shape: cache[(shape[1], shape[0])].stream("group") for shape in groups}
 
     def on_stream(shape, idx):
         torch.cuda.set_device(dev_i)
@@ -171,12 +183,16 @@ class _HeatAdjoint:
     density term of the solve and the lift term.  ``result()`` joins the thread and
     orders the caller's stream after the side stream."""
 
-    def __init__(self, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info):
+    def __init__(self, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info, threaded=True):
         import concurrent.futures
 
         self.dev = _device_index(P.device)
         self.main = torch.cuda.current_stream(self.dev)
-        self.side = torch.cuda.Stream(device=self.dev)
+        if not threaded:  # in order on the caller's stream
+            self.side, self.pool = self.main, None
+            self.g_chi = self._run(P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info)
+            return
+        self.side = P.stream("heat_adjoint")
         self.side.wait_stream(self.main)
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=1)
         self.fut = self.pool.submit(self._run, P, hl, T, T_free, heat_rhs, Ws, rtol, max_iter, info)
@@ -195,6 +211,8 @@ class _HeatAdjoint:
             return torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h.reshape(G, nnode))["gdens"]
 
     def result(self):
+        if self.pool is None:
+            return self.g_chi
         try:
             g_chi = self.fut.result()
         finally:
@@ -205,6 +223,8 @@ class _HeatAdjoint:
 
     def abandon(self):
         """Wait for the side work and drop it (the caller is unwinding an error)."""
+        if self.pool is None:
+            return
         self.pool.shutdown(wait=True)
         self.main.wait_stream(self.side)
 
@@ -212,7 +232,7 @@ class _HeatAdjoint:
 def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
                  precision: str, rtol: float, max_iter: int, drain_beta: float, conduction_penal: float,
                  Emin: float, Emax: float, penal: float, max_coarse_elements: int, gradient: bool,
-                 batched: bool, info: dict | None) -> list[dict]:
+                 batched: bool, info: dict | None, overlap: bool = True) -> list[dict]:
     """G problems on one grid: batched heat solve, all stage rows in one batched solve."""
     L = _lib.lib()
     st = _lib.stream()
@@ -249,7 +269,8 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
     # bandwidth-bound stage kernels instead of adding to the step.
     heat_adj = None
     if gradient:
-        heat_adj = _HeatAdjoint(P, hl, T, T_free, heat_rhs, (W / scale).contiguous(), rtol, max_iter, info)
+        heat_adj = _HeatAdjoint(P, hl, T, T_free, heat_rhs, (W / scale).contiguous(), rtol, max_iter, info,
+                                threaded=overlap)
 
     try:
         # 2.-3. stage rows of every problem, then the batched stage solves
