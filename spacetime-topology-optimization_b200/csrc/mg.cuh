@@ -1136,7 +1136,26 @@ __global__ void __launch_bounds__(kQThreads) prolong2_kernel(
   crow(R, a0, a1);
   crow(R + 1, b0, b1);
   crow(R + 2, n0, n1);
-  for (int r = r0; r < r1; ++r) {
+  // fine rows r + 1 .. r + AHEAD of x and flags in flight (raw loads)
+  constexpr int AHEAD = 4;
+  T qx[AHEAD][D];
+  uint8_t qf[AHEAD];
+  auto frow = [&](int rr, T(&v)[D], uint8_t& fl) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    fl = 0;
+    if (!col_ok || rr >= r1) return;
+    const long long node = (long long)rr * fnnx + c;
+    load_node<D, T>(x, node, v);
+    fl = __ldg(ffixed + node);
+  };
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) frow(r0 + k, qx[k], qf[k]);
+  for (int rb = r0; rb < r1; rb += AHEAD) {
+#pragma unroll
+   for (int k = 0; k < AHEAD; ++k) {
+    const int r = rb + k;
+    if (r >= r1) break;
     const int Rr = div_k(r, ky), jy = r - Rr * ky;
     if (Rr != R) {  // advance one coarse row (the band steps rows one at a time)
 #pragma unroll
@@ -1149,11 +1168,13 @@ __global__ void __launch_bounds__(kQThreads) prolong2_kernel(
       R = Rr;
       crow(R + 2, n0, n1);
     }
+    T v[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = qx[k][d];
+    const uint8_t fl = qf[k];
+    frow(r + AHEAD, qx[k], qf[k]);
     if (!col_ok) continue;
     const long long node = (long long)r * fnnx + c;
-    T v[D];
-    load_node<D, T>(x, node, v);
-    const uint8_t fl = __ldg(ffixed + node);
     const T wy = T((double)jy / ky);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -1166,6 +1187,7 @@ __global__ void __launch_bounds__(kQThreads) prolong2_kernel(
       if (!((fl >> d) & 1)) v[d] += pv;
     }
     store_node<D, T>(x, node, v);
+   }
   }
 }
 

@@ -74,6 +74,7 @@ static void galerkin_table(const double* S, const double* K, int nm, int nk, dou
 
 constexpr int kTableStride = 9 * 64;   // doubles per table (max 9 children x 8 x 8)
 constexpr int kGrandStride = 81 * 64;  // doubles per grandchild table (max 81 x 8 x 8)
+constexpr int kChildStencilSize = 2 * 5 * 4 * 4 * 9;  // stencil_children_kernel tables, D = 2, 9 children
 
 // H[g] = S1_{m1}^T G[m0] S1_{m1} for the level-0 grandchild g = (m1, m0) of a level-2
 // element, with G the level-0 -> 1 child tables (S0^T K S0) and S1 the level-1 -> 2
@@ -199,7 +200,7 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     co.blocks = (double*)carve(p, used, 8LL * h.hrows * co.nb * 4 * co.B * co.B);
   }
   h.tables = (double*)carve(p, used, 8LL * kMaxLevels * 3 * kTableStride);
-  h.gtables = (double*)carve(p, used, 8LL * 2 * kGrandStride);
+  h.gtables = (double*)carve(p, used, 8LL * (2 * kGrandStride + kChildStencilSize));
   // level 1 is assembled straight from the level-0 densities and level 2's element
   // matrices from its level-0 grandchildren, so the element-matrix buffers start at
   // level 2 (keffB: even levels, keffA: odd levels >= 3)
@@ -429,6 +430,96 @@ __global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int n
   }
 }
 
+// Level-1 stencil straight from the level-0 densities.  Block b (centre, E, S, SE, SW) of
+// node N, entry (i, j), is a fixed linear form in the densities of the level-0 children
+// of N's (up to four) level-1 elements: W[b][i, j][element position][child] =
+// Gs_m[corner of N * D + i][corner of M * D + j] when the element holds both N and the
+// block's neighbour M, else 0, with Gs_m = (G_m + G_m^T) / 2 the symmetrised
+// S_m^T KE S_m (the reference averages its coarse matrix with its transpose,
+// torch_mg.py:286).  The table sits in shared memory; a thread per node loads the
+// 4 x NM child densities once and forms its 5 D^2 coefficients, rows and columns of
+// fixed dofs zeroed.  RD adds the reaction's share with its own table.
+template <int D, bool RD, int NM>
+__global__ void __launch_bounds__(256) stencil_children_kernel(
+    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ reac, long long r_rs,
+    const double* __restrict__ Wg, int fnelx, int kx, int ky, const uint8_t* __restrict__ fixed, int nelx,
+    int nely, double* __restrict__ st) {
+  constexpr int DD = D * D, NS = 5 * DD, NW = NS * 4 * NM;
+  __shared__ double W[(RD ? 2 : 1) * NW];
+  for (int i = threadIdx.x; i < (RD ? 2 : 1) * NW; i += blockDim.x) W[i] = Wg[i];
+  __syncthreads();
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = blockIdx.y;
+  if (n >= nnx * nny) return;
+  const long long nnode = (long long)nnx * nny;
+  const int r = n / nnx, c = n - r * nnx;
+  const double* rr = rho + (size_t)h * rho_rs;
+  const double* ar = RD ? reac + (size_t)h * r_rs : nullptr;
+  double rv[4][NM], av[RD ? 4 : 1][NM];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int er = r - 1 + p / 2, ec = c - 1 + p % 2;
+    const bool ok = er >= 0 && er < nely && ec >= 0 && ec < nelx;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const int my = m / kx, mx = m - my * kx;
+      const size_t fe = ok ? (size_t)(er * ky + my) * fnelx + (ec * kx + mx) : 0;
+      rv[p][m] = ok ? __ldg(rr + fe) : 0.0;
+      if constexpr (RD) av[p][m] = ok ? __ldg(ar + fe) : 0.0;
+    }
+  }
+  const uint8_t fN = fixed[n];
+  double* out = st + (size_t)h * NS * nnode + n;
+#pragma unroll
+  for (int blk = 0; blk < 5; ++blk) {
+    const int dr = (blk == 0 || blk == 1) ? 0 : 1;
+    const int dc = blk == 0 ? 0 : (blk == 1 ? 1 : (blk == 2 ? 0 : (blk == 3 ? 1 : -1)));
+    const int mr = r + dr, mc = c + dc;
+    const bool m_ok = mr >= 0 && mr < nny && mc >= 0 && mc < nnx;
+    const uint8_t fM = m_ok ? fixed[mr * nnx + mc] : 0;
+#pragma unroll
+    for (int q = 0; q < DD; ++q) {
+      const int i = q / D, j = q % D;
+      const double* w = W + (size_t)(blk * DD + q) * 4 * NM;
+      double v = 0.0;
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+          v = fma(rv[p][m], w[p * NM + m], v);
+          if constexpr (RD) v = fma(av[p][m], w[NW + p * NM + m], v);
+        }
+      if (!m_ok || ((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
+      out[(size_t)(blk * DD + q) * nnode] = v;
+    }
+  }
+}
+
+// The table of stencil_children_kernel from the child tables G (and GM), [5 D^2][4][nm].
+static void children_stencil_table(const double* G, int nm, int d, std::vector<double>& W) {
+  const int nk = 4 * d, dd = d * d;
+  W.assign((size_t)5 * dd * 4 * nm, 0.0);
+  for (int blk = 0; blk < 5; ++blk) {
+    const int dr = (blk == 0 || blk == 1) ? 0 : 1;
+    const int dc = blk == 0 ? 0 : (blk == 1 ? 1 : (blk == 2 ? 0 : (blk == 3 ? 1 : -1)));
+    for (int p = 0; p < 4; ++p) {
+      const int a = p / 2, b = p % 2;   // element (r - 1 + a, c - 1 + b) around node (r, c)
+      const int ddr = dr + 1 - a, ddc = dc + 1 - b;  // M relative to the element's top-left node
+      if (ddr < 0 || ddr > 1 || ddc < 0 || ddc > 1) continue;
+      const int kN = corner_of(a, b);
+      const int kM = ddr == 1 ? (ddc == 0 ? 0 : 1) : (ddc == 1 ? 2 : 3);
+      for (int i = 0; i < d; ++i)
+        for (int j = 0; j < d; ++j)
+          for (int m = 0; m < nm; ++m) {
+            const double* Gm = G + (size_t)m * nk * nk;
+            const int P = kN * d + i, Q = kM * d + j;
+            W[(((size_t)blk * dd + i * d + j) * 4 + p) * nm + m] = 0.5 * (Gm[P * nk + Q] + Gm[Q * nk + P]);
+          }
+    }
+  }
+}
+
 // Banded coarse matrix from the coarsest stencil, written into the factor's storage:
 // diagonal blocks in slot 0, sub-diagonal blocks A_{k,k-1} in slot 2.  Fixed dofs get
 // a unit diagonal (torch_mg.py:287-289); padding rows are identity.
@@ -654,6 +745,16 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   if (D == 2 && h->modal && !reaction && h->nlevels > 2 && h->lv[0].kx >= 2 && h->lv[0].ky >= 2)
     h->l1 = l1_tables(&tab[kTableStride], h->lv[0].kx * h->lv[0].ky, h->l1m) ? 1 : 0;
 
+  // level 1's stencil tables (after the two grandchild tables)
+  if (h->nlevels > 1) {
+    const int nm = h->lv[0].kx * h->lv[0].ky;
+    std::vector<double> W, WM;
+    children_stencil_table(&tab[kTableStride], nm, D, W);
+    children_stencil_table(&tab[2 * kTableStride], nm, D, WM);
+    W.insert(W.end(), WM.begin(), WM.end());
+    STT_TRY(check_cuda(cudaMemcpyAsync(h->gtables + 2 * kGrandStride, W.data(), W.size() * 8,
+                                       cudaMemcpyHostToDevice, st), "children stencil tables"));
+  }
   // level 2's element matrices from the level-0 grandchildren
   if (h->nlevels > 2) {
     const LevelDesc& f0 = h->lv[0];
@@ -672,11 +773,29 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     const double* S = h->tables + (size_t)(l - 1) * 3 * kTableStride;
     coarse_fixed_kernel<<<grid1(c.nnode), 256, 0, st>>>(f.fixed, f.nnx, f.kx, f.ky, c.fixed, c.nnx, c.nny);
     if (l == 1) {
-      // level 1: keff[E] = sum_m rho_m G_m (+ reaction) evaluated inside the assembly
-      stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
-          ChildSource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
-                         f.kx, f.ky, c.nelx},
-          c.fixed, c.nelx, c.nely, c.st64);
+      // level 1: keff[E] = sum_m rho_m G_m (+ reaction), assembled from the densities
+      const int nm = f.kx * f.ky;
+      if (nm == 4 || nm == 6 || nm == 9) {
+#define STT_CHILD_ST(RD, NM)                                                                          \
+  stencil_children_kernel<D, RD, NM><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                        \
+      l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, \
+      c.nelx, c.nely, c.st64)
+        if (reaction) {
+          if (nm == 4) STT_CHILD_ST(true, 4);
+          else if (nm == 6) STT_CHILD_ST(true, 6);
+          else STT_CHILD_ST(true, 9);
+        } else {
+          if (nm == 4) STT_CHILD_ST(false, 4);
+          else if (nm == 6) STT_CHILD_ST(false, 6);
+          else STT_CHILD_ST(false, 9);
+        }
+#undef STT_CHILD_ST
+      } else {  // a single coarsening direction (factor 1 in the other)
+        stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
+            ChildSource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
+                           f.kx, f.ky, c.nelx},
+            c.fixed, c.nelx, c.nely, c.st64);
+      }
     } else {
       double* kc = (l % 2 == 0) ? h->keffB : h->keffA;
       const dim3 g(grid1(c.nel * NK), H);

@@ -532,12 +532,32 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
   const double* as = Ap + (size_t)s * rs;
   float* r32s = r32 ? r32 + (size_t)s * r32_rs : nullptr;
   double vals[1] = {0.0};
-  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kEwThreads) {
+  auto one = [&](long long i) {
     const double rv = rsv[i] - alpha * as[i];
     rsv[i] = rv;
     if (r32s) r32s[i] = (float)rv;  // the FP32 V-cycle's right-hand side
     vals[0] = fma(rv, rv, vals[0]);
+  };
+  if ((rs & 1) == 0) {
+    // pairs of dofs (128-bit loads): with an even row stride every row starts 16-byte
+    // aligned (the workspace is 256-byte aligned; the FP32 copy's stride is a multiple of 4)
+    const long long n2 = n / 2;
+    double2* r2 = reinterpret_cast<double2*>(rsv);
+    const double2* a2 = reinterpret_cast<const double2*>(as);
+    for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n2;
+         i += (long long)gridDim.x * kEwThreads) {
+      const double2 rr = r2[i], aa = __ldg(a2 + i);
+      const double2 rv = make_double2(rr.x - alpha * aa.x, rr.y - alpha * aa.y);
+      r2[i] = rv;
+      if (r32s) reinterpret_cast<float2*>(r32s)[i] = make_float2((float)rv.x, (float)rv.y);
+      vals[0] = fma(rv.x, rv.x, vals[0]);
+      vals[0] = fma(rv.y, rv.y, vals[0]);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) one(n - 1);  // odd-length rows
+  } else {
+    for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kEwThreads)
+      one(i);
   }
   grid_reduce<1, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
     RowState& S = rst[s];
