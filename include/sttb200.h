@@ -17,6 +17,8 @@
  *   stt_q4_diag         sttopt/torch_fem.py:86-98 (matvec_diagonal), :162-181 (jacobi diag)
  *   stt_lumped_reaction sttopt/torch_fem.py:117-132
  *   stt_ke_modal        sttopt/fem.py:17-30, :98-111 (the element matrices it recognises)
+ *   stt_cone_filter*    sttopt/filters.py:38-85 (density_filter, apply_density_filter),
+ *                       :109-133 (heaviside_projection and its derivative)
  *   stt_hier_*          sttopt/torch_mg.py:293-400 (build_hierarchy), :257-266 (select)
  *   stt_level_apply     sttopt/torch_mg.py:239-255 (_Level.__call__), :179-193 (keff_matvec)
  *   stt_vcycle          sttopt/torch_mg.py:403-476 (VCycle.__call__)
@@ -80,6 +82,21 @@ int stt_lumped_reaction(int d, int nelx, int nely, int nrows, const double* reac
  * apply through the element's edge modes; returns 0 for any other KE (those take the
  * generic 8 x 8 product).  m = {m00, m01, m11, m22, m44, m55, kd0, kd1}. */
 int stt_ke_modal(int d, const double* KE, double* m);
+
+/* ---- density filter ------------------------------------------------------------ */
+
+/* xt[s] = H x[s] / Hs with H[e1, e2] = max(0, rmin - dist(e1, e2)) over the offsets
+ * |d| <= ceil(rmin) - 1 (zero outside the grid) and Hs its row sums; when beta > 0 also
+ * xp[s] = P(xt[s]), the Heaviside projection at threshold eta (beta = +inf: the step,
+ * 1/2 at the threshold).  Element fields (nely x nelx, row-major), FP64, rmin in (0, 8]. */
+int stt_cone_filter(int nelx, int nely, int nrows, double rmin, const double* x, long long x_rs,
+                    double* xt, double* xp, long long o_rs, double beta, double eta,
+                    stt_stream_t stream);
+
+/* The adjoint: out[s] = H (g[s] * P'(xt[s]) / Hs) (beta > 0, xt given) or H (g[s] / Hs). */
+int stt_cone_filter_adjoint(int nelx, int nely, int nrows, double rmin, const double* g,
+                            long long g_rs, const double* xt, long long xt_rs, double beta,
+                            double eta, double* out, long long o_rs, stt_stream_t stream);
 
 /* ---- multigrid hierarchy ------------------------------------------------------- */
 

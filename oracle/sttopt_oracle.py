@@ -765,3 +765,53 @@ def smoothed_density(nelx, nely, seed, rmin=4.0, lo=1e-3, hi=1.0):
     sm = cone_filter(noise, rmin)
     sm = (sm - sm.min()) / (sm.max() - sm.min())
     return lo + (hi - lo) * sm
+
+
+# ---- density filter and projection (sttopt/filters.py) ----------------------------------
+
+def density_filter(nelx, nely, rmin):
+    """``H[e1, e2] = max(0, rmin - dist)`` over offsets ``|d| <= ceil(rmin) - 1`` and its row
+    sums ``Hs`` (filters.py:38-64), as a SciPy CSR matrix."""
+    import math
+
+    import scipy.sparse as sp
+
+    r = int(math.ceil(rmin)) - 1
+    e = np.arange(nelx * nely)
+    i, j = e % nelx, e // nelx
+    rows, cols, vals = [], [], []
+    for di in range(-r, r + 1):
+        for dj in range(-r, r + 1):
+            w = max(0.0, rmin - math.hypot(di, dj))
+            if w == 0.0:
+                continue
+            ok = (i + di >= 0) & (i + di < nelx) & (j + dj >= 0) & (j + dj < nely)
+            rows.append(e[ok])
+            cols.append(((j + dj) * nelx + (i + di))[ok])
+            vals.append(np.full(ok.sum(), w))
+    H = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(nelx * nely, nelx * nely)).tocsr()
+    return H, np.asarray(H.sum(axis=1)).ravel()
+
+
+def apply_density_filter(field, H, Hs):
+    """``H @ field / Hs``, shape-preserving (filters.py:67-78)."""
+    return (H @ np.asarray(field).ravel() / Hs).reshape(np.shape(field))
+
+
+def heaviside_projection(xt, beta, eta):
+    """Smoothed threshold (filters.py:109-127); ``beta = inf`` is the step, 1/2 at eta."""
+    import math
+
+    if math.isinf(beta):
+        return np.where(xt > eta, 1.0, np.where(xt < eta, 0.0, 0.5))
+    den = math.tanh(beta * eta) + math.tanh(beta * (1 - eta))
+    return (math.tanh(beta * eta) + np.tanh(beta * (xt - eta))) / den
+
+
+def heaviside_projection_derivative(xt, beta, eta):
+    """(filters.py:128-133)"""
+    import math
+
+    den = math.tanh(beta * eta) + math.tanh(beta * (1 - eta))
+    return beta * (1 - np.tanh(beta * (xt - eta)) ** 2) / den

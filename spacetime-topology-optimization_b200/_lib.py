@@ -40,6 +40,10 @@ _SIGS = {
     "stt_q4_diag": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _p, _c_ll, _pd, _p]),
     "stt_lumped_reaction": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
     "stt_ke_modal": (_c_int, [_c_int, _pd, _pd]),
+    "stt_cone_filter": (_c_int, [_c_int, _c_int, _c_int, _c_double, _p, _c_ll, _p, _p, _c_ll, _c_double,
+                                 _c_double, _p]),
+    "stt_cone_filter_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_double, _p, _c_ll, _p, _c_ll, _c_double,
+                                         _c_double, _p, _c_ll, _p]),
     "stt_hier_workspace_bytes": (_c_ll, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int]),
     "stt_hier_create": (_c_int, [ctypes.POINTER(_p), _p, _c_ll, _c_int, _c_int, _c_int, _c_int, _p, _c_ll,
                                  _p, _c_ll, _p, _pd, _c_int, _c_int, _p]),

@@ -26,6 +26,7 @@ sys.path.insert(0, str(HERE.parents[1]))
 import torch  # noqa: E402
 
 import sttopt.compliance as compliance  # noqa: E402
+import sttopt.filters as filters  # noqa: E402
 import sttopt.fem as fem  # noqa: E402
 import sttopt.gravity as gravity  # noqa: E402
 import sttopt.load_cases as load_cases  # noqa: E402
@@ -370,6 +371,34 @@ def gen_spacetime_512():
          fwd_iter=res["fwd_iter"], bwd_iter=res["bwd_iter"])
 
 
+def gen_filters():
+    """The cone density filter and the Heaviside projection, as the reference computes
+    them (filters.density_filter / apply_density_filter / heaviside_projection*), and the
+    gradient of sum(w * P(H x / Hs)) through the reference's autograd (symmetric_matmul)."""
+    out = {}
+    for nelx, nely, rmin, seed in [(37, 23, 1.5, 11), (37, 23, 2.5, 12), (64, 40, 4.0, 13), (20, 11, 8.0, 14)]:
+        k = f"{nelx}x{nely}r{rmin}"
+        H, Hs = filters.density_filter(nelx, nely, rmin)
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(0, 1, (nely, nelx))
+        w = rng.uniform(-1, 1, (nely, nelx))
+        Ht = torch_util.symmetric_csr_to_tensor(H, "cpu", F64)
+        xt_t = t(x).requires_grad_(True)
+        xTilde = filters.apply_density_filter(xt_t, Ht, t(Hs))
+        out[f"{k}_x"], out[f"{k}_w"], out[f"{k}_Hs"] = x, w, Hs
+        out[f"{k}_xTilde"] = xTilde.detach().numpy()
+        for beta in (1.0, 8.0, float("inf")):
+            xp = filters.heaviside_projection(xTilde, beta, 0.5)
+            out[f"{k}_b{beta}_xPhys"] = xp.detach().numpy()
+            if not np.isinf(beta):
+                out[f"{k}_b{beta}_dP"] = filters.heaviside_projection_derivative(xTilde, beta, 0.5).detach().numpy()
+                (g,) = torch.autograd.grad(torch.sum(t(w) * xp), [xt_t], retain_graph=True)
+                out[f"{k}_b{beta}_grad"] = g.numpy()
+        (g,) = torch.autograd.grad(torch.sum(t(w) * xTilde), [xt_t])
+        out[f"{k}_grad_filter"] = g.numpy()
+    save("filters", **out)
+
+
 def gen_pcg_cases():
     """Retirement, zero rows, warm starts and non-convergence, as the reference does them."""
     nelx, nely = 18, 12
@@ -406,5 +435,6 @@ if __name__ == "__main__":
     gen_cantilever()
     gen_heat()
     gen_spacetime()
+    gen_filters()
     if "--with-512" in sys.argv:
         gen_spacetime_512()

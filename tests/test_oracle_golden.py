@@ -227,3 +227,24 @@ def test_stage_membership_is_bit_exact_on_identical_tphys():
     g = golden("spacetime")
     for k, n_stage in [("48x24s4", 4), ("64x32s16", 16)]:
         np.testing.assert_array_equal(O.stage_membership(g[f"{k}_tPhys"], n_stage), g[f"{k}_member"])
+
+
+@pytest.mark.parametrize("key", ["37x23r1.5", "37x23r2.5", "64x40r4.0", "20x11r8.0"])
+def test_density_filter_and_projection_against_the_reference(key, pkg):
+    """The oracle's cone filter / projection and the package's host-side filter (row
+    sums, explicit matrix) against the reference's outputs."""
+    from sttopt_b200 import filters
+
+    g = golden("filters")
+    nelx, nely = (int(v) for v in key.split("r")[0].split("x"))
+    rmin = float(key.split("r")[1])
+    H, Hs = O.density_filter(nelx, nely, rmin)
+    np.testing.assert_allclose(Hs, g[f"{key}_Hs"], rtol=1e-15)
+    xt = O.apply_density_filter(g[f"{key}_x"], H, Hs)
+    np.testing.assert_allclose(xt, g[f"{key}_xTilde"], rtol=1e-14, atol=1e-15)
+    for beta in (1.0, 8.0, float("inf")):
+        np.testing.assert_allclose(O.heaviside_projection(xt, beta, 0.5), g[f"{key}_b{beta}_xPhys"],
+                                   rtol=1e-13, atol=1e-14)
+    Hb, Hsb = filters.density_filter(nelx, nely, rmin)
+    np.testing.assert_allclose(Hsb, g[f"{key}_Hs"], rtol=1e-14)  # summation order differs
+    assert (Hb.tocsr() != H).nnz == 0
