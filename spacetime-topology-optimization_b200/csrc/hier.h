@@ -43,6 +43,7 @@ struct CoarseDesc {
   int nb;            // blocks, n padded to nb * B
   int by_col;        // dof ordering: 1 = column-major nodes (nny < nnx), 0 = row-major
   double* blocks;    // [hrows][nb][4][B][B]: Dinv, Dinv^T, E, E^T (E_k = L_{k,k-1})
+  double* inv;       // [hrows][nb B][nb B] explicit inverse (FP32 cycles, B <= 64), or null
 };
 
 struct stt_hier_impl {

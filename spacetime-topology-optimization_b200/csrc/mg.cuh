@@ -1314,6 +1314,63 @@ __global__ void __launch_bounds__(4 * 4 * NC) coarse_solve_kernel(
   }
 }
 
+// The coarsest level by its explicit inverse (FP32 cycles): x = A^{-1} b as one GEMV in
+// the band ordering.  Grid (np / 32, rows): each CTA stages b (permuted, FP64) in shared
+// memory and its 8 warps produce 4 output rows each, lanes striding a row of the
+// inverse (coalesced) and a warp reduction; fixed dofs come back zero.
+constexpr int kInvRowsPerCta = 32;
+
+template <int D, typename T>
+__global__ void __launch_bounds__(256) coarse_inv_solve_kernel(
+    const T* __restrict__ b, T* __restrict__ x, long long rs, const double* __restrict__ inv, int np, int by_col,
+    int nnx, int nny, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows,
+    const RowState* __restrict__ rst) {
+  extern __shared__ double yv[];  // [np]
+  const int s = blockIdx.y;
+  if (rst && !rst[s].active) return;
+  const int h = hier_row(row_map, hrows, s);
+  const long long nnode = (long long)nnx * nny, n = nnode * D;
+  auto node_of = [&](long long P, int& r, int& c, int& d) {
+    const long long nd = P / D;
+    d = (int)(P - nd * D);
+    if (by_col) {
+      c = (int)(nd / nny);
+      r = (int)(nd - (long long)c * nny);
+    } else {
+      r = (int)(nd / nnx);
+      c = (int)(nd - (long long)r * nnx);
+    }
+  };
+  const T* bs = b + (size_t)s * rs;
+  for (int P = threadIdx.x; P < np; P += blockDim.x) {
+    double v = 0.0;
+    if (P < n) {
+      int r, c, d;
+      node_of(P, r, c, d);
+      v = (double)bs[((size_t)r * nnx + c) * D + d];
+    }
+    yv[P] = v;
+  }
+  __syncthreads();
+  const double* ih = inv + (size_t)h * np * np;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T* xs = x + (size_t)s * rs;
+  for (int q = 0; q < kInvRowsPerCta / 8; ++q) {
+    const int P = blockIdx.x * kInvRowsPerCta + warp * (kInvRowsPerCta / 8) + q;
+    if (P >= n) break;
+    const double* row = ih + (size_t)P * np;
+    double acc = 0.0;
+    for (int Q = lane; Q < np; Q += 32) acc = fma(__ldg(row + Q), yv[Q], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      int r, c, d;
+      node_of(P, r, c, d);
+      const long long node = (long long)r * nnx + c;
+      xs[node * D + d] = ((fixed[node] >> d) & 1) ? T(0) : T(acc);
+    }
+  }
+}
+
 // ---- small vector kernels ---------------------------------------------------------
 
 template <typename TI, typename TO>

@@ -3,6 +3,7 @@
 // level (torch_mg._dense_cholesky, :269-290).
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "errors.h"
@@ -198,6 +199,9 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     if (co.B < 32) co.B = 32;
     co.nb = (co.n + co.B - 1) / co.B;
     co.blocks = (double*)carve(p, used, 8LL * h.hrows * co.nb * 4 * co.B * co.B);
+    // the FP32 cycle solves the coarsest level with the explicit inverse (one GEMV)
+    const long long np = (long long)co.nb * co.B;
+    co.inv = (f32 && co.B <= 64) ? (double*)carve(p, used, 8LL * h.hrows * np * np) : nullptr;
   }
   h.tables = (double*)carve(p, used, 8LL * kMaxLevels * 3 * kTableStride);
   h.gtables = (double*)carve(p, used, 8LL * (2 * kGrandStride + kChildStencilSize));
@@ -826,6 +830,114 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   return STT_OK;
 }
 
+// The explicit inverse of the coarsest matrix from its block-bidiagonal Cholesky factor
+// (for the FP32 cycle, whose coarse solve is then one GEMV instead of 2 nb dependent
+// block steps).  CTA (kc, h) solves A X = I for the B columns of block kc: forward
+// Y_k = Dinv_k (I_k - E_k Y_{k-1}) from block kc on (Y is zero above it), then backward
+// X_k = Dinv_k^T (Y_k - E_{k+1}^T X_{k+1}); Y is parked in the output rows it precedes.
+// Same arithmetic as coarse_solve_kernel, so the GEMV's result matches the block solve
+// to the conditioning of the coarse matrix.  B <= 64 (three B x B FP64 tiles in shared
+// memory).
+__global__ void __launch_bounds__(256) coarse_inverse_kernel(const double* __restrict__ blocks, int B, int nb,
+                                                             double* __restrict__ inv) {
+  extern __shared__ double sm[];
+  double* Y = sm;              // the current block of the solution, B x B (row-major)
+  double* R = Y + B * B;       // right-hand side of the step
+  double* M = R + B * B;       // the step's matrix
+  const int kc = blockIdx.x, h = blockIdx.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const long long np = (long long)nb * B;
+  const double* bh = blocks + (size_t)h * nb * 4 * B * B;
+  double* ih = inv + (size_t)h * np * np;
+  auto load = [&](const double* src, double* dst) {
+    for (int t = tid; t < B * B; t += nt) dst[t] = src[t];
+  };
+  // dst = A src (all B x B); A from shared memory
+  auto mm = [&](const double* A, const double* src, double* dst, double sign) {
+    for (int t = tid; t < B * B; t += nt) {
+      const int i = t / B, j = t % B;
+      double acc = 0.0;
+      for (int l = 0; l < B; ++l) acc = fma(A[i * B + l], src[l * B + j], acc);
+      dst[t] = sign * acc;
+    }
+  };
+  auto park = [&](int k, const double* src) {  // rows of block k, columns of block kc
+    for (int t = tid; t < B * B; t += nt) {
+      const int i = t / B, j = t % B;
+      ih[((size_t)k * B + i) * np + (size_t)kc * B + j] = src[t];
+    }
+  };
+  // forward
+  for (int k = kc; k < nb; ++k) {
+    if (k == kc) {
+      for (int t = tid; t < B * B; t += nt) R[t] = (t / B == t % B) ? 1.0 : 0.0;
+    } else {
+      load(bh + ((size_t)k * 4 + 2) * B * B, M);  // E_k
+      __syncthreads();
+      mm(M, Y, R, -1.0);
+    }
+    __syncthreads();
+    load(bh + ((size_t)k * 4 + 0) * B * B, M);  // Dinv_k
+    __syncthreads();
+    mm(M, R, Y, 1.0);
+    __syncthreads();
+    park(k, Y);
+    __syncthreads();
+  }
+  // backward (Y holds X_{k+1} after each step)
+  for (int k = nb - 1; k >= 0; --k) {
+    for (int t = tid; t < B * B; t += nt) {
+      const int i = t / B, j = t % B;
+      R[t] = k >= kc ? ih[((size_t)k * B + i) * np + (size_t)kc * B + j] : 0.0;
+    }
+    if (k < nb - 1) {
+      __syncthreads();
+      load(bh + ((size_t)(k + 1) * 4 + 3) * B * B, M);  // E_{k+1}^T
+      __syncthreads();
+      for (int t = tid; t < B * B; t += nt) {
+        const int i = t / B, j = t % B;
+        double acc = 0.0;
+        for (int l = 0; l < B; ++l) acc = fma(M[i * B + l], Y[l * B + j], acc);
+        R[t] -= acc;
+      }
+    }
+    __syncthreads();
+    load(bh + ((size_t)k * 4 + 1) * B * B, M);  // Dinv_k^T
+    __syncthreads();
+    mm(M, R, Y, 1.0);
+    __syncthreads();
+    park(k, Y);
+    __syncthreads();
+  }
+}
+
+// The dynamic shared-memory ceiling of the coarse kernels, raised once per device to the
+// device's opt-in maximum.  (Setting it per call to the call's own size raced between
+// host threads building hierarchies of different block sizes: a launch could meet
+// another thread's smaller ceiling and fail.)
+static int allow_large_smem() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  STT_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return STT_OK;
+  int max_optin = 0;
+  STT_TRY(check_cuda(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                     "smem attribute"));
+  // the ceiling counts the kernel's static shared memory too
+  auto raise_to = [&](const void* fn) -> int {
+    cudaFuncAttributes fa;
+    STT_TRY(check_cuda(cudaFuncGetAttributes(&fa, fn), "function attributes"));
+    return check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           max_optin - (int)fa.sharedSizeBytes), "smem attr");
+  };
+  STT_TRY(raise_to((const void*)band_factor_kernel));
+  STT_TRY(raise_to((const void*)coarse_inverse_kernel));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return STT_OK;
+}
+
 template <int D>
 static int build_coarse(stt_hier* h, cudaStream_t st) {
   CoarseDesc& co = h->co;
@@ -838,9 +950,15 @@ static int build_coarse(stt_hier* h, cudaStream_t st) {
       cl.st64, cl.fixed, cl.nnx, cl.nny, co.by_col, co.B, co.nb, co.blocks, h->status);
   STT_TRY(check_launch("band assemble"));
   const size_t smem = (size_t)3 * co.B * (co.B + 1) * sizeof(double);
-  STT_TRY(check_cuda(cudaFuncSetAttribute(band_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr"));
+  STT_TRY(allow_large_smem());
   band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
-  return check_launch("band factor");
+  STT_TRY(check_launch("band factor"));
+  if (co.inv) {
+    const size_t ism = (size_t)3 * co.B * co.B * sizeof(double);
+    coarse_inverse_kernel<<<dim3(co.nb, H), 256, ism, st>>>(co.blocks, co.B, co.nb, co.inv);
+    STT_TRY(check_launch("coarse inverse"));
+  }
+  return STT_OK;
 }
 
 extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_bytes, int d, int nelx,

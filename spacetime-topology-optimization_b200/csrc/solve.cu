@@ -198,6 +198,14 @@ struct Cycle {
   void coarse(int l, const T* b, T* x) {
     const LevelDesc& lv = h->lv[l];
     const CoarseDesc& co = h->co;
+    if (sizeof(T) == 4 && co.inv) {
+      const int np = co.nb * co.B;
+      coarse_inv_solve_kernel<D, T><<<dim3((np + kInvRowsPerCta - 1) / kInvRowsPerCta, nrows), 256,
+                                      sizeof(double) * np, st>>>(b, x, vstride(lv.ndof), co.inv, np, co.by_col,
+                                                                 lv.nnx, lv.nny, lv.fixed, h->row_map, h->hrows,
+                                                                 rst);
+      return;
+    }
 #define STT_COARSE(NC)                                                                          \
   coarse_solve_kernel<D, T, NC><<<nrows, 16 * NC, 0, st>>>(b, x, vstride(lv.ndof), co.blocks, co.nb, co.by_col, \
                                                           lv.nnx, lv.nny, lv.fixed, w.cscratch,       \
