@@ -620,17 +620,18 @@ __global__ void __launch_bounds__(256) band_factor_kernel(double* __restrict__ b
       }
       __syncthreads();
     }
-    // unblocked right-looking Cholesky, lower triangle
+    // unblocked right-looking Cholesky, lower triangle; two barriers per column: every
+    // thread forms the pivot itself, and the diagonal entry is written back during the
+    // trailing update (which does not read it)
     for (int j = 0; j < B; ++j) {
-      if (tid == 0) {
-        const double p = A[j * ld + j];
-        if (!(p > 0.0)) bad = 1;
-        A[j * ld + j] = sqrt(p > 0.0 ? p : 1.0);
-      }
-      __syncthreads();
-      const double piv = A[j * ld + j];
+      const double p = A[j * ld + j];
+      const double piv = sqrt(p > 0.0 ? p : 1.0);
       for (int i = j + 1 + tid; i < B; i += nt) A[i * ld + j] /= piv;
       __syncthreads();
+      if (tid == 0) {
+        if (!(p > 0.0)) bad = 1;
+        A[j * ld + j] = piv;
+      }
       const int m = B - j - 1;
       for (int t = tid; t < m * m; t += nt) {
         const int i = j + 1 + t / m, l = j + 1 + t % m;
@@ -638,14 +639,28 @@ __global__ void __launch_bounds__(256) band_factor_kernel(double* __restrict__ b
       }
       __syncthreads();
     }
-    // X = A^{-1}, one column per thread
-    for (int c = tid; c < B; c += nt) {
-      for (int i = 0; i < c; ++i) X[i * ld + c] = 0.0;
-      X[c * ld + c] = 1.0 / A[c * ld + c];
-      for (int i = c + 1; i < B; ++i) {
-        double s = 0.0;
-        for (int l = c; l < i; ++l) s = fma(A[i * ld + l], X[l * ld + c], s);
-        X[i * ld + c] = -s / A[i * ld + i];
+    // X = A^{-1} by forward substitution, a quad of threads per column: the four split
+    // each row's dot product and combine it by shuffles.  Loop bounds are uniform over the
+    // warp (the shuffles need every lane); lanes without a column do no arithmetic.
+    {
+      const int q = tid & 3;
+      for (int c0 = 0; c0 < B; c0 += nt / 4) {
+        const int c = c0 + tid / 4;
+        const bool col = c < B;
+        if (col && q == 0) {
+          for (int i = 0; i < c; ++i) X[i * ld + c] = 0.0;
+          X[c * ld + c] = 1.0 / A[c * ld + c];
+        }
+        __syncwarp();
+        for (int i = c0 + 1; i < B; ++i) {
+          double s = 0.0;
+          if (col && i > c)
+            for (int l = c + q; l < i; l += 4) s = fma(A[i * ld + l], X[l * ld + c], s);
+          s += __shfl_xor_sync(0xffffffffu, s, 1);
+          s += __shfl_xor_sync(0xffffffffu, s, 2);
+          if (col && i > c && q == 0) X[i * ld + c] = -s / A[i * ld + i];
+          __syncwarp();
+        }
       }
     }
     __syncthreads();
