@@ -218,6 +218,36 @@ int stt_heat_element_means(int nelx, int nely, const double* T, double* t_e,
 int stt_heat_adjoint_load(int nelx, int nely, const double* w, double scale, double* g,
                           stt_stream_t stream);
 
+/* ---- element <-> node transfers of the stage glue and the time fields ----------- */
+
+/* Gravity load matrix C of the self-weight load (replaces gravity.gravity_load_matrix,
+ * sttopt/gravity.py:15-36, and its SpMV in compliance._gravity_load,
+ * sttopt/compliance.py:156): transpose == 0: out[s][n] = (fe / 4) * sum of x[s][e] over
+ * the elements of node n (C x); transpose != 0: out[s][e] = (fe / 4) * sum of x[s][n]
+ * over the corners of e (C^T g).  fe = 1 / (nelx nely).  FP64. */
+int stt_gravity_load(int nelx, int nely, int nrows, const double* x, long long x_rs,
+                     double* out, long long o_rs, int transpose, stt_stream_t stream);
+
+/* Element means (virtual_heat.element_means, sttopt/virtual_heat.py:162-166):
+ * transpose == 0: out[s][e] = mean of u[s] over e's corners; transpose != 0:
+ * out[s][n] = sum over the elements of n of u[s][e] / 4 (the adjoint).  FP64. */
+int stt_element_means(int nelx, int nely, int nrows, const double* u, long long u_rs,
+                      double* out, long long o_rs, int transpose, stt_stream_t stream);
+
+/* Load of the Poisson distance fit (ScalarMesh.divergence_load(w, direction_field(s)),
+ * sttopt/virtual_heat.py:290-320): F[n] = sum over elements of w[e] / 4 * sum over the
+ * 2 x 2 Gauss points of X . grad N_n, X = grad s / sqrt(|grad s|^2 + DBL_MIN).  FP64. */
+int stt_poisson_load(int nelx, int nely, int nrows, const double* s, long long s_rs,
+                     const double* w, long long w_rs, double* F, long long F_rs,
+                     stt_stream_t stream);
+
+/* Its adjoint for an output weight gF: gs = (dF/ds)^T gF (per node), gw = (dF/dw)^T gF
+ * (per element); either output may be NULL. */
+int stt_poisson_load_adjoint(int nelx, int nely, int nrows, const double* s, long long s_rs,
+                             const double* w, long long w_rs, const double* gF, long long gF_rs,
+                             double* gs, long long gs_rs, double* gw, long long gw_rs,
+                             stt_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,7 +2,8 @@
 
 Drop-in modules with the reference's names and call signatures:
 ``torch_fem``, ``torch_mg``, ``torch_solve``, ``sensitivity``, ``virtual_heat``,
-``compliance``; plus ``spacetime``, the batched space-time objective + gradient.
+``compliance``, ``gravity``, ``filters``; plus ``spacetime``, the batched space-time
+objective + gradient.
 All compute runs in ``libsttb200.so`` (C ABI: ``include/sttb200.h``) on the caller's
 CUDA stream; there is no CPU path.
 """
@@ -10,7 +11,7 @@ CUDA stream; there is no CPU path.
 from . import _lib  # noqa: F401
 
 __all__ = ["torch_fem", "torch_mg", "torch_solve", "sensitivity", "virtual_heat", "compliance",
-           "spacetime", "fem"]
+           "spacetime", "fem", "gravity", "filters"]
 
 
 def __getattr__(name):

@@ -399,6 +399,121 @@ def gen_filters():
     save("filters", **out)
 
 
+def gen_compliance_smooth():
+    """The production stage glue with the smooth stage mask: batched_whole_and_gravity_compliance
+    (row 0 = the point-load whole structure, then one self-weight row per stage time) on an MBB
+    grid, and the gradient of c + sum_s w_s c_s in xPhys and tPhys through the reference's
+    autograd (its dcx and dct)."""
+    out = {}
+    for nelx, nely, beta_t, times, seed in [(48, 24, 10.0, (0.25, 0.5, 0.75, 1.0), 21),
+                                            (40, 16, 40.0, (0.2, 0.45, 0.7), 22)]:
+        k = f"{nelx}x{nely}"
+        ndof = 2 * (nelx + 1) * (nely + 1)
+        # the MBB point load on the whole-structure row; the build plate (the bottom row of
+        # nodes, both dofs) clamped, as the space-time stages are supported
+        F, _ = load_cases.load_case(load_cases.LoadCase.MBB, nelx, nely, 0.0, 0.0, 1.0)
+        plate = fem.node_grid(nelx, nely)[-1, :]
+        free = np.setdiff1d(np.arange(ndof), np.concatenate([2 * plate, 2 * plate + 1]))
+        rng = np.random.default_rng(seed)
+        x = smoothed_density(nelx, nely, seed)
+        # a layered build from the bottom (the supports' side) with a mild seeded ripple,
+        # so every stage's material is connected to the supports
+        rows = (nely - 0.5 - np.arange(nely)[:, None]) / nely
+        tp = np.clip(rows + 0.05 * np.sin(0.3 * np.arange(nelx))[None, :] + 0.02 * rng.uniform(-1, 1, (nely, nelx)),
+                     0.0, 1.0)
+        w = rng.uniform(0.5, 1.5, len(times))
+        C = torch_util.csr_to_tensor(gravity.gravity_load_matrix(nelx, nely), "cpu", F64)
+        xT, tT = t(x).requires_grad_(True), t(tp).requires_grad_(True)
+        c, stages, U = compliance.batched_whole_and_gravity_compliance(
+            xT, tT, t(fem.plane_stress_KE(NU)), t(fem.element_dof_map(nelx, nely), torch.int64), EMIN, EMAX,
+            PENAL, t(free, torch.int64), t(F), ndof, C, beta_t, list(times))
+        L = c + sum(float(wi) * cs for wi, cs in zip(w, stages))
+        gx, gt = torch.autograd.grad(L, [xT, tT])
+        out.update({f"{k}_x": x, f"{k}_t": tp, f"{k}_w": w, f"{k}_beta_t": beta_t, f"{k}_times": np.array(times),
+                    f"{k}_F": F, f"{k}_free": free, f"{k}_c": c, f"{k}_stages": torch.stack(stages), f"{k}_U": U,
+                    f"{k}_L": L, f"{k}_gx": gx, f"{k}_gt": gt})
+    out["C_7x4"] = gravity.gravity_load_matrix(7, 4).toarray()
+    save("compliance_smooth", **out)
+
+
+def laplace_config(time_map):
+    """A LaplaceRunConfig-shaped object carrying only the fields laplace_time_field reads."""
+
+    class Cfg:
+        pass
+
+    c = Cfg()
+    c.chi_contrast = 100.0
+    c.chi_density_floor = 1e-2
+    c.chi_density_sensitivity = True
+    c.laplace_cg_rtol = 1e-10
+    c.poisson_cg_rtol = 1e-10
+    c.time_map = time_map
+    return c
+
+
+def gen_time_maps():
+    """The poisson map of heat_time_field and laplace_time_field (identity and poisson maps)
+    with the reference's autograd gradients of sum(w tPhys); and the fused Poisson load
+    divergence_load(w, direction_field(s)) with its vector-Jacobian products."""
+    out = {}
+    nelx, nely, seed = 40, 20, 31
+    rng = np.random.default_rng(seed)
+    x = smoothed_density(nelx, nely, seed)
+    mu = rng.uniform(0.2, 0.8, (nely, nelx))
+    w = rng.uniform(-1, 1, (nely, nelx))
+    mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device("cpu"), F64)
+    cfg = heat_config(nelx, nely, time_map="poisson", heat_cg_rtol=1e-10, poisson_cg_rtol=1e-10)
+    xT, muT = t(x).requires_grad_(True), t(mu).requires_grad_(True)
+    sol = vh.heat_time_field(cfg, mesh, xT, muT, conduction_penal=3.0)
+    J = torch.sum(t(w) * sol.tPhys)
+    gx, gmu = torch.autograd.grad(J, [xT, muT])
+    out.update({"heat_x": x, "heat_mu": mu, "heat_w": w, "heat_tPhys": sol.tPhys, "heat_T": sol.primary,
+                "heat_phi": sol.poisson, "heat_J": J, "heat_gx": gx, "heat_gmu": gmu})
+
+    # Poisson load alone, on a random field, with random output weights
+    s_field = rng.normal(size=mesh.ndof)
+    we = rng.uniform(0.1, 1.0, nelx * nely)
+    gF = rng.normal(size=mesh.ndof)
+    sT, weT = t(s_field).requires_grad_(True), t(we).requires_grad_(True)
+    Fp = mesh.divergence_load(weT, mesh.direction_field(sT))
+    gs, gw = torch.autograd.grad(torch.sum(t(gF) * Fp), [sT, weT])
+    u = rng.normal(size=(2, mesh.ndof))
+    out.update({"pl_s": s_field, "pl_w": we, "pl_gF": gF, "pl_F": Fp, "pl_gs": gs, "pl_gw": gw,
+                "em_u": u, "em_means": vh.element_means(t(u), mesh.edof)})
+
+    for nelx, nely, base, tmap, dexp, seed in [(36, 18, "bottom_edge", "identity", 0.0, 32),
+                                              (36, 18, "left_edge", "identity", 1.0, 33),
+                                              (32, 16, "bottom_edge", "poisson", 1.0, 34)]:
+        k = f"lap_{nelx}x{nely}_{base}_{tmap}_{dexp}"
+        rng = np.random.default_rng(seed)
+        x = smoothed_density(nelx, nely, seed)
+        mu = rng.uniform(0.2, 0.8, (nely, nelx))
+        w = rng.uniform(-1, 1, (nely, nelx))
+        mesh = vh.ScalarMesh.build(nelx, nely, base, torch.device("cpu"), F64)
+        n_arc = mesh.arc.numel()
+        b = 0.5 * np.sin(np.linspace(0.1, 3.0, n_arc)) + 0.6 + 0.05 * rng.uniform(size=n_arc)
+        xT, muT, bT = t(x).requires_grad_(True), t(mu).requires_grad_(True), t(b).requires_grad_(True)
+        sol = vh.laplace_time_field(laplace_config(tmap), mesh, xT, muT, bT, density_exponent=dexp)
+        J = torch.sum(t(w) * sol.tPhys)
+        grads = torch.autograd.grad(J, [xT, muT, bT], allow_unused=True)
+        gx, gmu, gb = [torch.zeros(1, dtype=F64) if g is None else g for g in grads]
+        out.update({f"{k}_x": x, f"{k}_mu": mu, f"{k}_w": w, f"{k}_b": b, f"{k}_arc": mesh.arc,
+                    f"{k}_tPhys": sol.tPhys, f"{k}_u": sol.primary, f"{k}_J": J, f"{k}_gx": gx,
+                    f"{k}_gmu": gmu, f"{k}_gb": gb})
+        if sol.poisson is not None:
+            out[f"{k}_phi"] = sol.poisson
+    # wall arcs: every plate side, and an L-shaped domain (a re-entrant corner)
+    lshape = np.ones((8, 12), bool)
+    lshape[:4, 6:] = False
+    for base in ("bottom_edge", "left_edge", "right_edge"):
+        out[f"arc_rect_{base}"] = vh.wall_arc(13, 7, base)
+        out[f"arc_L_{base}"] = vh.wall_arc(12, 8, base, lshape)
+        out[f"plate_L_{base}"] = vh.plate_nodes(12, 8, base, lshape)
+    out["lshape"] = lshape
+    save("time_maps", **out)
+
+
 def gen_pcg_cases():
     """Retirement, zero rows, warm starts and non-convergence, as the reference does them."""
     nelx, nely = 18, 12
@@ -436,5 +551,7 @@ if __name__ == "__main__":
     gen_heat()
     gen_spacetime()
     gen_filters()
+    gen_compliance_smooth()
+    gen_time_maps()
     if "--with-512" in sys.argv:
         gen_spacetime_512()

@@ -1,0 +1,150 @@
+"""GPU parity of the smooth-mask stage glue and of the other time maps against the
+reference's outputs (golden fixtures made by running it on the same seeded inputs).
+
+* ``compliance.batched_whole_and_gravity_compliance`` with the smooth ``time_mask``, the
+  point-load row 0 and the device gravity stencil: compliances and displacements 1e-9
+  relative, the gradients in xPhys and tPhys 5e-8 (converged FP64 solves at rtol 1e-8).
+* The fused Poisson load and its adjoint, element means: 1e-13 (same arithmetic to
+  rounding).
+* ``heat_time_field`` with the ``poisson`` map and ``laplace_time_field`` (identity and
+  poisson maps; solves at rtol 1e-10): fields 1e-8, gradients 1e-7.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+EMIN, EMAX, PENAL, NU = 1e-9, 1.0, 3.0, 0.3
+DEV = "cuda"
+
+
+def T(a, dtype=torch.float64):
+    return torch.as_tensor(np.asarray(a), dtype=dtype, device=DEV)
+
+
+@pytest.mark.parametrize("key", ["48x24", "40x16"])
+@pytest.mark.parametrize("sparse_C", [False, True])
+def test_batched_whole_and_gravity_compliance_smooth(pkg, key, sparse_C):
+    from sttopt_b200 import compliance, fem, gravity
+
+    g = golden("compliance_smooth")
+    nelx, nely = (int(v) for v in key.split("x"))
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    C = gravity.gravity_load_matrix(nelx, nely)
+    if sparse_C:  # the production loop's torch CSR form of the matrix (a library SpMV)
+        csr = C.tocsr()
+        C = torch.sparse_csr_tensor(torch.as_tensor(csr.indptr), torch.as_tensor(csr.indices),
+                                    torch.as_tensor(csr.data), size=csr.shape).to(DEV)
+    x = T(g[f"{key}_x"]).requires_grad_(True)
+    tp = T(g[f"{key}_t"]).requires_grad_(True)
+    c, stages, U = compliance.batched_whole_and_gravity_compliance(
+        x, tp, T(fem.plane_stress_KE(NU)), T(fem.element_dof_map(nelx, nely), torch.int64), EMIN, EMAX, PENAL,
+        T(g[f"{key}_free"], torch.int64), T(g[f"{key}_F"]), ndof, C, float(g[f"{key}_beta_t"]),
+        [float(v) for v in g[f"{key}_times"]])
+    L = c + sum(float(wi) * cs for wi, cs in zip(g[f"{key}_w"], stages))
+    gx, gt = torch.autograd.grad(L, [x, tp])
+    assert abs(float(c) - float(g[f"{key}_c"])) <= 1e-9 * abs(float(g[f"{key}_c"]))
+    assert rel_err(torch.stack(stages).detach().cpu(), g[f"{key}_stages"]) < 1e-9
+    assert rel_err(U.detach().cpu(), g[f"{key}_U"]) < 1e-9
+    assert rel_err(gx.cpu(), g[f"{key}_gx"]) < 5e-8
+    assert rel_err(gt.cpu(), g[f"{key}_gt"]) < 5e-8
+
+
+def test_gravity_stencil_and_transpose(pkg):
+    from sttopt_b200 import gravity
+
+    rng = np.random.default_rng(5)
+    nelx, nely = 37, 19
+    C = gravity.gravity_load_matrix(nelx, nely)
+    csr = C.tocsr()
+    x = rng.uniform(size=(3, nelx * nely))
+    y = rng.normal(size=(2, (nelx + 1) * (nely + 1)))
+    assert rel_err((C @ T(x)).cpu(), (csr @ x.T).T) < 1e-15
+    assert rel_err((C.T @ T(y)).cpu(), (csr.T @ y.T).T) < 1e-15
+
+
+def test_poisson_load_adjoint_and_element_means(pkg):
+    from sttopt_b200 import virtual_heat as vh
+
+    g = golden("time_maps")
+    mesh = vh.ScalarMesh.build(40, 20, "bottom_edge", torch.device(DEV), torch.float64)
+    s = T(g["pl_s"]).requires_grad_(True)
+    w = T(g["pl_w"]).requires_grad_(True)
+    F = mesh.poisson_load(s, w)
+    assert rel_err(F.detach().cpu(), g["pl_F"]) < 1e-13
+    gs, gw = torch.autograd.grad(torch.sum(T(g["pl_gF"]) * F), [s, w])
+    assert rel_err(gs.cpu(), g["pl_gs"]) < 1e-13
+    assert rel_err(gw.cpu(), g["pl_gw"]) < 1e-13
+    # the unfused form on the device agrees with the kernel
+    F2 = mesh.divergence_load(w.detach(), mesh.direction_field(s.detach()))
+    assert rel_err(F2.cpu(), F.detach().cpu()) < 1e-13
+    u = T(g["em_u"]).requires_grad_(True)
+    means = vh.element_means(u, mesh.edof)
+    assert rel_err(means.detach().cpu(), g["em_means"]) < 1e-15
+    (gu,) = torch.autograd.grad(means.sum(), [u])
+    counts = torch.zeros(mesh.ndof, dtype=torch.float64, device=DEV).index_add_(
+        0, mesh.edof.reshape(-1), torch.full((mesh.edof.numel(),), 0.25, dtype=torch.float64, device=DEV))
+    assert torch.allclose(gu, counts.expand_as(gu), rtol=0, atol=1e-15)
+
+
+def test_heat_time_field_poisson_map(pkg):
+    from sttopt_b200 import virtual_heat as vh
+
+    g = golden("time_maps")
+    mesh = vh.ScalarMesh.build(40, 20, "bottom_edge", torch.device(DEV), torch.float64)
+
+    class Cfg:
+        chi_contrast, drain_beta, time_map = 1000.0, 25.0, "poisson"
+        heat_cg_rtol = poisson_cg_rtol = 1e-10
+
+    x = T(g["heat_x"]).requires_grad_(True)
+    mu = T(g["heat_mu"]).requires_grad_(True)
+    sol = vh.heat_time_field(Cfg, mesh, x, mu, conduction_penal=3.0)
+    J = torch.sum(T(g["heat_w"]) * sol.tPhys)
+    gx, gmu = torch.autograd.grad(J, [x, mu])
+    assert rel_err(sol.primary.detach().cpu(), g["heat_T"]) < 1e-8
+    assert rel_err(sol.poisson.detach().cpu(), g["heat_phi"]) < 1e-8
+    assert rel_err(sol.tPhys.detach().cpu(), g["heat_tPhys"]) < 1e-8
+    assert abs(float(J) - float(g["heat_J"])) <= 1e-8 * abs(float(g["heat_J"]))
+    assert rel_err(gx.cpu(), g["heat_gx"]) < 1e-7
+    assert rel_err(gmu.cpu(), g["heat_gmu"]) < 1e-7
+
+
+LAPLACE = ["lap_36x18_bottom_edge_identity_0.0", "lap_36x18_left_edge_identity_1.0",
+           "lap_32x16_bottom_edge_poisson_1.0"]
+
+
+@pytest.mark.parametrize("key", LAPLACE)
+def test_laplace_time_field(pkg, key):
+    from sttopt_b200 import virtual_heat as vh
+
+    g = golden("time_maps")
+    _, dims, edge, side, tmap, dexp = key.split("_")
+    nelx, nely = (int(v) for v in dims.split("x"))
+    mesh = vh.ScalarMesh.build(nelx, nely, f"{edge}_{side}", torch.device(DEV), torch.float64)
+    assert np.array_equal(mesh.arc.cpu().numpy(), g[f"{key}_arc"])
+
+    class Cfg:
+        chi_contrast, chi_density_floor, chi_density_sensitivity = 100.0, 1e-2, True
+        laplace_cg_rtol = poisson_cg_rtol = 1e-10
+        time_map = tmap
+
+    x = T(g[f"{key}_x"]).requires_grad_(True)
+    mu = T(g[f"{key}_mu"]).requires_grad_(True)
+    b = T(g[f"{key}_b"]).requires_grad_(True)
+    sol = vh.laplace_time_field(Cfg, mesh, x, mu, b, density_exponent=float(dexp))
+    J = torch.sum(T(g[f"{key}_w"]) * sol.tPhys)
+    grads = torch.autograd.grad(J, [x, mu, b], allow_unused=True)
+    assert rel_err(sol.primary.detach().cpu(), g[f"{key}_u"]) < 1e-8
+    assert rel_err(sol.tPhys.detach().cpu(), g[f"{key}_tPhys"]) < 1e-8
+    if tmap == "poisson":
+        assert rel_err(sol.poisson.detach().cpu(), g[f"{key}_phi"]) < 1e-8
+    for gr, name in zip(grads, ["gx", "gmu", "gb"]):
+        ref = g[f"{key}_{name}"]
+        if gr is None:
+            assert ref.size == 1 and ref[0] == 0.0
+        else:
+            assert rel_err(gr.cpu(), ref) < 1e-7, name
