@@ -224,12 +224,17 @@ __global__ void convert_kernel(const TI* __restrict__ in, TO* __restrict__ out, 
     out[i] = (TO)in[i];
 }
 
+// Row copy of the densities, with the FP32 copy written in the same pass (out32 may be null).
 __global__ void copy_rows_kernel(const double* __restrict__ in, long long in_rs,
-                                 double* __restrict__ out, long long out_rs, long long n) {
+                                 double* __restrict__ out, float* __restrict__ out32, long long out_rs,
+                                 long long n) {
   const int row = blockIdx.y;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    out[(size_t)row * out_rs + i] = in[(size_t)row * in_rs + i];
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = in[(size_t)row * in_rs + i];
+    out[(size_t)row * out_rs + i] = v;
+    if (out32) out32[(size_t)row * out_rs + i] = (float)v;
+  }
 }
 
 // Coarse fixed flags: the fine flags at the collocated nodes (torch_mg.py:376).
@@ -277,6 +282,70 @@ __global__ void keff_from_density_kernel(const double* __restrict__ rho, long lo
   double* out = keff + (((size_t)h * cnel + E) * NK + i) * NK;
 #pragma unroll
   for (int j = 0; j < NK; ++j) out[j] = reac ? acc[j] + acc2[j] : acc[j];
+}
+
+// keff_from_density_kernel for NM = 16 grandchildren (2 x 2 coarsening twice), a warp per
+// element (D = 2: lane l holds entries l and l + 32) or per two elements (D = 1: a group of
+// 16 lanes per element): the NM tables live in registers, the first NM lanes of a group
+// load the child densities and shuffles broadcast them, and a warp's stores are 256
+// contiguous bytes.  (The per-(E, i) kernel re-reads the tables from L1 for every
+// element and is bound by it.)
+template <int D, int NM, bool RD>
+__global__ void __launch_bounds__(256) keff_from_density_warp_kernel(
+    const double* __restrict__ rho, long long rho_rs, const double* __restrict__ reac, long long r_rs,
+    const double* __restrict__ G, const double* __restrict__ GM, int fnelx, int kx, int cnelx, int cnel,
+    int H, double* __restrict__ keff) {
+  constexpr int NK = 4 * D, NE = NK * NK;       // 64 or 16 entries
+  constexpr int GW = NE >= 32 ? 32 : NE;        // lanes per element
+  constexpr int EPL = NE / GW;                  // entries per lane
+  constexpr int EPW = 32 / GW;                  // elements per warp step
+  static_assert(NM <= GW, "the children of an element must fit its lane group");
+  const int lane = threadIdx.x & 31, sub = lane / GW, gl = lane % GW;
+  double g[NM][EPL], gm[RD ? NM : 1][EPL];
+#pragma unroll
+  for (int m = 0; m < NM; ++m)
+#pragma unroll
+    for (int k = 0; k < EPL; ++k) {
+      g[m][k] = __ldg(G + (size_t)m * NE + gl + GW * k);
+      if constexpr (RD) gm[m][k] = __ldg(GM + (size_t)m * NE + gl + GW * k);
+    }
+  const int ky = NM / kx;
+  const long long total = (long long)H * cnel;
+  const long long nw = (long long)gridDim.x * (blockDim.x / 32);
+  for (long long base = (blockIdx.x * (long long)(blockDim.x / 32) + threadIdx.x / 32) * EPW; base < total;
+       base += nw * EPW) {  // the same trip count for every lane of the warp
+    const long long idx = base + sub;
+    const bool ok = idx < total;
+    const int h = ok ? (int)(idx / cnel) : 0;
+    const int E = ok ? (int)(idx - (long long)h * cnel) : 0;
+    const int R = E / cnelx, C = E - R * cnelx;
+    double rv = 0.0, av = 0.0;
+    if (ok && gl < NM) {
+      const int my = gl / kx, mx = gl - my * kx;
+      const size_t fe = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
+      rv = __ldg(rho + (size_t)h * rho_rs + fe);
+      if constexpr (RD) av = __ldg(reac + (size_t)h * r_rs + fe);
+    }
+    double acc[EPL];
+#pragma unroll
+    for (int k = 0; k < EPL; ++k) acc[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const double r = __shfl_sync(0xffffffffu, rv, sub * GW + m);
+#pragma unroll
+      for (int k = 0; k < EPL; ++k) acc[k] = fma(r, g[m][k], acc[k]);
+      if constexpr (RD) {
+        const double a = __shfl_sync(0xffffffffu, av, sub * GW + m);
+#pragma unroll
+        for (int k = 0; k < EPL; ++k) acc[k] = fma(a, gm[m][k], acc[k]);
+      }
+    }
+    if (ok) {
+      double* out = keff + ((size_t)h * cnel + E) * NE + gl;
+#pragma unroll
+      for (int k = 0; k < EPL; ++k) out[GW * k] = acc[k];
+    }
+  }
 }
 
 // Galerkin product of the level above: keff_c[E] = sum_m S_m^T keff_f[child m] S_m
@@ -375,9 +444,11 @@ struct DensitySource {  // rho_e KE (+ reaction_e I / 4), level 0 used as the co
 // sums the (corner N, corner M) blocks of the elements holding both nodes, averaged
 // with the transpose of (M, N) as the reference symmetrises its dense coarse matrix
 // (torch_mg.py:286), with rows and columns of fixed dofs zeroed.
+// st32 (may be null) receives the FP32 copy in the same pass: every entry, or with
+// diag32 only the centre block's diagonal (all a level swept from the densities reads).
 template <int D, typename Src>
 __global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int nelx, int nely,
-                               double* __restrict__ st) {
+                               double* __restrict__ st, float* __restrict__ st32, int diag32) {
   constexpr int NS = 5 * D * D;
   const int nnx = nelx + 1, nny = nely + 1;
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -429,7 +500,9 @@ __global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int n
       for (int j = 0; j < D; ++j) {
         double v = (A[i][j] + AT[i][j]) / 2;
         if (((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
-        out[(size_t)(blk * D * D + i * D + j) * nnode] = v;
+        const size_t o = (size_t)(blk * D * D + i * D + j) * nnode;
+        out[o] = v;
+        if (st32 && (!diag32 || (blk == 0 && i == j))) st32[(size_t)h * NS * nnode + n + o] = (float)v;
       }
   }
 }
@@ -447,7 +520,7 @@ template <int D, bool RD, int NM>
 __global__ void __launch_bounds__(256) stencil_children_kernel(
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ reac, long long r_rs,
     const double* __restrict__ Wg, int fnelx, int kx, int ky, const uint8_t* __restrict__ fixed, int nelx,
-    int nely, double* __restrict__ st) {
+    int nely, double* __restrict__ st, float* __restrict__ st32, int diag32) {
   constexpr int DD = D * D, NS = 5 * DD, NW = NS * 4 * NM;
   __shared__ double W[(RD ? 2 : 1) * NW];
   for (int i = threadIdx.x; i < (RD ? 2 : 1) * NW; i += blockDim.x) W[i] = Wg[i];
@@ -495,7 +568,9 @@ __global__ void __launch_bounds__(256) stencil_children_kernel(
           if constexpr (RD) v = fma(av[p][m], w[NW + p * NM + m], v);
         }
       if (!m_ok || ((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
-      out[(size_t)(blk * DD + q) * nnode] = v;
+      const size_t o = (size_t)(blk * DD + q) * nnode;
+      out[o] = v;
+      if (st32 && (!diag32 || (blk == 0 && i == j))) st32[(size_t)h * NS * nnode + n + o] = (float)v;
     }
   }
 }
@@ -696,6 +771,196 @@ __global__ void __launch_bounds__(256) band_factor_kernel(double* __restrict__ b
   if (tid == 0 && bad) atomicOr(status, 1);
 }
 
+// 16-byte asynchronous global -> shared copies (sm_80+ cp.async), for prefetching the
+// next blocks while the current one factors.
+STT_DEV void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+STT_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+STT_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The same factorisation for B = 16 NA (NA = 2, 4), 256 threads as a 16 x 16 grid:
+//   * thread (ty, tx) owns the strided tile of entries (ty + 16 a, tx + 16 b), a, b < NA,
+//     of every B x B product, so each shared-memory load feeds NA multiply-adds (a warp
+//     reads 2 rows of one operand, broadcast, and 16 rows of the other at a stride of
+//     B + 1 doubles, conflict-free);
+//   * the Cholesky takes two columns per pair of barriers: every thread forms both
+//     pivots and the two scaled columns of its rows and columns in registers (column
+//     j + 1 updated by column j on the fly), then applies the rank-2 trailing update;
+//   * A_{k+1,k+1} and A_{k+1,k} are copied into staging buffers with cp.async while
+//     block k factors; the Schur update and E = A_{k+1,k} X^T read them from there.
+// Upper triangles of the work arrays carry harmless values (only lower triangles are
+// read); X = D^{-1} keeps exact zeros above its diagonal.
+template <int NA>
+__global__ void __launch_bounds__(256) band_factor_tiled_kernel(double* __restrict__ blocks, int nb,
+                                                                int* __restrict__ status) {
+  constexpr int B = 16 * NA, ld = B + 1;
+  extern __shared__ __align__(16) double sm[];
+  double* P0 = sm;           // staged A_{k,k} (B x B, dense rows)
+  double* P1 = P0 + B * B;   // staged A_{k+1,k}
+  double* A = P1 + B * B;    // current diagonal block, then its Cholesky factor (ld)
+  double* X = A + B * ld;    // D_k^{-1}
+  double* Y = X + B * ld;    // E_k
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  double* bh = blocks + (size_t)blockIdx.x * nb * 4 * B * B;
+  __shared__ int bad;
+  if (tid == 0) bad = 0;
+  auto stage = [&](double* dst, const double* src) {
+    for (int t = tid; t < B * B / 2; t += 256) cp_async16(dst + 2 * t, src + 2 * t);
+  };
+  stage(P0, bh);
+  cp_async_commit();
+  for (int k = 0; k < nb; ++k) {
+    double* Dk = bh + (size_t)k * 4 * B * B;
+    cp_async_wait_all();
+    __syncthreads();
+    // A = A_kk - E_k E_k^T (k > 0)
+    {
+      double acc[NA][NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) acc[a][b] = 0.0;
+      if (k > 0) {
+#pragma unroll 4
+        for (int m = 0; m < B; ++m) {
+          double yi[NA], yl[NA];
+#pragma unroll
+          for (int a = 0; a < NA; ++a) yi[a] = Y[(ty + 16 * a) * ld + m];
+#pragma unroll
+          for (int b = 0; b < NA; ++b) yl[b] = Y[(tx + 16 * b) * ld + m];
+#pragma unroll
+          for (int a = 0; a < NA; ++a)
+#pragma unroll
+            for (int b = 0; b < NA; ++b) acc[a][b] = fma(yi[a], yl[b], acc[a][b]);
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) {
+          const int i = ty + 16 * a, l = tx + 16 * b;
+          A[i * ld + l] = P0[i * B + l] - acc[a][b];
+        }
+    }
+    __syncthreads();  // P0 consumed, A complete
+    if (k + 1 < nb) {
+      double* Dn = bh + (size_t)(k + 1) * 4 * B * B;
+      stage(P0, Dn);                    // A_{k+1,k+1}
+      stage(P1, Dn + (size_t)2 * B * B);  // A_{k+1,k}
+      cp_async_commit();
+    }
+    // Cholesky, columns j and j + 1 per step
+    for (int j = 0; j < B; j += 2) {
+      const double p0 = A[j * ld + j];
+      const double piv0 = sqrt(p0 > 0.0 ? p0 : 1.0), r0 = 1.0 / piv0;
+      const double c1 = A[(j + 1) * ld + j] * r0;  // scaled (j + 1, j)
+      const double p1 = A[(j + 1) * ld + j + 1] - c1 * c1;
+      const double piv1 = sqrt(p1 > 0.0 ? p1 : 1.0), r1 = 1.0 / piv1;
+      double ci[NA], di[NA], cl[NA], dl[NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        const int i = ty + 16 * a;
+        const double c = i > j ? A[i * ld + j] * r0 : 0.0;
+        ci[a] = c;
+        di[a] = i > j + 1 ? (A[i * ld + j + 1] - c * c1) * r1 : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < NA; ++b) {
+        const int l = tx + 16 * b;
+        const double c = l > j ? A[l * ld + j] * r0 : 0.0;
+        cl[b] = c;
+        dl[b] = l > j + 1 ? (A[l * ld + j + 1] - c * c1) * r1 : 0.0;
+      }
+      __syncthreads();
+      if (tx == 0) {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+          const int i = ty + 16 * a;
+          if (i > j) A[i * ld + j] = ci[a];
+          if (i > j + 1) A[i * ld + j + 1] = di[a];
+        }
+      }
+      if (tid == 0) {
+        if (!(p0 > 0.0) || !(p1 > 0.0)) bad = 1;
+        A[j * ld + j] = piv0;
+        A[(j + 1) * ld + j + 1] = piv1;
+      }
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) {
+          const int i = ty + 16 * a, l = tx + 16 * b;
+          if (i > j + 1 && l > j + 1) A[i * ld + l] = fma(-di[a], dl[b], fma(-ci[a], cl[b], A[i * ld + l]));
+        }
+      __syncthreads();
+    }
+    // X = A^{-1}: forward substitution, a quad of threads per column (as band_factor_kernel)
+    {
+      const int q = tid & 3;
+      for (int c0 = 0; c0 < B; c0 += 64) {
+        const int c = c0 + tid / 4;
+        const bool col = c < B;
+        if (col && q == 0) {
+          for (int i = 0; i < c; ++i) X[i * ld + c] = 0.0;
+          X[c * ld + c] = 1.0 / A[c * ld + c];
+        }
+        __syncwarp();
+        for (int i = c0 + 1; i < B; ++i) {
+          double sacc = 0.0;
+          if (col && i > c)
+            for (int l = c + q; l < i; l += 4) sacc = fma(A[i * ld + l], X[l * ld + c], sacc);
+          sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+          sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+          if (col && i > c && q == 0) X[i * ld + c] = -sacc / A[i * ld + i];
+          __syncwarp();
+        }
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < B * B; t += 256) {
+      const int i = t / B, j = t % B;
+      Dk[t] = X[i * ld + j];                  // Dinv
+      Dk[(size_t)B * B + t] = X[j * ld + i];  // Dinv^T
+    }
+    if (k + 1 < nb) {
+      double* Dn = bh + (size_t)(k + 1) * 4 * B * B;
+      cp_async_wait_all();
+      __syncthreads();  // P1 (and P0) landed for every thread
+      // E = A_{k+1,k} X^T (X is zero above its diagonal)
+      double acc[NA][NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) acc[a][b] = 0.0;
+#pragma unroll 4
+      for (int l = 0; l < B; ++l) {
+        double ai[NA], xj[NA];
+#pragma unroll
+        for (int a = 0; a < NA; ++a) ai[a] = P1[(ty + 16 * a) * B + l];
+#pragma unroll
+        for (int b = 0; b < NA; ++b) xj[b] = X[(tx + 16 * b) * ld + l];
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int b = 0; b < NA; ++b) acc[a][b] = fma(ai[a], xj[b], acc[a][b]);
+      }
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) {
+          const int i = ty + 16 * a, j = tx + 16 * b;
+          Y[i * ld + j] = acc[a][b];
+          Dn[(size_t)2 * B * B + i * B + j] = acc[a][b];  // E
+        }
+      __syncthreads();
+      for (int t = tid; t < B * B; t += 256) Dn[(size_t)3 * B * B + t] = Y[(t % B) * ld + t / B];  // E^T
+    }
+  }
+  if (tid == 0 && bad) atomicOr(status, 1);
+}
+
 }  // namespace stt
 
 using namespace stt;
@@ -726,21 +991,18 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   const int H = h->hrows;
   LevelDesc& l0 = h->lv[0];
   // level 0: copies of the densities, the lumped reaction diagonal, the flags
-  copy_rows_kernel<<<dim3(grid1(l0.nel), H), 256, 0, st>>>(rho, rho_rs, l0.rho64, l0.rs_rho, l0.nel);
-  if (reaction) {
+  const bool f32 = h->precision == STT_FP32;
+  copy_rows_kernel<<<dim3(grid1(l0.nel), H), 256, 0, st>>>(rho, rho_rs, l0.rho64, f32 ? l0.rho32 : nullptr,
+                                                           l0.rs_rho, l0.nel);
+  if (reaction)  // (without a reaction nothing reads the diagonal)
     STT_TRY(stt_lumped_reaction(D, h->nelx, h->nely, H, reaction, r_rs, l0.rdiag64, l0.ndof,
                                 (stt_stream_t)st));
-  } else {
-    STT_TRY(check_cuda(cudaMemsetAsync(l0.rdiag64, 0, 8 * H * l0.ndof, st), "memset"));
-  }
   if (fixed)
     STT_TRY(check_cuda(cudaMemcpyAsync(l0.fixed, fixed, l0.nnode, cudaMemcpyDeviceToDevice, st), "copy fixed"));
   else
     STT_TRY(check_cuda(cudaMemsetAsync(l0.fixed, 0, l0.nnode, st), "memset"));
-  if (h->precision == STT_FP32) {
-    convert_kernel<double, float><<<grid1(H * l0.rs_rho), 256, 0, st>>>(l0.rho64, l0.rho32, H * l0.rs_rho);
+  if (f32 && reaction)
     convert_kernel<double, float><<<grid1(H * l0.ndof), 256, 0, st>>>(l0.rdiag64, l0.rdiag32, H * l0.ndof);
-  }
   STT_TRY(check_launch("level0 copies"));
 
   // tables: per transition S, and G/GM for the first
@@ -798,7 +1060,7 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
 #define STT_CHILD_ST(RD, NM)                                                                          \
   stencil_children_kernel<D, RD, NM><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                        \
       l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, \
-      c.nelx, c.nely, c.st64)
+      c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, h->l1)
         if (reaction) {
           if (nm == 4) STT_CHILD_ST(true, 4);
           else if (nm == 6) STT_CHILD_ST(true, 6);
@@ -813,26 +1075,37 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
         stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
             ChildSource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
                            f.kx, f.ky, c.nelx},
-            c.fixed, c.nelx, c.nely, c.st64);
+            c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
       }
     } else {
       double* kc = (l % 2 == 0) ? h->keffB : h->keffA;
       const dim3 g(grid1(c.nel * NK), H);
       if (l == 2) {
         const LevelDesc& f0 = h->lv[0];
-        keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables,
-                                                       h->gtables + kGrandStride, f0.nelx, f0.kx * f.kx,
-                                                       f0.ky * f.ky, c.nelx, (int)c.nel, kc);
+        const int KX = f0.kx * f.kx, KY = f0.ky * f.ky;
+        if (KX * KY == 16) {
+          constexpr int per_block = D == 2 ? 8 : 16;  // elements a 256-thread block takes a step
+          const long long blocks = std::min<long long>((H * c.nel + per_block - 1) / per_block, 148LL * 8);
+          if (reaction)
+            keff_from_density_warp_kernel<D, 16, true><<<(int)blocks, 256, 0, st>>>(
+                l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables, h->gtables + kGrandStride, f0.nelx, KX, c.nelx,
+                (int)c.nel, H, kc);
+          else
+            keff_from_density_warp_kernel<D, 16, false><<<(int)blocks, 256, 0, st>>>(
+                l0.rho64, l0.rs_rho, nullptr, 0, h->gtables, nullptr, f0.nelx, KX, c.nelx, (int)c.nel, H, kc);
+        } else {
+          keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables,
+                                                         h->gtables + kGrandStride, f0.nelx, KX, KY, c.nelx,
+                                                         (int)c.nel, kc);
+        }
       } else {
         keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
                                                    (int)c.nel, kc);
       }
       stencil_kernel<D, KeffSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
-          KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64);
+          KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
       kprev = kc;
     }
-    if (h->precision == STT_FP32)
-      convert_kernel<double, float><<<grid1(H * NS * c.nnode), 256, 0, st>>>(c.st64, c.st32, H * NS * c.nnode);
     STT_TRY(check_launch("galerkin level"));
   }
   LevelDesc& cl = h->lv[h->nlevels - 1];
@@ -840,7 +1113,8 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     KEq<D, double> ke;
     for (int i = 0; i < NK * NK; ++i) ke.v[i] = h->KE[i];
     stencil_kernel<D, DensitySource<D>><<<dim3(grid1(cl.nnode), H), 256, 0, st>>>(
-        DensitySource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, ke}, cl.fixed, cl.nelx, cl.nely, cl.st64);
+        DensitySource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, ke}, cl.fixed, cl.nelx, cl.nely, cl.st64, nullptr,
+        0);
   }
   return STT_OK;
 }
@@ -948,6 +1222,8 @@ static int allow_large_smem() {
                                            max_optin - (int)fa.sharedSizeBytes), "smem attr");
   };
   STT_TRY(raise_to((const void*)band_factor_kernel));
+  STT_TRY(raise_to((const void*)band_factor_tiled_kernel<2>));
+  STT_TRY(raise_to((const void*)band_factor_tiled_kernel<4>));
   STT_TRY(raise_to((const void*)coarse_inverse_kernel));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return STT_OK;
@@ -966,7 +1242,13 @@ static int build_coarse(stt_hier* h, cudaStream_t st) {
   STT_TRY(check_launch("band assemble"));
   const size_t smem = (size_t)3 * co.B * (co.B + 1) * sizeof(double);
   STT_TRY(allow_large_smem());
-  band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
+  const size_t tsmem = smem + (size_t)2 * co.B * co.B * sizeof(double);  // + two staging blocks
+  if (co.B == 32)
+    band_factor_tiled_kernel<2><<<H, 256, tsmem, st>>>(co.blocks, co.nb, h->status);
+  else if (co.B == 64)
+    band_factor_tiled_kernel<4><<<H, 256, tsmem, st>>>(co.blocks, co.nb, h->status);
+  else
+    band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
   STT_TRY(check_launch("band factor"));
   if (co.inv) {
     const size_t ism = (size_t)3 * co.B * co.B * sizeof(double);
@@ -1072,7 +1354,8 @@ extern "C" int stt_hier_level_diag(const stt_hier* h, int level, double* out, st
   const LevelDesc& lv = h->lv[level];
   cudaStream_t st = (cudaStream_t)stream;
   if (level == 0)
-    return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.rs_rho, lv.rdiag64, lv.ndof,
+    return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.rs_rho,
+                       h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof,
                        lv.fixed, out, lv.ndof, h->KE, stream);
   if (h->d == 2)
     stencil_diag_kernel<2><<<dim3(grid1(lv.nnode), h->hrows), 256, 0, st>>>(lv.st64, lv.fixed, lv.nnode, out);
