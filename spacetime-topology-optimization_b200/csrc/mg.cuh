@@ -1064,6 +1064,114 @@ __global__ void __launch_bounds__(kQThreads) restrict_kernel(
   }
 }
 
+// Restriction as restrict_kernel with the coarsening factors as template parameters
+// (constant weights, no divisions) and the next coarse row's fine rows loaded while the
+// current one is combined.
+template <int D, typename T, int KX, int KY>
+__global__ void __launch_bounds__(kQThreads) restrict_t_kernel(
+    const T* __restrict__ rf, long long f_rs, int fnnx, int fnny, T* __restrict__ rc, long long c_rs,
+    int cnnx, int cnny, const uint8_t* __restrict__ cfixed, const RowState* __restrict__ rst) {
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const T* f = rf + (size_t)s * f_rs;
+  T* o = rc + (size_t)s * c_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int C = strip * kQCols - 1 + lane;
+  const bool out_lane = lane >= 1 && lane <= kQCols && C < cnnx;
+  const bool col_ok = C >= 0 && C < cnnx;
+  const int band = (cnny + gridDim.y - 1) / gridDim.y;  // coarse rows per block (any grid.y)
+  const int R0 = blockIdx.y * band;
+  const int R1 = min(R0 + band, cnny);
+  struct FRow {
+    T v[KX][D];
+  };
+  auto fload = [&](int fr, FRow& q) {
+#pragma unroll
+    for (int j = 0; j < KX; ++j) {
+      const int fc = KX * C + j;
+      if (col_ok && fr >= 0 && fr < fnny && fc < fnnx) {
+        load_node<D, T>(f, (long long)fr * fnnx + fc, q.v[j]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) q.v[j][d] = T(0);
+      }
+    }
+  };
+  auto xpass = [&](const FRow& q, T(&g)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      if constexpr (KX == 1) {
+        g[d] = q.v[0][d];
+      } else {
+        T lo = T(0), hi = T(0);
+#pragma unroll
+        for (int j = 0; j < KX; ++j) lo += q.v[j][d] * T(1.0 - (double)j / KX);
+#pragma unroll
+        for (int j = 1; j < KX; ++j) hi += __shfl_up_sync(0xffffffffu, q.v[j][d], 1) * T((double)j / KX);
+        g[d] = lo + hi;
+      }
+    }
+  };
+  T gprev[KY][D];  // x-pass values of fine rows KY (R - 1) + j, j = 1 .. KY - 1
+#pragma unroll
+  for (int j = 0; j < KY; ++j) {
+    if (j >= 1 && R0 >= 1) {
+      FRow q;
+      fload(KY * (R0 - 1) + j, q);
+      xpass(q, gprev[j]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d) gprev[j][d] = T(0);
+    }
+  }
+  FRow q[KY];
+#pragma unroll
+  for (int j = 0; j < KY; ++j) fload(KY * R0 + j, q[j]);
+  for (int R = R0; R < R1; ++R) {
+    FRow nq[KY];
+#pragma unroll
+    for (int j = 0; j < KY; ++j) {
+      if (R + 1 < R1) {
+        fload(KY * (R + 1) + j, nq[j]);
+      } else {
+#pragma unroll
+        for (int jj = 0; jj < KX; ++jj)
+#pragma unroll
+          for (int d = 0; d < D; ++d) nq[j].v[jj][d] = T(0);
+      }
+    }
+    T gcur[KY][D];
+#pragma unroll
+    for (int j = 0; j < KY; ++j) xpass(q[j], gcur[j]);
+    if (out_lane) {
+      const uint8_t fl = __ldg(cfixed + (size_t)R * cnnx + C);
+      T v[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        if constexpr (KY == 1) {
+          v[d] = gcur[0][d];
+        } else {
+          T lo = T(0), hi = T(0);
+#pragma unroll
+          for (int j = 0; j < KY; ++j) lo += gcur[j][d] * T(1.0 - (double)j / KY);
+#pragma unroll
+          for (int j = 1; j < KY; ++j) hi += gprev[j][d] * T((double)j / KY);
+          v[d] = lo + hi;
+        }
+        if ((fl >> d) & 1) v[d] = T(0);
+      }
+      store_node<D, T>(o, (long long)R * cnnx + C, v);
+    }
+#pragma unroll
+    for (int j = 0; j < KY; ++j) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) gprev[j][d] = gcur[j][d];
+      q[j] = nq[j];
+    }
+  }
+}
+
 // ---- prolongation -----------------------------------------------------------------
 //
 // x_f += P_f (P e_c), the x pass then the y pass of torch_mg._interp_axis
@@ -1188,6 +1296,98 @@ __global__ void __launch_bounds__(kQThreads) prolong2_kernel(
     }
     store_node<D, T>(x, node, v);
    }
+  }
+}
+
+// Prolongation as prolong2_kernel with the coarsening factors as template parameters:
+// a block's band of fine rows starts on a coarse row, so the rows are walked as coarse
+// rows of KY fine rows each, with the y weights constants of the unrolled inner loop
+// (no per-row division), and NQ fine rows of x and flags in flight.
+template <int D, typename T, int KX, int KY>
+__global__ void __launch_bounds__(kQThreads) prolong_t_kernel(
+    const T* __restrict__ ec, long long c_rs, int cnnx, int cnny, T* __restrict__ xf, long long f_rs, int fnnx,
+    int fnny, const uint8_t* __restrict__ ffixed, const RowState* __restrict__ rst) {
+  constexpr int NQ = KY == 3 ? 6 : 4;  // fine rows in flight, a multiple of KY
+  constexpr int CR = NQ / KY;          // coarse rows a step
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const T* e = ec + (size_t)s * c_rs;
+  T* x = xf + (size_t)s * f_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = (blockIdx.x * kQWarps + warp) * 32 + lane;
+  const bool col_ok = c < fnnx;
+  const int C = col_ok ? c / KX : 0, jx = c - C * KX;
+  const T wx = jx == 0 ? T(0) : (jx == 1 ? T(1.0 / KX) : T(2.0 / KX));
+  const bool c1 = col_ok && jx != 0;  // needs coarse column C + 1
+  int band = (fnny + gridDim.y - 1) / gridDim.y;
+  band = (band + KY - 1) / KY * KY;  // bands start on coarse rows
+  const int r0 = blockIdx.y * band;
+  if (r0 >= fnny) return;
+  const int r1 = min(r0 + band, fnny);
+  auto crow = [&](int RR, T(&v0)[D], T(&v1)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v0[d] = v1[d] = T(0);
+    if (!col_ok || RR >= cnny) return;
+    const long long n0 = (long long)RR * cnnx + C;
+    load_node<D, T>(e, n0, v0);
+    if (c1) load_node<D, T>(e, n0 + 1, v1);
+  };
+  auto frow = [&](int rr, T(&v)[D], uint8_t& fl) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = T(0);
+    fl = 0;
+    if (!col_ok || rr >= r1) return;
+    const long long node = (long long)rr * fnnx + c;
+    load_node<D, T>(x, node, v);
+    fl = __ldg(ffixed + node);
+  };
+  int R = r0 / KY;
+  T a0[D], a1[D], b0[D], b1[D], n0[D], n1[D];  // coarse rows R, R + 1, and R + 2 in flight
+  crow(R, a0, a1);
+  crow(R + 1, b0, b1);
+  crow(R + 2, n0, n1);
+  T qx[NQ][D];
+  uint8_t qf[NQ];
+#pragma unroll
+  for (int k = 0; k < NQ; ++k) frow(r0 + k, qx[k], qf[k]);
+  for (int rb = r0; rb < r1; rb += NQ) {
+#pragma unroll
+    for (int cr = 0; cr < CR; ++cr) {
+#pragma unroll
+      for (int jy = 0; jy < KY; ++jy) {
+        const int k = cr * KY + jy;
+        const int r = rb + k;
+        T v[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[d] = qx[k][d];
+        const uint8_t fl = qf[k];
+        frow(r + NQ, qx[k], qf[k]);
+        if (col_ok && r < r1) {
+          const T wy = jy == 0 ? T(0) : (jy == 1 ? T(1.0 / KY) : T(2.0 / KY));
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            T t0 = a0[d], t1 = b0[d];
+            if (jx) {
+              t0 = a0[d] * (T(1) - wx) + a1[d] * wx;
+              t1 = b0[d] * (T(1) - wx) + b1[d] * wx;
+            }
+            const T pv = jy ? t0 * (T(1) - wy) + t1 * wy : t0;
+            if (!((fl >> d) & 1)) v[d] += pv;
+          }
+          store_node<D, T>(x, (long long)r * fnnx + c, v);
+        }
+      }
+      // advance one coarse row
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        a0[d] = b0[d];
+        a1[d] = b1[d];
+        b0[d] = n0[d];
+        b1[d] = n1[d];
+      }
+      ++R;
+      crow(R + 2, n0, n1);
+    }
   }
 }
 

@@ -288,19 +288,21 @@ __global__ void keff_from_density_kernel(const double* __restrict__ rho, long lo
 // element (D = 2: lane l holds entries l and l + 32) or per two elements (D = 1: a group of
 // 16 lanes per element): the NM tables live in registers, the first NM lanes of a group
 // load the child densities and shuffles broadcast them, and a warp's stores are 256
-// contiguous bytes.  (The per-(E, i) kernel re-reads the tables from L1 for every
-// element and is bound by it.)
+// contiguous bytes.  A warp takes U element steps at once (their density loads in flight
+// together).  Grid: (blocks, hierarchy rows).
 template <int D, int NM, bool RD>
 __global__ void __launch_bounds__(256) keff_from_density_warp_kernel(
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ reac, long long r_rs,
     const double* __restrict__ G, const double* __restrict__ GM, int fnelx, int kx, int cnelx, int cnel,
-    int H, double* __restrict__ keff) {
+    double* __restrict__ keff) {
   constexpr int NK = 4 * D, NE = NK * NK;       // 64 or 16 entries
   constexpr int GW = NE >= 32 ? 32 : NE;        // lanes per element
   constexpr int EPL = NE / GW;                  // entries per lane
   constexpr int EPW = 32 / GW;                  // elements per warp step
+  constexpr int U = 4;                          // warp steps in flight
   static_assert(NM <= GW, "the children of an element must fit its lane group");
   const int lane = threadIdx.x & 31, sub = lane / GW, gl = lane % GW;
+  const int h = blockIdx.y;
   double g[NM][EPL], gm[RD ? NM : 1][EPL];
 #pragma unroll
   for (int m = 0; m < NM; ++m)
@@ -310,40 +312,46 @@ __global__ void __launch_bounds__(256) keff_from_density_warp_kernel(
       if constexpr (RD) gm[m][k] = __ldg(GM + (size_t)m * NE + gl + GW * k);
     }
   const int ky = NM / kx;
-  const long long total = (long long)H * cnel;
-  const long long nw = (long long)gridDim.x * (blockDim.x / 32);
-  for (long long base = (blockIdx.x * (long long)(blockDim.x / 32) + threadIdx.x / 32) * EPW; base < total;
-       base += nw * EPW) {  // the same trip count for every lane of the warp
-    const long long idx = base + sub;
-    const bool ok = idx < total;
-    const int h = ok ? (int)(idx / cnel) : 0;
-    const int E = ok ? (int)(idx - (long long)h * cnel) : 0;
-    const int R = E / cnelx, C = E - R * cnelx;
-    double rv = 0.0, av = 0.0;
-    if (ok && gl < NM) {
-      const int my = gl / kx, mx = gl - my * kx;
-      const size_t fe = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
-      rv = __ldg(rho + (size_t)h * rho_rs + fe);
-      if constexpr (RD) av = __ldg(reac + (size_t)h * r_rs + fe);
-    }
-    double acc[EPL];
+  const int my = gl / kx, mx = gl - my * kx;
+  const double* rr = rho + (size_t)h * rho_rs;
+  const double* ar = RD ? reac + (size_t)h * r_rs : nullptr;
+  double* kh = keff + (size_t)h * cnel * NE;
+  const int nw = gridDim.x * (blockDim.x / 32);
+  const int w0 = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  for (int base = w0 * U * EPW; base < cnel; base += nw * U * EPW) {  // uniform per warp
+    double rv[U], av[U];
 #pragma unroll
-    for (int k = 0; k < EPL; ++k) acc[k] = 0.0;
-#pragma unroll
-    for (int m = 0; m < NM; ++m) {
-      const double r = __shfl_sync(0xffffffffu, rv, sub * GW + m);
-#pragma unroll
-      for (int k = 0; k < EPL; ++k) acc[k] = fma(r, g[m][k], acc[k]);
-      if constexpr (RD) {
-        const double a = __shfl_sync(0xffffffffu, av, sub * GW + m);
-#pragma unroll
-        for (int k = 0; k < EPL; ++k) acc[k] = fma(a, gm[m][k], acc[k]);
+    for (int u = 0; u < U; ++u) {
+      const int E = base + u * EPW + sub;
+      rv[u] = av[u] = 0.0;
+      if (E < cnel && gl < NM) {
+        const int R = E / cnelx, C = E - R * cnelx;
+        const size_t fe = (size_t)(R * ky + my) * fnelx + (C * kx + mx);
+        rv[u] = __ldg(rr + fe);
+        if constexpr (RD) av[u] = __ldg(ar + fe);
       }
     }
-    if (ok) {
-      double* out = keff + ((size_t)h * cnel + E) * NE + gl;
 #pragma unroll
-      for (int k = 0; k < EPL; ++k) out[GW * k] = acc[k];
+    for (int u = 0; u < U; ++u) {
+      const int E = base + u * EPW + sub;
+      double acc[EPL];
+#pragma unroll
+      for (int k = 0; k < EPL; ++k) acc[k] = 0.0;
+#pragma unroll
+      for (int m = 0; m < NM; ++m) {
+        const double r = __shfl_sync(0xffffffffu, rv[u], sub * GW + m);
+#pragma unroll
+        for (int k = 0; k < EPL; ++k) acc[k] = fma(r, g[m][k], acc[k]);
+        if constexpr (RD) {
+          const double a = __shfl_sync(0xffffffffu, av[u], sub * GW + m);
+#pragma unroll
+          for (int k = 0; k < EPL; ++k) acc[k] = fma(a, gm[m][k], acc[k]);
+        }
+      }
+      if (E < cnel) {
+#pragma unroll
+        for (int k = 0; k < EPL; ++k) kh[(size_t)E * NE + gl + GW * k] = acc[k];
+      }
     }
   }
 }
@@ -1084,15 +1092,17 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
         const LevelDesc& f0 = h->lv[0];
         const int KX = f0.kx * f.kx, KY = f0.ky * f.ky;
         if (KX * KY == 16) {
-          constexpr int per_block = D == 2 ? 8 : 16;  // elements a 256-thread block takes a step
-          const long long blocks = std::min<long long>((H * c.nel + per_block - 1) / per_block, 148LL * 8);
+          // about four resident blocks' worth a row, at least one warp step per warp
+          const long long per_block = 8LL * 4 * (D == 2 ? 1 : 2);  // elements a block takes per step
+          const long long want = std::max<long long>(1, 148LL * 4 / H);
+          const dim3 kg((unsigned)std::min<long long>(want, (c.nel + per_block - 1) / per_block), H);
           if (reaction)
-            keff_from_density_warp_kernel<D, 16, true><<<(int)blocks, 256, 0, st>>>(
+            keff_from_density_warp_kernel<D, 16, true><<<kg, 256, 0, st>>>(
                 l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables, h->gtables + kGrandStride, f0.nelx, KX, c.nelx,
-                (int)c.nel, H, kc);
+                (int)c.nel, kc);
           else
-            keff_from_density_warp_kernel<D, 16, false><<<(int)blocks, 256, 0, st>>>(
-                l0.rho64, l0.rs_rho, nullptr, 0, h->gtables, nullptr, f0.nelx, KX, c.nelx, (int)c.nel, H, kc);
+            keff_from_density_warp_kernel<D, 16, false><<<kg, 256, 0, st>>>(
+                l0.rho64, l0.rs_rho, nullptr, 0, h->gtables, nullptr, f0.nelx, KX, c.nelx, (int)c.nel, kc);
         } else {
           keff_from_density_kernel<D><<<g, 256, 0, st>>>(l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables,
                                                          h->gtables + kGrandStride, f0.nelx, KX, KY, c.nelx,

@@ -20,6 +20,20 @@ namespace stt {
 
 constexpr int kEwThreads = 256;
 
+// Calls M(KX, KY) for the coarsening factors (kx, ky), each 1, 2 or 3; else runs FALLBACK.
+#define STT_KXKY_DISPATCH(kx, ky, M, FALLBACK)   \
+  do {                                          \
+    if ((kx) == 2 && (ky) == 2) M(2, 2);         \
+    else if ((kx) == 2 && (ky) == 3) M(2, 3);    \
+    else if ((kx) == 3 && (ky) == 2) M(3, 2);    \
+    else if ((kx) == 3 && (ky) == 3) M(3, 3);    \
+    else if ((kx) == 1 && (ky) == 2) M(1, 2);    \
+    else if ((kx) == 2 && (ky) == 1) M(2, 1);    \
+    else if ((kx) == 1 && (ky) == 3) M(1, 3);    \
+    else if ((kx) == 3 && (ky) == 1) M(3, 1);    \
+    else FALLBACK;                               \
+  } while (0)
+
 static int grid1(long long n, int bs = 256) {
   long long g = (n + bs - 1) / bs;
   if (g > (1 << 30)) g = 1 << 30;
@@ -162,6 +176,30 @@ struct Cycle {
     }
   }
 
+  // Restriction of the fine residual rf into the coarse right-hand side, and the
+  // prolongation of the coarse correction ec added into xf, with the level's coarsening
+  // factors as template parameters (every combination of 1, 2 and 3).
+  void transfer_down(const LevelDesc& lv, const LevelDesc& cl, const T* rf, long long nd, T* rc, long long cnd) {
+    const dim3 g = coarse_grid(cl.nelx, cl.nely, nrows);
+#define STT_RESTRICT(KX, KY)                                                                       \
+  restrict_t_kernel<D, T, KX, KY><<<g, kQThreads, 0, st>>>(rf, nd, lv.nnx, lv.nny, rc, cnd, cl.nnx, \
+                                                           cl.nny, cl.fixed, rst)
+    STT_KXKY_DISPATCH(lv.kx, lv.ky, STT_RESTRICT,
+                      (restrict_kernel<D, T><<<g, kQThreads, 0, st>>>(rf, nd, lv.nnx, lv.nny, rc, cnd, cl.nnx,
+                                                                      cl.nny, lv.kx, lv.ky, cl.fixed, rst)));
+#undef STT_RESTRICT
+  }
+  void transfer_up(const LevelDesc& lv, const LevelDesc& cl, const T* ec, long long cnd, T* xf, long long nd) {
+    const dim3 g = prolong2_grid(lv.nnx, lv.nny, nrows);
+#define STT_PROLONG(KX, KY)                                                                         \
+  prolong_t_kernel<D, T, KX, KY><<<g, kQThreads, 0, st>>>(ec, cnd, cl.nnx, cl.nny, xf, nd, lv.nnx, lv.nny, \
+                                                          lv.fixed, rst)
+    STT_KXKY_DISPATCH(lv.kx, lv.ky, STT_PROLONG,
+                      (prolong2_kernel<D, T><<<g, kQThreads, 0, st>>>(ec, cnd, cl.nnx, cl.nny, xf, nd, lv.nnx,
+                                                                      lv.nny, lv.kx, lv.ky, lv.fixed, rst)));
+#undef STT_PROLONG
+  }
+
   // One smoother / residual / apply pass at level l: out = op(x, b); SW_POST reads
   // x + P(pro.ec) (the coarse correction) in place of x.
   template <int MODE>
@@ -291,11 +329,9 @@ struct Cycle {
     const LevelDesc& cl = h->lv[l + 1];
     const long long cnd = vstride(cl.ndof);
     T* bc = (T*)w.b[l + 1];
-    restrict_kernel<D, T><<<coarse_grid(cl.nelx, cl.nely, nrows), kQThreads, 0, st>>>(
-        xb, nd, lv.nnx, lv.nny, bc, cnd, cl.nnx, cl.nny, lv.kx, lv.ky, cl.fixed, rst);
+    transfer_down(lv, cl, xb, nd, bc, cnd);
     T* ec = coarse_correction(l, bc);
-    prolong2_kernel<D, T><<<prolong2_grid(lv.nnx, lv.nny, nrows), kQThreads, 0, st>>>(
-        ec, cnd, cl.nnx, cl.nny, xa, nd, lv.nnx, lv.nny, lv.kx, lv.ky, lv.fixed, rst);
+    transfer_up(lv, cl, ec, cnd, xa, nd);
     // post-smoothing; level 0's last sweep writes straight into final_out when given
     for (int k = 0; k < n_smooth; ++k) {
       T* dst = (l == 0 && final_out && k == n_smooth - 1) ? final_out : xb;
