@@ -421,6 +421,137 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
   }
 }
 
+// ---- level 0: post-smoothing in one pass (modal form, n_smooth = 2) -------------------
+//
+// The two post-smoothing sweeps after the prolongation, chained like l0_presmooth_kernel:
+//   x1 = x0 + omega (b - A x0) / D;  x2 = x1 + omega (b - A x1) / D.  Writes x2.
+// x0 (the prolonged iterate) is loaded with the front row; stage A sweeps at row f - 1,
+// stage B at row f - 2.  Lanes 2..29 are output (28 columns a warp).  Per node the
+// arithmetic is the unfused sweeps'.
+constexpr int kPostCols = 28;
+
+inline dim3 postsmooth_grid(int nelx, int nely, int rows) {
+  const int strips = (nelx + 1 + kPostCols - 1) / kPostCols;
+  return dim3((strips + kQWarps - 1) / kQWarps, (nely + 1 + kQRows - 1) / kQRows, rows);
+}
+
+template <int D, typename T, bool RD, int AHEAD = 2>
+__global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmooth_kernel(
+    const T* __restrict__ x0, long long x_rs, const T* __restrict__ b, long long b_rs, T* __restrict__ out,
+    long long o_rs, const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag, long long rd_rs,
+    const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows,
+    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q) {
+  constexpr int LO = 2, HI = 29;
+  static_assert(HI - LO + 1 == kPostCols, "strip width");
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int h = hier_row(row_map, hrows, s);
+  const T* rh = rho + (size_t)h * rho_rs;
+  const T* rdh = RD ? rdiag + (size_t)h * rd_rs : nullptr;
+  const T* xs = x0 + (size_t)s * x_rs;
+  const T* bs = b + (size_t)s * b_rs;
+  T* os = out + (size_t)s * o_rs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kPostCols - LO + lane;
+  const bool out_lane = lane >= LO && lane <= HI && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const bool ecol_ok = c >= 0 && c < nelx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  struct Front {
+    FrontRow<D, T, RD> F;
+    T x[D];
+  };
+  auto load_front = [&](int f, Front& Q) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) Q.F.b[d] = Q.x[d] = T(0);
+    if constexpr (RD) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) Q.F.rd[d] = T(0);
+    }
+    Q.F.fl = 0;
+    Q.F.rho = (ecol_ok && f >= 0 && f < nely) ? __ldg(rh + (size_t)f * nelx + c) : T(0);
+    if (!col_ok || f < 0 || f >= nny) return;
+    const long long node = (long long)f * nnx + c;
+    Q.F.fl = __ldg(fixed + node);
+    load_node<D, T>(bs, node, Q.F.b);
+    load_node<D, T>(xs, node, Q.x);
+    if constexpr (RD) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) Q.F.rd[d] = __ldg(rdh + node * D + d);
+    }
+  };
+  ModalStage<D, T> A, B;
+  A.reset();
+  B.reset();
+  DelayRow<D, T, RD> d1{}, d2{};  // rows f - 1 and f - 2
+  const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
+  T rho_prev = (ecol_ok && f0 - 1 >= 0 && f0 - 1 < nely) ? __ldg(rh + (size_t)(f0 - 1) * nelx + c) : T(0);
+  Front qf[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) load_front(f0 + k, qf[k]);
+  for (int fb = f0; fb <= f1; fb += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int f = fb + k;
+      const Front Q = qf[k];
+      load_front(f + AHEAD, qf[k]);
+      DelayRow<D, T, RD> cur;
+      {
+        const T rs = Q.F.rho + rho_prev;
+        const T dsum = rs + __shfl_up_sync(0xffffffffu, rs, 1);
+        cur.dg[0] = q.kd0 * dsum;
+        if constexpr (D == 2) cur.dg[1] = q.kd1 * dsum;
+      }
+      rho_prev = Q.F.rho;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        cur.b[d] = Q.F.b[d];
+        if constexpr (RD) cur.rd[d] = Q.F.rd[d];
+      }
+      cur.rho = Q.F.rho;
+      cur.fl = Q.F.fl;
+      // stage A: element row f - 1 -> first sweep at node row f - 1
+      T KA[D], xa[D], xo_a[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
+      A.step(q, Q.x, d1.rho, KA);
+      {
+        T rd1[D], dg[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          rd1[d] = RD ? d1.rd[d] : T(0);
+          dg[d] = d1.dg[d];
+        }
+        l0_result<D, T, SW_SWEEP>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
+        if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
+#pragma unroll
+          for (int d = 0; d < D; ++d) xa[d] = T(0);
+        }
+      }
+      // stage B: element row f - 2 -> second sweep at node row f - 2
+      T KB[D], xb[D], xo_b[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
+      B.step(q, xa, d2.rho, KB);
+      {
+        T rd2[D], dg[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          rd2[d] = RD ? d2.rd[d] : T(0);
+          dg[d] = d2.dg[d];
+        }
+        l0_result<D, T, SW_SWEEP>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, xb);
+      }
+      if (out_lane && f - 2 >= r0 && f - 2 < r1) store_node<D, T>(os, (long long)(f - 2) * nnx + c, xb);
+      d2 = d1;
+      d1 = cur;
+    }
+  }
+}
+
 // Rows a block marches on the coarse levels: 32 where the grid then fills the GPU,
 // shorter bands on small grids (the heat solve's single row, the coarse levels), whose
 // launches are otherwise latency-bound by the sequential march down 32 rows.  The

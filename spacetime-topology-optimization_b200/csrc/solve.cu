@@ -273,6 +273,20 @@ struct Cycle {
 #undef STT_PRE
   }
 
+  // Level 0's two post-smoothing sweeps in one pass: x0 (the prolonged iterate) -> out.
+  void postsmooth(const T* x0, const T* b, long long b_rs, T* out) {
+    const LevelDesc& lv = h->lv[0];
+    const long long nd = vstride(lv.ndof);
+    const dim3 g = postsmooth_grid(lv.nelx, lv.nely, nrows);
+#define STT_POST(RD)                                                                                  \
+  l0_postsmooth_kernel<D, T, RD><<<g, kQThreads, 0, st>>>(x0, nd, b, b_rs, out, nd, rho0(), lv.rs_rho,     \
+                                                        rdiag0(), lv.ndof, lv.fixed, h->row_map, h->hrows, \
+                                                        rst, lv.nelx, lv.nely, omega, mq)
+    if (h->has_reaction) STT_POST(true);
+    else STT_POST(false);
+#undef STT_POST
+  }
+
   // The correction from level l + 1 for its right-hand side bc (gamma visits).
   T* coarse_correction(int l, T* bc) {
     const LevelDesc& cl = h->lv[l + 1];
@@ -333,6 +347,13 @@ struct Cycle {
     T* ec = coarse_correction(l, bc);
     transfer_up(lv, cl, ec, cnd, xa, nd);
     // post-smoothing; level 0's last sweep writes straight into final_out when given
+    if (modal0 && n_smooth == 2) {
+      // the fused pass reads b a few rows ahead of its writes, so it never writes over b
+      // (an in-place V-cycle, z = r, goes through xb and the final copy)
+      T* dst = (final_out && final_out != b) ? final_out : xb;
+      postsmooth(xa, b, b_rs, dst);
+      return dst;
+    }
     for (int k = 0; k < n_smooth; ++k) {
       T* dst = (l == 0 && final_out && k == n_smooth - 1) ? final_out : xb;
       pass<SW_SWEEP>(l, xa, nd, b, b_rs, dst, nd);
