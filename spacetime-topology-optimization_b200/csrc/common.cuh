@@ -131,6 +131,14 @@ STT_DEV void grid_reduce(const GridRed& g, int row, int bid, const double (&v)[K
 
 STT_DEV double safe_div(double num, double den) { return den != 0.0 ? num / den : 0.0; }
 
+// Signs of the six plane-stress edge modes (Gx(ux), Gy(uy), Gy(ux), Gx(uy), H(ux), H(uy))
+// under the x and the y reflection of an element: the Gx and H patterns change sign under
+// x, Gy and H under y, and so do ux under x and uy under y.
+__host__ __device__ constexpr int mode_dx(int i) { return (i == 2 || i == 3 || i == 5) ? -1 : 1; }
+__host__ __device__ constexpr int mode_dy(int i) { return (i == 2 || i == 3 || i == 4) ? -1 : 1; }
+constexpr double kModeDX[6] = {1, 1, -1, -1, 1, -1};
+constexpr double kModeDY[6] = {1, 1, -1, -1, -1, 1};
+
 // n / k and n % k for the coarsening factors k in {1, 2, 3} and 0 <= n < 2^30, without
 // an integer division (0x55555556 = ceil(2^32 / 3) gives floor(n / 3) exactly there).
 STT_DEV int div_k(int n, int k) {

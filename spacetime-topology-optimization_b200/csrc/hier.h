@@ -55,6 +55,7 @@ struct stt_hier_impl {
   double mq[8];
   int l1;            // level 1 is applied from the level-0 densities (l1_sweep_kernel)
   double l1m[9][21]; // per child m of a level-1 element: T G_m T^T / 16, packed upper triangle
+  int l1par;         // 2 x 2 children whose M_m are mirror images of M_0 (l1_mirror_classes)
   double* tables;    // device: per transition S[9][64], G[9][64], GM[9][64]
   double* gtables;   // device: level-0 grandchildren of a level-2 element, H[81][64], HM[81][64]
   double* keffA;     // build temporaries: element matrices of levels 3, 5, ...

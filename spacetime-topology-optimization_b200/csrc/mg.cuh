@@ -932,12 +932,15 @@ struct L1Mat {
   T m[NM][21];  // packed upper triangle, row-major
 };
 
-template <typename T, int MODE, int KX, int KY, int AHEAD = 2>
+// MIR (2 x 2 children whose M_m mirror M_0): M = sum_m rho_m M_m takes four signed
+// density sums and one product per entry, M[e] = M_0[e] (rho_00 + sx rho_10 + sy rho_01
+// + sx sy rho_11), instead of four multiply-adds per entry.
+template <typename T, int MODE, int KX, int KY, int AHEAD = 2, bool MIR = false>
 __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
     const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
     const T* __restrict__ rho0, long long rho_rs, int fnelx, const T* __restrict__ st,
     const uint8_t* __restrict__ fixed, int nnx, int nny, const int* __restrict__ row_map, int hrows,
-    const RowState* __restrict__ rst, T omega, L1Mat<T, KX * KY> M) {
+    const RowState* __restrict__ rst, T omega, L1Mat<T, MIR ? 1 : KX * KY> M) {
   static_assert(MODE == SW_SWEEP || MODE == SW_RESID, "sweep and residual only");
   constexpr int D = 2, NM = KX * KY;
   const int s = blockIdx.z;
@@ -1005,12 +1008,25 @@ __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
     md[4] = dT[0] - dB[0];  // H(ux)
     md[5] = dT[1] - dB[1];  // H(uy)
     T Me[21];
+    if constexpr (MIR && NM == 4) {
+      const T p0 = rm[0] + rm[1], p1 = rm[0] - rm[1], q0 = rm[2] + rm[3], q1 = rm[2] - rm[3];
+      const T cpp = p0 + q0, cmp = p1 + q1, cpm = p0 - q0, cmm = p1 - q1;  // (sx, sy) = (+,+), (-,+), ...
+      int e = 0;
 #pragma unroll
-    for (int e = 0; e < 21; ++e) {
-      T a = rm[0] * M.m[0][e];
+      for (int i = 0; i < 6; ++i)
 #pragma unroll
-      for (int m = 1; m < NM; ++m) a = fma(rm[m], M.m[m][e], a);
-      Me[e] = a;
+        for (int j = i; j < 6; ++j, ++e) {
+          const bool sxn = mode_dx(i) * mode_dx(j) < 0, syn = mode_dy(i) * mode_dy(j) < 0;
+          Me[e] = M.m[0][e] * (sxn ? (syn ? cmm : cmp) : (syn ? cpm : cpp));
+        }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 21; ++e) {
+        T a = rm[0] * M.m[0][e];
+#pragma unroll
+        for (int m = 1; m < NM; ++m) a = fma(rm[m], M.m[m][e], a);
+        Me[e] = a;
+      }
     }
     T q[6];
 #pragma unroll

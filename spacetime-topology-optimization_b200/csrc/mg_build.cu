@@ -97,6 +97,26 @@ static void grand_table(const double* S1, const double* G, int kx0, int ky0, int
     }
 }
 
+// For 2 x 2 children (m = my * 2 + mx): true when each M_m is the mirror image of M_0,
+// M_m[i][j] = sx^mx sy^my M_0[i][j] with sx = DX_i DX_j, sy = DY_i DY_j and DX / DY the
+// modes' signs under the x / y reflection of the element (l1_sweep_kernel's mirror path;
+// the reference's plane-stress KE and the bilinear interpolation have this symmetry).
+static bool l1_mirror_classes(const double (*m)[21]) {
+  double big = 0.0;
+  for (int e = 0; e < 21; ++e) big = std::max(big, std::fabs(m[0][e]));
+  for (int c = 1; c < 4; ++c) {
+    const int mx = c & 1, my = c >> 1;
+    int e = 0;
+    for (int i = 0; i < 6; ++i)
+      for (int j = i; j < 6; ++j, ++e) {
+        const double sx = kModeDX[i] * kModeDX[j], sy = kModeDY[i] * kModeDY[j];
+        const double want = (mx ? sx : 1.0) * (my ? sy : 1.0) * m[0][e];
+        if (std::fabs(m[c][e] - want) > 1e-12 * big) return false;
+      }
+  }
+  return true;
+}
+
 // M_m = T G_m T^T / 16 for the nm plane-stress child matrices G (8 x 8 each), packed as
 // the upper triangle of the symmetric 6 x 6 (row-major, i <= j); mode order Gx(ux),
 // Gy(uy), Gy(ux), Gx(uy), H(ux), H(uy) as modal_from_ke.  False unless T^T M_m T
@@ -1031,8 +1051,10 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
   // bilinear edge modes (q4.cuh); kept when M_m rebuilds G_m to 1e-12 (plane stress, no
   // reaction, 2 or 3 children a direction, level 1 not the coarsest)
   h->l1 = 0;
+  h->l1par = 0;
   if (D == 2 && h->modal && !reaction && h->nlevels > 2 && h->lv[0].kx >= 2 && h->lv[0].ky >= 2)
     h->l1 = l1_tables(&tab[kTableStride], h->lv[0].kx * h->lv[0].ky, h->l1m) ? 1 : 0;
+  if (h->l1 && h->lv[0].kx == 2 && h->lv[0].ky == 2) h->l1par = l1_mirror_classes(h->l1m) ? 1 : 0;
 
   // level 1's stencil tables (after the two grandchild tables)
   if (h->nlevels > 1) {

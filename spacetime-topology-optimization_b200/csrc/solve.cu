@@ -166,7 +166,13 @@ struct Cycle {
                                                               f.nelx, stl(1), lv.fixed, lv.nnx, lv.nny,  \
                                                               h->row_map, h->hrows, rst, omega, M);      \
   } while (0)
-      if (f.kx == 2 && f.ky == 2) STT_L1(2, 2);
+      if (f.kx == 2 && f.ky == 2 && h->l1par) {
+        L1Mat<T, 1> M;  // M_0 only
+        for (int e = 0; e < 21; ++e) M.m[0][e] = T(h->l1m[0][e]);
+        l1_sweep_kernel<T, MODE, 2, 2, 2, true><<<g, kQThreads, 0, st>>>(
+            x, b, out, vstride(lv.ndof), r0, f.rs_rho, f.nelx, stl(1), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows,
+            rst, omega, M);
+      } else if (f.kx == 2 && f.ky == 2) STT_L1(2, 2);
       else if (f.kx == 2 && f.ky == 3) STT_L1(2, 3);
       else if (f.kx == 3 && f.ky == 2) STT_L1(3, 2);
       else if (f.kx == 3 && f.ky == 3) STT_L1(3, 3);
