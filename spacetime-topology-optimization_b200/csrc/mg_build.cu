@@ -1232,7 +1232,132 @@ __global__ void __launch_bounds__(256) coarse_inverse_kernel(const double* __res
   }
 }
 
-// The dynamic shared-memory ceiling of the coarse kernels, raised once per device to the
+// coarse_inverse_kernel for B = 16 NA (NA = 2, 4) with register-tiled products (thread
+// (ty, tx) owns entries (ty + 16 a, tx + 16 b), as band_factor_tiled_kernel), computing only
+// the block rows k >= kc of column block kc: A^{-1} is symmetric, so coarse_mirror_kernel
+// fills the blocks above the diagonal from their transposes afterwards.
+template <int NA>
+__global__ void __launch_bounds__(256) coarse_inverse_tiled_kernel(const double* __restrict__ blocks, int nb,
+                                                                   double* __restrict__ inv) {
+  constexpr int B = 16 * NA, ld = B + 1;
+  extern __shared__ double sm[];
+  double* Y = sm;           // the current block of the solution (ld)
+  double* R = Y + B * ld;   // right-hand side of the step
+  double* M = R + B * ld;   // the step's matrix
+  const int kc = blockIdx.x, h = blockIdx.y;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const long long np = (long long)nb * B;
+  const double* bh = blocks + (size_t)h * nb * 4 * B * B;
+  double* ih = inv + (size_t)h * np * np;
+  auto load = [&](const double* src, double* dst) {
+    for (int t = tid; t < B * B; t += 256) dst[(t / B) * ld + t % B] = src[t];
+  };
+  // acc = A src over this thread's tile
+  auto mm = [&](const double* A, const double* src, double (&acc)[NA][NA]) {
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NA; ++b) acc[a][b] = 0.0;
+#pragma unroll 4
+    for (int l = 0; l < B; ++l) {
+      double ai[NA], sj[NA];
+#pragma unroll
+      for (int a = 0; a < NA; ++a) ai[a] = A[(ty + 16 * a) * ld + l];
+#pragma unroll
+      for (int b = 0; b < NA; ++b) sj[b] = src[l * ld + tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) acc[a][b] = fma(ai[a], sj[b], acc[a][b]);
+    }
+  };
+  auto park_ptr = [&](int k, int i, int j) { return ih + ((size_t)k * B + i) * np + (size_t)kc * B + j; };
+  double acc[NA][NA];
+  // forward: Y_k = Dinv_k (I_k - E_k Y_{k-1}), k = kc .. nb - 1
+  for (int k = kc; k < nb; ++k) {
+    if (k == kc) {
+      for (int t = tid; t < B * B; t += 256) R[(t / B) * ld + t % B] = (t / B == t % B) ? 1.0 : 0.0;
+    } else {
+      load(bh + ((size_t)k * 4 + 2) * B * B, M);  // E_k
+      __syncthreads();
+      mm(M, Y, acc);
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) R[(ty + 16 * a) * ld + tx + 16 * b] = -acc[a][b];
+    }
+    __syncthreads();
+    load(bh + ((size_t)k * 4 + 0) * B * B, M);  // Dinv_k
+    __syncthreads();
+    mm(M, R, acc);
+    __syncthreads();  // everyone has read Y (the E_k product) and R
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NA; ++b) {
+        const int i = ty + 16 * a, j = tx + 16 * b;
+        Y[i * ld + j] = acc[a][b];
+        *park_ptr(k, i, j) = acc[a][b];
+      }
+    __syncthreads();
+  }
+  // backward: X_k = Dinv_k^T (Y_k - E_{k+1}^T X_{k+1}), k = nb - 1 .. kc (Y holds X_{k+1})
+  for (int k = nb - 1; k >= kc; --k) {
+    double rv[NA][NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NA; ++b) rv[a][b] = *park_ptr(k, ty + 16 * a, tx + 16 * b);
+    if (k < nb - 1) {
+      load(bh + ((size_t)(k + 1) * 4 + 3) * B * B, M);  // E_{k+1}^T
+      __syncthreads();
+      mm(M, Y, acc);
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NA; ++b) rv[a][b] -= acc[a][b];
+    }
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NA; ++b) R[(ty + 16 * a) * ld + tx + 16 * b] = rv[a][b];
+    __syncthreads();
+    load(bh + ((size_t)k * 4 + 1) * B * B, M);  // Dinv_k^T
+    __syncthreads();
+    mm(M, R, acc);
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NA; ++b) {
+        const int i = ty + 16 * a, j = tx + 16 * b;
+        Y[i * ld + j] = acc[a][b];
+        *park_ptr(k, i, j) = acc[a][b];
+      }
+    __syncthreads();
+  }
+}
+
+// inv[r][c] = inv[c][r] for the block rows above the diagonal block (row block < column
+// block), a 32 x 32 tile through shared memory per CTA (reads and writes coalesced).
+// Grid: (np / 32, np / 32, rows); tiles wholly below the block diagonal return at once.
+__global__ void __launch_bounds__(256) coarse_mirror_kernel(double* __restrict__ inv, int B, long long np) {
+  __shared__ double tile[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;  // destination tile (rows r0.., cols c0..)
+  if (r0 / B >= (c0 + 31) / B) return;                    // no destination entry above the block diagonal
+  double* ih = inv + (size_t)blockIdx.z * np * np;
+  for (int j = threadIdx.y; j < 32; j += 8) {  // source rows c0 + j, columns r0 + threadIdx.x
+    const long long sr = c0 + j, sc = r0 + threadIdx.x;
+    tile[j][threadIdx.x] = (sr < np && sc < np) ? ih[sr * np + sc] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const long long r = r0 + i, c = c0 + threadIdx.x;
+    if (r < np && c < np && r / B < c / B) ih[r * np + c] = tile[threadIdx.x][i];
+  }
+}
+
+// The dynamic shared-memory ceiling of the coarse kernels, raised once per device to the// The dynamic shared-memory ceiling of the coarse kernels, raised once per device to the
 // device's opt-in maximum.  (Setting it per call to the call's own size raced between
 // host threads building hierarchies of different block sizes: a launch could meet
 // another thread's smaller ceiling and fail.)
@@ -1257,6 +1382,8 @@ static int allow_large_smem() {
   STT_TRY(raise_to((const void*)band_factor_tiled_kernel<2>));
   STT_TRY(raise_to((const void*)band_factor_tiled_kernel<4>));
   STT_TRY(raise_to((const void*)coarse_inverse_kernel));
+  STT_TRY(raise_to((const void*)coarse_inverse_tiled_kernel<2>));
+  STT_TRY(raise_to((const void*)coarse_inverse_tiled_kernel<4>));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return STT_OK;
 }
@@ -1283,8 +1410,19 @@ static int build_coarse(stt_hier* h, cudaStream_t st) {
     band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
   STT_TRY(check_launch("band factor"));
   if (co.inv) {
-    const size_t ism = (size_t)3 * co.B * co.B * sizeof(double);
-    coarse_inverse_kernel<<<dim3(co.nb, H), 256, ism, st>>>(co.blocks, co.B, co.nb, co.inv);
+    if (co.B == 32 || co.B == 64) {
+      const size_t tsm = (size_t)3 * co.B * (co.B + 1) * sizeof(double);
+      if (co.B == 32)
+        coarse_inverse_tiled_kernel<2><<<dim3(co.nb, H), 256, tsm, st>>>(co.blocks, co.nb, co.inv);
+      else
+        coarse_inverse_tiled_kernel<4><<<dim3(co.nb, H), 256, tsm, st>>>(co.blocks, co.nb, co.inv);
+      const long long np = (long long)co.nb * co.B;
+      const unsigned nt = (unsigned)((np + 31) / 32);
+      coarse_mirror_kernel<<<dim3(nt, nt, H), dim3(32, 8), 0, st>>>(co.inv, co.B, np);
+    } else {
+      const size_t ism = (size_t)3 * co.B * co.B * sizeof(double);
+      coarse_inverse_kernel<<<dim3(co.nb, H), 256, ism, st>>>(co.blocks, co.B, co.nb, co.inv);
+    }
     STT_TRY(check_launch("coarse inverse"));
   }
   return STT_OK;

@@ -183,6 +183,25 @@ def test_vcycle_matches_oracle_and_is_spd(m, gamma):
     assert np.all(Mu[~mask] == 0.0)
 
 
+@pytest.mark.parametrize("nelx,nely,mce", [(64, 32, 700), (96, 48, 700), (48, 36, 20)])
+def test_vcycle_fp32_matches_fp64(m, nelx, nely, mce):
+    """The mixed-precision cycle (FP32 smoothing and transfers, the coarsest level solved
+    by its explicit FP64 inverse) against the FP64 cycle (block Cholesky solves), on
+    coarse matrices of band widths 32 and 64: agreement to FP32 rounding."""
+    rng = np.random.default_rng(7)
+    x = rng.uniform(1e-3, 1.0, nelx * nely)
+    F, mask = O.cantilever_point_load(nelx, nely)
+    M64 = m.mg.VCycle(_levels(m, nelx, nely, x, mask, mce))
+    M32 = m.mg.VCycle(_levels(m, nelx, nely, x, mask, mce, precision="mixed"))
+    u = O.project(rng.standard_normal((3, len(F))), mask)
+    z64, z32 = M64(T(u)).cpu().numpy(), M32(T(u)).cpu().numpy()
+    assert rel_err(z32, z64) < 1e-4
+    # and the inverse is symmetric: M is symmetric to FP32 rounding
+    v = O.project(rng.standard_normal(len(F)), mask)
+    a, b = M32(T(u[0])).cpu().numpy() @ v, u[0] @ M32(T(v)).cpu().numpy()
+    assert abs(a - b) <= 1e-4 * abs(a)
+
+
 def test_mbb_config_solve_compliance_and_sensitivities(m):
     """120 x 40 MBB, rho = 0.5: U, iterations, compliance, dc/dx vs the reference."""
     g = golden("mbb120x40")
