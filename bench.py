@@ -275,20 +275,30 @@ def main():
         if world > 1:
             torch.distributed.barrier()
 
+    def device_allocs():
+        st = torch.cuda.memory_stats(dev)
+        return int(st.get("num_device_alloc", 0))
+
     # timed region: inputs resident in HBM
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     with ClockSampler(local) as clk:
         barrier()
         torch.cuda.synchronize()
+        allocs0 = device_allocs()
         start.record()
-        for _ in range(args.steps):
+        for k in range(args.steps):
+            marks[k].record()
             torch.cuda.nvtx.range_push("timed_step")  # lets a profiler select one step's launches
             out = step(x, w)
             torch.cuda.nvtx.range_pop()
+        marks[-1].record()
         end.record()
         torch.cuda.synchronize()
         barrier()
     elapsed_ms = start.elapsed_time(end)
+    timed_detail = {"step_ms": [round(marks[k].elapsed_time(marks[k + 1]), 3) for k in range(args.steps)],
+                    "device_allocs": device_allocs() - allocs0}
     if world > 1:
         t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -312,17 +322,23 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    emarks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    allocs0 = device_allocs()
     e0.record()
-    for _ in range(args.steps):
+    for k in range(args.steps):
+        emarks[k].record()
         xd.copy_(xh, non_blocking=True)
         wd.copy_(wh, non_blocking=True)
         o = step(xd, wd)
         gh.copy_(o["gradient"], non_blocking=True)
         oh.copy_(o["objective"].reshape(1), non_blocking=True)
+    emarks[-1].record()
     e1.record()
     torch.cuda.synchronize()
     barrier()
     e2e_ms = e0.elapsed_time(e1)
+    e2e_detail = {"step_ms": [round(emarks[k].elapsed_time(emarks[k + 1]), 3) for k in range(args.steps)],
+                  "device_allocs": device_allocs() - allocs0}
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -374,7 +390,8 @@ def main():
             "iterations": iters,
             "clocks": clk.summary(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "full_gradient_ms": e2e_ms / args.steps},
+                    "full_gradient_ms": e2e_ms / args.steps, "detail": e2e_detail},
+            "timed_detail": timed_detail,
             "gpu_launches": None if launches is None else launches * args.steps,
         }
         line.update(extra)

@@ -1101,6 +1101,234 @@ __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
   }
 }
 
+// ---- level 1: smoothing chained in one pass (plane stress, 2 x 2 children) ---------------
+//
+// l1_sweep_kernel's passes chained like level 0's (l0_presmooth_kernel): PRE runs the
+// first sweep from zero, a sweep and the residual (writes x2 and r); POST runs two sweeps
+// from the prolonged iterate x0 (writes x2).  Stage A works on element row f - 1 for the
+// front row f, stage B on element row f - 2 with the element matrices stage A assembled a
+// step earlier, so each element's M = sum_m rho_m M_m is formed once per pass.  The
+// Jacobi diagonal is the stored stencil's centre diagonal (as l1_sweep_kernel).  Lanes
+// 2..29 are output (28 columns a warp).
+constexpr int kL1ChainCols = 28;
+
+inline dim3 l1_chain_grid(int nelx, int nely, int rows) {
+  const int strips = (nelx + 1 + kL1ChainCols - 1) / kL1ChainCols;
+  return dim3((strips + kQWarps - 1) / kQWarps, (nely + 1 + kQRows - 1) / kQRows, rows);
+}
+
+// One element-row stage of the level-1 modal operator (l1_sweep_kernel's step).
+template <typename T>
+struct L1Stage {
+  T sT[2], dT[2], co[2], cr[2], ut[2];
+  STT_DEV void reset() {
+#pragma unroll
+    for (int d = 0; d < 2; ++d) sT[d] = dT[d] = co[d] = cr[d] = ut[d] = T(0);
+  }
+  STT_DEV void step(const T (&Me)[21], const T (&ub)[2], T (&Ku)[2]) {
+    T sB[2], dB[2];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const T vr = __shfl_down_sync(0xffffffffu, ub[d], 1);
+      sB[d] = ub[d] + vr;
+      dB[d] = vr - ub[d];
+    }
+    T md[6];
+    md[0] = dB[0] + dT[0];  // Gx(ux)
+    md[1] = sT[1] - sB[1];  // Gy(uy)
+    md[2] = sT[0] - sB[0];  // Gy(ux)
+    md[3] = dB[1] + dT[1];  // Gx(uy)
+    md[4] = dT[0] - dB[0];  // H(ux)
+    md[5] = dT[1] - dB[1];  // H(uy)
+    T q[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) q[i] = T(0);
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j, ++e) {
+        q[i] = fma(Me[e], md[j], q[i]);
+        if (j != i) q[j] = fma(Me[e], md[i], q[j]);
+      }
+    T own[2], send[2];
+    modal_corners(q[0], q[2], q[4], co[0], cr[0], own[0], send[0]);
+    modal_corners(q[3], q[1], q[5], co[1], cr[1], own[1], send[1]);
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      Ku[d] = own[d] + __shfl_up_sync(0xffffffffu, send[d], 1);
+      sT[d] = sB[d];
+      dT[d] = dB[d];
+      ut[d] = ub[d];
+    }
+  }
+};
+
+// M = sum over the 2 x 2 children of rho_m M_m (mirror form when MIR, as l1_sweep_kernel).
+template <typename T, bool MIR>
+STT_DEV void l1_assemble(const T (&rm)[4], const L1Mat<T, MIR ? 1 : 4>& M, T (&Me)[21]) {
+  if constexpr (MIR) {
+    const T p0 = rm[0] + rm[1], p1 = rm[0] - rm[1], q0 = rm[2] + rm[3], q1 = rm[2] - rm[3];
+    const T cpp = p0 + q0, cmp = p1 + q1, cpm = p0 - q0, cmm = p1 - q1;
+    int e = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j, ++e) {
+        const bool sxn = mode_dx(i) * mode_dx(j) < 0, syn = mode_dy(i) * mode_dy(j) < 0;
+        Me[e] = M.m[0][e] * (sxn ? (syn ? cmm : cmp) : (syn ? cpm : cpp));
+      }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 21; ++e) {
+      T a = rm[0] * M.m[0][e];
+#pragma unroll
+      for (int m = 1; m < 4; ++m) a = fma(rm[m], M.m[m][e], a);
+      Me[e] = a;
+    }
+  }
+}
+
+template <typename T, bool PRE, bool MIR, int AHEAD = 2>
+__global__ void __launch_bounds__(kQThreads, 4) l1_chain_kernel(
+    const T* __restrict__ x0, const T* __restrict__ b, T* __restrict__ out_x, T* __restrict__ out_r,
+    long long vec_rs, const T* __restrict__ rho0, long long rho_rs, int fnelx, const T* __restrict__ st,
+    const uint8_t* __restrict__ fixed, int nnx, int nny, const int* __restrict__ row_map, int hrows,
+    const RowState* __restrict__ rst, T omega, L1Mat<T, MIR ? 1 : 4> M) {
+  constexpr int D = 2, LO = 2, HI = 29;
+  static_assert(HI - LO + 1 == kL1ChainCols, "strip width");
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const long long nnode = (long long)nnx * nny;
+  const int h = hier_row(row_map, hrows, s);
+  const T* rh = rho0 + (size_t)h * rho_rs;
+  const T* dgh = st + (size_t)h * 5 * D * D * nnode;  // centre block: coefficients 0 and 3
+  const T* xs = PRE ? nullptr : x0 + (size_t)s * vec_rs;
+  const T* bs = b + (size_t)s * vec_rs;
+  T* ox = out_x + (size_t)s * vec_rs;
+  T* orr = PRE ? out_r + (size_t)s * vec_rs : nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kL1ChainCols - LO + lane;
+  const bool out_lane = lane >= LO && lane <= HI && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const int nelx = nnx - 1, nely = nny - 1;
+  const bool ecol_ok = c >= 0 && c < nelx;
+  const int r0 = blockIdx.y * kQRows;
+  const int r1 = min(r0 + kQRows, nny);
+  struct Front {
+    T b[D], dg[D], x[D], rm[4];
+    uint8_t fl;
+  };
+  auto load_rm = [&](int f, T(&rm)[4]) {
+    const bool ok = ecol_ok && f >= 0 && f < nely;
+#pragma unroll
+    for (int my = 0; my < 2; ++my)
+#pragma unroll
+      for (int mx = 0; mx < 2; ++mx)
+        rm[my * 2 + mx] = ok ? __ldg(rh + (size_t)(2 * f + my) * fnelx + 2 * c + mx) : T(0);
+  };
+  auto load_front = [&](int f, Front& Q) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) Q.b[d] = Q.dg[d] = Q.x[d] = T(0);
+    Q.fl = 0;
+    load_rm(f, Q.rm);
+    if (!col_ok || f < 0 || f >= nny) return;
+    const long long node = (long long)f * nnx + c;
+    Q.fl = __ldg(fixed + node);
+    load_node<D, T>(bs, node, Q.b);
+    Q.dg[0] = __ldg(dgh + node);
+    Q.dg[1] = __ldg(dgh + 3 * nnode + node);
+    if constexpr (!PRE) load_node<D, T>(xs, node, Q.x);
+  };
+  struct Delay {
+    T b[D], dg[D];
+    uint8_t fl;
+  };
+  // the sweep / residual at a node from K x there
+  auto result = [&](bool sweep, const T(&Kx)[D], const T(&xo)[D], const Delay& e, T(&res)[D]) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const bool fx = (e.fl >> i) & 1;
+      const T Ax = fx ? T(0) : Kx[i];
+      if (sweep) {
+        const T dg = fx ? T(1) : e.dg[i];
+        res[i] = xo[i] + sweep_div(omega * (e.b[i] - Ax), dg);
+      } else {
+        res[i] = e.b[i] - Ax;
+      }
+    }
+  };
+  L1Stage<T> A, B;
+  A.reset();
+  B.reset();
+  Delay d1{}, d2{};  // node rows f - 1 and f - 2
+  const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
+  T rm_prev[4];  // children of element row f - 1
+  load_rm(f0 - 1, rm_prev);
+  T MeB[21];  // element row f - 2's matrix, from stage A a step earlier
+#pragma unroll
+  for (int e = 0; e < 21; ++e) MeB[e] = T(0);
+  Front qf[AHEAD];
+#pragma unroll
+  for (int k = 0; k < AHEAD; ++k) load_front(f0 + k, qf[k]);
+  for (int fb = f0; fb <= f1; fb += AHEAD) {
+#pragma unroll
+    for (int k = 0; k < AHEAD; ++k) {
+      const int f = fb + k;
+      const Front Q = qf[k];
+      load_front(f + AHEAD, qf[k]);
+      const bool row_f = col_ok && f >= 0 && f < nny;
+      Delay cur;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        cur.b[d] = Q.b[d];
+        cur.dg[d] = Q.dg[d];
+      }
+      cur.fl = Q.fl;
+      // stage A's input at row f: the first sweep from zero (PRE) or the loaded x0
+      T xin[D];
+      if constexpr (PRE) {
+        const T zero[D] = {T(0), T(0)};
+        result(true, zero, zero, cur, xin);
+        if (!row_f) xin[0] = xin[1] = T(0);
+      } else {
+#pragma unroll
+        for (int d = 0; d < D; ++d) xin[d] = Q.x[d];
+      }
+      // stage A: element row f - 1 -> a sweep at node row f - 1
+      T MeA[21];
+      l1_assemble<T, MIR>(rm_prev, M, MeA);
+      T KA[D], xa[D], xo_a[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
+      A.step(MeA, xin, KA);
+      result(true, KA, xo_a, d1, xa);
+      if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) xa[0] = xa[1] = T(0);
+      // stage B: element row f - 2 -> the residual (PRE) or a second sweep at node row f - 2
+      T KB[D], xbr[D], xo_b[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
+      B.step(MeB, xa, KB);
+      result(!PRE, KB, xo_b, d2, xbr);
+      if (out_lane) {
+        if constexpr (PRE) {
+          if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);
+          if (f - 2 >= r0 && f - 2 < r1) store_node<D, T>(orr, (long long)(f - 2) * nnx + c, xbr);
+        } else {
+          if (f - 2 >= r0 && f - 2 < r1) store_node<D, T>(ox, (long long)(f - 2) * nnx + c, xbr);
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 21; ++e) MeB[e] = MeA[e];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) rm_prev[m] = Q.rm[m];
+      d2 = d1;
+      d1 = cur;
+    }
+  }
+}
+
 // ---- restriction: column-marching full weighting ---------------------------------
 //
 // rc = P_c (R r_f), the x pass then the y pass of torch_mg._restrict_axis

@@ -279,6 +279,36 @@ struct Cycle {
 #undef STT_PRE
   }
 
+  // Level 1's smoothing chained in one pass from the level-0 densities (FP32, 2 x 2
+  // mirror-form children, two sweeps each way): PRE writes x2 to ox and the residual to
+  // orr; POST sweeps twice from x0 into ox.  False when the hierarchy does not allow it
+  // (the FP64 cycle keeps the unchained passes: the chained state does not fit its
+  // registers).
+  bool l1_chain(bool pre, const T* x0, const T* b, T* ox, T* orr) {
+    if constexpr (D != 2 || sizeof(T) != 4) {
+      return false;
+    } else {
+      const LevelDesc& f = h->lv[0];
+      const LevelDesc& lv = h->lv[1];
+      if (!h->l1 || !h->l1par || n_smooth != 2 || f.kx != 2 || f.ky != 2) return false;
+      const dim3 g = l1_chain_grid(lv.nelx, lv.nely, nrows);
+      const long long vs = vstride(lv.ndof);
+#define STT_L1C(PRE, MIR, NM)                                                                                 \
+  do {                                                                                                        \
+    L1Mat<T, NM> M;                                                                                           \
+    for (int m = 0; m < NM; ++m)                                                                              \
+      for (int e = 0; e < 21; ++e) M.m[m][e] = T(h->l1m[m][e]);                                               \
+    l1_chain_kernel<T, PRE, MIR><<<g, kQThreads, 0, st>>>(x0, b, ox, orr, vs, rho0(), f.rs_rho, f.nelx, stl(1), \
+                                                          lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst,  \
+                                                          omega, M);                                            \
+  } while (0)
+      if (pre) STT_L1C(true, true, 1);
+      else STT_L1C(false, true, 1);
+#undef STT_L1C
+      return true;
+    }
+  }
+
   // Level 0's two post-smoothing sweeps in one pass: x0 (the prolonged iterate) -> out.
   void postsmooth(const T* x0, const T* b, long long b_rs, T* out) {
     const LevelDesc& lv = h->lv[0];
@@ -334,8 +364,11 @@ struct Cycle {
     // the prolongation into the first post-smoothing sweep, SW_POST, measured slower on
     // B200 than the separate prolongation: 600 us against 277 + 151 us at 2048x1024 x 16.)
     const bool modal0 = l == 0 && h->modal;
+    bool chained1 = false;  // level 1's smoothing chained in one pass each way
     if (modal0 && n_smooth == 2) {
       presmooth(b, b_rs, xa, xb);
+    } else if (l == 1 && b_rs == nd && l1_chain(true, nullptr, b, xa, xb)) {
+      chained1 = true;
     } else {
       pass<SW_FIRST>(l, nullptr, nd, b, b_rs, xa, nd);
       for (int k = 1; k < n_smooth; ++k) {
@@ -359,6 +392,10 @@ struct Cycle {
       T* dst = (final_out && final_out != b) ? final_out : xb;
       postsmooth(xa, b, b_rs, dst);
       return dst;
+    }
+    if (chained1) {
+      l1_chain(false, xa, b, xb, nullptr);
+      return xb;
     }
     for (int k = 0; k < n_smooth; ++k) {
       T* dst = (l == 0 && final_out && k == n_smooth - 1) ? final_out : xb;
