@@ -915,6 +915,216 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
   }
 }
 
+// ---- stencil levels: smoothing chained in one pass ---------------------------------------
+//
+// st_sweep2_kernel's passes chained like l0_presmooth_kernel: PRE runs the first sweep from
+// zero, a sweep and the residual (writes x2 and r); POST runs two sweeps from x0 (writes
+// x2).  Stage A emits node row f - 1 for the front row f, stage B node row f - 2 from stage
+// A's output, so the intermediate iterate never leaves registers.  Stage A's coefficient
+// row streams from HBM one step ahead; stage B reads the same rows one step later, from
+// cache.  Lanes 2..29 are output (28 columns a warp).
+constexpr int kStChainCols = 28;
+
+inline dim3 st_chain_grid(int nelx, int nely, int rows) {
+  const int strips = (nelx + 1 + kStChainCols - 1) / kStChainCols;
+  const int xb = (strips + kQWarps - 1) / kQWarps;
+  const int band = band_rows(xb, nely + 1, rows);
+  return dim3(xb, (nely + 1 + band - 1) / band, rows);
+}
+
+// One stage of the half-stencil operator (st_sweep2_kernel's march): the x of the row
+// being emitted and of its right neighbour, and the N / NW / NE products carried from the
+// row above.
+template <int D, typename T>
+struct StStage {
+  T xr[D], xrr[D], nN[D], nNW[D], nNE[D];
+  STT_DEV void reset() {
+#pragma unroll
+    for (int d = 0; d < D; ++d) xr[d] = xrr[d] = nN[d] = nNW[d] = nNE[d] = T(0);
+  }
+  // (A x) at the current row from its coefficients co (Cc, E, S, SE, SW) and the next
+  // row's x; then the next row becomes current
+  STT_DEV void step(const T* co, const T (&xn)[D], T (&Ax)[D]) {
+    constexpr int DD = D * D;
+    const T* Cc = co;
+    const T* E = co + DD;
+    const T* S = co + 2 * DD;
+    const T* SE = co + 3 * DD;
+    const T* SW = co + 4 * DD;
+    T xnl[D], xnr[D], wp[D], pse[D], psw[D], pn[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      xnl[d] = __shfl_up_sync(0xffffffffu, xn[d], 1);
+      xnr[d] = __shfl_down_sync(0xffffffffu, xn[d], 1);
+      wp[d] = pse[d] = psw[d] = pn[d] = Ax[d] = T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        wp[j] = fma(E[i * D + j], xr[i], wp[j]);    // W term of the right neighbour
+        pn[j] = fma(S[i * D + j], xr[i], pn[j]);    // N term of the node below
+        pse[j] = fma(SE[i * D + j], xr[i], pse[j]);  // NW term of the node below-right
+        psw[j] = fma(SW[i * D + j], xr[i], psw[j]);  // NE term of the node below-left
+      }
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        Ax[i] = fma(Cc[i * D + j], xr[j], Ax[i]);
+        Ax[i] = fma(E[i * D + j], xrr[j], Ax[i]);
+        Ax[i] = fma(S[i * D + j], xn[j], Ax[i]);
+        Ax[i] = fma(SE[i * D + j], xnr[j], Ax[i]);
+        Ax[i] = fma(SW[i * D + j], xnl[j], Ax[i]);
+      }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      Ax[d] += __shfl_up_sync(0xffffffffu, wp[d], 1);
+      Ax[d] += nN[d] + nNW[d] + nNE[d];
+      nN[d] = pn[d];
+      nNW[d] = __shfl_up_sync(0xffffffffu, pse[d], 1);
+      nNE[d] = __shfl_down_sync(0xffffffffu, psw[d], 1);
+      xr[d] = xn[d];
+      xrr[d] = xnr[d];
+    }
+  }
+};
+
+template <int D, typename T, bool PRE>
+__global__ void __launch_bounds__(kQThreads, 4) st_chain_kernel(
+    const T* __restrict__ x0, const T* __restrict__ b, T* __restrict__ out_x, T* __restrict__ out_r,
+    long long vec_rs, const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega) {
+  constexpr int DD = D * D, NS = 5 * DD, LO = 2, HI = 29;
+  static_assert(HI - LO + 1 == kStChainCols, "strip width");
+  const int s = blockIdx.z;
+  if (rst && !rst[s].active) return;
+  const long long nnode = (long long)nnx * nny;
+  const int h = hier_row(row_map, hrows, s);
+  const T* sth = st + (size_t)h * NS * nnode;
+  const T* xs = PRE ? nullptr : x0 + (size_t)s * vec_rs;
+  const T* bs = b + (size_t)s * vec_rs;
+  T* ox = out_x + (size_t)s * vec_rs;
+  T* orr = PRE ? out_r + (size_t)s * vec_rs : nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * kQWarps + warp;
+  const int c = strip * kStChainCols - LO + lane;
+  const bool out_lane = lane >= LO && lane <= HI && c < nnx;
+  const bool col_ok = c >= 0 && c < nnx;
+  const int band = (nny + gridDim.y - 1) / gridDim.y;  // rows per block (any grid.y)
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
+  // a node row's coefficients, right-hand side and flags (zero outside the grid)
+  struct Row {
+    T co[NS];
+    T b[D];
+    uint8_t fl;
+  };
+  auto load_row = [&](int r, Row& R) {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) R.co[k] = T(0);
+#pragma unroll
+    for (int d = 0; d < D; ++d) R.b[d] = T(0);
+    R.fl = 0;
+    if (!col_ok || r < 0 || r >= nny) return;
+    const long long node = (long long)r * nnx + c;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) R.co[k] = __ldg(sth + (size_t)k * nnode + node);
+    load_node<D, T>(bs, node, R.b);
+    R.fl = __ldg(fixed + node);
+  };
+  // stage A's input at the front row f: the first sweep from zero (PRE: the diagonal,
+  // b, flags) or the loaded x0 (POST)
+  struct Front {
+    T v[D];
+    T dg[PRE ? D : 1];
+    uint8_t fl;
+  };
+  auto load_front = [&](int f, Front& F) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) F.v[d] = T(0);
+    F.fl = 0;
+    if constexpr (PRE) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) F.dg[d] = T(0);
+    }
+    if (!col_ok || f < 0 || f >= nny) return;
+    const long long node = (long long)f * nnx + c;
+    if constexpr (PRE) {
+      load_node<D, T>(bs, node, F.v);
+#pragma unroll
+      for (int d = 0; d < D; ++d) F.dg[d] = __ldg(sth + (size_t)(d * D + d) * nnode + node);
+      F.fl = __ldg(fixed + node);
+    } else {
+      load_node<D, T>(xs, node, F.v);
+    }
+  };
+  auto sweep_at = [&](const T(&Ax)[D], const T(&xo)[D], const Row& R, T(&res)[D]) {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const T dg = ((R.fl >> i) & 1) ? T(1) : R.co[i * D + i];
+      res[i] = xo[i] + sweep_div(omega * (R.b[i] - Ax[i]), dg);
+    }
+  };
+  StStage<D, T> A, B;
+  A.reset();
+  B.reset();
+  const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
+  Front qf;
+  Row qa;  // stage A's row (f - 1), one step ahead
+  load_front(f0, qf);
+  load_row(f0 - 1, qa);
+  for (int f = f0; f <= f1; ++f) {
+    const Front F = qf;
+    const Row RA = qa;
+    load_front(f + 1, qf);
+    load_row(f, qa);
+    Row RB;  // stage B's row (f - 2): stage A's row of the previous step, from cache
+    load_row(f - 2, RB);
+    T xin[D];
+    if constexpr (PRE) {
+      const bool in = col_ok && f >= 0 && f < nny;  // (outside, the diagonal is zero)
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        const T dg = ((F.fl >> i) & 1) ? T(1) : F.dg[i];
+        xin[i] = in ? sweep_div(omega * F.v[i], dg) : T(0);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < D; ++d) xin[d] = F.v[d];
+    }
+    // stage A: a sweep at node row f - 1
+    T KA[D], xa[D], xo_a[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) xo_a[d] = A.xr[d];
+    A.step(RA.co, xin, KA);
+    sweep_at(KA, xo_a, RA, xa);
+    if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) xa[d] = T(0);
+    }
+    // stage B: the residual (PRE) or a second sweep (POST) at node row f - 2
+    T KB[D], xbr[D], xo_b[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) xo_b[d] = B.xr[d];
+    B.step(RB.co, xa, KB);
+    if constexpr (PRE) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) xbr[d] = RB.b[d] - KB[d];
+    } else {
+      sweep_at(KB, xo_b, RB, xbr);
+    }
+    if (out_lane) {
+      if constexpr (PRE) {
+        if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);
+        if (f - 2 >= r0 && f - 2 < r1) store_node<D, T>(orr, (long long)(f - 2) * nnx + c, xbr);
+      } else {
+        if (f - 2 >= r0 && f - 2 < r1) store_node<D, T>(ox, (long long)(f - 2) * nnx + c, xbr);
+      }
+    }
+  }
+}
+
 // ---- level 1 from the level-0 densities (plane stress) --------------------------------
 //
 // The Galerkin element matrices of level 1 are keff[E] = sum over E's KX x KY children

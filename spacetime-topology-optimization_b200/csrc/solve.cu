@@ -309,6 +309,28 @@ struct Cycle {
     }
   }
 
+  // A stored-stencil level's smoothing chained in one pass each way (FP32, two sweeps each
+  // way): PRE writes x2 to ox and the residual to orr; POST sweeps twice from x0 into ox.
+  // False where it does not apply (FP64 cycles, other sweep counts, and level 1 when it
+  // is swept from the densities: its FP32 stencil then holds only the diagonal).
+  bool st_chain(int l, bool pre, const T* x0, const T* b, T* ox, T* orr) {
+    if constexpr (sizeof(T) != 4) {
+      return false;
+    } else {
+      if (l < 1 || n_smooth != 2 || (l == 1 && h->l1)) return false;
+      const LevelDesc& lv = h->lv[l];
+      const dim3 g = st_chain_grid(lv.nelx, lv.nely, nrows);
+      const long long vs = vstride(lv.ndof);
+      if (pre)
+        st_chain_kernel<D, T, true><<<g, kQThreads, 0, st>>>(x0, b, ox, orr, vs, stl(l), lv.fixed, lv.nnx, lv.nny,
+                                                             h->row_map, h->hrows, rst, omega);
+      else
+        st_chain_kernel<D, T, false><<<g, kQThreads, 0, st>>>(x0, b, ox, orr, vs, stl(l), lv.fixed, lv.nnx,
+                                                              lv.nny, h->row_map, h->hrows, rst, omega);
+      return true;
+    }
+  }
+
   // Level 0's two post-smoothing sweeps in one pass: x0 (the prolonged iterate) -> out.
   void postsmooth(const T* x0, const T* b, long long b_rs, T* out) {
     const LevelDesc& lv = h->lv[0];
@@ -365,10 +387,13 @@ struct Cycle {
     // B200 than the separate prolongation: 600 us against 277 + 151 us at 2048x1024 x 16.)
     const bool modal0 = l == 0 && h->modal;
     bool chained1 = false;  // level 1's smoothing chained in one pass each way
+    bool chainedS = false;  // a stencil level's, likewise
     if (modal0 && n_smooth == 2) {
       presmooth(b, b_rs, xa, xb);
     } else if (l == 1 && b_rs == nd && l1_chain(true, nullptr, b, xa, xb)) {
       chained1 = true;
+    } else if (b_rs == nd && st_chain(l, true, nullptr, b, xa, xb)) {
+      chainedS = true;
     } else {
       pass<SW_FIRST>(l, nullptr, nd, b, b_rs, xa, nd);
       for (int k = 1; k < n_smooth; ++k) {
@@ -395,6 +420,10 @@ struct Cycle {
     }
     if (chained1) {
       l1_chain(false, xa, b, xb, nullptr);
+      return xb;
+    }
+    if (chainedS) {
+      st_chain(l, false, xa, b, xb, nullptr);
       return xb;
     }
     for (int k = 0; k < n_smooth; ++k) {

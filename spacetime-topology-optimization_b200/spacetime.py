@@ -317,7 +317,11 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
                                   2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
                                   _lib.STT_PROJECT_OUT, P.ke, st))
         gK = 2 * gK
-        a_ = torch_fem.safe_div(torch_fem._dots(U, gK), torch_fem._dots(U, F))
+        # U . gK and U . F in one pass over U
+        d2 = torch.empty(S, 2, dtype=torch.float64, device=dev)
+        _lib.check(L.stt_vec_dots(S, 2 * nnode, _lib.ptr(U), _lib.ptr(gK), _lib.ptr(U), _lib.ptr(F), None, None,
+                                  2 * nnode, _lib.ptr(d2), st))
+        a_ = torch_fem.safe_div(d2[:, 0], d2[:, 1])
         x0 = (a_[:, None] * U).contiguous()
         if batched:
             lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
