@@ -11,7 +11,7 @@ CUDA stream; there is no CPU path.
 from . import _lib  # noqa: F401
 
 __all__ = ["torch_fem", "torch_mg", "torch_solve", "sensitivity", "virtual_heat", "compliance",
-           "spacetime", "fem", "gravity", "filters"]
+           "spacetime", "fem", "gravity", "filters", "sharding"]
 
 
 def __getattr__(name):
