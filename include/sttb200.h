@@ -22,6 +22,8 @@
  *   stt_hier_*          sttopt/torch_mg.py:293-400 (build_hierarchy), :257-266 (select)
  *   stt_level_apply     sttopt/torch_mg.py:239-255 (_Level.__call__), :179-193 (keff_matvec)
  *   stt_vcycle          sttopt/torch_mg.py:403-476 (VCycle.__call__)
+ *   stt_grid_transfer   sttopt/torch_mg.py:75-109 (_interp_axis, _restrict_axis, _on_node_grid)
+ *   stt_keff_apply      sttopt/torch_mg.py:168-193 (_scatter, keff_matvec)
  *   stt_pcg_mg          sttopt/torch_fem.py:201-343 (pcg with a multigrid preconditioner)
  *   stt_vec_*           sttopt/torch_fem.py:253-331 (the PCG vector updates, any operator)
  *   stt_element_sens    sttopt/torch_solve.py:144-152 (FemSolve.backward element terms),
@@ -132,7 +134,24 @@ int stt_hier_level_fixed(const stt_hier* h, int level, uint8_t* out, stt_stream_
 int stt_level_apply(const stt_hier* h, int level, int nrows, const double* v, long long v_rs,
                     double* out, long long out_rs, stt_stream_t stream);
 
-/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
+/* The grid transfers of torch_mg._on_node_grid with _interp_axis (restrict_ == 0:
+ * out = P in, in on the cnnx x cnny coarse node grid) or _restrict_axis (restrict_ != 0:
+ * out = R in = P^T in, in on the fine grid), sttopt/torch_mg.py:75-109: the x pass then
+ * the y pass, factors kx, ky in {1, 2, 3}, d interleaved dofs per node, no projection.
+ * FP64; nrows batch rows with their own strides. */
+int stt_grid_transfer(int d, int kx, int ky, int cnnx, int cnny, int nrows, int restrict_,
+                      const double* in, long long in_rs, double* out, long long out_rs,
+                      stt_stream_t stream);
+
+/* keff_matvec (sttopt/torch_mg.py:179-193): out[s] = sum_e scatter(U_e[s]^T keff[s][e]) with
+ * explicit element matrices keff[s] ((4d)^2 doubles per element, row-major, the
+ * reference's local dof order; k_rs = 0 shares one set over the rows).  FP64,
+ * deterministic (node-centric gather, no atomics). */
+int stt_keff_apply(int d, int nelx, int nely, int nrows, const double* U, long long u_rs,
+                   const double* keff, long long k_rs, double* out, long long o_rs,
+                   stt_stream_t stream);
+
+/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. *//* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
 long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int gamma);
 
 /* z[s] = M r[s], one V-cycle (damped Jacobi omega, n_smooth sweeps each way, gamma

@@ -71,6 +71,8 @@ _SIGS = {
     "stt_heat_element_means": (_c_int, [_c_int, _c_int, _p, _p, _p]),
     "stt_heat_adjoint_load": (_c_int, [_c_int, _c_int, _p, _c_double, _p, _p]),
     "stt_gravity_load": (_c_int, [_c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _c_int, _p]),
+    "stt_grid_transfer": (_c_int, [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_keff_apply": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _c_ll, _p]),
     "stt_element_means": (_c_int, [_c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _c_int, _p]),
     "stt_poisson_load": (_c_int, [_c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _c_ll, _p]),
     "stt_poisson_load_adjoint": (_c_int, [_c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _c_ll, _p, _c_ll,

@@ -1622,7 +1622,7 @@ __global__ void __launch_bounds__(kQThreads) restrict_kernel(
       }
     }
     if (out_lane) {
-      const uint8_t fl = __ldg(cfixed + (size_t)R * cnnx + C);
+      const uint8_t fl = cfixed ? __ldg(cfixed + (size_t)R * cnnx + C) : uint8_t(0);  // null: no projection
       T v[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
@@ -1780,7 +1780,7 @@ __global__ void __launch_bounds__(kProlongThreads) prolong_kernel(
   T v[D], pv[D];
   load_node<D, T>(x, node, v);
   prolong_at<D, T>(e, cnnx, kx, ky, r, c, pv);
-  const uint8_t fl = __ldg(ffixed + node);
+  const uint8_t fl = ffixed ? __ldg(ffixed + node) : uint8_t(0);  // null: no projection
 #pragma unroll
   for (int d = 0; d < D; ++d)
     if (!((fl >> d) & 1)) v[d] += pv[d];

@@ -337,3 +337,121 @@ def child_interpolation_matrices(kx: int, ky: int, device=None, dtype=torch.floa
                     for i in range(d):
                         S[my * kx + mx, qf * d + i, qc * d + i] = v
     return torch.tensor(S, dtype=dtype, device=device)
+
+
+# ---- grid transfers and explicit element matrices (the reference's helpers) ---------
+
+
+def _transfer(v: Tensor, cnnx: int, cnny: int, kx: int, ky: int, d: int, restrict: bool) -> Tensor:
+    _lib.require_cuda(v)
+    fnnx, fnny = kx * (cnnx - 1) + 1, ky * (cnny - 1) + 1
+    n_in, n_out = (d * fnnx * fnny, d * cnnx * cnny) if restrict else (d * cnnx * cnny, d * fnnx * fnny)
+    if v.shape[-1] != n_in:
+        raise ValueError(f"expected a trailing dimension of {n_in}, got {tuple(v.shape)}")
+    V = v.detach().to(torch.float64).reshape(-1, n_in).contiguous()
+    out = torch.empty(V.shape[0], n_out, dtype=torch.float64, device=V.device)
+    _lib.check(_lib.lib().stt_grid_transfer(d, kx, ky, cnnx, cnny, V.shape[0], int(restrict), _lib.ptr(V), n_in,
+                                            _lib.ptr(out), n_out, _lib.stream()))
+    return out.reshape(*v.shape[:-1], n_out).to(v.dtype)
+
+
+class _Transfer(torch.autograd.Function):
+    """P (restrict = False) or R = P^T (True); the backward pass is the other one."""
+
+    @staticmethod
+    def forward(ctx, v, cnnx, cnny, kx, ky, d, restrict):
+        ctx.args = (cnnx, cnny, kx, ky, d, restrict)
+        return _transfer(v, cnnx, cnny, kx, ky, d, restrict)
+
+    @staticmethod
+    def backward(ctx, g):
+        cnnx, cnny, kx, ky, d, restrict = ctx.args
+        return _transfer(g, cnnx, cnny, kx, ky, d, not restrict), None, None, None, None, None, None
+
+
+def _interp_axis(c: Tensor, k: int) -> Tensor:
+    """Piecewise-linear interpolation by ``k`` along the last axis, ``nc + 1 -> k nc + 1``
+    (sttopt/torch_mg.py:75-81), on the device (``stt_grid_transfer``, x pass only)."""
+    if k == 1:
+        return c
+    lead = c.shape[:-1]
+    rows = int(np.prod(lead)) if lead else 1
+    out = _Transfer.apply(c.reshape(1, rows * c.shape[-1]), c.shape[-1], rows, k, 1, 1, False)
+    return out.reshape(*lead, k * (c.shape[-1] - 1) + 1)
+
+
+def _restrict_axis(f: Tensor, k: int) -> Tensor:
+    """The exact transpose of ``_interp_axis`` along the last axis (sttopt/torch_mg.py:84-93)."""
+    if k == 1:
+        return f
+    if (f.shape[-1] - 1) % k:
+        raise ValueError(f"{f.shape[-1]} nodes do not coarsen by {k}")
+    lead = f.shape[:-1]
+    rows = int(np.prod(lead)) if lead else 1
+    nc = (f.shape[-1] - 1) // k + 1
+    out = _Transfer.apply(f.reshape(1, rows * f.shape[-1]), nc, rows, k, 1, 1, True)
+    return out.reshape(*lead, nc)
+
+
+def _on_node_grid(v: Tensor, nnx: int, nny: int, kx: int, ky: int, axis_op) -> Tensor:
+    """``axis_op`` along the node grid's x then y axes of a dof vector (sttopt/torch_mg.py:96-109).
+    ``_interp_axis`` / ``_restrict_axis`` with 1 or 2 dofs per node run as one device pass
+    (``stt_grid_transfer``); any other operator runs through its own calls."""
+    d = v.shape[-1] // (nny * nnx)
+    if d in (1, 2) and axis_op in (_interp_axis, _restrict_axis):
+        if axis_op is _interp_axis:
+            return _Transfer.apply(v, nnx, nny, kx, ky, d, False)
+        if (nnx - 1) % kx or (nny - 1) % ky:
+            raise ValueError("the node grid does not coarsen by these factors")
+        return _Transfer.apply(v, (nnx - 1) // kx + 1, (nny - 1) // ky + 1, kx, ky, d, True)
+    g = v.reshape(*v.shape[:-1], nny, nnx, d)
+    g = axis_op(g.movedim(-2, -1), kx).movedim(-1, -2)
+    g = axis_op(g.movedim(-3, -1), ky).movedim(-1, -3)
+    return g.reshape(*v.shape[:-1], -1)
+
+
+@functools.lru_cache(maxsize=None)
+def _child_elements(nelx: int, nely: int, kx: int, ky: int, device) -> Tensor:
+    """Fine element indices under each coarse element, in the child order of
+    ``fem.element_dof_map(kx, ky)`` (sttopt/torch_mg.py:130-137)."""
+    e = torch.arange(nelx * nely, device=device).reshape(nely, nelx)
+    return e.reshape(nely // ky, ky, nelx // kx, kx).permute(0, 2, 1, 3).reshape(-1, ky * kx)
+
+
+def _scatter(per_element: Tensor, edofMat: Tensor, ndof: int) -> Tensor:
+    """Scatter-add of per-element dof values into a dof vector (sttopt/torch_mg.py:168-176)."""
+    batch = per_element.shape[:-2]
+    flat = per_element.reshape(*batch, -1)
+    return flat.new_zeros(*batch, ndof).index_add_(-1, edofMat.reshape(-1), flat)
+
+
+def keff_matvec(U: Tensor, keff: Tensor, edofMat: Tensor, ndof: int) -> Tensor:
+    """``sum_e scatter(keff_e U_e)`` for explicit per-element matrices (sttopt/torch_mg.py:179-193),
+    batch dims broadcasting as in the reference, by ``stt_keff_apply`` (FP64)."""
+    _lib.require_cuda(U, keff)
+    k = keff.shape[-1]
+    d = k // 4
+    nelx, nely = _geom.grid_shape(edofMat, ndof, d)
+    nel = nelx * nely
+    if keff.shape[-3:] != (nel, k, k):
+        raise ValueError(f"keff of shape {tuple(keff.shape)} does not match {nel} elements of {k} dofs")
+    batch = torch.broadcast_shapes(U.shape[:-1], keff.shape[:-3])
+    Ub = U.detach().to(torch.float64).expand(*batch, ndof).reshape(-1, ndof).contiguous()
+    if keff.dim() == 3:
+        Kb, k_rs = keff.detach().to(torch.float64).contiguous(), 0
+    else:
+        Kb, k_rs = keff.detach().to(torch.float64).expand(*batch, nel, k, k).reshape(-1, nel, k, k).contiguous(), nel * k * k
+    out = torch.empty_like(Ub)
+    _lib.check(_lib.lib().stt_keff_apply(d, nelx, nely, Ub.shape[0], _lib.ptr(Ub), ndof, _lib.ptr(Kb), k_rs,
+                                         _lib.ptr(out), ndof, _lib.stream()))
+    return out.reshape(*batch, ndof).to(U.dtype)
+
+
+def _select_rows(t: Tensor | None, rows: Tensor, core_ndim: int):
+    """``t[rows]`` along its batch dim; an unbatched tensor passes through (sttopt/torch_mg.py:196-209)."""
+    if t is None or t.ndim == core_ndim:
+        return t
+    if t.ndim != core_ndim + 1:
+        raise ValueError(f"row selection needs a single batch dim, got shape {tuple(t.shape)}")
+    return t[rows]
+

@@ -202,6 +202,42 @@ def test_vcycle_fp32_matches_fp64(m, nelx, nely, mce):
     assert abs(a - b) <= 1e-4 * abs(a)
 
 
+@pytest.mark.parametrize("kx,ky,d", [(2, 2, 2), (3, 2, 2), (2, 3, 1), (3, 3, 1), (1, 2, 2)])
+def test_grid_transfer_helpers_match_oracle_and_are_adjoint(m, kx, ky, d):
+    """torch_mg._on_node_grid with _interp_axis / _restrict_axis (stt_grid_transfer) against
+    the oracle's restatement, the 1-D helpers alone, and R = P^T (the reference's test)."""
+    rng = np.random.default_rng(kx * 10 + ky + d)
+    ncx, ncy = 5, 4
+    cnnx, cnny, fnnx, fnny = ncx + 1, ncy + 1, ncx * kx + 1, ncy * ky + 1
+    c = rng.standard_normal((3, d * cnnx * cnny))
+    f = rng.standard_normal((3, d * fnnx * fnny))
+    Pc = m.mg._on_node_grid(T(c), cnnx, cnny, kx, ky, m.mg._interp_axis).cpu().numpy()
+    Rf = m.mg._on_node_grid(T(f), fnnx, fnny, kx, ky, m.mg._restrict_axis).cpu().numpy()
+    assert rel_err(Pc, O.on_node_grid(c, cnnx, cnny, kx, ky, O.interp_axis)) < 1e-15
+    assert rel_err(Rf, O.on_node_grid(f, fnnx, fnny, kx, ky, O.restrict_axis)) < 1e-15
+    assert abs((Pc * f).sum() - (c * Rf).sum()) <= 1e-12 * abs((Pc * f).sum())
+    a = rng.standard_normal((2, 3, 7))
+    assert rel_err(m.mg._interp_axis(T(a), kx).cpu().numpy(), O.interp_axis(a, kx)) < 1e-15
+    b = rng.standard_normal((2, 3, 6 * ky + 1))
+    assert rel_err(m.mg._restrict_axis(T(b), ky).cpu().numpy(), O.restrict_axis(b, ky)) < 1e-15
+
+
+@pytest.mark.parametrize("d", [2, 1])
+def test_keff_matvec_matches_oracle(m, d):
+    """torch_mg.keff_matvec (stt_keff_apply) with per-row and shared element matrices."""
+    rng = np.random.default_rng(4 + d)
+    nelx, nely = 9, 7
+    nel, k = nelx * nely, 4 * d
+    ndof = d * (nelx + 1) * (nely + 1)
+    edof = O.element_dof_map(nelx, nely, d)
+    keff = rng.standard_normal((2, nel, k, k))
+    U = rng.standard_normal((2, ndof))
+    got = m.mg.keff_matvec(T(U), T(keff), T(edof, torch.int64), ndof).cpu().numpy()
+    assert rel_err(got, O.keff_matvec(U, keff, edof, ndof)) < 1e-14
+    got1 = m.mg.keff_matvec(T(U), T(keff[0]), T(edof, torch.int64), ndof).cpu().numpy()
+    assert rel_err(got1, O.keff_matvec(U, keff[0], edof, ndof)) < 1e-14
+
+
 def test_mbb_config_solve_compliance_and_sensitivities(m):
     """120 x 40 MBB, rho = 0.5: U, iterations, compliance, dc/dx vs the reference."""
     g = golden("mbb120x40")
