@@ -63,6 +63,14 @@ def shape_gradients() -> np.ndarray:
                      for xi, eta in _GAUSS])
 
 
+_shape_gradients = shape_gradients
+
+
+def _whole(nelx: int, nely: int) -> np.ndarray:
+    """The whole mesh as the design domain."""
+    return np.ones((nely, nelx), bool)
+
+
 def _boundary_loop(active: np.ndarray) -> np.ndarray:
     """The domain's boundary nodes, once each, clockwise from its top-left node
     (sttopt/virtual_heat.py:111-140); raises unless the boundary is one simple loop."""
@@ -326,3 +334,98 @@ def laplace_time_field(config, mesh: ScalarMesh, xPhys: Tensor, mu: Tensor, b: T
         raise ValueError(f"time_map {time_map!r} is not one of identity, poisson")
     t_e = element_means(t, mesh.edof).reshape(shape)
     return TimeFieldSolution(normalize(t_e, xPhys), u, phi, t)
+
+
+# ---- host helpers of the Laplace time field's wall design and the start check -------
+
+
+def _node_edges(active: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """The 8-connected node adjacencies through the design domain, both directions, with
+    their Euclidean lengths (sttopt/virtual_heat.py:465-489): an axis step along an edge of
+    a domain element, a diagonal across one."""
+    nely, nelx = active.shape
+    inside = np.pad(active, 1)  # element (r, c) at inside[r + 1, c + 1]
+    node = np.arange((nely + 1) * (nelx + 1)).reshape(nely + 1, nelx + 1)
+    src, dst, length = [], [], []
+    for dr, dc in ((0, 1), (1, 0), (1, 1), (1, -1)):
+        r, c = np.mgrid[0:nely + 1 - dr, max(0, -dc):nelx + 1 - max(0, dc)]
+        cl = np.minimum(c, c + dc)  # the element column the step runs beside or across
+        if dr == 0:
+            ok = inside[r, cl + 1] | inside[r + 1, cl + 1]
+        elif dc == 0:
+            ok = inside[r + 1, cl] | inside[r + 1, cl + 1]
+        else:
+            ok = inside[r + 1, cl + 1]
+        a, b = node[r, c][ok], node[r + dr, c + dc][ok]
+        src += [a, b]
+        dst += [b, a]
+        length.append(np.full(2 * a.size, float(np.hypot(dr, dc))))
+    return np.concatenate(src), np.concatenate(dst), np.concatenate(length)
+
+
+def _plate_distance(mesh: "ScalarMesh") -> Tensor:
+    """The wall arc's grid-graph distance to the plate through the domain, in
+    ``unit_length`` (sttopt/virtual_heat.py:492-507)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import dijkstra
+
+    active = mesh.active.cpu().numpy().reshape(mesh.nely, mesh.nelx)
+    src, dst, length = _node_edges(active)
+    graph = csr_matrix((length, (src, dst)), shape=(mesh.ndof, mesh.ndof))
+    plate = np.flatnonzero(mesh.plate.cpu().numpy())
+    dist = dijkstra(graph, indices=plate, min_only=True)[mesh.arc.cpu().numpy()]
+    return torch.as_tensor(dist / mesh.unit_length, device=mesh.arc.device, dtype=mesh.KE.dtype)
+
+
+def distance_wall(mesh: "ScalarMesh") -> Tensor:
+    """The wall data of the distance to the plate, scaled to a largest value of 1/2
+    (sttopt/virtual_heat.py:510-520)."""
+    d = _plate_distance(mesh)
+    return d / (2 * d.max())
+
+
+def wall_filter(n_arc: int, rmin: float) -> np.ndarray:
+    """Cone weights ``max(0, rmin - distance)`` along the wall arc, reflected with the sign
+    flipped past either end (into the plate, where t = 0), normalised by the full cone's
+    sum (sttopt/virtual_heat.py:523-543)."""
+    k = np.arange(n_arc)
+    cone = lambda dist: np.maximum(0.0, rmin - np.abs(dist))  # noqa: E731
+    H = cone(k[:, None] - k[None, :])
+    H[k, k] = max(rmin, 1.0)
+    # the plate corners sit at -1 and n_arc: node j reflects to -2 - j and 2 n_arc - j
+    H -= cone(k[:, None] + 2 + k[None, :])
+    H -= cone(2 * n_arc - k[None, :] - k[:, None])
+    full = max(rmin, 1.0) + 2 * cone(np.arange(1, int(np.ceil(rmin)))).sum()
+    return H / full
+
+
+def start_report(mesh: "ScalarMesh", solution: TimeFieldSolution, solid: np.ndarray, base: np.ndarray) -> dict:
+    """The print-start check (sttopt/virtual_heat.py:356-390): the part touches the plate,
+    and every node of a solid element off the plate has ``t > 0``."""
+    t = solution.t.detach().cpu().numpy()
+    tPhys = solution.tPhys.detach().cpu().numpy().ravel()
+    edof = mesh.edof.cpu().numpy()
+    solid = np.asarray(solid).ravel()
+    on_base = np.zeros(solid.size, bool)
+    on_base[np.asarray(base)] = True
+    nodes = np.unique(edof[solid])
+    nodes = nodes[~mesh.plate.cpu().numpy()[nodes]]
+    earliest = float(t[nodes].min()) if nodes.size else None
+    base_t = tPhys[solid & on_base]
+    off_t = tPhys[solid & ~on_base]
+    return dict(
+        passed=bool(base_t.size) and (earliest is None or earliest > 0),
+        solid_base_elements=int(base_t.size),
+        earliest_node_t=earliest,
+        max_base_t=float(base_t.max()) if base_t.size else None,
+        earliest_off_base_t=float(off_t.min()) if off_t.size else None,
+    )
+
+
+def warn_start(start: dict) -> None:
+    """Warns that a ``start_report`` failed (sttopt/virtual_heat.py:393-398)."""
+    import warnings
+
+    warnings.warn(f"print start: {start['solid_base_elements']} solid base element(s), and the earliest node of "
+                  f"the part off the plate at t = {start['earliest_node_t']} (must be > 0)")
+

@@ -511,6 +511,23 @@ def gen_time_maps():
         out[f"arc_L_{base}"] = vh.wall_arc(12, 8, base, lshape)
         out[f"plate_L_{base}"] = vh.plate_nodes(12, 8, base, lshape)
     out["lshape"] = lshape
+    # the Laplace loop's wall design helpers and the start check
+    for n_arc, rmin in [(30, 1.0), (30, 3.5), (45, 6.0), (5, 8.0)]:
+        out[f"wf_{n_arc}_{rmin}"] = vh.wall_filter(n_arc, rmin)
+    for key, (nx, ny, base, act) in {"rect": (13, 7, "bottom_edge", None), "L": (12, 8, "left_edge", lshape),
+                                     "Lb": (12, 8, "bottom_edge", lshape)}.items():
+        mesh = vh.ScalarMesh.build(nx, ny, base, torch.device("cpu"), F64, act)
+        out[f"dw_{key}"] = vh.distance_wall(mesh)
+    rng = np.random.default_rng(41)
+    mesh = vh.ScalarMesh.build(10, 6, "bottom_edge", torch.device("cpu"), F64)
+    t_nodes = rng.uniform(-0.05, 1.0, mesh.ndof)
+    t_el = rng.uniform(0.0, 1.0, (6, 10))
+    solid = rng.uniform(size=(6, 10)) > 0.4
+    base_el = np.arange(50, 60)
+    sol = vh.TimeFieldSolution(t(t_el), t(t_nodes), None, t(t_nodes))
+    rep = vh.start_report(mesh, sol, solid, base_el)
+    out.update({"sr_t": t_nodes, "sr_tPhys": t_el, "sr_solid": solid, "sr_base": base_el,
+                "sr_report": np.array(repr(sorted(rep.items())))})
     save("time_maps", **out)
 
 

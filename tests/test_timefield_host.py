@@ -53,3 +53,28 @@ def test_gravity_matrix_explicit_form(pkg):
     assert C.shape == (40, 28)
     np.testing.assert_array_equal(C.tocsr().toarray(), g["C_7x4"])
     np.testing.assert_array_equal(C.T.tocsr().toarray(), g["C_7x4"].T)
+
+
+def test_wall_filter_distance_wall_and_start_report(pkg):
+    import torch
+
+    from sttopt_b200 import virtual_heat as vh
+
+    g = golden("time_maps")
+    for n_arc, rmin in [(30, 1.0), (30, 3.5), (45, 6.0), (5, 8.0)]:
+        np.testing.assert_allclose(vh.wall_filter(n_arc, rmin), g[f"wf_{n_arc}_{rmin}"], rtol=0, atol=1e-15)
+    for key, (nx, ny, base, act) in {"rect": (13, 7, "bottom_edge", None), "L": (12, 8, "left_edge", g["lshape"]),
+                                     "Lb": (12, 8, "bottom_edge", g["lshape"])}.items():
+        mesh = vh.ScalarMesh.build(nx, ny, base, torch.device("cpu"), torch.float64, act)
+        np.testing.assert_allclose(vh.distance_wall(mesh).numpy(), g[f"dw_{key}"], rtol=1e-14, atol=0)
+    mesh = vh.ScalarMesh.build(10, 6, "bottom_edge", torch.device("cpu"), torch.float64)
+    t_nodes = torch.as_tensor(g["sr_t"])
+    sol = vh.TimeFieldSolution(torch.as_tensor(g["sr_tPhys"]), t_nodes, None, t_nodes)
+    rep = vh.start_report(mesh, sol, g["sr_solid"], g["sr_base"])
+    assert repr(sorted(rep.items())) == str(g["sr_report"])
+    import warnings
+
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        vh.warn_start(rep)
+    assert len(w) == 1 and "print start" in str(w[0].message)
