@@ -731,22 +731,23 @@ __global__ void pcg_xclear_kernel(RowState* __restrict__ rst, int nrows) {
 
 // rz = r . z (and r . z_old for the flexible beta); first: p = z, rz_old = rz;
 // otherwise beta = safe_div(rz - rz_mix, rz_old), rz_old = rz.
-template <typename TZ>
+template <typename TZ, typename TR>
 __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
-    const double* __restrict__ r, const TZ* __restrict__ z, const TZ* __restrict__ zold,
+    const TR* __restrict__ r, const TZ* __restrict__ z, const TZ* __restrict__ zold,
     double* __restrict__ p, long long rs, long long z_rs, long long n, RowState* __restrict__ rst,
     GridRed red, int first, int flexible) {
   const int s = blockIdx.y;
   if (!rst[s].active) return;
-  const double* rsv = r + (size_t)s * rs;
+  const TR* rsv = r + (size_t)s * rs;
   const TZ* zs = z + (size_t)s * z_rs;
   const TZ* zo = zold + (size_t)s * z_rs;
   double vals[2] = {0.0, 0.0};
   for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kEwThreads) {
     const double zv = (double)zs[i];
-    vals[0] = fma(rsv[i], zv, vals[0]);
-    if (flexible && !first) vals[1] = fma(rsv[i], (double)zo[i], vals[1]);
+    const double rv = (double)rsv[i];
+    vals[0] = fma(rv, zv, vals[0]);
+    if (flexible && !first) vals[1] = fma(rv, (double)zo[i], vals[1]);
     if (first && p) p[(size_t)s * rs + i] = zv;
   }
   grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
@@ -868,7 +869,17 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     };
     bool pending = false;  // the rows still iterating have an x update pending
     STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
-    pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 1, flexible);
+    // r . z: the mixed cycle's z carries FP32 rounding, so its dots read the FP32 copy of r
+    // the cycle itself read (written by the update, or by the cycle's own conversion)
+    auto rz = [&](int first) {
+      if constexpr (sizeof(T) == 4)
+        pcg_rz_kernel<T, float><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(
+            (const float*)w.b0, z, zold, nullptr, vstride(nd), vstride(nd), nd, w.rs, red_ew, first, flexible);
+      else
+        pcg_rz_kernel<T, double><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd),
+                                                                           nd, w.rs, red_ew, first, flexible);
+    };
+    rz(1);
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
@@ -905,7 +916,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       }
       if (flexible) std::swap(z, zold);
       STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
-      pcg_rz_kernel<T><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd), nd, w.rs, red_ew, 0, flexible);
+      rz(0);
       STT_TRY(check_launch("pcg iteration"));
       if (it % check_every == 0 || it == max_iter) {
         STT_TRY(pull());
