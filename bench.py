@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the roofline kernel's timing (the small case for an ncu capture)")
+    ap.add_argument("--vcycle-only", action="store_true",
+                    help="run only V-cycles of the stage solve's 16-row mixed hierarchy (the small case for "
+                         "ncu captures of the cycle's kernels; seeded uniform densities in [1e-3, 1])")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the batched uneven multi-problem measurement")
     ap.add_argument("--uneven-only", action="store_true",
@@ -139,6 +142,37 @@ def uneven_workload(dev, seed=SEED):
         xs.append(synthetic.smoothed_density(nx, ny, 1000 * seed + k, device=dev))
         ws.append(synthetic.time_weights(nx, ny, 1000 * seed + k, device=dev))
     return xs, ws, [int(n) for n in stages]
+
+
+def run_vcycles(dev, steps, warmup):
+    """V-cycles z = M r on the 2048x1024 x 16-row mixed hierarchy of the stage solve (the
+    bench's mesh and build-plate clamp; seeded densities): ms per cycle."""
+    import numpy as np
+    import torch
+
+    from sttopt_b200 import fem, torch_mg
+
+    rng = np.random.default_rng(SEED)
+    rho = torch.as_tensor(rng.uniform(1e-3, 1.0, (N_STAGE, NELX * NELY)), device=dev)
+    edof = torch.as_tensor(fem.element_dof_map(NELX, NELY, 2), device=dev)
+    KE = torch.as_tensor(fem.plane_stress_KE(0.3), device=dev)
+    ndof = 2 * (NELX + 1) * (NELY + 1)
+    mask = torch.ones(ndof, dtype=torch.bool, device=dev)
+    mask[-2 * (NELX + 1):] = False
+    levels = torch_mg.build_hierarchy(rho, edof, KE, mask, NELX, NELY, precision="mixed")
+    M = torch_mg.VCycle(levels)
+    r = torch.as_tensor(rng.standard_normal((N_STAGE, ndof)), device=dev) * mask
+    for _ in range(warmup):
+        M(r)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        z = M(r)
+    b.record()
+    torch.cuda.synchronize()
+    return {"ms_per_cycle": a.elapsed_time(b) / steps, "levels": len(levels), "rows": N_STAGE,
+            "z_norm": float(z.norm())}
 
 
 def run_uneven(dev, steps=2, warmup=1):
@@ -259,6 +293,9 @@ def main():
         u = torch.randn(N_STAGE, 2 * problem.nnode, device=dev, dtype=torch.float64)
         roof, detail = roofline(_lib, problem, {"U": u}, dev)
         print(json.dumps({"roofline": roof, "roofline_detail": detail}), flush=True)
+        return 0
+    if args.vcycle_only:
+        print(json.dumps({"vcycle": run_vcycles(dev, max(args.steps, 1), max(args.warmup, 0))}), flush=True)
         return 0
     if args.uneven_only:
         print(json.dumps({"batched_uneven": run_uneven(dev, steps=max(args.steps, 1), warmup=max(args.warmup, 1))}),
