@@ -10,6 +10,7 @@
 
 #include "common.cuh"
 #include "errors.h"
+#include "modal.h"
 
 namespace cg = cooperative_groups;
 
@@ -189,6 +190,99 @@ __global__ void heat_adjoint_load_kernel(const double* __restrict__ w, double sc
   g[n] = -acc;
 }
 
+// ce and gdens of plane-stress elements whose KE has the modal form KE = T^T M T (the
+// level-0 kernels' edge modes Gx, Gy, H per component): U^T KE U = (T U) . M (T U), about
+// 20 flops an element instead of the 8 x 8 product.  A warp marches down a strip of 31
+// element columns (lane c holds node column c, the right neighbour's values come by
+// shuffle), a row of nodes loaded once and coalesced per step; ce / gdens stores are
+// coalesced.  Grid: (strips / 4, bands, rows).
+struct ModalE {
+  double m00, m01, m11, m22, m44, m55;
+};
+
+constexpr int kSensCols = 31;
+
+STT_DEV void modal_modes(const double (&t)[2], const double (&b)[2], double (&md)[6]) {
+  // t, b: this lane's top / bottom node; the right neighbour's by shuffle
+  double tr[2], br[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    tr[d] = __shfl_down_sync(0xffffffffu, t[d], 1);
+    br[d] = __shfl_down_sync(0xffffffffu, b[d], 1);
+  }
+  double Gx[2], Gy[2], H[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const double dB = br[d] - b[d], dT = tr[d] - t[d];
+    Gx[d] = dB + dT;
+    Gy[d] = (t[d] + tr[d]) - (b[d] + br[d]);
+    H[d] = dT - dB;
+  }
+  md[0] = Gx[0];
+  md[1] = Gy[1];
+  md[2] = Gy[0] + Gx[1];  // the shear pair enters M once
+  md[3] = H[0];
+  md[4] = H[1];
+  md[5] = 0.0;
+}
+
+template <bool LAM>
+__global__ void __launch_bounds__(128) element_sens_modal_kernel(
+    const double* __restrict__ U, long long U_rs, const double* __restrict__ lam, long long lam_rs,
+    double* __restrict__ ce, double* __restrict__ gdens, double* __restrict__ greac, long long e_rs, int nelx,
+    int nely, ModalE q) {
+  const int s = blockIdx.z;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int strip = blockIdx.x * 4 + warp;
+  const int c = strip * kSensCols + lane;  // node column; element column when lane < 31
+  const int nnx = nelx + 1;
+  const bool col_ok = c < nnx;
+  const bool el_ok = lane < kSensCols && c < nelx;
+  const int band = (nely + gridDim.y - 1) / gridDim.y;
+  const int r0 = blockIdx.y * band, r1 = min(r0 + band, nely);
+  if (r0 >= r1) return;
+  const double* us = U + (size_t)s * U_rs;
+  const double* ls = LAM ? lam + (size_t)s * lam_rs : nullptr;
+  auto load = [&](const double* v, int r, double(&o)[2]) {
+    o[0] = o[1] = 0.0;
+    if (col_ok) {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(v) + (size_t)r * nnx + c);
+      o[0] = t.x;
+      o[1] = t.y;
+    }
+  };
+  double ut[2], lt[2] = {0.0, 0.0};
+  load(us, r0, ut);
+  if (LAM) load(ls, r0, lt);
+  for (int r = r0; r < r1; ++r) {
+    double ub[2], lb[2] = {0.0, 0.0};
+    load(us, r + 1, ub);
+    if (LAM) load(ls, r + 1, lb);
+    double mu[6];
+    modal_modes(ut, ub, mu);
+    // q = M (T u): normal pair, shear, hourglass
+    const double q0 = fma(q.m01, mu[1], q.m00 * mu[0]);
+    const double q1 = fma(q.m01, mu[0], q.m11 * mu[1]);
+    const double q2 = q.m22 * mu[2], q3 = q.m44 * mu[3], q4 = q.m55 * mu[4];
+    const size_t e = (size_t)s * e_rs + (size_t)r * nelx + c;
+    if (ce && el_ok) ce[e] = mu[0] * q0 + mu[1] * q1 + mu[2] * q2 + mu[3] * q3 + mu[4] * q4;
+    if (LAM) {
+      double ml[6];
+      modal_modes(lt, lb, ml);
+      if (gdens && el_ok) gdens[e] = -(ml[0] * q0 + ml[1] * q1 + ml[2] * q2 + ml[3] * q3 + ml[4] * q4);
+      if (greac) {  // -lam_e . U_e / 4: this node column's two nodes and the right neighbour's
+        const double pl = fma(ut[0], lt[0], fma(ut[1], lt[1], fma(ub[0], lb[0], ub[1] * lb[1])));
+        const double pr = __shfl_down_sync(0xffffffffu, pl, 1);
+        if (el_ok) greac[e] = -(pl + pr) * 0.25;
+      }
+#pragma unroll
+      for (int d = 0; d < 2; ++d) lt[d] = lb[d];
+    }
+#pragma unroll
+    for (int d = 0; d < 2; ++d) ut[d] = ub[d];
+  }
+}
+
 // ---- PCG vector steps (arbitrary operator path) -----------------------------------
 
 // Dot products of up to three vector pairs per row.  One thread-block cluster of
@@ -198,37 +292,51 @@ __global__ void heat_adjoint_load_kernel(const double* __restrict__ w, double sc
 constexpr int kDotCluster = 8;
 constexpr int kDotThreads = 512;
 
+// K pairs, U strided loads of each in flight per thread (U kDotThreads apart): the
+// accumulators are summed in a fixed order, so the result stays deterministic.
+template <int K>
 __global__ void __cluster_dims__(kDotCluster, 1, 1) __launch_bounds__(kDotThreads)
     vec_dots_kernel(long long n, const double* __restrict__ a0, const double* __restrict__ b0,
                     const double* __restrict__ a1, const double* __restrict__ b1,
-                    const double* __restrict__ a2, const double* __restrict__ b2, long long rs, int k,
+                    const double* __restrict__ a2, const double* __restrict__ b2, long long rs,
                     double* __restrict__ dots) {
+  constexpr int U = 4;
   __shared__ double scratch[kDotThreads / 32];
   __shared__ double part[3];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int s = blockIdx.y;
   const long long lo = n * rank / kDotCluster, hi = n * (rank + 1) / kDotCluster;
-  const double* A[3] = {a0, a1, a2};
-  const double* Bv[3] = {b0, b1, b2};
-  for (int j = 0; j < k; ++j) {
-    const double* a = A[j] + (size_t)s * rs;
-    const double* b = Bv[j] + (size_t)s * rs;
-    double acc0 = 0.0, acc1 = 0.0;
+  const double* A[3] = {a0 + (size_t)s * rs, K > 1 ? a1 + (size_t)s * rs : nullptr,
+                        K > 2 ? a2 + (size_t)s * rs : nullptr};
+  const double* Bv[3] = {b0 + (size_t)s * rs, K > 1 ? b1 + (size_t)s * rs : nullptr,
+                         K > 2 ? b2 + (size_t)s * rs : nullptr};
+  // one pair after the other (a pass over each pair's chunk), U loads of each in flight
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    double acc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc[u] = 0.0;
     long long i = lo + threadIdx.x;
-    for (; i + kDotThreads < hi; i += 2 * kDotThreads) {
-      acc0 = fma(__ldg(a + i), __ldg(b + i), acc0);
-      acc1 = fma(__ldg(a + i + kDotThreads), __ldg(b + i + kDotThreads), acc1);
+    for (; i + (U - 1) * kDotThreads < hi; i += U * kDotThreads) {
+      double va[U], vb[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        va[u] = __ldg(A[j] + i + u * kDotThreads);
+        vb[u] = __ldg(Bv[j] + i + u * kDotThreads);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) acc[u] = fma(va[u], vb[u], acc[u]);
     }
-    if (i < hi) acc0 = fma(__ldg(a + i), __ldg(b + i), acc0);
-    const double t = block_sum<kDotThreads>(acc0 + acc1, scratch);
+    for (; i < hi; i += kDotThreads) acc[0] = fma(__ldg(A[j] + i), __ldg(Bv[j] + i), acc[0]);
+    const double t = block_sum<kDotThreads>((acc[0] + acc[1]) + (acc[2] + acc[3]), scratch);
     if (threadIdx.x == 0) part[j] = t;
   }
   cluster.sync();
-  if (rank == 0 && threadIdx.x < k) {
+  if (rank == 0 && threadIdx.x < K) {
     double t = 0.0;
     for (int r = 0; r < kDotCluster; ++r) t += cluster.map_shared_rank(part, r)[threadIdx.x];
-    dots[(size_t)s * k + threadIdx.x] = t;
+    dots[(size_t)s * K + threadIdx.x] = t;
   }
   cluster.sync();
 }
@@ -274,7 +382,22 @@ extern "C" int stt_element_sens(int d, int nelx, int nely, int nrows, const doub
   const int nel = nelx * nely;
   cudaStream_t st = (cudaStream_t)stream;
   dim3 grid(grid1(nel), nrows);
-  if (d == 2) {
+  double m[8];
+  if (d == 2 && (((uintptr_t)U | (uintptr_t)lam) & 15) == 0 && (U_rs & 1) == 0 && (lam_rs & 1) == 0 &&
+      modal_from_ke(2, KE, m)) {
+    // the modal form: a column-marching pass (16-byte node loads need aligned rows)
+    const int strips = (nelx + kSensCols - 1) / kSensCols;
+    int band = 32;
+    while (band > 4 && (long long)((strips + 3) / 4) * ((nely + band - 1) / band) * nrows < 4 * 148) band /= 2;
+    const dim3 g((strips + 3) / 4, (nely + band - 1) / band, nrows);
+    const ModalE q{m[0], m[1], m[2], m[3], m[4], m[5]};
+    if (lam)
+      element_sens_modal_kernel<true><<<g, 128, 0, st>>>(U, U_rs, lam, lam_rs, ce, gdens, greac, e_rs, nelx, nely,
+                                                         q);
+    else
+      element_sens_modal_kernel<false><<<g, 128, 0, st>>>(U, U_rs, nullptr, 0, ce, nullptr, nullptr, e_rs, nelx,
+                                                          nely, q);
+  } else if (d == 2) {
     KEd<2> k;
     for (int i = 0; i < 64; ++i) k.v[i] = KE[i];
     element_sens_kernel<2><<<grid, 256, 0, st>>>(U, U_rs, lam, lam_rs, ce, gdens, greac, e_rs, nelx, nel, k);
@@ -336,8 +459,14 @@ extern "C" int stt_vec_dots(int nrows, long long n, const double* a0, const doub
   if (nrows <= 0 || n <= 0 || !a0 || !b0 || !dots) return set_error(STT_ERR_INVALID, "stt_vec_dots: bad arguments");
   if (nrows > 65535) return set_error(STT_ERR_INVALID, "stt_vec_dots: too many rows");
   const int k = (a1 && b1) ? ((a2 && b2) ? 3 : 2) : 1;
-  vec_dots_kernel<<<dim3(kDotCluster, nrows), kDotThreads, 0, (cudaStream_t)stream>>>(n, a0, b0, a1, b1, a2,
-                                                                                       b2, rs, k, dots);
+  const dim3 g(kDotCluster, nrows);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (k == 1)
+    vec_dots_kernel<1><<<g, kDotThreads, 0, st>>>(n, a0, b0, a1, b1, a2, b2, rs, dots);
+  else if (k == 2)
+    vec_dots_kernel<2><<<g, kDotThreads, 0, st>>>(n, a0, b0, a1, b1, a2, b2, rs, dots);
+  else
+    vec_dots_kernel<3><<<g, kDotThreads, 0, st>>>(n, a0, b0, a1, b1, a2, b2, rs, dots);
   return check_launch("vec_dots");
 }
 
