@@ -420,7 +420,80 @@ __global__ void keff_galerkin_kernel(const double* __restrict__ kf, int fnelx, i
   for (int j = 0; j < NK; ++j) o[j] = out[j];
 }
 
-// Element-matrix sources for the stencil assembly.
+// keff_galerkin_kernel for plane stress (8 x 8 element matrices), a warp per coarse
+// element: per child m the child's matrix K is staged in the warp's shared tile (two
+// entries a lane, 512 coalesced bytes), T = K S_m and then S_m^T T are formed two entries
+// a lane (each a dot of length 8 over shared rows), and the accumulated matrix is stored
+// 256 bytes at a time.  The interpolation tables S (nm x 8 x 8) sit in shared memory.
+constexpr int kGalWarps = 8;
+
+__global__ void __launch_bounds__(32 * kGalWarps) keff_galerkin_warp_kernel(
+    const double* __restrict__ kf, int fnelx, int fnel, const double* __restrict__ S, int kx, int ky, int cnelx,
+    int cnel, double* __restrict__ kc) {
+  constexpr int NK = 8, NE = 64;
+  __shared__ double Ss[9 * NE];
+  __shared__ double Ks[kGalWarps][NE], Ts[kGalWarps][NE];
+  const int nm = kx * ky;
+  for (int t = threadIdx.x; t < nm * NE; t += blockDim.x) Ss[t] = S[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int h = blockIdx.y;
+  const double* kh = kf + (size_t)h * fnel * NE;
+  double* ch = kc + (size_t)h * cnel * NE;
+  // this lane's two entries (i, j): e = lane and lane + 32
+  const int i0 = lane >> 3, j0 = lane & 7, i1 = i0 + 4;
+  // the child matrices of the warp's elements stream through two registers a lane, the
+  // next child's loads in flight while the current one is multiplied
+  auto child = [&](int E, int m) {
+    const int R = E / cnelx, C = E - R * cnelx, my = m / kx, mx = m - my * kx;
+    return kh + ((size_t)(R * ky + my) * fnelx + (C * kx + mx)) * NE;
+  };
+  const int E0 = blockIdx.x * kGalWarps + w, dE = gridDim.x * kGalWarps;
+  double n0 = 0.0, n1 = 0.0;
+  if (E0 < cnel) {
+    n0 = __ldg(child(E0, 0) + lane);
+    n1 = __ldg(child(E0, 0) + lane + 32);
+  }
+  for (int E = E0; E < cnel; E += dE) {  // uniform per warp
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int m = 0; m < nm; ++m) {
+      Ks[w][lane] = n0;
+      Ks[w][lane + 32] = n1;
+      // prefetch the next child (of this element, or of the warp's next element)
+      const int En = m + 1 < nm ? E : E + dE, mn = m + 1 < nm ? m + 1 : 0;
+      if (En < cnel) {
+        n0 = __ldg(child(En, mn) + lane);
+        n1 = __ldg(child(En, mn) + lane + 32);
+      }
+      __syncwarp();
+      const double* Sm = Ss + m * NE;
+      // T[p][j] = sum_q K[p][q] S_m[q][j] for (p, j) = (i0, j0) and (i1, j0)
+      double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+      for (int q = 0; q < NK; ++q) {
+        const double sq = Sm[q * NK + j0];
+        t0 = fma(Ks[w][i0 * NK + q], sq, t0);
+        t1 = fma(Ks[w][i1 * NK + q], sq, t1);
+      }
+      Ts[w][lane] = t0;
+      Ts[w][lane + 32] = t1;
+      __syncwarp();
+      // out[i][j] += sum_p S_m[p][i] T[p][j]
+#pragma unroll
+      for (int pp = 0; pp < NK; ++pp) {
+        const double tp = Ts[w][pp * NK + j0];
+        acc0 = fma(Sm[pp * NK + i0], tp, acc0);
+        acc1 = fma(Sm[pp * NK + i1], tp, acc1);
+      }
+      __syncwarp();  // the tiles are rewritten for the next child
+    }
+    double* out = ch + (size_t)E * NE;
+    out[lane] = acc0;
+    out[lane + 32] = acc1;
+  }
+}
+
+// Element-matrix sources for the stencil assembly.// Element-matrix sources for the stencil assembly.
 template <int D>
 struct KeffSource {  // explicit element matrices
   const double* keff;
@@ -1131,8 +1204,15 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
                                                          (int)c.nel, kc);
         }
       } else {
-        keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
-                                                   (int)c.nel, kc);
+        if (D == 2) {
+          const long long want = std::max<long long>(1, 148LL * 8 / H);
+          const dim3 gw((unsigned)std::min<long long>(want, (c.nel + kGalWarps - 1) / kGalWarps), H);
+          keff_galerkin_warp_kernel<<<gw, 32 * kGalWarps, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
+                                                                   (int)c.nel, kc);
+        } else {
+          keff_galerkin_kernel<D><<<g, 256, 0, st>>>(kprev, f.nelx, (int)f.nel, S, f.kx, f.ky, c.nelx,
+                                                     (int)c.nel, kc);
+        }
       }
       stencil_kernel<D, KeffSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
           KeffSource<D>{kc, (int)c.nel}, c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
