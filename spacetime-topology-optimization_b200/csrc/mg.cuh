@@ -920,9 +920,9 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
 // st_sweep2_kernel's passes chained like l0_presmooth_kernel: PRE runs the first sweep from
 // zero, a sweep and the residual (writes x2 and r); POST runs two sweeps from x0 (writes
 // x2).  Stage A emits node row f - 1 for the front row f, stage B node row f - 2 from stage
-// A's output, so the intermediate iterate never leaves registers.  Stage A's coefficient
-// row streams from HBM one step ahead; stage B reads the same rows one step later, from
-// cache.  Lanes 2..29 are output (28 columns a warp).
+// A's output, so the intermediate iterate never leaves registers.  Stage B reads stage
+// A's coefficient rows one step later, from cache.  Lanes 2..29 are output (28 columns a
+// warp).
 constexpr int kStChainCols = 28;
 
 inline dim3 st_chain_grid(int nelx, int nely, int rows) {
@@ -991,7 +991,7 @@ struct StStage {
 };
 
 template <int D, typename T, bool PRE>
-__global__ void __launch_bounds__(kQThreads, 4) st_chain_kernel(
+__global__ void __launch_bounds__(kQThreads, 6) st_chain_kernel(
     const T* __restrict__ x0, const T* __restrict__ b, T* __restrict__ out_x, T* __restrict__ out_r,
     long long vec_rs, const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
     const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega) {
@@ -1069,16 +1069,24 @@ __global__ void __launch_bounds__(kQThreads, 4) st_chain_kernel(
   StStage<D, T> A, B;
   A.reset();
   B.reset();
+  // D = 1: stage A's coefficient row streams one step ahead; D = 2: loaded at the step
+  // (its 20 coefficients a row would cost the registers of two more blocks an SM)
+  constexpr bool PF = D == 1;
   const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
   Front qf;
-  Row qa;  // stage A's row (f - 1), one step ahead
+  Row qa;
   load_front(f0, qf);
-  load_row(f0 - 1, qa);
+  if constexpr (PF) load_row(f0 - 1, qa);
   for (int f = f0; f <= f1; ++f) {
     const Front F = qf;
-    const Row RA = qa;
     load_front(f + 1, qf);
-    load_row(f, qa);
+    Row RA;  // stage A's row (f - 1)
+    if constexpr (PF) {
+      RA = qa;
+      load_row(f, qa);
+    } else {
+      load_row(f - 1, RA);
+    }
     Row RB;  // stage B's row (f - 2): stage A's row of the previous step, from cache
     load_row(f - 2, RB);
     T xin[D];
