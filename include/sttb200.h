@@ -118,6 +118,11 @@ int stt_hier_create(stt_hier** out, void* workspace, long long ws_bytes, int d, 
                     const double* KE, int max_coarse_elements, int precision,
                     stt_stream_t stream);
 
+/* The build does not synchronise: its device checks (a coarse pivot <= 0, a coarse
+ * operator beyond its planned band) are reported by stt_hier_status (which synchronises
+ * the stream) and by the first convergence check of stt_pcg_mg on the hierarchy. */
+int stt_hier_status(const stt_hier* h, stt_stream_t stream);
+
 /* A view of h restricted to batch rows: batch row s uses hierarchy row row_map[s]
  * (device int32, caller-owned, kept alive while the view is used). */
 int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier** out);

@@ -72,6 +72,9 @@ inline int level_node_count(int nelx, int nely) { return (nelx + 1) * (nely + 1)
 // Returns the bytes needed.
 long long plan_hierarchy(stt_hier_impl& h, char* base);
 
+// The build's device status word (copied to the host) as an STT error code.
+int hier_status_code(int s);
+
 }  // namespace stt
 
 struct stt_hier : stt::stt_hier_impl {};

@@ -1541,21 +1541,30 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   if (rc == STT_OK) rc = d == 2 ? build_levels<2>(h, rho, rho_rs, reaction, r_rs, fixed, st)
                                 : build_levels<1>(h, rho, rho_rs, reaction, r_rs, fixed, st);
   if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, st) : build_coarse<1>(h, st);
-  if (rc == STT_OK) {
-    int s = 0;
-    rc = check_cuda(cudaMemcpyAsync(&s, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy");
-    if (rc == STT_OK) rc = check_cuda(cudaStreamSynchronize(st), "hierarchy build");
-    if (rc == STT_OK && (s & 1))
-      rc = set_error(STT_ERR_INVALID, "coarse operator is not positive definite (Cholesky pivot <= 0)");
-    if (rc == STT_OK && (s & 2))
-      rc = set_error(STT_ERR_INVALID, "coarse operator exceeds its planned band");
-  }
   if (rc != STT_OK) {
     delete h;
     return rc;
   }
+  // no synchronisation here: the build's device checks (coarse pivots, band) are read by
+  // stt_hier_status, and by the first convergence check of a solve on the hierarchy
   *out = h;
   return STT_OK;
+}
+
+// The build's device status word as an error code (host int s, already copied).
+int stt::hier_status_code(int s) {
+  if (s & 1) return set_error(STT_ERR_INVALID, "coarse operator is not positive definite (Cholesky pivot <= 0)");
+  if (s & 2) return set_error(STT_ERR_INVALID, "coarse operator exceeds its planned band");
+  return STT_OK;
+}
+
+extern "C" int stt_hier_status(const stt_hier* h, stt_stream_t stream) {
+  if (!h) return set_error(STT_ERR_INVALID, "stt_hier_status: null hierarchy");
+  cudaStream_t st = (cudaStream_t)stream;
+  int s = 0;
+  STT_TRY(check_cuda(cudaMemcpyAsync(&s, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy"));
+  STT_TRY(check_cuda(cudaStreamSynchronize(st), "hierarchy build"));
+  return hier_status_code(s);
 }
 
 extern "C" int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier** out) {

@@ -844,9 +844,20 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   init(has_x0 ? x : nullptr, pp, 0);
   STT_TRY(check_launch("pcg init"));
   std::vector<RowState> host(nrows);
+  // the first read also carries the hierarchy build's status word (the build does not
+  // synchronise): a failed coarse factorisation surfaces here
+  int hstatus = 0;
+  bool hchecked = false;
   auto pull = [&]() -> int {
     STT_TRY(check_cuda(cudaMemcpyAsync(host.data(), w.rs, sizeof(RowState) * nrows, cudaMemcpyDeviceToHost, st), "row state"));
-    return check_cuda(cudaStreamSynchronize(st), "pcg sync");
+    if (!hchecked)
+      STT_TRY(check_cuda(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy"));
+    STT_TRY(check_cuda(cudaStreamSynchronize(st), "pcg sync"));
+    if (!hchecked) {
+      hchecked = true;
+      STT_TRY(hier_status_code(hstatus));
+    }
+    return STT_OK;
   };
   auto n_active = [&]() {
     int a = 0;

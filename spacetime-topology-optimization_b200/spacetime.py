@@ -259,7 +259,7 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
     alpha = drain_beta / (nelx * nely)
     reac = torch.full_like(chi, alpha)
     hl = torch_mg.build_hierarchy(chi, P.edof1, P.KEh, P.heat_mask, nelx, nely, reaction=reac,
-                                  max_coarse_elements=max_coarse_elements, precision=precision)
+                                  max_coarse_elements=max_coarse_elements, precision=precision, check=False)
     rdiag = hl[0].reaction_diag.reshape(G, nnode).contiguous()
     Klift = torch.empty(G, nnode, dtype=torch.float64, device=dev)
     _lib.check(L.stt_q4_apply(_lib.STT_FP64, 1, nelx, nely, G, _lib.ptr(P.lift), 0, _lib.ptr(Klift),
@@ -301,14 +301,14 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
             members.append(m)
         if batched:
             sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
-                                          max_coarse_elements=max_coarse_elements, precision=precision)
+                                          max_coarse_elements=max_coarse_elements, precision=precision, check=False)
             U = _pcg(sl, F, None, rtol, max_iter, "stage_n_iter", info)
             stage_levels = [sl]
         else:
             Us, stage_levels = [], []
             for s in range(S):
                 sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
-                                              max_coarse_elements=max_coarse_elements, precision=precision)
+                                              max_coarse_elements=max_coarse_elements, precision=precision, check=False)
                 Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
                 stage_levels.append(sl)
             U = torch.stack(Us)

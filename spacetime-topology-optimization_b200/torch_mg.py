@@ -78,7 +78,8 @@ class _Hierarchy:
 
     @classmethod
     def build(cls, density: Tensor, mask: Tensor, KE: Tensor, nelx: int, nely: int,
-              reaction: Tensor | None, max_coarse_elements: int, precision: str | None):
+              reaction: Tensor | None, max_coarse_elements: int, precision: str | None,
+              check: bool = True):
         _lib.require_cuda(density, mask, reaction)
         d = KE.shape[-1] // 4
         nel = nelx * nely
@@ -102,6 +103,8 @@ class _Hierarchy:
             max_coarse_elements, prec, _lib.stream()))
         h = cls(handle, ws, d, hrows, batch_shape, density.device, ke_host)
         h.precision = "fp64" if prec == _lib.STT_FP64 else "mixed"
+        if check:  # the reference raises at build time on a failed coarse factorisation
+            _lib.check(_lib.lib().stt_hier_status(handle, _lib.stream()))
         return h
 
     def select(self, rows: Tensor) -> "_Hierarchy":
@@ -246,13 +249,15 @@ class _Level:
 def build_hierarchy(density: Tensor, edofMat: Tensor, KE: Tensor, mask: Tensor, nelx: int,
                     nely: int, *, reaction: Tensor | None = None,
                     max_coarse_elements: int = MAX_COARSE_ELEMENTS,
-                    precision: str | None = None) -> list[_Level]:
-    """Levels from finest to coarsest (sttopt/torch_mg.py:293-400), built on the device."""
+                    precision: str | None = None, check: bool = True) -> list[_Level]:
+    """Levels from finest to coarsest (sttopt/torch_mg.py:293-400), built on the device.
+    ``check=False`` skips the build-time synchronisation of the coarse factorisation's
+    checks; a failure then surfaces at the first solve on the hierarchy."""
     ndof = mask.shape[-1]
     d = KE.shape[-1] // 4
     if d * (nelx + 1) * (nely + 1) != ndof:
         raise ValueError("mask does not match the grid")
-    h = _Hierarchy.build(density, mask, KE, nelx, nely, reaction, max_coarse_elements, precision)
+    h = _Hierarchy.build(density, mask, KE, nelx, nely, reaction, max_coarse_elements, precision, check)
     reaction_diag = None
     if reaction is not None:
         reaction_diag = torch_fem.lumped_reaction(reaction.detach(), edofMat, ndof)

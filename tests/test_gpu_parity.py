@@ -238,6 +238,23 @@ def test_keff_matvec_matches_oracle(m, d):
     assert rel_err(got1, O.keff_matvec(U, keff[0], edof, ndof)) < 1e-14
 
 
+def test_coarse_factorisation_failure_is_reported(m, pkg):
+    """A coarse operator that is not positive definite (a negated KE): the default build
+    raises at once; the unsynchronised build (check=False) raises at the first solve."""
+    from sttopt_b200 import _lib
+
+    nelx, nely = 24, 12
+    F, mask = O.cantilever_point_load(nelx, nely)
+    KE, edof = T(-O.plane_stress_KE(0.3)), T(O.element_dof_map(nelx, nely), torch.int64)
+    dens = T(np.full(nelx * nely, 0.5))
+    with pytest.raises(_lib.SttError, match="positive definite"):
+        m.mg.build_hierarchy(dens, edof, KE, T(mask, torch.bool), nelx, nely, max_coarse_elements=50)
+    levels = m.mg.build_hierarchy(dens, edof, KE, T(mask, torch.bool), nelx, nely, max_coarse_elements=50,
+                                  check=False)
+    with pytest.raises(_lib.SttError, match="positive definite"):
+        m.fem.pcg(levels[0], T(F), m.mg.VCycle(levels), rtol=1e-8, max_iter=5)
+
+
 def test_mbb_config_solve_compliance_and_sensitivities(m):
     """120 x 40 MBB, rho = 0.5: U, iterations, compliance, dc/dx vs the reference."""
     g = golden("mbb120x40")
