@@ -73,6 +73,7 @@ static void galerkin_table(const double* S, const double* K, int nm, int nk, dou
   }
 }
 
+constexpr int kCoarseInvMaxRows = 48;  // hierarchy rows up to which the FP32 cycle uses the coarse inverse
 constexpr int kTableStride = 9 * 64;   // doubles per table (max 9 children x 8 x 8)
 constexpr int kGrandStride = 81 * 64;  // doubles per grandchild table (max 81 x 8 x 8)
 constexpr int kChildStencilSize = 2 * 5 * 4 * 4 * 9;  // stencil_children_kernel tables, D = 2, 9 children
@@ -219,9 +220,13 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     if (co.B < 32) co.B = 32;
     co.nb = (co.n + co.B - 1) / co.B;
     co.blocks = (double*)carve(p, used, 8LL * h.hrows * co.nb * 4 * co.B * co.B);
-    // the FP32 cycle solves the coarsest level with the explicit inverse (one GEMV)
+    // the FP32 cycle solves the coarsest level with the explicit inverse (one GEMV) while
+    // the hierarchy has few rows: the GEMV streams np^2 doubles a row per cycle, the block
+    // solves ~8 B^2 nb, and from about 48 rows on (one CTA a row filling the SMs) the
+    // latency-bound block solves cost less than the inverse's bytes and its build
     const long long np = (long long)co.nb * co.B;
-    co.inv = (f32 && co.B <= 64) ? (double*)carve(p, used, 8LL * h.hrows * np * np) : nullptr;
+    co.inv = (f32 && co.B <= 64 && h.hrows <= kCoarseInvMaxRows) ? (double*)carve(p, used, 8LL * h.hrows * np * np)
+                                                                   : nullptr;
   }
   h.tables = (double*)carve(p, used, 8LL * kMaxLevels * 3 * kTableStride);
   h.gtables = (double*)carve(p, used, 8LL * (2 * kGrandStride + kChildStencilSize));

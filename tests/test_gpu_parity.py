@@ -238,6 +238,22 @@ def test_keff_matvec_matches_oracle(m, d):
     assert rel_err(got1, O.keff_matvec(U, keff[0], edof, ndof)) < 1e-14
 
 
+def test_vcycle_fp32_many_rows_uses_block_solves(m):
+    """With more hierarchy rows than the coarse inverse is kept for, the FP32 cycle solves
+    the coarsest level by the block-banded Cholesky solves: same agreement with FP64."""
+    rng = np.random.default_rng(9)
+    nelx, nely, rows = 64, 32, 50
+    x = rng.uniform(1e-3, 1.0, (rows, nelx * nely))
+    F, mask = O.cantilever_point_load(nelx, nely)
+    dens = O.simp_density(x, EMIN, EMAX, PENAL)
+    KE, edof = T(O.plane_stress_KE(0.3)), T(O.element_dof_map(nelx, nely), torch.int64)
+    lv = [m.mg.build_hierarchy(T(dens), edof, KE, T(mask, torch.bool), nelx, nely, precision=p)
+          for p in ("fp64", "mixed")]
+    u = O.project(rng.standard_normal((rows, len(F))), mask)
+    z64, z32 = (m.mg.VCycle(levels)(T(u)).cpu().numpy() for levels in lv)
+    assert rel_err(z32, z64) < 1e-4
+
+
 def test_coarse_factorisation_failure_is_reported(m, pkg):
     """A coarse operator that is not positive definite (a negated KE): the default build
     raises at once; the unsynchronised build (check=False) raises at the first solve."""
