@@ -19,6 +19,7 @@ Multi-GPU: the path has no exchange step, so N ranks run N independent replicas
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -34,9 +35,10 @@ NELX, NELY, N_STAGE = 2048, 1024, 16
 SEED = 3
 METRIC = "stage solves/s (space-time objective + full gradient, 2048x1024 Q4, 16 stages, rtol 1e-8)"
 UNIT = "stage solves/s"
-# Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the roofline
-# kernel from the ncu capture summarised in profiles/q4_apply_fp32_2048x1024_16rows.md.
-NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576}
+# Per-launch DRAM bytes of the roofline kernels from ncu captures: the FP32 apply at 16 rows
+# (profiles/q4_apply_fp32_2048x1024_16rows.md), and the FP64 p.Ap pass per stage row, from a
+# 2-row capture scaled by the rows (profiles/pcg_pap_fp64_2048x1024.md).
+NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576, "pcg_pap_fp64_per_row": 186447000}
 
 
 def parse():
@@ -53,6 +55,9 @@ def parse():
     ap.add_argument("--vcycle-only", action="store_true",
                     help="run only V-cycles of the stage solve's 16-row mixed hierarchy (the small case for "
                          "ncu captures of the cycle's kernels; seeded uniform densities in [1e-3, 1])")
+    ap.add_argument("--pcg-only", action="store_true",
+                    help="run only a 2-row plane-stress PCG on the 2048x1024 grid (the small case for ncu "
+                         "captures of the outer PCG's p.Ap pass; seeded densities and loads)")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the batched uneven multi-problem measurement")
     ap.add_argument("--uneven-only", action="store_true",
@@ -175,6 +180,31 @@ def run_vcycles(dev, steps, warmup):
             "z_norm": float(z.norm())}
 
 
+def run_pcg_small(dev, rows=2):
+    """One mixed-precision PCG solve of `rows` plane-stress rows on the 2048x1024 grid (the
+    bench's mesh and clamp; seeded densities and loads): iterations and time."""
+    import numpy as np
+    import torch
+
+    from sttopt_b200 import fem, torch_fem, torch_mg
+
+    rng = np.random.default_rng(SEED)
+    rho = torch.as_tensor(rng.uniform(1e-3, 1.0, (rows, NELX * NELY)), device=dev)
+    edof = torch.as_tensor(fem.element_dof_map(NELX, NELY, 2), device=dev)
+    KE = torch.as_tensor(fem.plane_stress_KE(0.3), device=dev)
+    ndof = 2 * (NELX + 1) * (NELY + 1)
+    mask = torch.ones(ndof, dtype=torch.bool, device=dev)
+    mask[-2 * (NELX + 1):] = False
+    levels = torch_mg.build_hierarchy(rho, edof, KE, mask, NELX, NELY, precision="mixed")
+    F = torch.as_tensor(rng.standard_normal((rows, ndof)), device=dev) * mask
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    _, n = torch_fem.pcg(levels[0], F, torch_mg.VCycle(levels), rtol=1e-8, max_iter=200)
+    b.record()
+    torch.cuda.synchronize()
+    return {"rows": rows, "n_iter": n, "ms": a.elapsed_time(b)}
+
+
 def run_uneven(dev, steps=2, warmup=1):
     """Stage solves per second over the 64 uneven problems (objective + full gradient of
     each), grouped per grid size into batched solves on concurrent streams."""
@@ -294,6 +324,9 @@ def main():
         roof, detail = roofline(_lib, problem, {"U": u}, dev)
         print(json.dumps({"roofline": roof, "roofline_detail": detail}), flush=True)
         return 0
+    if args.pcg_only:
+        print(json.dumps({"pcg": run_pcg_small(dev)}), flush=True)
+        return 0
     if args.vcycle_only:
         print(json.dumps({"vcycle": run_vcycles(dev, max(args.steps, 1), max(args.warmup, 0))}), flush=True)
         return 0
@@ -322,10 +355,12 @@ def main():
     # timed region: inputs resident in HBM
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    L = _lib.lib()
     with ClockSampler(local) as clk:
         barrier()
         torch.cuda.synchronize()
         allocs0 = device_allocs()
+        L.stt_pap_timing(1)  # events around the plane-stress p.Ap passes (the dominant kernel)
         start.record()
         for k in range(args.steps):
             marks[k].record()
@@ -337,6 +372,10 @@ def main():
         torch.cuda.synchronize()
         barrier()
     elapsed_ms = start.elapsed_time(end)
+    pap = (ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong())
+    L.stt_pap_timing_read(ctypes.byref(pap[0]), ctypes.byref(pap[1]), ctypes.byref(pap[2]))
+    L.stt_pap_timing(0)
+    pap_live = {"ms": pap[0].value, "launches": pap[1].value, "rows": pap[2].value}
     timed_detail = {"step_ms": [round(marks[k].elapsed_time(marks[k + 1]), 3) for k in range(args.steps)],
                     "device_allocs": device_allocs() - allocs0}
     if world > 1:
@@ -391,7 +430,7 @@ def main():
 
     extra = {}
     if rank == 0:
-        extra["roofline"], extra["roofline_detail"] = roofline(_lib, problem, out, dev)
+        extra["roofline"], extra["roofline_detail"] = roofline(_lib, problem, out, dev, pap_live)
         # the plain FP64 GPU form: unbatched stages, FP64 V-cycle
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -444,9 +483,10 @@ def main():
     return 0
 
 
-def roofline(_lib, P, out, dev):
-    """Live CUDA-event timing of the level-0 operator apply over the 16 stage rows:
-    FP32 (the V-cycle's fine-level kernel) and FP64 (the outer PCG's)."""
+def roofline(_lib, P, out, dev, pap_live=None):
+    """The dominant kernel of the step, the outer PCG's FP64 p.Ap pass, timed live inside
+    the timed region (CUDA events around its launches, stt_pap_timing); and, beside it,
+    the level-0 operator apply over the 16 stage rows timed alone in FP32 and FP64."""
     import torch
 
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -480,10 +520,28 @@ def roofline(_lib, P, out, dev):
         alg = rows * (2 * ndof * es + nel * es)  # read u, write Ku, read rho (flags: 1 B/node not counted)
         gbs = alg / (ms * 1e-3) / 1e9
         detail[name] = {"achieved": gbs, "ms_per_launch": ms, "algorithmic_bytes": alg, "frac": gbs / peak}
-    main_k = detail["l0_apply_fp32_16rows"]
-    roof = {"bound": "hbm", "achieved": main_k["achieved"], "peak": peak, "unit": "GB/s",
-            "frac": main_k["frac"], "peak_source": peak_src, "kernel": "l0 Q4 apply, FP32, 16 stage rows",
-            "traffic": NCU_TRAFFIC["l0_apply_fp32_16rows"]}
+    for k in ("l0_apply_fp32_16rows",):
+        detail[k]["traffic"] = NCU_TRAFFIC[k]
+    if pap_live and pap_live["launches"]:
+        # per row and launch: read p_old 8 ndof, z 4 ndof, x 8 ndof and rho 8 nel; write p, Ap and
+        # x 8 ndof each (flags, 1 B a node, not counted)
+        per_row = 44 * ndof + 8 * nel
+        alg = per_row * pap_live["rows"] / pap_live["launches"]
+        ms = pap_live["ms"] / pap_live["launches"]
+        gbs = alg / (ms * 1e-3) / 1e9
+        rows_per = pap_live["rows"] / pap_live["launches"]
+        traffic = NCU_TRAFFIC.get("pcg_pap_fp64_per_row")
+        roof = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                "peak_source": peak_src,
+                "kernel": "pcg_pap_kernel (FP64 outer PCG: p = beta p + z, A p, p.Ap, deferred x update), "
+                          f"{rows_per:.0f} stage rows, timed live over {pap_live['launches']} launches",
+                "algorithmic_bytes": alg, "ms_per_launch": ms,
+                "traffic": None if traffic is None else traffic * rows_per}
+    else:
+        main_k = detail["l0_apply_fp32_16rows"]
+        roof = {"bound": "hbm", "achieved": main_k["achieved"], "peak": peak, "unit": "GB/s",
+                "frac": main_k["frac"], "peak_source": peak_src, "kernel": "l0 Q4 apply, FP32, 16 stage rows",
+                "traffic": NCU_TRAFFIC["l0_apply_fp32_16rows"]}
     return roof, detail
 
 

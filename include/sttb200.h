@@ -156,7 +156,15 @@ int stt_keff_apply(int d, int nelx, int nely, int nrows, const double* U, long l
                    const double* keff, long long k_rs, double* out, long long o_rs,
                    stt_stream_t stream);
 
-/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. *//* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
+/* Live timing of the plane-stress solves' steady-state p.Ap passes (pcg_pap_kernel with a
+ * deferred x update), for measurement: while enabled (stt_pap_timing(1), which also resets
+ * the totals) each such launch of stt_pcg_mg is bracketed by CUDA events on its stream;
+ * stt_pap_timing_read returns the summed milliseconds, the launches and the batch rows
+ * summed over the launches.  No reference counterpart. */
+int stt_pap_timing(int enable);
+int stt_pap_timing_read(double* total_ms, long long* launches, long long* rows);
+
+/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
 long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int gamma);
 
 /* z[s] = M r[s], one V-cycle (damped Jacobi omega, n_smooth sweeps each way, gamma

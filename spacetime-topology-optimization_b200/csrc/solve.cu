@@ -808,6 +808,59 @@ static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r,
   return check_launch("vcycle");
 }
 
+// Optional live timing of the plane-stress solves' steady-state p.Ap passes (the step's
+// dominant kernel, pcg_pap_kernel<2, ..., PMODE 2, XP>): while enabled, every such launch
+// is bracketed by CUDA events on its stream, and the solve adds the elapsed times at its
+// end (after its final synchronisation).  Off by default; stt_pap_timing.
+struct PapTiming {
+  std::mutex mu;
+  bool on = false;
+  double total_ms = 0.0;
+  long long launches = 0;
+  long long rows = 0;  // summed over the launches (bytes scale with the rows)
+};
+static PapTiming g_pap;
+
+struct PapEvents {
+  std::vector<cudaEvent_t> ev;  // pairs (start, stop)
+  std::vector<int> rows;
+  size_t used = 0;
+  ~PapEvents() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+  int record(cudaStream_t st, bool start, int nrows) {
+    const size_t i = start ? used : used + 1;
+    while (ev.size() <= i) {
+      cudaEvent_t e;
+      STT_TRY(check_cuda(cudaEventCreate(&e), "timing event"));
+      ev.push_back(e);
+    }
+    STT_TRY(check_cuda(cudaEventRecord(ev[i], st), "timing record"));
+    if (!start) {
+      rows.push_back(nrows);
+      used += 2;
+    }
+    return STT_OK;
+  }
+  // after the stream has synchronised
+  void flush() {
+    if (!used) return;
+    double ms = 0.0;
+    long long nr = 0;
+    for (size_t i = 0; i + 1 < used; i += 2) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[i], ev[i + 1]) == cudaSuccess) ms += t;
+    }
+    for (int r : rows) nr += r;
+    std::lock_guard<std::mutex> lock(g_pap.mu);
+    g_pap.total_ms += ms;
+    g_pap.launches += (long long)(used / 2);
+    g_pap.rows += nr;
+    used = 0;
+    rows.clear();
+  }
+};
+
 template <int D, typename T>
 static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, long long b_rs,
                    double* x, long long x_rs, int has_x0, double rtol, int max_iter, double omega,
@@ -825,6 +878,12 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   STT_TRY(check_cuda(cudaMemsetAsync(w.rs, 0, sizeof(RowState) * nrows, st), "memset rows"));
   if (!has_x0) rows_zero_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(x, x_rs, nd);
   const MQ<double> mq = mq_cast<double>(h->mq);
+  bool timing = false;
+  if (D == 2) {
+    std::lock_guard<std::mutex> lock(g_pap.mu);
+    timing = g_pap.on;
+  }
+  PapEvents pev;
   // r = b - A x (x may be null: r = b); replace = 1 keeps ||b|| (true-residual replacement)
   auto init = [&](const double* xx, const PcgParams& pq, int replace) {
 #define STT_INIT(MODAL, RD)                                                                              \
@@ -908,9 +967,15 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       else STT_PAP(false, false, PM, XP);     \
     }                                       \
   } while (0)
-      if (it == 1) STT_PAP2(1, false);
-      else if (pending) STT_PAP2(2, true);
-      else STT_PAP2(2, false);
+      if (it == 1) {
+        STT_PAP2(1, false);
+      } else if (pending) {
+        if (timing) STT_TRY(pev.record(st, true, nrows));
+        STT_PAP2(2, true);
+        if (timing) STT_TRY(pev.record(st, false, nrows));
+      } else {
+        STT_PAP2(2, false);
+      }
 #undef STT_PAP2
 #undef STT_PAP
       float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
@@ -941,6 +1006,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     STT_TRY(check_launch("pcg flush"));
   }
   STT_TRY(pull());
+  if (timing) pev.flush();
   int worst = 0, status = STT_OK;
   for (int s = 0; s < nrows; ++s) {
     rel_out[s] = host[s].rel;
@@ -1122,4 +1188,22 @@ extern "C" int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r,
   void* scratch = nullptr;
   STT_TRY(vcycle_scratch_address(&scratch));
   return stt_vcycle(h, nrows, r, r_rs, z, z_rs, omega, n_smooth, gamma, scratch, kVCycleScratchBytes, stream);
+}
+
+extern "C" int stt_pap_timing(int enable) {
+  std::lock_guard<std::mutex> lock(g_pap.mu);
+  g_pap.on = enable != 0;
+  g_pap.total_ms = 0.0;
+  g_pap.launches = 0;
+  g_pap.rows = 0;
+  return STT_OK;
+}
+
+extern "C" int stt_pap_timing_read(double* total_ms, long long* launches, long long* rows) {
+  if (!total_ms || !launches || !rows) return set_error(STT_ERR_INVALID, "stt_pap_timing_read: null output");
+  std::lock_guard<std::mutex> lock(g_pap.mu);
+  *total_ms = g_pap.total_ms;
+  *launches = g_pap.launches;
+  *rows = g_pap.rows;
+  return STT_OK;
 }
