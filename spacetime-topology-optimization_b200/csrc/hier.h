@@ -9,6 +9,10 @@
 // The coarsest level is factorised by a block-banded FP64 Cholesky.
 #pragma once
 
+#include <atomic>
+
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 
@@ -46,6 +50,16 @@ struct CoarseDesc {
   double* inv;       // [hrows][nb B][nb B] explicit inverse (FP32 cycles, B <= 64), or null
 };
 
+// The coarsest level's factorisation runs on a stream of its own, concurrently with the
+// caller's next work (a solve's initialisation and first descent); `ready` marks its end.
+// Shared by a hierarchy and its row-selected views; the last one destroyed waits for it.
+struct CoarseSync {
+  int device = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t built = nullptr, ready = nullptr;
+  std::atomic<int> refs{1};
+};
+
 struct stt_hier_impl {
   int d, nelx, nely, hrows, precision, nlevels, mce;
   LevelDesc lv[kMaxLevels];
@@ -63,6 +77,7 @@ struct stt_hier_impl {
   const int* row_map;  // batch row -> hierarchy row (device), or null
   int has_reaction;    // level 0 carries a lumped reaction (drain) term
   int* status;         // device status word of the build (bit 0: pivot <= 0, bit 1: band)
+  CoarseSync* sync;    // the coarse factorisation's stream and completion event
   long long ws_bytes;
 };
 

@@ -1473,6 +1473,54 @@ static int allow_large_smem() {
   return STT_OK;
 }
 
+// Pool of coarse-factorisation streams and events (creating a stream per hierarchy would
+// cost more than the overlap gains). The side streams have the highest priority: the
+// factorisation is on the critical path of the first coarse solve, and its few CTAs
+// should not wait behind the caller's wide kernels.
+static std::mutex g_sync_mu;
+static std::vector<CoarseSync*> g_sync_free;
+
+static int acquire_sync(CoarseSync** out) {
+  int dev = 0;
+  STT_TRY(check_cuda(cudaGetDevice(&dev), "get device"));
+  {
+    std::lock_guard<std::mutex> lock(g_sync_mu);
+    for (size_t i = 0; i < g_sync_free.size(); ++i)
+      if (g_sync_free[i]->device == dev) {
+        CoarseSync* s = g_sync_free[i];
+        g_sync_free.erase(g_sync_free.begin() + (long)i);
+        s->refs.store(1);
+        *out = s;
+        return STT_OK;
+      }
+  }
+  CoarseSync* s = new CoarseSync();
+  s->device = dev;
+  int lo = 0, hi = 0;
+  int rc = check_cuda(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities");
+  if (rc == STT_OK) rc = check_cuda(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi), "side stream");
+  if (rc == STT_OK) rc = check_cuda(cudaEventCreateWithFlags(&s->built, cudaEventDisableTiming), "event");
+  if (rc == STT_OK) rc = check_cuda(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event");
+  if (rc != STT_OK) {
+    if (s->ready) cudaEventDestroy(s->ready);
+    if (s->built) cudaEventDestroy(s->built);
+    if (s->side) cudaStreamDestroy(s->side);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return STT_OK;
+}
+
+// Drops one reference; the last waits for the factorisation (it writes the workspace,
+// which the caller may free or reuse after the destroy) and returns the object to the pool.
+static void release_sync(CoarseSync* s) {
+  if (!s || s->refs.fetch_sub(1) != 1) return;
+  cudaEventSynchronize(s->ready);
+  std::lock_guard<std::mutex> lock(g_sync_mu);
+  g_sync_free.push_back(s);
+}
+
 template <int D>
 static int build_coarse(stt_hier* h, cudaStream_t st) {
   CoarseDesc& co = h->co;
@@ -1545,13 +1593,21 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   int rc = check_cuda(cudaMemsetAsync(h->status, 0, 256, st), "memset status");
   if (rc == STT_OK) rc = d == 2 ? build_levels<2>(h, rho, rho_rs, reaction, r_rs, fixed, st)
                                 : build_levels<1>(h, rho, rho_rs, reaction, r_rs, fixed, st);
-  if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, st) : build_coarse<1>(h, st);
+  // the coarsest level's factorisation runs on the side stream, after the levels, while
+  // the caller's stream goes on (a solve's initialisation and first descent); the coarse
+  // solves wait for `ready`
+  if (rc == STT_OK) rc = acquire_sync(&h->sync);
+  if (rc == STT_OK) rc = check_cuda(cudaEventRecord(h->sync->built, st), "record build");
+  if (rc == STT_OK) rc = check_cuda(cudaStreamWaitEvent(h->sync->side, h->sync->built, 0), "side wait");
+  if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, h->sync->side) : build_coarse<1>(h, h->sync->side);
+  if (rc == STT_OK) rc = check_cuda(cudaEventRecord(h->sync->ready, h->sync->side), "record coarse");
   if (rc != STT_OK) {
+    if (h->sync) release_sync(h->sync);
     delete h;
     return rc;
   }
   // no synchronisation here: the build's device checks (coarse pivots, band) are read by
-  // stt_hier_status, and by the first convergence check of a solve on the hierarchy
+  // stt_hier_status, and by the first convergence check after a solve's first V-cycle
   *out = h;
   return STT_OK;
 }
@@ -1567,6 +1623,7 @@ extern "C" int stt_hier_status(const stt_hier* h, stt_stream_t stream) {
   if (!h) return set_error(STT_ERR_INVALID, "stt_hier_status: null hierarchy");
   cudaStream_t st = (cudaStream_t)stream;
   int s = 0;
+  STT_TRY(check_cuda(cudaStreamWaitEvent(st, h->sync->ready, 0), "wait coarse"));
   STT_TRY(check_cuda(cudaMemcpyAsync(&s, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy"));
   STT_TRY(check_cuda(cudaStreamSynchronize(st), "hierarchy build"));
   return hier_status_code(s);
@@ -1576,11 +1633,13 @@ extern "C" int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier**
   if (!h || !out) return set_error(STT_ERR_INVALID, "stt_hier_select: null");
   stt_hier* v = new stt_hier(*h);
   v->row_map = row_map;
+  v->sync->refs.fetch_add(1);  // the view shares the coarse factorisation
   *out = v;
   return STT_OK;
 }
 
 extern "C" int stt_hier_destroy(stt_hier* h) {
+  if (h) release_sync(h->sync);
   delete h;
   return STT_OK;
 }

@@ -127,6 +127,7 @@ struct Cycle {
   KEq<D, T> ke;
   MQ<T> mq;
   T* final_out = nullptr;  // where level 0's last sweep writes (row stride vstride(ndof0))
+  bool coarse_waited = false;  // the stream has waited for the coarse factorisation
 
   T* X(int l) const { return (T*)w.x[l]; }
   T* Tt(int l) const { return (T*)w.t[l]; }
@@ -242,6 +243,10 @@ struct Cycle {
   void coarse(int l, const T* b, T* x) {
     const LevelDesc& lv = h->lv[l];
     const CoarseDesc& co = h->co;
+    if (!coarse_waited) {  // the factorisation runs on the hierarchy's side stream
+      cudaStreamWaitEvent(st, h->sync->ready, 0);
+      coarse_waited = true;
+    }
     if (sizeof(T) == 4 && co.inv) {
       const int np = co.nb * co.B;
       coarse_inv_solve_kernel<D, T><<<dim3((np + kInvRowsPerCta - 1) / kInvRowsPerCta, nrows), 256,
@@ -903,16 +908,21 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   init(has_x0 ? x : nullptr, pp, 0);
   STT_TRY(check_launch("pcg init"));
   std::vector<RowState> host(nrows);
-  // the first read also carries the hierarchy build's status word (the build does not
-  // synchronise): a failed coarse factorisation surfaces here
+  // the reads after the first V-cycle also carry the hierarchy build's status word (the
+  // build does not synchronise, and the coarse factorisation runs on the hierarchy's side
+  // stream, overlapping the initialisation and the first descent): a failed coarse
+  // factorisation surfaces there
   int hstatus = 0;
   bool hchecked = false;
-  auto pull = [&]() -> int {
+  auto pull = [&](bool with_status) -> int {
     STT_TRY(check_cuda(cudaMemcpyAsync(host.data(), w.rs, sizeof(RowState) * nrows, cudaMemcpyDeviceToHost, st), "row state"));
-    if (!hchecked)
+    with_status = with_status && !hchecked;
+    if (with_status) {
+      STT_TRY(check_cuda(cudaStreamWaitEvent(st, h->sync->ready, 0), "wait coarse"));
       STT_TRY(check_cuda(cudaMemcpyAsync(&hstatus, h->status, sizeof(int), cudaMemcpyDeviceToHost, st), "status copy"));
+    }
     STT_TRY(check_cuda(cudaStreamSynchronize(st), "pcg sync"));
-    if (!hchecked) {
+    if (with_status) {
       hchecked = true;
       STT_TRY(hier_status_code(hstatus));
     }
@@ -923,7 +933,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     for (auto& s : host) a += s.active;
     return a;
   };
-  STT_TRY(pull());
+  STT_TRY(pull(false));
   int it = 0;
   if (n_active() > 0) {
     T* z = (T*)w.z;
@@ -995,7 +1005,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       rz(0);
       STT_TRY(check_launch("pcg iteration"));
       if (it % check_every == 0 || it == max_iter) {
-        STT_TRY(pull());
+        STT_TRY(pull(true));
         if (n_active() == 0) break;
         // a wider check interval once the solve is evidently long
         if (it >= 8) check_every = 2;
@@ -1005,7 +1015,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     flush_x();
     STT_TRY(check_launch("pcg flush"));
   }
-  STT_TRY(pull());
+  STT_TRY(pull(true));
   if (timing) pev.flush();
   int worst = 0, status = STT_OK;
   for (int s = 0; s < nrows; ++s) {

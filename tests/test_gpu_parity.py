@@ -256,7 +256,8 @@ def test_vcycle_fp32_many_rows_uses_block_solves(m):
 
 def test_coarse_factorisation_failure_is_reported(m, pkg):
     """A coarse operator that is not positive definite (a negated KE): the default build
-    raises at once; the unsynchronised build (check=False) raises at the first solve."""
+    raises at once; the unsynchronised build (check=False) raises at the first solve, also
+    when the solve ends before its first V-cycle (a zero load)."""
     from sttopt_b200 import _lib
 
     nelx, nely = 24, 12
@@ -269,6 +270,10 @@ def test_coarse_factorisation_failure_is_reported(m, pkg):
                                   check=False)
     with pytest.raises(_lib.SttError, match="positive definite"):
         m.fem.pcg(levels[0], T(F), m.mg.VCycle(levels), rtol=1e-8, max_iter=5)
+    levels = m.mg.build_hierarchy(dens, edof, KE, T(mask, torch.bool), nelx, nely, max_coarse_elements=50,
+                                  check=False)
+    with pytest.raises(_lib.SttError, match="positive definite"):
+        m.fem.pcg(levels[0], T(np.zeros_like(F)), m.mg.VCycle(levels), rtol=1e-8, max_iter=5)
 
 
 def test_mbb_config_solve_compliance_and_sensitivities(m):
