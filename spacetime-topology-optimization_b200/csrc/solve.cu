@@ -747,14 +747,45 @@ __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
   const TZ* zs = z + (size_t)s * z_rs;
   const TZ* zo = zold + (size_t)s * z_rs;
   double vals[2] = {0.0, 0.0};
-  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kEwThreads) {
+  auto one = [&](long long i) {
     const double zv = (double)zs[i];
     const double rv = (double)rsv[i];
     vals[0] = fma(rv, zv, vals[0]);
     if (flexible && !first) vals[1] = fma(rv, (double)zo[i], vals[1]);
     if (first && p) p[(size_t)s * rs + i] = zv;
+  };
+  bool vec = false;
+  if constexpr (sizeof(TZ) == 4 && sizeof(TR) == 4) {
+    // FP32 vectors with row strides a multiple of 4 (16-byte aligned rows): 128-bit loads
+    vec = !p && ((rs | z_rs) & 3) == 0 && (((uintptr_t)r | (uintptr_t)z | (uintptr_t)zold) & 15) == 0;
+    if (vec) {
+      const long long n4 = n / 4;
+      const float4* r4 = reinterpret_cast<const float4*>(rsv);
+      const float4* z4 = reinterpret_cast<const float4*>(zs);
+      const float4* o4 = reinterpret_cast<const float4*>(zo);
+      const bool mix = flexible && !first;
+      for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n4;
+           i += (long long)gridDim.x * kEwThreads) {
+        const float4 rv = __ldg(r4 + i), zv = __ldg(z4 + i);
+        vals[0] = fma((double)rv.x, (double)zv.x, vals[0]);
+        vals[0] = fma((double)rv.y, (double)zv.y, vals[0]);
+        vals[0] = fma((double)rv.z, (double)zv.z, vals[0]);
+        vals[0] = fma((double)rv.w, (double)zv.w, vals[0]);
+        if (mix) {
+          const float4 ov = __ldg(o4 + i);
+          vals[1] = fma((double)rv.x, (double)ov.x, vals[1]);
+          vals[1] = fma((double)rv.y, (double)ov.y, vals[1]);
+          vals[1] = fma((double)rv.z, (double)ov.z, vals[1]);
+          vals[1] = fma((double)rv.w, (double)ov.w, vals[1]);
+        }
+      }
+      if (blockIdx.x == 0 && threadIdx.x < (n & 3)) one(n4 * 4 + threadIdx.x);  // the row's tail
+    }
   }
+  if (!vec)
+    for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kEwThreads)
+      one(i);
   grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
     RowState& S = rst[s];
     if (first) {
@@ -877,6 +908,10 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   const int ewb = ew_blocks(nd);
   GridRed red_tile{w.partials, w.counters, (int)(tg.x * tg.y)};
   GridRed red_ew{w.partials, w.counters, ewb};
+  // the FP32 r.z pass: eight 128-bit loads of each vector a thread (its block partials
+  // and reduction cost less than with one block per 1024 values)
+  const int rzb = (int)std::max<long long>(1, std::min<long long>(ewb, (nd / 4 + 8 * kEwThreads - 1) / (8 * kEwThreads)));
+  GridRed red_rz{w.partials, w.counters, rzb};
   const KEq<D, double> ke = ke_of<D, double>(h);
   const double* rd0 = h->has_reaction ? l0.rdiag64 : nullptr;
   STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4LL * nrows, st), "memset counters"));
@@ -953,8 +988,8 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     // the cycle itself read (written by the update, or by the cycle's own conversion)
     auto rz = [&](int first) {
       if constexpr (sizeof(T) == 4)
-        pcg_rz_kernel<T, float><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(
-            (const float*)w.b0, z, zold, nullptr, vstride(nd), vstride(nd), nd, w.rs, red_ew, first, flexible);
+        pcg_rz_kernel<T, float><<<dim3(rzb, nrows), kEwThreads, 0, st>>>(
+            (const float*)w.b0, z, zold, nullptr, vstride(nd), vstride(nd), nd, w.rs, red_rz, first, flexible);
       else
         pcg_rz_kernel<T, double><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd),
                                                                            nd, w.rs, red_ew, first, flexible);
