@@ -912,6 +912,9 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   // and reduction cost less than with one block per 1024 values)
   const int rzb = (int)std::max<long long>(1, std::min<long long>(ewb, (nd / 4 + 8 * kEwThreads - 1) / (8 * kEwThreads)));
   GridRed red_rz{w.partials, w.counters, rzb};
+  // the r update likewise: eight 128-bit pairs of r and Ap a thread
+  const int upb = (int)std::max<long long>(1, std::min<long long>(ewb, (nd / 2 + 8 * kEwThreads - 1) / (8 * kEwThreads)));
+  GridRed red_up{w.partials, w.counters, upb};
   const KEq<D, double> ke = ke_of<D, double>(h);
   const double* rd0 = h->has_reaction ? l0.rdiag64 : nullptr;
   STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4LL * nrows, st), "memset counters"));
@@ -1026,7 +1029,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       float* r32 = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
       std::swap(pcur, pnext);
       pnext_buf ^= 1;
-      pcg_update_kernel<<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, w.Ap, nd, nd, w.rs, red_ew, pp, r32,
+      pcg_update_kernel<<<dim3(upb, nrows), kEwThreads, 0, st>>>(w.r, w.Ap, nd, nd, w.rs, red_up, pp, r32,
                                                                   vstride(nd));
       pending = true;
       const bool replaced = replace_every > 0 && it % replace_every == 0;
