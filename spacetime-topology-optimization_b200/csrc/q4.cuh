@@ -80,8 +80,10 @@ struct RhsX {  // a right-hand side value and the node's fixed flags
   uint8_t fl;
 };
 
-template <int D, typename T, bool KU, bool DG, typename Extra = NoExtra, typename LoadU, typename LoadR,
-          typename LoadX, typename Emit>
+// BAND: grid rows a warp marches; 0 takes them from the launch (nny / gridDim.y, rounded
+// up), for launches that choose shorter bands when they have few rows.
+template <int D, typename T, bool KU, bool DG, typename Extra = NoExtra, int BAND = kQRows, typename LoadU,
+          typename LoadR, typename LoadX, typename Emit>
 STT_DEV void march(const KEq<D, T>& ke, int nnx, int nny, LoadU loadu, LoadR loadr, LoadX loadx, Emit emit) {
   // FP64: the element matrix is read from shared memory per use (volatile, so it is not
   // hoisted): DFMA takes no constant-bank operand and 64 doubles in registers would cost
@@ -100,8 +102,9 @@ STT_DEV void march(const KEq<D, T>& ke, int nnx, int nny, LoadU loadu, LoadR loa
   const int strip = blockIdx.x * kQWarps + warp;
   const int c = strip * kQCols - 1 + lane;  // this lane's column
   const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
-  const int r0 = blockIdx.y * kQRows;
-  const int r1 = min(r0 + kQRows, nny);
+  const int band = BAND > 0 ? BAND : (nny + (int)gridDim.y - 1) / (int)gridDim.y;
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
   const int nelx = nnx - 1, nely = nny - 1;
   const bool col_ok = c >= 0 && c < nnx;
   const bool ecol_ok = c >= 0 && c < nelx;
@@ -286,8 +289,9 @@ STT_DEV void march_modal(const MQ<T>& q, int nnx, int nny, LoadF loadf, LoadU lo
   const int strip = blockIdx.x * kQWarps + warp;
   const int c = strip * kQCols - 1 + lane;  // this lane's column
   const bool out_lane = lane >= 1 && lane <= kQCols && c < nnx;
-  const int r0 = blockIdx.y * BAND;
-  const int r1 = min(r0 + BAND, nny);
+  const int band = BAND > 0 ? BAND : (nny + (int)gridDim.y - 1) / (int)gridDim.y;  // 0: from the launch
+  const int r0 = blockIdx.y * band;
+  const int r1 = min(r0 + band, nny);
   const int nelx = nnx - 1, nely = nny - 1;
   const bool col_ok = c >= 0 && c < nnx;
   const bool ecol_ok = c >= 0 && c < nelx;

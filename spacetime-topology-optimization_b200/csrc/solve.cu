@@ -47,6 +47,18 @@ static int ew_blocks(long long n) {
 
 static dim3 tile_grid(int nelx, int nely, int rows) { return q4_grid(nelx, nely, rows); }
 
+// The PCG's level-0 passes (initial residual, p.Ap): bands of 32 grid rows, or shorter
+// ones (down to 8) while the rows give fewer blocks than two waves of six 128-thread
+// blocks on each of the 148 SMs (a single scalar row: the heat solves).  The kernels
+// take the band from the launch (BAND = 0).
+static dim3 pcg_tile_grid(int nelx, int nely, int rows) {
+  const dim3 g = q4_grid(nelx, nely, rows);
+  const int nny = nely + 1;
+  int band = kQRows;
+  while (band > 8 && (long long)g.x * ((nny + band - 1) / band) * rows < 2LL * 148 * 6) band /= 2;
+  return dim3(g.x, (nny + band - 1) / band, rows);
+}
+
 // prolong_kernel: one thread per fine node, x = fine columns, y = fine rows.
 static dim3 prolong_grid(int fnnx, int fnny, int rows) {
   return dim3((fnnx + kProlongThreads - 1) / kProlongThreads, fnny, rows);
@@ -86,7 +98,7 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
   long long used = 0;
   const int es = h->precision == STT_FP32 ? 4 : 8;
   const LevelDesc& l0 = h->lv[0];
-  const dim3 tg = tile_grid(h->nelx, h->nely, 1);
+  const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows);
   w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
   w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
   w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
@@ -496,12 +508,12 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
       return e;
     };
     if (xs)
-      march_modal<D, double, true, false, true, RhsB<D, double>>(
+      march_modal<D, double, true, false, true, RhsB<D, double>, double[D], 2, 0>(
           mq, nnx, nny, loadf, loadu, loadr, loadx,
           [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl,
               const RhsB<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, fl, true); });
     else
-      march_modal<D, double, false, false, false, RhsB<D, double>>(
+      march_modal<D, double, false, false, false, RhsB<D, double>, double[D], 2, 0>(
           mq, nnx, nny, loadf, loadu, loadr, loadx,
           [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D], uint8_t fl,
               const RhsB<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, fl, false); });
@@ -524,9 +536,9 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
     auto emit = [&](int rr, int cc, double(&Ax)[D], double(&)[D], const double(&uc)[D],
                     const RhsX<D, double>& ex) { finish(rr, cc, Ax, uc, ex.b, ex.fl, xs != nullptr); };
     if (xs)
-      march<D, double, true, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+      march<D, double, true, false, RhsX<D, double>, 0>(ke, nnx, nny, loadu, loadr, loadx, emit);
     else
-      march<D, double, false, false, RhsX<D, double>>(ke, nnx, nny, loadu, loadr, loadx, emit);
+      march<D, double, false, false, RhsX<D, double>, 0>(ke, nnx, nny, loadu, loadr, loadx, emit);
   }
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
   grid_reduce<2, kQThreads>(red, s, bid, vals, [&](const double* t) {
@@ -619,7 +631,7 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
   };
   auto loadr = [&](int rr, int cc) { return __ldg(rh + (size_t)rr * nelx + cc); };
   if constexpr (MODAL) {
-    march_modal<D, double, true, false, false, XPExtra<D>, PZIn<TZ, D>>(
+    march_modal<D, double, true, false, false, XPExtra<D>, PZIn<TZ, D>, 2, 0>(
         mq, nnx, nny, [&](int rr, int cc) { return __ldg(fixed + rr * nnx + cc); },
         [&](int rr, int cc, uint8_t, PZIn<TZ, D>& in) {
           const long long node = (long long)rr * nnx + cc;
@@ -634,7 +646,7 @@ __global__ void __launch_bounds__(kQThreads) pcg_pap_kernel(
           for (int d = 0; d < D; ++d) v[d] = PMODE == 2 ? fma(in.p[d], beta, (double)in.z[d]) : (double)in.z[d];
         });
   } else {
-    march<D, double, true, false, FlagX>(
+    march<D, double, true, false, FlagX, 0>(
         ke, nnx, nny,
         [&](int rr, int cc, double(&v)[D]) {
           const long long node = (long long)rr * nnx + cc;
@@ -904,7 +916,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
                    int* conv_out, int* n_iter_out, cudaStream_t st) {
   const LevelDesc& l0 = h->lv[0];
   const long long nd = l0.ndof;
-  const dim3 tg = tile_grid(h->nelx, h->nely, nrows);
+  const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows);
   const int ewb = ew_blocks(nd);
   GridRed red_tile{w.partials, w.counters, (int)(tg.x * tg.y)};
   GridRed red_ew{w.partials, w.counters, ewb};
