@@ -38,7 +38,7 @@ UNIT = "stage solves/s"
 # Per-launch DRAM bytes of the roofline kernels from ncu captures: the FP32 apply at 16 rows
 # (profiles/q4_apply_fp32_2048x1024_16rows.md), and the FP64 p.Ap pass per stage row, from a
 # 2-row capture scaled by the rows (profiles/pcg_pap_fp64_2048x1024.md).
-NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576, "pcg_pap_fp64_per_row": 186447000}
+NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576, "pcg_pap_fp64_per_row": 198669505}
 
 
 def parse():
@@ -56,8 +56,9 @@ def parse():
                     help="run only V-cycles of the stage solve's 16-row mixed hierarchy (the small case for "
                          "ncu captures of the cycle's kernels; seeded uniform densities in [1e-3, 1])")
     ap.add_argument("--pcg-only", action="store_true",
-                    help="run only a 2-row plane-stress PCG on the 2048x1024 grid (the small case for ncu "
-                         "captures of the outer PCG's p.Ap pass; seeded densities and loads)")
+                    help="run only a 4-row plane-stress PCG on the 2048x1024 grid (the small case for ncu "
+                         "captures of the outer PCG's p.Ap pass, with the 32-row bands of the 16-row solve; "
+                         "seeded densities and loads)")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the batched uneven multi-problem measurement")
     ap.add_argument("--uneven-only", action="store_true",
@@ -180,7 +181,7 @@ def run_vcycles(dev, steps, warmup):
             "z_norm": float(z.norm())}
 
 
-def run_pcg_small(dev, rows=2):
+def run_pcg_small(dev, rows=4):
     """One mixed-precision PCG solve of `rows` plane-stress rows on the 2048x1024 grid (the
     bench's mesh and clamp; seeded densities and loads): iterations and time."""
     import numpy as np
