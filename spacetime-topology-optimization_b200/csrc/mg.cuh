@@ -56,7 +56,9 @@ STT_DEV void prolong_at(const T* __restrict__ e, int cnnx, int kx, int ky, int r
 
 // The per-node result of a level-0 pass from A x (unprojected, without reaction), the
 // diagonal of K, the node's x and b, its fixed flags and its reaction value.
-template <int D, typename T, int MODE>
+// RDT: the reaction term is present (false skips its zero terms, which the compiler must
+// otherwise keep: fma(0, x, y) is not y for every x and signed zero y).
+template <int D, typename T, int MODE, bool RDT = true>
 STT_DEV void l0_result(T (&Ax)[D], T (&dg)[D], const T (&xo)[D], const T (&bv)[D], uint8_t fl,
                        const T (&rd)[D], T omega, T (&res)[D]) {
   constexpr bool KU = MODE != SW_FIRST;
@@ -64,14 +66,14 @@ STT_DEV void l0_result(T (&Ax)[D], T (&dg)[D], const T (&xo)[D], const T (&bv)[D
   if (KU) {
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      Ax[i] = fma(rd[i], xo[i], Ax[i]);
+      if constexpr (RDT) Ax[i] = fma(rd[i], xo[i], Ax[i]);
       if ((fl >> i) & 1) Ax[i] = T(0);
     }
   }
   if (DG) {
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      dg[i] += rd[i];
+      if constexpr (RDT) dg[i] += rd[i];
       if ((fl >> i) & 1) dg[i] = T(1);
       const T x0 = MODE == SW_FIRST ? T(0) : xo[i];
       res[i] = x0 + sweep_div(omega * (bv[i] - (KU ? Ax[i] : T(0))), dg[i]);
@@ -187,7 +189,7 @@ __global__ void __launch_bounds__(kQThreads) l0_sweep_modal_kernel(
     T rd[D], res[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) rd[i] = RD ? __ldg(rdh + node * D + i) : T(0);
-    l0_result<D, T, MODE>(Ax, dg, xo, ex.b, fl, rd, omega, res);
+    l0_result<D, T, MODE, RD>(Ax, dg, xo, ex.b, fl, rd, omega, res);
     store_node<D, T>(os, node, res);
   };
   static_assert(MODE != SW_POST, "the cycle prolongs with prolong_kernel");
@@ -258,6 +260,55 @@ struct ModalStage {
       dT[d] = dB[d];
       ut[d] = ub[d];
     }
+  }
+};
+
+// The plane-stress FP32 stage with the two displacement components in float2 pairs:
+// Blackwell's paired FP32 add / multiply / fma issue one instruction for both components
+// (the chained level-0 passes are issue-bound).  Every operation rounds as the scalar
+// stage's does (the same operations on each component, subtraction as addition of the
+// negation, which is exact).
+STT_DEV float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+
+template <>
+struct ModalStage<2, float> {
+  float2 sT, dT, co, cr;
+  float ut[2];
+
+  STT_DEV void reset() {
+    sT = dT = co = cr = make_float2(0.f, 0.f);
+    ut[0] = ut[1] = 0.f;
+  }
+  STT_DEV void step(const MQ<float>& q, const float (&ub)[2], float rho, float (&Ku)[2]) {
+    const float2 u = make_float2(ub[0], ub[1]);
+    const float2 vr = make_float2(__shfl_down_sync(0xffffffffu, ub[0], 1), __shfl_down_sync(0xffffffffu, ub[1], 1));
+    const float2 sB = __fadd2_rn(u, vr);
+    const float2 dB = sub2(vr, u);
+    const float2 Gx = __fadd2_rn(dB, dT);
+    const float2 Gy = sub2(sT, sB);
+    const float2 H = sub2(dT, dB);
+    const float2 rr = make_float2(rho, rho);
+    const float2 P = __fmul2_rn(rr, make_float2(Gx.x, Gy.y));  // p = rho Gx(ux), pq = rho Gy(uy)
+    // a = m01 pq + m00 p, cc = m01 p + m11 pq
+    const float2 AC = __ffma2_rn(make_float2(q.m01, q.m01), make_float2(P.y, P.x),
+                                 __fmul2_rn(make_float2(q.m00, q.m11), P));
+    const float b = (rho * q.m22) * (Gy.x + Gx.y);
+    const float2 GA = __fmul2_rn(__fmul2_rn(rr, make_float2(q.m44, q.m55)), H);
+    // modal_corners of (a, b, GA.x) and (b, cc, GA.y)
+    const float2 AL = make_float2(AC.x, b), BE = make_float2(b, AC.y);
+    const float2 s = __fadd2_rn(AL, BE), t = sub2(AL, BE);
+    const float2 own = sub2(co, __fadd2_rn(t, GA));
+    const float2 send = __fadd2_rn(cr, __fadd2_rn(s, GA));
+    co = sub2(GA, s);
+    cr = sub2(t, GA);
+    const float2 K = __fadd2_rn(own, make_float2(__shfl_up_sync(0xffffffffu, send.x, 1),
+                                                 __shfl_up_sync(0xffffffffu, send.y, 1)));
+    Ku[0] = K.x;
+    Ku[1] = K.y;
+    sT = sB;
+    dT = dB;
+    ut[0] = ub[0];
+    ut[1] = ub[1];
   }
 };
 
@@ -373,7 +424,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
           dg[d] = cur.dg[d];
           rdv[d] = RD ? F.rd[d] : T(0);
         }
-        l0_result<D, T, SW_FIRST>(Ax, dg, zero, F.b, F.fl, rdv, omega, x1);
+        l0_result<D, T, SW_FIRST, RD>(Ax, dg, zero, F.b, F.fl, rdv, omega, x1);
         if (!(col_ok && f >= 0 && f < nny)) {
 #pragma unroll
           for (int d = 0; d < D; ++d) x1[d] = T(0);
@@ -391,7 +442,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
           rd1[d] = RD ? d1.rd[d] : T(0);
           dg[d] = d1.dg[d];
         }
-        l0_result<D, T, SW_SWEEP>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
+        l0_result<D, T, SW_SWEEP, RD>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
         if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
 #pragma unroll
           for (int d = 0; d < D; ++d) xa[d] = T(0);
@@ -409,7 +460,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
           rd2[d] = RD ? d2.rd[d] : T(0);
           dg[d] = d2.dg[d];
         }
-        l0_result<D, T, SW_RESID>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, rb);
+        l0_result<D, T, SW_RESID, RD>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, rb);
       }
       if (out_lane) {
         if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);
@@ -525,7 +576,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
           rd1[d] = RD ? d1.rd[d] : T(0);
           dg[d] = d1.dg[d];
         }
-        l0_result<D, T, SW_SWEEP>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
+        l0_result<D, T, SW_SWEEP, RD>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
         if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
 #pragma unroll
           for (int d = 0; d < D; ++d) xa[d] = T(0);
@@ -543,7 +594,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
           rd2[d] = RD ? d2.rd[d] : T(0);
           dg[d] = d2.dg[d];
         }
-        l0_result<D, T, SW_SWEEP>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, xb);
+        l0_result<D, T, SW_SWEEP, RD>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, xb);
       }
       if (out_lane && f - 2 >= r0 && f - 2 < r1) store_node<D, T>(os, (long long)(f - 2) * nnx + c, xb);
       d2 = d1;
