@@ -341,6 +341,66 @@ __global__ void __cluster_dims__(kDotCluster, 1, 1) __launch_bounds__(kDotThread
   cluster.sync();
 }
 
+// The two dots a.b0 and a.b1 of one first operand (k = 2, a0 == a1: U.gK and U.F of the
+// stage adjoint's warm start, and the heat adjoint's) in one pass over a: 128-bit loads of
+// the three vectors, U pairs in flight per thread (every row 16-byte aligned: an even
+// stride or a single row; an odd length's last value is added by one fixed thread); the
+// accumulators are summed in a fixed order, so the result stays deterministic.
+__global__ void __cluster_dims__(kDotCluster, 1, 1) __launch_bounds__(kDotThreads)
+    vec_dots_shared_kernel(long long n, const double* __restrict__ a, const double* __restrict__ b0,
+                           const double* __restrict__ b1, long long rs, double* __restrict__ dots) {
+  constexpr int U = 4;
+  __shared__ double scratch[kDotThreads / 32];
+  __shared__ double part[2];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int s = blockIdx.y;
+  const long long n2 = n / 2;
+  const long long lo = n2 * rank / kDotCluster, hi = n2 * (rank + 1) / kDotCluster;
+  const double2* A = reinterpret_cast<const double2*>(a + (size_t)s * rs);
+  const double2* B0 = reinterpret_cast<const double2*>(b0 + (size_t)s * rs);
+  const double2* B1 = reinterpret_cast<const double2*>(b1 + (size_t)s * rs);
+  double acc0[U], acc1[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) acc0[u] = acc1[u] = 0.0;
+  long long i = lo + threadIdx.x;
+  for (; i + (U - 1) * kDotThreads < hi; i += U * kDotThreads) {
+    double2 va[U], v0[U], v1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      va[u] = __ldg(A + i + u * kDotThreads);
+      v0[u] = __ldg(B0 + i + u * kDotThreads);
+      v1[u] = __ldg(B1 + i + u * kDotThreads);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      acc0[u] = fma(va[u].y, v0[u].y, fma(va[u].x, v0[u].x, acc0[u]));
+      acc1[u] = fma(va[u].y, v1[u].y, fma(va[u].x, v1[u].x, acc1[u]));
+    }
+  }
+  for (; i < hi; i += kDotThreads) {
+    const double2 va = __ldg(A + i), v0 = __ldg(B0 + i), v1 = __ldg(B1 + i);
+    acc0[0] = fma(va.y, v0.y, fma(va.x, v0.x, acc0[0]));
+    acc1[0] = fma(va.y, v1.y, fma(va.x, v1.x, acc1[0]));
+  }
+  if ((n & 1) && rank == 0 && threadIdx.x == 0) {
+    const size_t last = (size_t)s * rs + n - 1;
+    acc0[0] = fma(__ldg(a + last), __ldg(b0 + last), acc0[0]);
+    acc1[0] = fma(__ldg(a + last), __ldg(b1 + last), acc1[0]);
+  }
+  const double t0 = block_sum<kDotThreads>((acc0[0] + acc0[1]) + (acc0[2] + acc0[3]), scratch);
+  if (threadIdx.x == 0) part[0] = t0;
+  const double t1 = block_sum<kDotThreads>((acc1[0] + acc1[1]) + (acc1[2] + acc1[3]), scratch);
+  if (threadIdx.x == 0) part[1] = t1;
+  cluster.sync();
+  if (rank == 0 && threadIdx.x < 2) {
+    double t = 0.0;
+    for (int r = 0; r < kDotCluster; ++r) t += cluster.map_shared_rank(part, r)[threadIdx.x];
+    dots[(size_t)s * 2 + threadIdx.x] = t;
+  }
+  cluster.sync();
+}
+
 __global__ void vec_cg_update_kernel(long long n, const double* __restrict__ alpha, double* __restrict__ x,
                                      double* __restrict__ r, const double* __restrict__ p,
                                      const double* __restrict__ Ap, long long rs, double* __restrict__ rr) {
@@ -461,6 +521,11 @@ extern "C" int stt_vec_dots(int nrows, long long n, const double* a0, const doub
   const int k = (a1 && b1) ? ((a2 && b2) ? 3 : 2) : 1;
   const dim3 g(kDotCluster, nrows);
   cudaStream_t st = (cudaStream_t)stream;
+  if (k == 2 && a0 == a1 && ((rs & 1) == 0 || nrows == 1) &&
+      (((uintptr_t)a0 | (uintptr_t)b0 | (uintptr_t)b1) & 15) == 0) {
+    vec_dots_shared_kernel<<<g, kDotThreads, 0, st>>>(n, a0, b0, b1, rs, dots);
+    return check_launch("vec_dots");
+  }
   if (k == 1)
     vec_dots_kernel<1><<<g, kDotThreads, 0, st>>>(n, a0, b0, a1, b1, a2, b2, rs, dots);
   else if (k == 2)

@@ -52,6 +52,8 @@ class SpaceTimeProblem:
         self.fixed1 = _geom.fixed_flags(self.heat_mask, self.nnode, 1)
         self.lift = plate.to(torch.float64)
         self.ke = _lib.dbl_array(_geom.host_KE(self.KE))
+        # 2 KE: the stage adjoint's load 2 K U in one apply (doubling is exact)
+        self.ke2 = _lib.dbl_array([2.0 * v for v in _geom.host_KE(self.KE)])
         self.keh = _lib.dbl_array(_geom.host_KE(self.KEh))
         self._streams: dict = {}
         self._worker = None
@@ -221,7 +223,12 @@ class _HeatAdjoint:
             for g in range(G):
                 _lib.check(L.stt_heat_adjoint_load(P.nelx, P.nely, _lib.ptr(Ws[g]), 1.0, _lib.ptr(gT[g]), st))
             gT = torch_fem.project(gT, P.heat_mask).contiguous()
-            ah = torch_fem.safe_div(torch_fem._dots(T_free, gT), torch_fem._dots(T_free, heat_rhs))
+            # T_free . gT and T_free . heat_rhs in one pass over T_free
+            Tf, hr = T_free.contiguous(), heat_rhs.contiguous()
+            d2 = torch.empty(G, 2, dtype=torch.float64, device=P.device)
+            _lib.check(L.stt_vec_dots(G, nnode, _lib.ptr(Tf), _lib.ptr(gT), _lib.ptr(Tf), _lib.ptr(hr), None, None,
+                                      nnode, _lib.ptr(d2), st))
+            ah = torch_fem.safe_div(d2[:, 0], d2[:, 1])
             lam_h = _pcg(hl, gT, (ah[:, None] * T_free).contiguous(), rtol, max_iter, "heat_adjoint_n_iter", info)
             return torch_fem.element_terms(T, P.edof1, P.KEh, lam=lam_h.reshape(G, nnode))["gdens"]
 
@@ -323,12 +330,12 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
         if not gradient:
             return outs
 
-        # 5a. stage adjoints: dL/dU = 2 K U; warm start alpha U (exact for compliance)
+        # 5a. stage adjoints: dL/dU = 2 K U (one apply with 2 KE); warm start alpha U
+        # (exact for compliance)
         gK = torch.empty_like(U)
         _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
                                   2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
-                                  _lib.STT_PROJECT_OUT, P.ke, st))
-        gK = 2 * gK
+                                  _lib.STT_PROJECT_OUT, P.ke2, st))
         # U . gK and U . F in one pass over U
         d2 = torch.empty(S, 2, dtype=torch.float64, device=dev)
         _lib.check(L.stt_vec_dots(S, 2 * nnode, _lib.ptr(U), _lib.ptr(gK), _lib.ptr(U), _lib.ptr(F), None, None,

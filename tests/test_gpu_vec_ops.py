@@ -1,0 +1,72 @@
+"""The PCG vector steps for arbitrary operators (``stt_vec_dots``, ``stt_vec_cg_update``,
+``stt_vec_xpay``) against torch FP64 on the same inputs: dots to 1e-13 relative (the
+kernels sum in another, fixed order), updates to three units in the last place of the
+terms' magnitude (the kernels may fuse the multiply-add into one rounding).  The dot
+cases cover one to three pairs, the shared-first-operand pass (two pairs with the same
+first vector, 128-bit loads) at even and odd lengths, a single row with an odd stride,
+and padded row strides."""
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _rows(g, rows, n, rs):
+    buf = torch.randn(rows, rs, generator=g, dtype=torch.float64).cuda()
+    return buf, buf[:, :n]
+
+
+@pytest.mark.parametrize("rows,n,rs", [(1, 2_100_225, 2_100_225), (3, 4_200_450, 4_200_450),
+                                       (4, 1001, 1002), (2, 999, 999), (5, 64, 70)])
+def test_vec_dots_match_torch(pkg, rows, n, rs):
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    g = torch.Generator().manual_seed(rows * 7 + n)
+    (A, a), (B0, b0), (B1, b1), (B2, b2) = (_rows(g, rows, n, rs) for _ in range(4))
+    ref = [(a * b0).sum(1), (a * b1).sum(1), (a * b2).sum(1), (b0 * b1).sum(1)]
+    scale = [(a.abs() * b.abs()).sum(1) for b in (b0, b1, b2)] + [(b0.abs() * b1.abs()).sum(1)]
+
+    def dots(pairs):
+        out = torch.full((rows, len(pairs)), float("nan"), dtype=torch.float64, device="cuda")
+        ptrs = [_lib.ptr(p) for pair in pairs for p in pair] + [None] * (6 - 2 * len(pairs))
+        _lib.check(lib.stt_vec_dots(rows, n, *ptrs, rs, _lib.ptr(out), _lib.stream()))
+        torch.cuda.synchronize()
+        return out
+
+    cases = [([(A, B0)], [0]), ([(A, B0), (A, B1)], [0, 1]), ([(A, B0), (B0, B1)], [0, 3]),
+             ([(A, B0), (A, B1), (A, B2)], [0, 1, 2])]
+    for pairs, idx in cases:
+        out = dots(pairs)
+        for j, k in enumerate(idx):
+            err = (out[:, j] - ref[k]).abs() / scale[k]
+            assert float(err.max()) <= 1e-13, (len(pairs), k)
+
+
+def _close(out, ref, mag):
+    return bool(((out - ref).abs() <= 6.7e-16 * mag).all())
+
+
+def test_vec_cg_update_and_xpay_match_torch(pkg):
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    g = torch.Generator().manual_seed(3)
+    rows, n = 3, 100_003
+    x, r, p, Ap = (torch.randn(rows, n, generator=g, dtype=torch.float64).cuda() for _ in range(4))
+    alpha = torch.tensor([0.5, -1.25, 3.0], dtype=torch.float64, device="cuda")
+    x_ref, r_ref = x + alpha[:, None] * p, r - alpha[:, None] * Ap
+    rr = torch.empty(rows, dtype=torch.float64, device="cuda")
+    _lib.check(lib.stt_vec_cg_update(rows, n, _lib.ptr(alpha), _lib.ptr(x), _lib.ptr(r), _lib.ptr(p), _lib.ptr(Ap),
+                                     n, _lib.ptr(rr), _lib.stream()))
+    torch.cuda.synchronize()
+    assert _close(x, x_ref, x_ref.abs() + (alpha[:, None] * p).abs())
+    assert _close(r, r_ref, r_ref.abs() + (alpha[:, None] * Ap).abs())
+    assert float(((rr - (r_ref * r_ref).sum(1)).abs() / (r_ref * r_ref).sum(1)).max()) <= 1e-13
+    z = torch.randn(rows, n, generator=g, dtype=torch.float64).cuda()
+    beta = torch.tensor([0.0, 2.0, -0.5], dtype=torch.float64, device="cuda")
+    p_ref = p * beta[:, None] + z
+    _lib.check(lib.stt_vec_xpay(rows, n, _lib.ptr(z), _lib.ptr(beta), _lib.ptr(p), n, _lib.stream()))
+    torch.cuda.synchronize()
+    assert _close(p, p_ref, p_ref.abs() + z.abs())
