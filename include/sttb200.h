@@ -118,14 +118,22 @@ int stt_hier_create(stt_hier** out, void* workspace, long long ws_bytes, int d, 
                     const double* KE, int max_coarse_elements, int precision,
                     stt_stream_t stream);
 
-/* The build does not synchronise: its device checks (a coarse pivot <= 0, a coarse
- * operator beyond its planned band) are reported by stt_hier_status (which synchronises
- * the stream) and by the first convergence check of stt_pcg_mg on the hierarchy. */
+/* The build does not synchronise.  The levels are built on `stream`; the coarsest
+ * level's factorisation (and its explicit inverse for STT_FP32) then runs on a stream of
+ * the library's own, ordered after them, while `stream` goes on: every coarse solve on
+ * any stream (stt_vcycle, stt_pcg_mg, ...) waits for it on the device.  The build's
+ * device checks (a coarse pivot <= 0, a coarse operator beyond its planned band) are
+ * reported by stt_hier_status (which waits for the factorisation and synchronises
+ * `stream`) and by the first convergence check of stt_pcg_mg after its first V-cycle.
+ * Work on other streams must be ordered after `stream` by the caller, as usual. */
 int stt_hier_status(const stt_hier* h, stt_stream_t stream);
 
 /* A view of h restricted to batch rows: batch row s uses hierarchy row row_map[s]
- * (device int32, caller-owned, kept alive while the view is used). */
+ * (device int32, caller-owned, kept alive while the view is used).  A view shares h's
+ * workspace and coarse factorisation and may outlive h's handle (not its workspace). */
 int stt_hier_select(const stt_hier* h, const int* row_map, stt_hier** out);
+/* Releases a hierarchy or view handle.  The last handle of a hierarchy waits (host) for
+ * its coarse factorisation, after which the caller may reuse the workspace. */
 int stt_hier_destroy(stt_hier* h);
 
 /* nlevels, and per level (nelx, nely, kx, ky) into dims[4 * level]. */
