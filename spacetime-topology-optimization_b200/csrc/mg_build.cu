@@ -1090,9 +1090,43 @@ extern "C" long long stt_hier_workspace_bytes(int d, int nelx, int nely, int hro
   return plan_hierarchy(h, nullptr);
 }
 
+// Level 1's stencil: keff[E] = sum_m rho_m G_m (+ reaction), assembled from the level-0
+// densities (level 1's flags must be built).
+template <int D>
+static int level1_stencil(stt_hier* h, const double* reaction, long long r_rs, cudaStream_t st) {
+  const int H = h->hrows;
+  const bool f32 = h->precision == STT_FP32;
+  const LevelDesc& f = h->lv[0];
+  LevelDesc& c = h->lv[1];
+  const double* S = h->tables;  // the level 0 -> 1 transition's tables
+  const int nm = f.kx * f.ky;
+  if (nm == 4 || nm == 6 || nm == 9) {
+#define STT_CHILD_ST(RD, NM)                                                                          \
+  stencil_children_kernel<D, RD, NM><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                        \
+      f.rho64, f.rs_rho, reaction, r_rs, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, \
+      c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, h->l1)
+    if (reaction) {
+      if (nm == 4) STT_CHILD_ST(true, 4);
+      else if (nm == 6) STT_CHILD_ST(true, 6);
+      else STT_CHILD_ST(true, 9);
+    } else {
+      if (nm == 4) STT_CHILD_ST(false, 4);
+      else if (nm == 6) STT_CHILD_ST(false, 6);
+      else STT_CHILD_ST(false, 9);
+    }
+#undef STT_CHILD_ST
+  } else {  // a single coarsening direction (factor 1 in the other)
+    stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
+        ChildSource<D>{f.rho64, f.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
+                       f.kx, f.ky, c.nelx},
+        c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
+  }
+  return check_launch("level-1 stencil");
+}
+
 template <int D>
 static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const double* reaction,
-                        long long r_rs, const uint8_t* fixed, cudaStream_t st) {
+                        long long r_rs, const uint8_t* fixed, cudaStream_t st, bool defer_l1) {
   constexpr int NK = 4 * D, NS = 5 * D * D;
   const int H = h->hrows;
   LevelDesc& l0 = h->lv[0];
@@ -1162,29 +1196,10 @@ static int build_levels(stt_hier* h, const double* rho, long long rho_rs, const 
     const double* S = h->tables + (size_t)(l - 1) * 3 * kTableStride;
     coarse_fixed_kernel<<<grid1(c.nnode), 256, 0, st>>>(f.fixed, f.nnx, f.kx, f.ky, c.fixed, c.nnx, c.nny);
     if (l == 1) {
-      // level 1: keff[E] = sum_m rho_m G_m (+ reaction), assembled from the densities
-      const int nm = f.kx * f.ky;
-      if (nm == 4 || nm == 6 || nm == 9) {
-#define STT_CHILD_ST(RD, NM)                                                                          \
-  stencil_children_kernel<D, RD, NM><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                        \
-      l0.rho64, l0.rs_rho, reaction, r_rs, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, \
-      c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, h->l1)
-        if (reaction) {
-          if (nm == 4) STT_CHILD_ST(true, 4);
-          else if (nm == 6) STT_CHILD_ST(true, 6);
-          else STT_CHILD_ST(true, 9);
-        } else {
-          if (nm == 4) STT_CHILD_ST(false, 4);
-          else if (nm == 6) STT_CHILD_ST(false, 6);
-          else STT_CHILD_ST(false, 9);
-        }
-#undef STT_CHILD_ST
-      } else {  // a single coarsening direction (factor 1 in the other)
-        stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
-            ChildSource<D>{l0.rho64, l0.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
-                           f.kx, f.ky, c.nelx},
-            c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
-      }
+      // level 1's stencil feeds no coarser level (level 2 is built from the level-0
+      // densities): with more than two levels it is assembled after the coarse
+      // factorisation has started (level1_stencil), so that it runs beside it
+      if (!defer_l1 || h->nlevels <= 2) STT_TRY((level1_stencil<D>(h, reaction, r_rs, st)));
     } else {
       double* kc = (l % 2 == 0) ? h->keffB : h->keffA;
       const dim3 g(grid1(c.nel * NK), H);
@@ -1591,8 +1606,8 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   h->status = (int*)((char*)workspace + need - 256);
   cudaStream_t st = (cudaStream_t)stream;
   int rc = check_cuda(cudaMemsetAsync(h->status, 0, 256, st), "memset status");
-  if (rc == STT_OK) rc = d == 2 ? build_levels<2>(h, rho, rho_rs, reaction, r_rs, fixed, st)
-                                : build_levels<1>(h, rho, rho_rs, reaction, r_rs, fixed, st);
+  if (rc == STT_OK) rc = d == 2 ? build_levels<2>(h, rho, rho_rs, reaction, r_rs, fixed, st, true)
+                                : build_levels<1>(h, rho, rho_rs, reaction, r_rs, fixed, st, true);
   // the coarsest level's factorisation runs on the side stream, after the levels, while
   // the caller's stream goes on (a solve's initialisation and first descent); the coarse
   // solves wait for `ready`
@@ -1601,6 +1616,9 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   if (rc == STT_OK) rc = check_cuda(cudaStreamWaitEvent(h->sync->side, h->sync->built, 0), "side wait");
   if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, h->sync->side) : build_coarse<1>(h, h->sync->side);
   if (rc == STT_OK) rc = check_cuda(cudaEventRecord(h->sync->ready, h->sync->side), "record coarse");
+  // level 1's stencil (deferred by build_levels) beside the factorisation
+  if (rc == STT_OK && h->nlevels > 2)
+    rc = d == 2 ? level1_stencil<2>(h, reaction, r_rs, st) : level1_stencil<1>(h, reaction, r_rs, st);
   if (rc != STT_OK) {
     if (h->sync) release_sync(h->sync);
     delete h;
