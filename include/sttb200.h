@@ -29,6 +29,9 @@
  *   stt_element_sens    sttopt/torch_solve.py:144-152 (FemSolve.backward element terms),
  *                       sttopt/compliance.py:49-59 (_element_strain_energy)
  *   stt_stage_*         sttopt/compliance.py:137-161,198-253 with a hard stage threshold
+ *   stt_stage_glue_*    sttopt/compliance.py:33-46 (time_mask), :137-161 (_gravity_load),
+ *                       :164-253 (gravity_compliance, batched_whole_and_gravity_compliance)
+ *   stt_lumped_reaction_adjoint  sttopt/torch_fem.py:117-132 (lumped_reaction's gradient)
  *   stt_heat_*          sttopt/virtual_heat.py:162-166,189-201,404-462
  */
 #ifndef STTB200_H
@@ -68,6 +71,11 @@ int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
                  const void* u, long long u_rs, void* out, long long out_rs,
                  const void* rho, long long rho_rs, const void* rdiag, long long rdiag_rs,
                  const uint8_t* fixed, int flags, const double* KE, stt_stream_t stream);
+
+/* The adjoint of stt_lumped_reaction: out[s][e] = (1/4) sum over e's 4 corners and their
+ * d dofs of g[s].  FP64. */
+int stt_lumped_reaction_adjoint(int d, int nelx, int nely, int nrows, const double* g, long long g_rs,
+                                double* out, long long o_rs, stt_stream_t stream);
 
 /* diag(K(rho)) (+ rdiag), with fixed dofs set to 1 when fixed != NULL.  FP64. */
 int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho, long long rho_rs,
@@ -172,8 +180,12 @@ int stt_keff_apply(int d, int nelx, int nely, int nrows, const double* U, long l
 int stt_pap_timing(int enable);
 int stt_pap_timing_read(double* total_ms, long long* launches, long long* rows);
 
-/* Bytes of device workspace for stt_vcycle / stt_pcg_mg over nrows batch rows. */
+/* Bytes of device workspace for stt_pcg_mg over nrows batch rows (enough for stt_vcycle
+ * too). */
 long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int gamma);
+/* Bytes of device workspace stt_vcycle needs over nrows batch rows (its per-level
+ * vectors and coarse scratch only). */
+long long stt_vcycle_workspace_bytes(const stt_hier* h, int nrows, int gamma);
 
 /* z[s] = M r[s], one V-cycle (damped Jacobi omega, n_smooth sweeps each way, gamma
  * coarse visits).  r and z are FP64; the cycle runs in the hierarchy's precision. */
@@ -187,11 +199,13 @@ int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, do
  * cannot afford cudaMalloc's implicit device synchronisation mid-run, and bindings that
  * can pass input and output buffers but cannot size and own scratch.
  * Its scratch is a fixed 32 MiB array inside this library, held by every GPU that loads
- * the library until exit; calls needing more (stt_solve_workspace_bytes) return
+ * the library until exit; calls needing more (stt_vcycle_workspace_bytes) return
  * STT_ERR_WORKSPACE without launching.  All calls on a device share that array: calls
  * that overlap on the GPU race, so order them on one stream.  The first call on each
- * device looks up the array's device address and should come before any stream capture.
- * Results equal stt_vcycle's for the same arguments. */
+ * device looks up the array's device address and keeps it for the process's lifetime:
+ * make that first call before any stream capture, and do not use the library across a
+ * reset of the device's primary context (cudaDeviceReset), which also invalidates its
+ * hierarchy handles and streams.  Results equal stt_vcycle's for the same arguments. */
 int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
                        long long z_rs, double omega, int n_smooth, int gamma, stt_stream_t stream);
 
@@ -250,6 +264,33 @@ int stt_stage_gradient(int nelx, int nely, int n_stage, const double* x,
                        const uint8_t* member, const double* ce, const double* gdens,
                        const double* gF, double Emin, double Emax, double penal, double* grad,
                        stt_stream_t stream);
+
+/* ---- production stage glue (any stage mask) ------------------------------------ */
+
+/* Rows of the one batched whole + self-weight solve.  For stage s < n_stage the mask row
+ * m_s is M[s] (M != NULL) or the smooth indicator
+ * max(0, 1 - (tanh(beta ti) + tanh(beta (t - ti))) / (tanh(beta ti) + tanh(beta (1 - ti))))
+ * with ti = times[s] (host array), written to M_out when non-NULL; xt[s] = x * m_s.  Row
+ * layout of rho and F: with has_row0, row 0 is the whole structure (rho = SIMP(x),
+ * F = F0) and stage s is row s + 1.  rho[r] = Emin + xt^penal (Emax - Emin);
+ * F[r][2n] = 0, F[r][2n+1] = -(fe / 4) * sum of xt over the elements of node n,
+ * fe = 1 / (nelx nely) (unprojected, as the reference builds it).  Any of M_out, xt,
+ * rho, F may be NULL (F needs xt).  FP64; n_stage <= 128. */
+int stt_stage_glue_rows(int nelx, int nely, int n_stage, int has_row0, const double* x,
+                        const double* t, const double* times, double beta, const double* M,
+                        double* M_out, const double* F0, double Emin, double Emax, double penal,
+                        double* xt, double* rho, double* F, stt_stream_t stream);
+
+/* The adjoint of stt_stage_glue_rows for output gradients g_xt [n_stage][nel],
+ * g_rho and g_F (rows as above; any may be NULL): gx[e] (overwritten), gt[e] (optional,
+ * the smooth indicator's t gradient; the clamp's gradient passes where the unclamped
+ * value is >= 0) and gM[s][e] = d/dm_s (optional).  The mask rows are the smooth
+ * indicator when t (with times and beta) is given, else M. */
+int stt_stage_glue_adjoint(int nelx, int nely, int n_stage, int has_row0, const double* x,
+                           const double* t, const double* times, double beta, const double* M,
+                           const double* g_xt, const double* g_rho, const double* g_F,
+                           double Emin, double Emax, double penal, double* gx, double* gt,
+                           double* gM, stt_stream_t stream);
 
 /* Heat glue: t_e = mean over corners of (1 - T); and the adjoint load
  * g[n] = -sum over elements of w[e] / (4 scale). */

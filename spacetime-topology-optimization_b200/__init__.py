@@ -2,7 +2,7 @@
 
 Drop-in modules with the reference's names and call signatures:
 ``torch_fem``, ``torch_mg``, ``torch_solve``, ``sensitivity``, ``virtual_heat``,
-``compliance``, ``gravity``, ``filters``; plus ``spacetime``, the batched space-time
+``compliance``, ``gravity``, ``filters``, ``load_cases``; plus ``spacetime``, the batched space-time
 objective + gradient.
 All compute runs in ``libsttb200.so`` (C ABI: ``include/sttb200.h``) on the caller's
 CUDA stream; there is no CPU path.
@@ -11,7 +11,7 @@ CUDA stream; there is no CPU path.
 from . import _lib  # noqa: F401
 
 __all__ = ["torch_fem", "torch_mg", "torch_solve", "sensitivity", "virtual_heat", "compliance",
-           "spacetime", "fem", "gravity", "filters", "sharding"]
+           "spacetime", "fem", "gravity", "filters", "load_cases", "sharding"]
 
 
 def __getattr__(name):

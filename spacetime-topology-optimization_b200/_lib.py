@@ -39,6 +39,11 @@ _SIGS = {
                               _p, _c_ll, _p, _c_int, _pd, _p]),
     "stt_q4_diag": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _p, _c_ll, _pd, _p]),
     "stt_lumped_reaction": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_lumped_reaction_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_stage_glue_rows": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p,
+                                     _c_double, _c_double, _c_double, _p, _p, _p, _p]),
+    "stt_stage_glue_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p, _p,
+                                        _c_double, _c_double, _c_double, _p, _p, _p, _p]),
     "stt_ke_modal": (_c_int, [_c_int, _pd, _pd]),
     "stt_cone_filter": (_c_int, [_c_int, _c_int, _c_int, _c_double, _p, _c_ll, _p, _p, _c_ll, _c_double,
                                  _c_double, _p]),
@@ -57,6 +62,7 @@ _SIGS = {
     "stt_hier_level_fixed": (_c_int, [_p, _c_int, _p, _p]),
     "stt_level_apply": (_c_int, [_p, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
     "stt_solve_workspace_bytes": (_c_ll, [_p, _c_int, _c_int]),
+    "stt_vcycle_workspace_bytes": (_c_ll, [_p, _c_int, _c_int]),
     "stt_vcycle": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p, _c_ll, _p]),
     "stt_vcycle_noalloc": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p]),
     "stt_pcg_mg": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_int, _c_double, _c_int, _c_double, _c_int,

@@ -93,22 +93,27 @@ static char* carve(char* base, long long& used, long long bytes) {
   return r;
 }
 
-static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base, SolveWS& w) {
+// The solve's buffers; with pcg == false only those a lone V-cycle uses (z, the FP32
+// copy of r, the per-level vectors and the coarse scratch), not the PCG's row states,
+// reduction partials and r / p / Ap / z_old.
+static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base, SolveWS& w, bool pcg = true) {
   std::memset(&w, 0, sizeof(w));
   long long used = 0;
   const int es = h->precision == STT_FP32 ? 4 : 8;
   const LevelDesc& l0 = h->lv[0];
-  const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows);
-  w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
-  w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
-  w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
-  w.counters = (unsigned*)carve(base, used, 4LL * nrows);
-  w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
-  w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
-  w.p2 = (double*)carve(base, used, 8LL * nrows * l0.ndof);
-  w.Ap = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  if (pcg) {
+    const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows);
+    w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
+    w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
+    w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
+    w.counters = (unsigned*)carve(base, used, 4LL * nrows);
+    w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+    w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+    w.p2 = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+    w.Ap = (double*)carve(base, used, 8LL * nrows * l0.ndof);
+  }
   w.z = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
-  w.zold = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
+  if (pcg) w.zold = carve(base, used, (long long)es * nrows * vstride(l0.ndof));
   if (h->precision == STT_FP32) w.b0 = carve(base, used, 4LL * nrows * vstride(l0.ndof));
   for (int l = 0; l < h->nlevels; ++l) {
     const long long nd = vstride(h->lv[l].ndof);
@@ -1092,6 +1097,12 @@ extern "C" long long stt_solve_workspace_bytes(const stt_hier* h, int nrows, int
   return plan_solve(h, nrows, gamma, nullptr, w);
 }
 
+extern "C" long long stt_vcycle_workspace_bytes(const stt_hier* h, int nrows, int gamma) {
+  if (!h || nrows <= 0) return -1;
+  SolveWS w;
+  return plan_solve(h, nrows, gamma, nullptr, w, false);
+}
+
 extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
                           long long z_rs, double omega, int n_smooth, int gamma, void* workspace,
                           long long ws_bytes, stt_stream_t stream) {
@@ -1100,9 +1111,9 @@ extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long lo
   if (h->d == 2 && (!aligned16(r) || !aligned16(z) || (r_rs % 2) || (z_rs % 2)))
     return set_error(STT_ERR_INVALID, "stt_vcycle: 2-dof vectors must be 16-byte aligned with even row strides");
   SolveWS w;
-  const long long need = plan_solve(h, nrows, gamma, nullptr, w);
+  const long long need = plan_solve(h, nrows, gamma, nullptr, w, false);
   if (ws_bytes < need) return set_error(STT_ERR_WORKSPACE, "stt_vcycle: workspace too small");
-  plan_solve(h, nrows, gamma, (char*)workspace, w);
+  plan_solve(h, nrows, gamma, (char*)workspace, w, false);
   cudaStream_t st = (cudaStream_t)stream;
   const long long nd = h->lv[0].ndof;
   int rc;
@@ -1200,15 +1211,17 @@ extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long lo
 // Limits and rules:
 //  * the scratch is kVCycleScratchBytes (32 MiB) per device; every GPU that loads the
 //    library holds it until the process exits.  A call whose V-cycle scratch
-//    (stt_solve_workspace_bytes for the same hierarchy, rows and gamma) exceeds it is
+//    (stt_vcycle_workspace_bytes for the same hierarchy, rows and gamma) exceeds it is
 //    rejected with STT_ERR_WORKSPACE before anything is launched;
 //  * all calls on a device share the one array and it keeps the last call's
 //    contents; the V-cycle writes every scratch word before reading it, so nothing has
 //    to start at zero.  Calls that overlap on the GPU (different streams, or threads
 //    without ordering) race on the array: order them on one stream;
 //  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call before
-//    any stream capture begins.
+//    (cudaGetSymbolAddress) with that device current and keeps it for the life of the
+//    process; make that first call before any stream capture begins.  Like the rest of
+//    the library (hierarchy handles, its pooled streams), it must not be used across a
+//    cudaDeviceReset or other reset of the device's primary context.
 
 namespace {
 
@@ -1240,7 +1253,7 @@ extern "C" int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r,
                                   stt_stream_t stream) {
   if (!h || nrows <= 0 || nrows > 65535 || gamma < 1)
     return set_error(STT_ERR_INVALID, "stt_vcycle_noalloc: bad arguments");
-  const long long need = stt_solve_workspace_bytes(h, nrows, gamma);
+  const long long need = stt_vcycle_workspace_bytes(h, nrows, gamma);
   if (need < 0 || need > kVCycleScratchBytes)
     return set_error(STT_ERR_WORKSPACE,
                      "stt_vcycle_noalloc: this V-cycle needs more scratch than the library's fixed 32 MiB; "

@@ -29,6 +29,27 @@ def diffusion_KE() -> np.ndarray:
     ) / 6
 
 
+def edge_load_shares(n_nodes: int, length: float) -> np.ndarray:
+    """Each edge node's share of a unit force spread uniformly over ``[0, length]``
+    elements from the edge's first node (sttopt/fem.py:33-57): the exact integral of the
+    node's hat function over the span, divided by the span, so the shares sum to 1;
+    ``length == 0`` is a point load on the first node."""
+    if not 0 <= length <= n_nodes - 1:
+        raise ValueError(f"a traction over {length} elements does not fit on an edge of {n_nodes - 1} elements")
+    if length == 0:
+        shares = np.zeros(n_nodes)
+        shares[0] = 1.0
+        return shares
+
+    def cumulative_hat(u):
+        # integral of the unit hat (support [-1, 1]) from -inf to u
+        u = np.clip(u, -1.0, 1.0)
+        return np.where(u < 0, 0.5 * (1.0 + u) ** 2, 1.0 - 0.5 * (1.0 - u) ** 2)
+
+    at = np.arange(n_nodes, dtype=np.float64)
+    return (cumulative_hat(length - at) - cumulative_hat(-at)) / length
+
+
 def node_grid(nelx: int, nely: int) -> np.ndarray:
     return np.arange((nely + 1) * (nelx + 1)).reshape(nely + 1, nelx + 1)
 

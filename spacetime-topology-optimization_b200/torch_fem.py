@@ -159,7 +159,7 @@ def project(v: Tensor, mask: Tensor) -> Tensor:
 class _LumpedReaction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, reaction, edofMat, ndof, d, nelx, nely):
-        ctx.edofMat, ctx.ndof = edofMat, ndof
+        ctx.grid = (ndof, d, nelx, nely)
         Rb, r_rs = _geom.rows2d(reaction, nelx * nely)
         out = torch.empty(*reaction.shape[:-1], ndof, dtype=torch.float64, device=reaction.device)
         _lib.check(_lib.lib().stt_lumped_reaction(d, nelx, nely, Rb.shape[0], _lib.ptr(Rb), r_rs,
@@ -168,8 +168,14 @@ class _LumpedReaction(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, g):
-        # each element's value reaches its 4 * d dofs with weight 1/4
-        return g[..., ctx.edofMat].sum(-1) / 4, None, None, None, None, None
+        # each element's value reaches its 4 * d dofs with weight 1/4: the element-centric
+        # gather of stt_lumped_reaction_adjoint
+        ndof, d, nelx, nely = ctx.grid
+        Gb, g_rs = _geom.rows2d(g.to(torch.float64), ndof)
+        out = torch.empty(*g.shape[:-1], nelx * nely, dtype=torch.float64, device=g.device)
+        _lib.check(_lib.lib().stt_lumped_reaction_adjoint(d, nelx, nely, Gb.shape[0], _lib.ptr(Gb), g_rs,
+                                                          _lib.ptr(out), nelx * nely, _lib.stream()))
+        return out.to(g.dtype), None, None, None, None, None
 
 
 def lumped_reaction(reaction: Tensor, edofMat: Tensor, ndof: int) -> Tensor:

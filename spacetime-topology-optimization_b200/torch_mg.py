@@ -292,7 +292,7 @@ class VCycle:
         n = self.levels[0].ndof
         flat, rows, batch = _rows_for(h, r.to(torch.float64))
         z = torch.empty_like(flat)
-        nbytes = _lib.lib().stt_solve_workspace_bytes(h.handle, rows, self.gamma)
+        nbytes = _lib.lib().stt_vcycle_workspace_bytes(h.handle, rows, self.gamma)
         ws = _lib.workspace(nbytes, flat.device)
         _lib.check(_lib.lib().stt_vcycle(h.handle, rows, _lib.ptr(flat), n, _lib.ptr(z), n, self.omega,
                                          self.n_smooth, self.gamma, _lib.ptr(ws), ws.numel(), _lib.stream()))

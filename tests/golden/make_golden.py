@@ -2,10 +2,15 @@
 
 The reference is pure Python (torch + NumPy/SciPy); its own LFS fixtures are absent,
 so its FP64 CPU torch path is run here, seeded, and its outputs saved as ``.npz``.
-Run from the repository root with the reference checkout on ``REFERENCE_ROOT``
-(default ``/root/reference``)::
+Run from the repository root with the path of a reference checkout, either in the
+``REFERENCE_ROOT`` environment variable or as ``--reference PATH``::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH [--only NAME,NAME] [--with-512] [--full-size]
+
+``--full-size`` adds the benchmark-size fixtures (config 2 at 1024x512, the space-time
+objective at 1024x512 and 2048x1024 x 16 stages); the 2048x1024 run takes about ten
+minutes and ~20 GB of host memory.  Large fields are stored as seeded random
+projections and a strided subsample (``field_summary``), small ones whole.
 
 The fixtures are inputs and outputs only; nothing here is imported at test time.
 """
@@ -19,7 +24,17 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE_ROOT = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+
+
+def _reference_root() -> Path:
+    if "--reference" in sys.argv:
+        return Path(sys.argv[sys.argv.index("--reference") + 1])
+    if "REFERENCE_ROOT" in os.environ:
+        return Path(os.environ["REFERENCE_ROOT"])
+    raise SystemExit("make_golden.py: give the reference checkout as --reference PATH or REFERENCE_ROOT")
+
+
+REFERENCE_ROOT = _reference_root()
 sys.path.insert(0, str(REFERENCE_ROOT))
 sys.path.insert(0, str(HERE.parents[1]))
 
@@ -39,6 +54,8 @@ import sttopt.virtual_heat as vh  # noqa: E402
 from sttopt.run_config import HeatRunConfig  # noqa: E402
 
 from oracle.sttopt_oracle import smoothed_density  # noqa: E402  (seeded input recipe)
+sys.path.insert(0, str(HERE))
+from summary import field_summary  # noqa: E402
 
 F64 = torch.float64
 EMIN, EMAX, PENAL, NU = 1e-9, 1.0, 3.0, 0.3
@@ -90,6 +107,26 @@ def gen_fem_basic():
         plate_bottom_6x4=vh.plate_nodes(6, 4, "bottom_edge"),
         plate_left_6x4=vh.plate_nodes(6, 4, "left_edge"),
     )
+
+
+def gen_load_cases():
+    """Every load case of the reference (load_cases.load_case, active_mask) on a few meshes
+    and load / support spans, with fem.edge_load_shares and units.in_elements."""
+    import sttopt.units as units
+
+    out = {}
+    for case in load_cases.LoadCase:
+        for nelx, nely, load_m, sup_m, h in [(12, 8, 0.0, 0.5, 0.25), (20, 10, 0.4, 0.3, 0.1),
+                                             (16, 12, 0.27, 0.13, 0.05)]:
+            k = f"{case.value}_{nelx}x{nely}_{load_m}_{sup_m}_{h}"
+            F, free = load_cases.load_case(case, nelx, nely, load_m, sup_m, h)
+            out[f"{k}_F"], out[f"{k}_free"] = F, free
+            out[f"{k}_active"] = load_cases.active_mask(case, nelx, nely)
+    for n, length in [(5, 0.0), (5, 1.0), (9, 2.5), (9, 8.0), (33, 7.3)]:
+        out[f"shares_{n}_{length}"] = fem.edge_load_shares(n, length)
+    out["in_elements"] = np.array([units.in_elements(a, b) for a, b in [(0.3, 0.1), (1.0, 0.25), (0.35, 0.1),
+                                                                        (0.7, 0.1), (1.0, 0.3)]])
+    save("load_cases", **out)
 
 
 def gen_operator():
@@ -292,16 +329,17 @@ def _hard_time_mask(tPhys, ti, beta):
     return (tPhys <= ti).to(tPhys.dtype)
 
 
-def spacetime_reference(x, w, n_stage):
+def spacetime_reference(x, w, n_stage, rtol=1e-8):
     """The space-time objective of the configs, composed from reference functions.
 
     ``compliance.time_mask`` is replaced by the hard threshold ``tPhys <= s/n_stage``;
     the stage rows go through one batched ``femsolve`` exactly as
-    ``batched_whole_and_gravity_compliance`` stacks them (without its row 0).
+    ``batched_whole_and_gravity_compliance`` stacks them (without its row 0).  ``rtol``
+    is the heat solve's and the stage solves' (and their adjoints') tolerance.
     """
     nely, nelx = x.shape
     mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device("cpu"), F64)
-    cfg = heat_config(nelx, nely)
+    cfg = heat_config(nelx, nely, heat_cg_rtol=rtol)
     xPhys = t(x).requires_grad_(True)
     mu = torch.full((nely, nelx), 0.5, dtype=F64)
     sol = vh.heat_time_field(cfg, mesh, xPhys, mu, conduction_penal=3.0)
@@ -328,7 +366,7 @@ def spacetime_reference(x, w, n_stage):
         compliance.time_mask = orig
     density = torch.stack(rows)
     info = {}
-    U = torch_solve.femsolve(density, torch.stack(Fs), edof, KE, mask, nelx, nely, info=info)
+    U = torch_solve.femsolve(density, torch.stack(Fs), edof, KE, mask, nelx, nely, info=info, rtol=rtol)
     cs = []
     for i, xt in enumerate(xts):
         ce = compliance._element_strain_energy(U[i], edof, KE, nely, nelx)
@@ -369,6 +407,79 @@ def gen_spacetime_512():
     save("spacetime512", x_sum=x.sum(), w_sum=w.sum(), tPhys=res["tPhys"], c_s=res["c_s"],
          J_t=res["J_t"], L=res["L"], grad=res["grad"], member_bits=np.packbits(res["member"], axis=-1),
          fwd_iter=res["fwd_iter"], bwd_iter=res["bwd_iter"])
+
+
+def gen_cantilever_full():
+    """Config 2 at its size: the 1024x512 cantilever (left edge clamped, unit -y load at the
+    mid-right node), seeded radius-4 smoothed density in [1e-3, 1], FP64, the reference's
+    6-level hierarchy; U, c and dc/dxPhys at the config's rtol 1e-8 (iteration counts) and
+    at rtol 1e-12 (values with the solve noise removed).  Inputs are regenerated by the
+    tests from the seed; fields are stored as summaries."""
+    nelx, nely, seed = 1024, 512, 2
+    x = smoothed_density(nelx, nely, seed)
+    nodes = fem.node_grid(nelx, nely)
+    ndof = 2 * nodes.size
+    F = np.zeros(ndof)
+    F[2 * nodes[nely // 2, -1] + 1] = -1.0
+    mask = np.ones(ndof, bool)
+    mask[2 * nodes[:, 0]] = False
+    mask[2 * nodes[:, 0] + 1] = False
+    KE = t(fem.plane_stress_KE(NU))
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    out = {"x_sum": x.sum(), "nelx": nelx, "nely": nely, "seed": seed}
+    for tag, rtol in (("r8", 1e-8), ("r12", 1e-12)):
+        xPhys = t(x).requires_grad_(True)
+        info = {}
+        density = torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL).flatten()
+        U = torch_solve.femsolve(density, t(F), edof, KE, torch.as_tensor(mask), nelx, nely, info=info, rtol=rtol)
+        ce = compliance._element_strain_energy(U, edof, KE, nely, nelx)
+        c = torch.sum(torch_fem.simp_density(xPhys, EMIN, EMAX, PENAL) * ce)
+        (dc,) = sensitivity.jacobian_rows(c[None], [xPhys])
+        out.update({f"{tag}_c": c.detach(), f"{tag}_fwd_iter": info["forward_n_iter"],
+                    f"{tag}_bwd_iter": info["backward_n_iter"]})
+        out.update(field_summary(f"{tag}_U", U.detach().numpy(), 101, 97))
+        out.update(field_summary(f"{tag}_dc", dc.numpy(), 102, 61))
+    levels = torch_mg.build_hierarchy(torch_fem.simp_density(t(x), EMIN, EMAX, PENAL).flatten(), edof, KE,
+                                      torch.as_tensor(mask), nelx, nely)
+    out["level_shapes"] = np.array([[lv.nelx, lv.nely] for lv in levels])
+    out["coarse_ndof"] = levels[-1].ndof
+    save("cantilever1024", **out)
+
+
+def _member_hash(member):
+    """Per stage: the member count and two index sums (int64, exact), pinning the stage
+    membership of millions of elements in three integers a stage."""
+    m = np.asarray(member, dtype=bool)
+    idx = np.arange(m.shape[-1], dtype=np.int64)
+    return np.stack([m.sum(-1), (m * idx).sum(-1), (m * (idx * idx % 1000003)).sum(-1)], axis=1)
+
+
+def gen_spacetime_full(nelx, nely, seed, rtols=(1e-8, 1e-12)):
+    """The space-time objective of the configs at a benchmark size, 16 stages: the
+    reference's heat solve, hard-threshold stages, one batched stage femsolve and the
+    sensitivity field, at each ``rtol``.  ``seed`` gives the density (``smoothed_density``)
+    and the time weights (``default_rng(seed).uniform(-1, 1)``), the benchmark's recipe."""
+    import time
+
+    n_stage = 16
+    x = smoothed_density(nelx, nely, seed)
+    w = np.random.default_rng(seed).uniform(-1, 1, (nely, nelx))
+    out = {"x_sum": x.sum(), "w_sum": w.sum(), "nelx": nelx, "nely": nely, "seed": seed, "n_stage": n_stage}
+    for rtol in rtols:
+        tag = f"r{round(-np.log10(rtol))}"
+        t0 = time.perf_counter()
+        res = spacetime_reference(x, w, n_stage, rtol=rtol)
+        print(f"  spacetime {nelx}x{nely} rtol {rtol:g}: {time.perf_counter() - t0:.1f} s", flush=True)
+        U = res["U"].detach().numpy()
+        out.update({f"{tag}_c_s": res["c_s"].detach(), f"{tag}_J_t": res["J_t"].detach(),
+                    f"{tag}_L": res["L"].detach(), f"{tag}_fwd_iter": res["fwd_iter"],
+                    f"{tag}_bwd_iter": res["bwd_iter"], f"{tag}_member": _member_hash(res["member"]),
+                    f"{tag}_U_norms": np.linalg.norm(U, axis=1)})
+        out.update(field_summary(f"{tag}_grad", res["grad"].numpy(), 201, 257))
+        out.update(field_summary(f"{tag}_tPhys", res["tPhys"].detach().numpy(), 202, 263))
+        out.update(field_summary(f"{tag}_U", U, 203, 4099))
+        del res, U
+    save(f"spacetime{nelx}", **out)
 
 
 def gen_filters():
@@ -434,6 +545,53 @@ def gen_compliance_smooth():
                     f"{k}_L": L, f"{k}_gx": gx, f"{k}_gt": gt})
     out["C_7x4"] = gravity.gravity_load_matrix(7, 4).toarray()
     save("compliance_smooth", **out)
+
+
+def gen_compliance_single():
+    """The single-solve glue (whole_compliance, gravity_compliance, _gravity_load) with its
+    autograd gradients, and the batched call with the stage mask replaced by the hard
+    threshold (the space-time configurations' membership), on one MBB-loaded grid with the
+    build plate clamped."""
+    nelx, nely, seed = 36, 20, 23
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    F, _ = load_cases.load_case(load_cases.LoadCase.MBB, nelx, nely, 0.0, 0.0, 1.0)
+    plate = fem.node_grid(nelx, nely)[-1, :]
+    free = np.setdiff1d(np.arange(ndof), np.concatenate([2 * plate, 2 * plate + 1]))
+    rng = np.random.default_rng(seed)
+    x = smoothed_density(nelx, nely, seed)
+    rows = (nely - 0.5 - np.arange(nely)[:, None]) / nely
+    tp = np.clip(rows + 0.03 * rng.uniform(-1, 1, (nely, nelx)), 0.0, 1.0)
+    wF = rng.normal(size=ndof)
+    wx = rng.normal(size=(nely, nelx))
+    KE = t(fem.plane_stress_KE(NU))
+    edof = t(fem.element_dof_map(nelx, nely), torch.int64)
+    C = torch_util.csr_to_tensor(gravity.gravity_load_matrix(nelx, nely), "cpu", F64)
+    out = {"x": x, "t": tp, "F": F, "free": free, "wF": wF, "wx": wx}
+    xT = t(x).requires_grad_(True)
+    c, U = compliance.whole_compliance(xT, KE, edof, EMIN, EMAX, PENAL, t(free, torch.int64), t(F), ndof)
+    (gx,) = torch.autograd.grad(c, [xT])
+    out.update(whole_c=c, whole_U=U, whole_gx=gx)
+    xT, tT = t(x).requires_grad_(True), t(tp).requires_grad_(True)
+    cg, Ug = compliance.gravity_compliance(xT, tT, KE, edof, EMIN, EMAX, PENAL, 0.55, C, 12.0,
+                                           t(free, torch.int64), ndof)
+    gx, gt = torch.autograd.grad(cg, [xT, tT])
+    out.update(grav_c=cg, grav_U=Ug, grav_gx=gx, grav_gt=gt)
+    xT, tT = t(x).requires_grad_(True), t(tp).requires_grad_(True)
+    tm, xj, Fg = compliance._gravity_load(xT, tT, 0.4, C, 8.0, ndof)
+    J = torch.sum(t(wF) * Fg) + torch.sum(t(wx) * xj)
+    gx, gt = torch.autograd.grad(J, [xT, tT])
+    out.update(gl_mask=tm, gl_xt=xj, gl_F=Fg, gl_gx=gx, gl_gt=gt)
+    orig = compliance.time_mask
+    compliance.time_mask = _hard_time_mask
+    try:
+        xT = t(x).requires_grad_(True)
+        c, stages, U = compliance.batched_whole_and_gravity_compliance(
+            xT, t(tp), KE, edof, EMIN, EMAX, PENAL, t(free, torch.int64), t(F), ndof, C, 10.0, [0.3, 0.6, 1.0])
+        (gx,) = torch.autograd.grad(c + 2.0 * stages[0] + stages[1] + 0.5 * stages[2], [xT])
+    finally:
+        compliance.time_mask = orig
+    out.update(hard_c=c, hard_stages=torch.stack(stages), hard_U=U, hard_gx=gx)
+    save("compliance_single", **out)
 
 
 def laplace_config(time_map):
@@ -531,6 +689,28 @@ def gen_time_maps():
     save("time_maps", **out)
 
 
+def gen_neg_log():
+    """``heat_time_field`` with the ``neg_log`` map (t = -log(max(T, 0) + floor), the floor
+    a fraction of the smallest element mean of T over the part) and the reference's
+    autograd gradients of sum(w tPhys) in xPhys and mu; solves at rtol 1e-10."""
+    out = {}
+    for nelx, nely, seed in [(40, 20, 51), (64, 24, 52)]:
+        rng = np.random.default_rng(seed)
+        x = smoothed_density(nelx, nely, seed)
+        mu = rng.uniform(0.2, 0.8, (nely, nelx))
+        w = rng.uniform(-1, 1, (nely, nelx))
+        mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device("cpu"), F64)
+        cfg = heat_config(nelx, nely, time_map="neg_log", heat_cg_rtol=1e-10)
+        xT, muT = t(x).requires_grad_(True), t(mu).requires_grad_(True)
+        sol = vh.heat_time_field(cfg, mesh, xT, muT, conduction_penal=3.0)
+        J = torch.sum(t(w) * sol.tPhys)
+        gx, gmu = torch.autograd.grad(J, [xT, muT])
+        k = f"{nelx}x{nely}"
+        out.update({f"{k}_x": x, f"{k}_mu": mu, f"{k}_w": w, f"{k}_tPhys": sol.tPhys, f"{k}_T": sol.primary,
+                    f"{k}_t_nodes": sol.t, f"{k}_J": J, f"{k}_gx": gx, f"{k}_gmu": gmu})
+    save("neg_log", **out)
+
+
 def gen_pcg_cases():
     """Retirement, zero rows, warm starts and non-convergence, as the reference does them."""
     nelx, nely = 18, 12
@@ -556,19 +736,30 @@ def gen_pcg_cases():
          fail_resid=resid, fail_msg=np.array(msg))
 
 
+GENERATORS = {
+    "fem_basic": gen_fem_basic, "load_cases": gen_load_cases, "operator": gen_operator, "transfers": gen_transfers,
+    "hierarchy": gen_hierarchy, "pcg_cases": gen_pcg_cases, "mbb120x40": gen_mbb_config,
+    "cantilever": gen_cantilever, "heat": gen_heat, "spacetime": gen_spacetime, "filters": gen_filters,
+    "compliance_smooth": gen_compliance_smooth, "compliance_single": gen_compliance_single,
+    "time_maps": gen_time_maps, "neg_log": gen_neg_log,
+}
+OPTIONAL = {
+    "spacetime512": gen_spacetime_512,
+    "cantilever1024": gen_cantilever_full,
+    "spacetime1024": lambda: gen_spacetime_full(1024, 512, 5),
+    "spacetime2048": lambda: gen_spacetime_full(2048, 1024, 3),
+}
+
+
 if __name__ == "__main__":
     torch.set_num_threads(os.cpu_count() or 1)
-    gen_fem_basic()
-    gen_operator()
-    gen_transfers()
-    gen_hierarchy()
-    gen_pcg_cases()
-    gen_mbb_config()
-    gen_cantilever()
-    gen_heat()
-    gen_spacetime()
-    gen_filters()
-    gen_compliance_smooth()
-    gen_time_maps()
-    if "--with-512" in sys.argv:
-        gen_spacetime_512()
+    if "--only" in sys.argv:
+        names = sys.argv[sys.argv.index("--only") + 1].split(",")
+    else:
+        names = list(GENERATORS)
+        if "--with-512" in sys.argv:
+            names.append("spacetime512")
+        if "--full-size" in sys.argv:
+            names += ["cantilever1024", "spacetime1024", "spacetime2048"]
+    for name in names:
+        (GENERATORS.get(name) or OPTIONAL[name])()

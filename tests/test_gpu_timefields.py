@@ -4,8 +4,12 @@ reference's outputs (golden fixtures made by running it on the same seeded input
 * ``compliance.batched_whole_and_gravity_compliance`` with the smooth ``time_mask``, the
   point-load row 0 and the device gravity stencil: compliances and displacements 1e-9
   relative, the gradients in xPhys and tPhys 5e-8 (converged FP64 solves at rtol 1e-8).
+* ``whole_compliance``, ``gravity_compliance`` and ``_gravity_load`` (fields 1e-9 /
+  1e-14, gradients 5e-9 / 5e-8 / 1e-13) and the batched call with the hard stage mask.
 * The fused Poisson load and its adjoint, element means: 1e-13 (same arithmetic to
   rounding).
+* ``heat_time_field`` with the ``neg_log`` map (solves at rtol 1e-10): fields 1e-9,
+  gradients 1e-8.
 * ``heat_time_field`` with the ``poisson`` map and ``laplace_time_field`` (identity and
   poisson maps; solves at rtol 1e-10): fields 1e-8, gradients 1e-7.
 """
@@ -51,6 +55,66 @@ def test_batched_whole_and_gravity_compliance_smooth(pkg, key, sparse_C):
     assert rel_err(U.detach().cpu(), g[f"{key}_U"]) < 1e-9
     assert rel_err(gx.cpu(), g[f"{key}_gx"]) < 5e-8
     assert rel_err(gt.cpu(), g[f"{key}_gt"]) < 5e-8
+
+
+def test_single_solve_glue_and_hard_mask(pkg):
+    """whole_compliance, gravity_compliance and _gravity_load with their gradients, and the
+    batched call with ``mask_fn=hard_time_mask``, against the reference (the hard mask by
+    replacing its ``time_mask``)."""
+    from sttopt_b200 import compliance, fem, gravity
+
+    g = golden("compliance_single")
+    nely, nelx = g["x"].shape
+    ndof = 2 * (nelx + 1) * (nely + 1)
+    KE, edof = T(fem.plane_stress_KE(NU)), T(fem.element_dof_map(nelx, nely), torch.int64)
+    free, F = T(g["free"], torch.int64), T(g["F"])
+    C = gravity.gravity_load_matrix(nelx, nely)
+    x = T(g["x"]).requires_grad_(True)
+    c, U = compliance.whole_compliance(x, KE, edof, EMIN, EMAX, PENAL, free, F, ndof)
+    (gx,) = torch.autograd.grad(c, [x])
+    assert abs(float(c) - float(g["whole_c"])) <= 1e-9 * abs(float(g["whole_c"]))
+    assert rel_err(U.detach().cpu(), g["whole_U"]) < 1e-9
+    assert rel_err(gx.cpu(), g["whole_gx"]) < 5e-9
+    x, tp = T(g["x"]).requires_grad_(True), T(g["t"]).requires_grad_(True)
+    cg, Ug = compliance.gravity_compliance(x, tp, KE, edof, EMIN, EMAX, PENAL, 0.55, C, 12.0, free, ndof)
+    gx, gt = torch.autograd.grad(cg, [x, tp])
+    assert abs(float(cg) - float(g["grav_c"])) <= 1e-9 * abs(float(g["grav_c"]))
+    assert rel_err(Ug.detach().cpu(), g["grav_U"]) < 1e-9
+    assert rel_err(gx.cpu(), g["grav_gx"]) < 5e-8
+    assert rel_err(gt.cpu(), g["grav_gt"]) < 5e-8
+    x, tp = T(g["x"]).requires_grad_(True), T(g["t"]).requires_grad_(True)
+    tm, xj, Fg = compliance._gravity_load(x, tp, 0.4, C, 8.0, ndof)
+    J = torch.sum(T(g["wF"]) * Fg) + torch.sum(T(g["wx"]) * xj)
+    gx, gt = torch.autograd.grad(J, [x, tp])
+    assert rel_err(tm.detach().cpu(), g["gl_mask"]) < 1e-14
+    assert rel_err(xj.detach().cpu(), g["gl_xt"]) < 1e-14
+    assert rel_err(Fg.detach().cpu(), g["gl_F"]) < 1e-14
+    assert rel_err(gx.cpu(), g["gl_gx"]) < 1e-13
+    assert rel_err(gt.cpu(), g["gl_gt"]) < 1e-13
+    x = T(g["x"]).requires_grad_(True)
+    c, stages, U = compliance.batched_whole_and_gravity_compliance(
+        x, T(g["t"]), KE, edof, EMIN, EMAX, PENAL, free, F, ndof, C, 10.0, [0.3, 0.6, 1.0],
+        mask_fn=compliance.hard_time_mask)
+    (gx,) = torch.autograd.grad(c + 2.0 * stages[0] + stages[1] + 0.5 * stages[2], [x])
+    assert abs(float(c) - float(g["hard_c"])) <= 1e-9 * abs(float(g["hard_c"]))
+    assert rel_err(torch.stack(stages).detach().cpu(), g["hard_stages"]) < 1e-9
+    assert rel_err(U.detach().cpu(), g["hard_U"]) < 1e-9
+    assert rel_err(gx.cpu(), g["hard_gx"]) < 5e-8
+
+
+def test_lumped_reaction_gradient(pkg):
+    """The lumped reaction's adjoint kernel against torch's gather of the same sum."""
+    from sttopt_b200 import fem, torch_fem
+
+    rng = np.random.default_rng(9)
+    for d, (nelx, nely) in [(1, (13, 7)), (2, (9, 6))]:
+        edof = T(fem.element_dof_map(nelx, nely, d), torch.int64)
+        ndof = d * (nelx + 1) * (nely + 1)
+        r = T(rng.uniform(size=(2, nelx * nely))).requires_grad_(True)
+        w = T(rng.normal(size=(2, ndof)))
+        (gr,) = torch.autograd.grad(torch.sum(w * torch_fem.lumped_reaction(r, edof, ndof)), [r])
+        expect = w[..., edof].sum(-1) / 4
+        assert rel_err(gr.cpu(), expect.cpu()) < 1e-15
 
 
 def test_gravity_stencil_and_transpose(pkg):
@@ -111,6 +175,33 @@ def test_heat_time_field_poisson_map(pkg):
     assert abs(float(J) - float(g["heat_J"])) <= 1e-8 * abs(float(g["heat_J"]))
     assert rel_err(gx.cpu(), g["heat_gx"]) < 1e-7
     assert rel_err(gmu.cpu(), g["heat_gmu"]) < 1e-7
+
+
+@pytest.mark.parametrize("key", ["40x20", "64x24"])
+def test_heat_time_field_neg_log_map(pkg, key):
+    """The ``neg_log`` map, t = -log(max(T, 0) + floor) with the floor a fraction of the
+    part's smallest element mean of T (sttopt/virtual_heat.py:443-449), against the
+    reference's fields and its autograd gradients (solves at rtol 1e-10)."""
+    from sttopt_b200 import virtual_heat as vh
+
+    g = golden("neg_log")
+    nelx, nely = (int(v) for v in key.split("x"))
+    mesh = vh.ScalarMesh.build(nelx, nely, "bottom_edge", torch.device(DEV), torch.float64)
+
+    class Cfg:
+        chi_contrast, drain_beta, time_map, heat_cg_rtol = 1000.0, 25.0, "neg_log", 1e-10
+
+    x = T(g[f"{key}_x"]).requires_grad_(True)
+    mu = T(g[f"{key}_mu"]).requires_grad_(True)
+    sol = vh.heat_time_field(Cfg, mesh, x, mu, conduction_penal=3.0)
+    J = torch.sum(T(g[f"{key}_w"]) * sol.tPhys)
+    gx, gmu = torch.autograd.grad(J, [x, mu])
+    assert rel_err(sol.primary.detach().cpu(), g[f"{key}_T"]) < 1e-9
+    assert rel_err(sol.t.detach().cpu(), g[f"{key}_t_nodes"]) < 1e-9
+    assert rel_err(sol.tPhys.detach().cpu(), g[f"{key}_tPhys"]) < 1e-9
+    assert abs(float(J) - float(g[f"{key}_J"])) <= 1e-9 * abs(float(g[f"{key}_J"]))
+    assert rel_err(gx.cpu(), g[f"{key}_gx"]) < 1e-8
+    assert rel_err(gmu.cpu(), g[f"{key}_gmu"]) < 1e-8
 
 
 LAPLACE = ["lap_36x18_bottom_edge_identity_0.0", "lap_36x18_left_edge_identity_1.0",
