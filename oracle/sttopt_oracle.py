@@ -18,10 +18,103 @@ top-right, top-left.
 
 from __future__ import annotations
 
+import ctypes
 import math
+from pathlib import Path
 
 import numpy as np
 import scipy.linalg
+
+# ---------------------------------------------------------------------------------
+# Optional C/OpenMP loops (oracle_kernels.c, built by oracle/build_oracle.py into
+# oracle/_build/): the element products, the Jacobi update and the PCG's row operations,
+# with the arithmetic of the NumPy forms below (only the summation order differs).
+# Without the library the NumPy forms run.
+# ---------------------------------------------------------------------------------
+
+_C_PATH = Path(__file__).resolve().parent / "_build" / "liboracle_kernels.so"
+_C_LIB = None
+
+
+def c_kernels():
+    """The C loops, or None when ``liboracle_kernels.so`` was not built."""
+    global _C_LIB
+    if _C_LIB is None:
+        if not _C_PATH.exists():
+            _C_LIB = False
+        else:
+            lib = ctypes.CDLL(str(_C_PATH))
+            P, I, LL, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double
+            lib.orc_element_apply.argtypes = [I, I, I, I, P, LL, P, LL, LL, P, LL, P, LL]
+            lib.orc_jacobi_update.argtypes = [I, LL, P, LL, P, LL, P, LL, P, LL, D]
+            lib.orc_row_dots.argtypes = [I, LL, P, LL, P, LL, P]
+            lib.orc_row_axpy.argtypes = [I, LL, P, P, LL, P, LL]
+            lib.orc_row_xpay.argtypes = [I, LL, P, LL, P, P, LL]
+            for f in (lib.orc_element_apply, lib.orc_jacobi_update, lib.orc_row_dots, lib.orc_row_axpy,
+                      lib.orc_row_xpay):
+                f.restype = None
+            _C_LIB = lib
+    return _C_LIB or None
+
+
+def _rows(a, n):
+    """``(array, row stride, rows)`` of a 1-D (one broadcast row, stride 0) or C-ordered
+    2-D float64 array."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        return a, 0, 1
+    return a, n, a.shape[0]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _grid_of(edof, d):
+    """``(nelx, nely)`` of the reference's structured element dof map."""
+    nelx = int(edof[0, 0]) // d - 1
+    nely = edof.shape[0] // nelx
+    return nelx, nely
+
+
+def _row_axpy(alpha, x, y):
+    """``y += alpha * x`` per row, in place (``alpha`` one value per row)."""
+    lib = c_kernels()
+    if lib is None or x.ndim > 2 or not y.flags.c_contiguous:
+        y += np.reshape(alpha, (-1, 1) if y.ndim == 2 else ()) * x
+        return y
+    n = y.shape[-1]
+    X, x_rs, _ = _rows(x, n)
+    a = np.ascontiguousarray(np.reshape(alpha, -1), dtype=np.float64)
+    lib.orc_row_axpy(a.size, n, _ptr(a), _ptr(X), x_rs, _ptr(y), n if y.ndim == 2 else 0)
+    return y
+
+
+def _row_xpay(z, beta, p):
+    """``p = p * beta + z`` per row, in place."""
+    lib = c_kernels()
+    if lib is None or z.ndim > 2 or not p.flags.c_contiguous:
+        p *= np.reshape(beta, (-1, 1) if p.ndim == 2 else ())
+        p += z
+        return p
+    n = p.shape[-1]
+    Z, z_rs, _ = _rows(z, n)
+    bt = np.ascontiguousarray(np.reshape(beta, -1), dtype=np.float64)
+    lib.orc_row_xpay(bt.size, n, _ptr(Z), z_rs, _ptr(bt), _ptr(p), n if p.ndim == 2 else 0)
+    return p
+
+
+def _row_dots(a, b):
+    lib = c_kernels()
+    if lib is None or a.ndim > 2 or b.ndim > 2:
+        return (a * b).sum(axis=-1)
+    n = a.shape[-1]
+    A, a_rs, ra = _rows(a, n)
+    B, b_rs, rb = _rows(b, n)
+    rows = max(ra, rb)
+    out = np.empty(rows)
+    lib.orc_row_dots(rows, n, _ptr(A), a_rs, _ptr(B), b_rs, _ptr(out))
+    return out if (a.ndim == 2 or b.ndim == 2) else out[0]
 
 # ---------------------------------------------------------------------------------
 # Mesh set-up (sttopt/fem.py)
@@ -144,6 +237,17 @@ def _scatter(per_element: np.ndarray, edof: np.ndarray, ndof: int) -> np.ndarray
 def matvec(U, density, edof, KE, ndof):
     """``K(density) U`` element by element: gather, ``@ KE``, scale, scatter
     (torch_fem.py:62-83).  Leading batch dims of ``U`` and ``density`` broadcast."""
+    lib = c_kernels()
+    if lib is not None and U.ndim <= 2 and np.ndim(density) <= 2:
+        d = KE.shape[-1] // 4
+        nelx, nely = _grid_of(edof, d)
+        Ub, u_rs, ru = _rows(U, ndof)
+        Db, d_rs, rd = _rows(density, edof.shape[0])
+        rows = max(ru, rd)
+        out = np.empty((rows, ndof))
+        K = np.ascontiguousarray(KE, dtype=np.float64)
+        lib.orc_element_apply(rows, nelx, nely, d, _ptr(Ub), u_rs, _ptr(K), 0, 0, _ptr(Db), d_rs, _ptr(out), ndof)
+        return out if (U.ndim == 2 or np.ndim(density) == 2) else out[0]
     Ue = U[..., edof]
     scaled = (Ue @ KE) * density[..., :, None]
     return _scatter(scaled, edof, ndof)
@@ -260,23 +364,25 @@ def pcg(apply_A, b, apply_M, *, rtol=1e-8, max_iter=10000, x0=None, info=None):
         keep = retire()
         x, r = x[keep], r[keep]
     z = apply_M(r)
-    p = z.copy()
-    rz_old = (r * z).sum(axis=-1)
+    p = np.array(z, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    rz_old = _row_dots(r, z)
     n_iter = 0
     for n_iter in range(1, max_iter + 1):
         row_iters += n_rows
         Ap = apply_A(p)
-        alpha = safe_div(rz_old, (p * Ap).sum(axis=-1))[..., None]
-        x = x + alpha * p
-        r = r - alpha * Ap
-        rel = np.linalg.norm(r, axis=-1) / b_norm_safe
+        alpha = safe_div(rz_old, _row_dots(p, Ap))
+        _row_axpy(alpha, p, x)
+        _row_axpy(-alpha, Ap, r)
+        rel = np.sqrt(_row_dots(r, r)) / b_norm_safe
         converged = rel <= rtol
         n_remaining = int(np.count_nonzero(~converged))
         if n_remaining == 0:
             break
         z = apply_M(r)
-        rz_new = (r * z).sum(axis=-1)
-        p = p * safe_div(rz_new, rz_old)[..., None] + z
+        rz_new = _row_dots(r, z)
+        _row_xpay(z, safe_div(rz_new, rz_old), p)
         rz_old = rz_new
         if worth():
             keep = retire()
@@ -398,6 +504,20 @@ class Level:
 
 def keff_matvec(U, keff, edof, ndof):
     """Coarse apply with one explicit matrix per element (torch_mg.py:179-193)."""
+    lib = c_kernels()
+    if lib is not None and U.ndim <= 2 and keff.ndim in (3, 4):
+        k = edof.shape[1]
+        d = k // 4
+        nelx, nely = _grid_of(edof, d)
+        nel = edof.shape[0]
+        Ub, u_rs, ru = _rows(U, ndof)
+        Kb = np.ascontiguousarray(keff, dtype=np.float64)
+        rk = Kb.shape[0] if Kb.ndim == 4 else 1
+        rows = max(ru, rk)
+        out = np.empty((rows, ndof))
+        lib.orc_element_apply(rows, nelx, nely, d, _ptr(Ub), u_rs, _ptr(Kb), k * k,
+                              nel * k * k if Kb.ndim == 4 else 0, None, 0, _ptr(out), ndof)
+        return out if (U.ndim == 2 or Kb.ndim == 4) else out[0]
     return _scatter(np.einsum("...ei,...eij->...ej", U[..., edof], keff), edof, ndof)
 
 
@@ -413,7 +533,10 @@ def dense_cholesky(keff, edof, ndof, mask):
     free = mask[:, None] & mask[None, :]
     dense = np.where(free, dense, 0.0)
     dense = dense + np.diag((~mask).astype(np.float64))
-    return np.linalg.cholesky(dense)
+    if dense.ndim == 2:
+        return scipy.linalg.cholesky(dense, lower=True)
+    return np.stack([scipy.linalg.cholesky(m, lower=True) for m in dense.reshape(-1, ndof, ndof)]).reshape(
+        dense.shape)
 
 
 def build_hierarchy(density, edof, KE, mask, nelx, nely, *, reaction=None,
@@ -447,6 +570,7 @@ def build_hierarchy(density, edof, KE, mask, nelx, nely, *, reaction=None,
                 keff = keff + np.einsum("...em,mij->...eij", reaction[..., children], GM)
         else:
             keff = np.einsum("mpi,...empq,mqj->...eij", S, keff[..., children, :, :], S)
+        keff = np.ascontiguousarray(keff)
         top.kx, top.ky = kx, ky
         cnelx, cnely = top.nelx // kx, top.nely // ky
         cedof = element_dof_map(cnelx, cnely, d)
@@ -475,6 +599,18 @@ class VCycle:
                       n_smooth=self.n_smooth, gamma=self.gamma)
 
     def _smooth(self, level, x, b):
+        lib = c_kernels()
+        if lib is not None and b.ndim <= 2:
+            n = b.shape[-1]
+            x = np.array(np.broadcast_to(x, b.shape), dtype=np.float64)
+            X, x_rs, rows = _rows(x, n)
+            B, b_rs, _ = _rows(b, n)
+            G, g_rs, _ = _rows(level.diag, n)
+            for _ in range(self.n_smooth):
+                Ax, a_rs, _ = _rows(level(X), n)
+                lib.orc_jacobi_update(rows, n, _ptr(X), x_rs, _ptr(B), b_rs, _ptr(Ax), a_rs, _ptr(G), g_rs,
+                                      self.omega)
+            return project(X, level.mask)
         for _ in range(self.n_smooth):
             x = x + self.omega * (b - level(x)) / level.diag
         return project(x, level.mask)
