@@ -56,6 +56,7 @@ enum {
 };
 
 enum { STT_FP64 = 0, STT_FP32 = 1 };
+enum { STT_FORM_MODAL = 0, STT_FORM_PRODUCT = 1 };
 enum { STT_PROJECT_IN = 1, STT_PROJECT_OUT = 2 };
 
 /* Last CUDA / argument error message of this thread (never NULL). */
@@ -85,6 +86,16 @@ int stt_q4_diag(int d, int nelx, int nely, int nrows, const double* rho, long lo
 /* rdiag[n * d + i] = sum over elements e touching node n of reaction[e] / 4.  FP64. */
 int stt_lumped_reaction(int d, int nelx, int nely, int nrows, const double* reaction,
                         long long r_rs, double* out, long long out_rs, stt_stream_t stream);
+
+/* How element matrices are applied, process-wide, by every later stt_hier_create and
+ * level-0 apply (not by hierarchies already built): STT_FORM_MODAL (default) through the
+ * element's edge modes when KE has the modal form (stt_ke_modal), else the 8 x 8 product;
+ * STT_FORM_PRODUCT always the 8 x 8 product of the corner values, as the reference's
+ * torch_fem.matvec (sttopt/torch_fem.py:76-82).  The modal form is faster and exact on
+ * rigid translations; the product form reproduces the reference's FP64 rounding (its
+ * float64 KE gives a translation a stiffness of ~1e-16 per element).  Returns the
+ * previous form, or -1 for an unknown one.  No reference counterpart. */
+int stt_set_element_form(int form);
 
 /* Host only (no device work).  Returns 1 and writes m[8] when KE ((4d)^2 doubles) has
  * the modal form KE = T^T M T of the unit-square bilinear element (the reference's
@@ -213,12 +224,16 @@ int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r, long long 
  * start when has_x0, else is zeroed; b must already be projected.  Outputs: rel_resid
  * [nrows] (host), conv_iter [nrows] (host, -1 = not converged), *n_iter (host).
  * flexible selects the Polak-Ribiere beta; replace_every > 0 recomputes the true
- * residual b - A x every that many iterations.  Returns STT_ERR_NOT_CONVERGED when a
- * row is above rtol after max_iter iterations. */
+ * residual b - A x every that many iterations.  retire selects when a converged row
+ * stops: 0 at once; 1 as the reference retires rows (torch_fem.py:270-331), a converged
+ * row iterating on with the others until the rows short of rtol are at most 3/4 of the
+ * rows left by the previous retirement, so that every row's x equals the reference's
+ * (conv_iter is then the iteration at which the row stopped).  Returns
+ * STT_ERR_NOT_CONVERGED when a row is above rtol after max_iter iterations. */
 int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long long b_rs, double* x,
                long long x_rs, int has_x0, double rtol, int max_iter, double omega,
-               int n_smooth, int gamma, int flexible, int replace_every, double* rel_resid,
-               int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
+               int n_smooth, int gamma, int flexible, int replace_every, int retire,
+               double* rel_resid, int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
                stt_stream_t stream);
 
 /* ---- PCG vector steps for arbitrary operators (FP64) ---------------------------- */

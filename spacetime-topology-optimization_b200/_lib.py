@@ -26,6 +26,9 @@ STT_FP64 = 0
 STT_FP32 = 1
 STT_PROJECT_IN = 1
 STT_PROJECT_OUT = 2
+STT_FORM_MODAL = 0
+STT_FORM_PRODUCT = 1
+_FORMS = {"modal": STT_FORM_MODAL, "product": STT_FORM_PRODUCT}
 
 _c_int, _c_ll, _c_double = ctypes.c_int, ctypes.c_longlong, ctypes.c_double
 _p = ctypes.c_void_p
@@ -45,6 +48,7 @@ _SIGS = {
     "stt_stage_glue_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p, _p,
                                         _c_double, _c_double, _c_double, _p, _p, _p, _p]),
     "stt_ke_modal": (_c_int, [_c_int, _pd, _pd]),
+    "stt_set_element_form": (_c_int, [_c_int]),
     "stt_cone_filter": (_c_int, [_c_int, _c_int, _c_int, _c_double, _p, _c_ll, _p, _p, _c_ll, _c_double,
                                  _c_double, _p]),
     "stt_cone_filter_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_double, _p, _c_ll, _p, _c_ll, _c_double,
@@ -66,7 +70,7 @@ _SIGS = {
     "stt_vcycle": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p, _c_ll, _p]),
     "stt_vcycle_noalloc": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_double, _c_int, _c_int, _p]),
     "stt_pcg_mg": (_c_int, [_p, _c_int, _p, _c_ll, _p, _c_ll, _c_int, _c_double, _c_int, _c_double, _c_int,
-                            _c_int, _c_int, _c_int, _pd, _pi, _pi, _p, _c_ll, _p]),
+                            _c_int, _c_int, _c_int, _c_int, _pd, _pi, _pi, _p, _c_ll, _p]),
     "stt_vec_dots": (_c_int, [_c_int, _c_ll, _p, _p, _p, _p, _p, _p, _c_ll, _p, _p]),
     "stt_vec_cg_update": (_c_int, [_c_int, _c_ll, _p, _p, _p, _p, _p, _c_ll, _p, _p]),
     "stt_vec_xpay": (_c_int, [_c_int, _c_ll, _p, _p, _p, _c_ll, _p]),
@@ -137,6 +141,32 @@ def require_cuda(*tensors: torch.Tensor | None) -> None:
                 "sttopt_b200 runs on CUDA tensors only (no CPU fallback); got a tensor on "
                 f"{t.device}"
             )
+
+
+def set_element_form(form: str) -> str:
+    """How the library applies element matrices from now on (hierarchies built and
+    applies launched after the call): ``"modal"`` (default; the element's edge modes,
+    faster and exact on rigid translations) or ``"product"`` (the 8 x 8 product of the
+    corner values, as the reference computes it, reproducing its FP64 rounding).
+    Returns the previous form."""
+    if form not in _FORMS:
+        raise ValueError(f"element form must be one of {sorted(_FORMS)}, got {form!r}")
+    prev = lib().stt_set_element_form(_FORMS[form])
+    return {v: k for k, v in _FORMS.items()}[prev]
+
+
+class element_form:
+    """``with element_form("product"): ...`` -- ``set_element_form`` for a block."""
+
+    def __init__(self, form: str):
+        self.form = form
+
+    def __enter__(self):
+        self.prev = set_element_form(self.form)
+        return self
+
+    def __exit__(self, *exc):
+        set_element_form(self.prev)
 
 
 def precision_of(dtype: torch.dtype) -> int:

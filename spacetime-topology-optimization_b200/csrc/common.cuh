@@ -43,6 +43,7 @@ struct RowState {
   int status;         // STT_OK, or STT_ERR_BREAKDOWN on a non-finite scalar
   int xpend;          // alpha p of the last update is not yet added to x
   int pbuf;           // which p buffer holds this row's last p (0 or 1)
+  int conv;           // rel <= rtol at the last check (the reference's retirement schedule)
 };
 
 STT_DEV int hier_row(const int* row_map, int hrows, int s) {

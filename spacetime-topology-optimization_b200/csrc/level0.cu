@@ -194,10 +194,15 @@ extern "C" int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
   return set_error(STT_ERR_INVALID, "stt_q4_apply: d must be 1 or 2, precision FP64 or FP32");
 }
 
+extern "C" int stt_set_element_form(int form) {
+  if (form != STT_FORM_MODAL && form != STT_FORM_PRODUCT) return -1;
+  return element_form().exchange(form);
+}
+
 extern "C" int stt_ke_modal(int d, const double* KE, double* m) {
   if (!KE || !m || (d != 1 && d != 2)) return 0;
   double t[8];
-  if (!modal_from_ke(d, KE, t)) return 0;
+  if (!ke_has_modal_form(d, KE, t)) return 0;
   for (int i = 0; i < 8; ++i) m[i] = t[i];
   return 1;
 }

@@ -8,14 +8,30 @@
 // M is T KE T^T / 16.  The KE is accepted only when T^T M T, rebuilt from the constants
 // the kernels use, reproduces it to 1e-12 of its largest entry and its diagonal is the
 // same at every corner; otherwise the caller uses the generic 8 x 8 product.
+//
+// stt_set_element_form(STT_FORM_PRODUCT) refuses every KE, so that the library applies
+// element matrices as the reference does (the 8 x 8 product of the corner values).  The
+// two forms round differently: the modal form annihilates rigid translations exactly,
+// while a float64 KE gives them a stiffness of ~1e-16 per element, which shifts the
+// compliance of large-displacement problems by ~1e-9 relative (measured on the 1024 x 512
+// cantilever); the product form reproduces the reference's results to ~1e-12.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 
 namespace stt {
 
+inline std::atomic<int>& element_form() {
+  static std::atomic<int> form{0};  // STT_FORM_MODAL
+  return form;
+}
+
+inline bool generic_ke_forced() { return element_form().load(std::memory_order_relaxed) != 0; }
+
 // m[8] = {m00, m01, m11, m22, m44, m55, kd0, kd1} in the meaning of MQ (q4.cuh).
-inline bool modal_from_ke(int d, const double* KE, double m[8]) {
+// Recognition only; modal_from_ke below also honours the selected element form.
+inline bool ke_has_modal_form(int d, const double* KE, double m[8]) {
   if (d != 1 && d != 2) return false;
   static const double pat[3][4] = {{-1, 1, 1, -1}, {-1, -1, 1, 1}, {1, -1, 1, -1}};  // Gx, Gy, H
   const int n = 4 * d, nm = 3 * d;
@@ -84,6 +100,12 @@ inline bool modal_from_ke(int d, const double* KE, double m[8]) {
   }
   if (d == 1) m[7] = 0.0;
   return true;
+}
+
+// The kernels' choice: the modal form when KE has it and the modal element form is
+// selected (stt_set_element_form).
+inline bool modal_from_ke(int d, const double* KE, double m[8]) {
+  return !generic_ke_forced() && ke_has_modal_form(d, KE, m);
 }
 
 }  // namespace stt

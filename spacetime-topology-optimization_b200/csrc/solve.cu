@@ -74,6 +74,7 @@ struct SolveWS {
   RowState* rs;
   double* partials;
   unsigned* counters;
+  int* sched_last;             // rows left by the last retirement (reference schedule)
   double *r, *p, *p2, *Ap;     // FP64 [nrows][ndof0]; p and p2 alternate
   void *z, *zold, *b0;         // cycle precision [nrows][ndof0]
   void* x[kMaxLevels];         // per level [nrows][ndof_l]
@@ -107,6 +108,7 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
     w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
     w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
     w.counters = (unsigned*)carve(base, used, 4LL * nrows);
+    w.sched_last = (int*)carve(base, used, 4);
     w.r = (double*)carve(base, used, 8LL * nrows * l0.ndof);
     w.p = (double*)carve(base, used, 8LL * nrows * l0.ndof);
     w.p2 = (double*)carve(base, used, 8LL * nrows * l0.ndof);
@@ -463,7 +465,21 @@ struct PcgParams {
   double rtol;
   int it;
   int flexible;
+  int sched;  // 1: a converged row iterates on until the reference's compaction retires it
 };
+
+// A row's convergence test after a residual: with the reference's schedule (sched) it
+// only records the test, and pcg_retire_kernel decides when the row stops; otherwise the
+// row stops at once.
+STT_DEV void pcg_converged(RowState& S, const PcgParams& pp) {
+  const bool c = S.rel <= pp.rtol;
+  if (pp.sched) {
+    S.conv = c ? 1 : 0;
+  } else if (c) {
+    S.active = 0;
+    S.conv_iter = pp.it;
+  }
+}
 
 // r = b - A x (or r = b when x is null), reductions ||r||^2 and ||b||^2.
 // replace: keep bnorm and only re-test convergence (true-residual replacement).
@@ -554,13 +570,11 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
       S.conv_iter = -1;
       S.status = STT_OK;
       S.active = 1;
+      S.conv = 0;
     }
     S.rel = sqrt(t[0]) / S.bnorm_safe;
     if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
-    if (S.rel <= pp.rtol) {
-      S.active = 0;
-      S.conv_iter = pp.it;
-    }
+    pcg_converged(S, pp);
   });
 }
 
@@ -723,11 +737,40 @@ __global__ void __launch_bounds__(kEwThreads) pcg_update_kernel(
     S.xpend = 1;
     S.rel = sqrt(t[0]) / S.bnorm_safe;
     if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
-    if (S.rel <= pp.rtol) {
-      S.active = 0;
-      S.conv_iter = pp.it;
-    }
+    pcg_converged(S, pp);
   });
+}
+
+// The reference's row retirement (torch_fem.pcg, sttopt/torch_fem.py:270-331): converged
+// rows keep iterating with the others until the rows still short of rtol are at most
+// COMPACTION_RATIO = 3/4 of the rows left by the previous retirement (*last); then every
+// converged row stops (its x stays as of this iteration), and when no row is short of
+// rtol all stop.  One warp; rows in order.
+__global__ void pcg_retire_kernel(RowState* __restrict__ rst, int nrows, int* __restrict__ last, int it) {
+  const int lane = threadIdx.x;
+  int n_left = 0;  // active rows not yet converged
+  for (int s = lane; s < nrows; s += 32) n_left += (rst[s].active && !rst[s].conv) ? 1 : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n_left += __shfl_xor_sync(0xffffffffu, n_left, o);
+  if (it == 0 && lane == 0) {
+    int n_act = 0;
+    for (int s = 0; s < nrows; ++s) n_act += rst[s].active;
+    *last = n_act;
+  }
+  __syncwarp();
+  const int prev = *last;
+  // n_left <= 0.75 * last, in integers; a single row is never compacted, it just finishes
+  const bool retire = n_left == 0 || (nrows > 1 && 4LL * n_left <= 3LL * prev);
+  __syncwarp();
+  if (!retire) return;
+  for (int s = lane; s < nrows; s += 32) {
+    RowState& S = rst[s];
+    if (S.active && S.conv) {
+      S.active = 0;
+      S.conv_iter = it;
+    }
+  }
+  if (lane == 0) *last = n_left;
 }
 
 // x += alpha p for every row whose last update is still pending (p from the buffer its
@@ -917,7 +960,7 @@ struct PapEvents {
 template <int D, typename T>
 static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, long long b_rs,
                    double* x, long long x_rs, int has_x0, double rtol, int max_iter, double omega,
-                   int n_smooth, int gamma, int flexible, int replace_every, double* rel_out,
+                   int n_smooth, int gamma, int flexible, int replace_every, int sched, double* rel_out,
                    int* conv_out, int* n_iter_out, cudaStream_t st) {
   const LevelDesc& l0 = h->lv[0];
   const long long nd = l0.ndof;
@@ -959,8 +1002,9 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     }
 #undef STT_INIT
   };
-  PcgParams pp{rtol, 0, flexible};
+  PcgParams pp{rtol, 0, flexible, sched ? 1 : 0};
   init(has_x0 ? x : nullptr, pp, 0);
+  if (sched) pcg_retire_kernel<<<1, 32, 0, st>>>(w.rs, nrows, w.sched_last, 0);
   STT_TRY(check_launch("pcg init"));
   std::vector<RowState> host(nrows);
   // the reads after the first V-cycle also carry the hierarchy build's status word (the
@@ -1048,6 +1092,7 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       pnext_buf ^= 1;
       pcg_update_kernel<<<dim3(upb, nrows), kEwThreads, 0, st>>>(w.r, w.Ap, nd, nd, w.rs, red_up, pp, r32,
                                                                   vstride(nd));
+      if (sched) pcg_retire_kernel<<<1, 32, 0, st>>>(w.rs, nrows, w.sched_last, it);
       pending = true;
       const bool replaced = replace_every > 0 && it % replace_every == 0;
       if (replaced) {
@@ -1178,8 +1223,8 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
 
 extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long long b_rs, double* x,
                           long long x_rs, int has_x0, double rtol, int max_iter, double omega,
-                          int n_smooth, int gamma, int flexible, int replace_every, double* rel_resid,
-                          int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
+                          int n_smooth, int gamma, int flexible, int replace_every, int retire,
+                          double* rel_resid, int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
                           stt_stream_t stream) {
   if (!h || !b || !x || !workspace || !rel_resid || !conv_iter || !n_iter || nrows <= 0 ||
       nrows > 65535 || max_iter < 0 || n_smooth < 1 || gamma < 1)
@@ -1192,10 +1237,10 @@ extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long lo
   plan_solve(h, nrows, gamma, (char*)workspace, w);
   cudaStream_t st = (cudaStream_t)stream;
   if (h->precision == STT_FP32)
-    return h->d == 2 ? run_pcg<2, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st)
-                     : run_pcg<1, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
-  return h->d == 2 ? run_pcg<2, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st)
-                   : run_pcg<1, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, rel_resid, conv_iter, n_iter, st);
+    return h->d == 2 ? run_pcg<2, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, retire, rel_resid, conv_iter, n_iter, st)
+                     : run_pcg<1, float>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, retire, rel_resid, conv_iter, n_iter, st);
+  return h->d == 2 ? run_pcg<2, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, retire, rel_resid, conv_iter, n_iter, st)
+                   : run_pcg<1, double>(h, w, nrows, b, b_rs, x, x_rs, has_x0, rtol, max_iter, omega, n_smooth, gamma, flexible, replace_every, retire, rel_resid, conv_iter, n_iter, st);
 }
 
 // ---- V-cycle without a caller workspace ---------------------------------------------

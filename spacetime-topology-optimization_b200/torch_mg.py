@@ -230,15 +230,23 @@ class _Level:
         conv = (ctypes.c_int * rows)()
         n_iter = ctypes.c_int()
         mixed = h.precision == "mixed"
+        # FP64 follows the reference's row retirement (a converged row iterates on until the
+        # compaction), so every row's x is the reference's; the mixed form stops a row when
+        # it converges (less work; its FP32 cycle makes the iterates differ anyway)
+        retire = 0 if mixed else 1
         rc = _lib.lib().stt_pcg_mg(
             h.handle, rows, _lib.ptr(flat), n, _lib.ptr(x), n, 1 if x0 is not None else 0, rtol, max_iter,
-            M.omega, M.n_smooth, M.gamma, 1 if mixed else 0, 0, rel, conv, ctypes.byref(n_iter),
+            M.omega, M.n_smooth, M.gamma, 1 if mixed else 0, 0, retire, rel, conv, ctypes.byref(n_iter),
             _lib.ptr(ws), ws.numel(), _lib.stream())
         conv_list = list(conv)
         n_rows_ref = b.shape[0] if b.ndim == 2 else 1
         if info is not None:
-            info["row_iters"] = torch_fem.row_iters_from_schedule(conv_list, n_rows_ref, max_iter) \
-                if b.ndim == 2 else (max(conv_list) if min(conv_list) >= 0 else max_iter)
+            if b.ndim != 2:
+                info["row_iters"] = max(conv_list) if min(conv_list) >= 0 else max_iter
+            elif retire:  # each row iterated until the iteration it stopped at
+                info["row_iters"] = sum(v if v >= 0 else max_iter for v in conv_list)
+            else:
+                info["row_iters"] = torch_fem.row_iters_from_schedule(conv_list, n_rows_ref, max_iter)
         if rc == _lib.STT_ERR_NOT_CONVERGED:
             resid = torch.tensor(list(rel), dtype=torch.float64, device=b.device)
             raise torch_fem.CGConvergenceError(resid.reshape(batch) if b.ndim == 2 else resid[0], max_iter, rtol)

@@ -2,18 +2,26 @@
 made by ``tests/golden/make_golden.py --full-size``, which runs the reference's FP64
 torch path on the CPU; inputs are regenerated here from the seeds).
 
-* Config 2, the 1024x512 cantilever in FP64 (6 levels, 1122-dof coarse Cholesky): at
-  the config's rtol 1e-8 the forward / adjoint iteration counts equal the reference's
-  and U, c agree with its rtol-1e-8 run to 1e-9, dc to 5e-9 (two rtol-1e-8 solves differ
-  by ~1e-9 on the adjoint factor: the reference's own rtol-1e-8 and rtol-1e-12 runs
-  differ by 9.3e-10 on dc); at rtol 1e-12, U, c and dc agree with its rtol-1e-12 run to
-  1e-9; the mixed form (FP32 V-cycle) at rtol 1e-8 to 1e-6.
+Two element forms (``sttopt_b200.element_form``): the default modal form applies each
+element through its edge modes and annihilates rigid translations exactly; the product
+form is the reference's 8 x 8 product of the corner values.  A float64 KE gives a rigid
+translation a stiffness of ~1e-16 per element, so on a large-displacement problem the two
+FP64 discretisations differ by ~1e-9 relative in compliance (measured: 7.5e-10 on the
+1024x512 cantilever, whose tip moves ~400 units; the oracle, a third FP64 code with the
+product form, agrees with the reference to 3e-12).  The product form therefore carries
+the north star's 1e-9 FP64 parity; the modal form is held to the bounds measured for it.
+
+* Config 2, the 1024x512 cantilever in FP64 (6 levels, 1122-dof coarse Cholesky): product
+  form at the config's rtol 1e-8 (iteration counts equal to the reference's) and at rtol
+  1e-12: U, c and dc to 1e-9; modal form: c to 1e-9, U and dc to 2e-9; the mixed form
+  (FP32 V-cycle) at rtol 1e-8 to 1e-6 against the reference's rtol-1e-12 run.
 * The space-time objective at 1024x512 and at 2048x1024 (the benchmark's grid, seed and
-  16 stages): the mixed form at rtol 1e-8 (the benchmark's form) against the
-  reference's rtol-1e-12 run to 1e-6 on the stage compliances, the objective, tPhys and
-  the gradient; FP64 at rtol 1e-12 to 1e-9; FP64 at rtol 1e-8 with the reference's
+  16 stages): the mixed form at rtol 1e-8 (the benchmark's form) against the reference's
+  rtol-1e-12 run to 1e-6 on the stage compliances, the objective, tPhys and the gradient;
+  FP64 modal at rtol 1e-12 to 1e-9; FP64 at the config's rtol 1e-8 with the reference's
   stage and adjoint iteration counts and its stage membership (three exact integers a
-  stage).
+  stage), to 1e-9 (product form; U of the modal form to the solve tolerance 1e-8, its
+  iterates rounding differently).
 
 Large fields are compared through ``summary_error`` (seeded projections and a strided
 subsample; relative L2).  Measured errors are printed and, with ``STT_PARITY_LOG`` set,
@@ -111,24 +119,29 @@ def test_cantilever1024_hierarchy_shapes(cantilever, pkg):
     assert levels[-1].ndof == int(g["coarse_ndof"])
 
 
-@pytest.mark.parametrize("precision,rtol,tag,tol_u,tol_dc", [
-    ("fp64", 1e-8, "r8", 1e-9, 5e-9),
-    ("fp64", 1e-12, "r12", 1e-9, 1e-9),
-    ("mixed", 1e-8, "r12", 1e-6, 1e-6),
+@pytest.mark.parametrize("precision,rtol,tag,form,tol_c,tol_u,tol_dc", [
+    ("fp64", 1e-8, "r8", "product", 1e-9, 1e-9, 1e-9),
+    ("fp64", 1e-12, "r12", "product", 1e-9, 1e-9, 1e-9),
+    ("fp64", 1e-8, "r8", "modal", 1e-9, 2e-9, 2e-9),
+    ("fp64", 1e-12, "r12", "modal", 1e-9, 2e-9, 2e-9),
+    ("mixed", 1e-8, "r12", "modal", 1e-6, 1e-6, 1e-6),
 ])
-def test_cantilever1024(cantilever, precision, rtol, tag, tol_u, tol_dc):
+def test_cantilever1024(cantilever, precision, rtol, tag, form, tol_c, tol_u, tol_dc):
+    from sttopt_b200 import element_form
+
     g, x, F, mask = cantilever
-    U, c, dc, info = _cantilever_solve(x, F, mask, rtol, precision)
+    with element_form(form):
+        U, c, dc, info = _cantilever_solve(x, F, mask, rtol, precision)
     eu, edc = summary_error(f"{tag}_U", g, U), summary_error(f"{tag}_dc", g, dc)
     ec = abs(c - float(g[f"{tag}_c"])) / abs(float(g[f"{tag}_c"]))
-    record(f"cantilever1024 {precision} rtol {rtol:g} vs reference rtol {'1e-8' if tag == 'r8' else '1e-12'}",
+    record(f"cantilever1024 {precision} {form} rtol {rtol:g} vs reference rtol {'1e-8' if tag == 'r8' else '1e-12'}",
            c=ec, U=max(eu["proj"], eu["sub"]), dc=max(edc["proj"], edc["sub"]), fwd_iter=info["forward_n_iter"],
            bwd_iter=info["backward_n_iter"], ref_fwd_iter=int(g[f"{tag}_fwd_iter"]),
            ref_bwd_iter=int(g[f"{tag}_bwd_iter"]))
     if precision == "fp64" and tag == "r8":
         assert info["forward_n_iter"] == int(g["r8_fwd_iter"])
         assert info["backward_n_iter"] == int(g["r8_bwd_iter"]) == 0
-    assert ec <= tol_u
+    assert ec <= tol_c
     assert eu["proj"] < tol_u and eu["sub"] < tol_u
     assert edc["proj"] < tol_dc and edc["sub"] < tol_dc
     # fixed dofs exactly zero
@@ -148,19 +161,22 @@ def _spacetime_case(name):
 
 
 @pytest.mark.parametrize("name", ["spacetime1024", "spacetime2048"])
-@pytest.mark.parametrize("precision,rtol,tag,tol,tol_g", [
-    ("mixed", 1e-8, "r12", 1e-6, 1e-6),
-    ("fp64", 1e-12, "r12", 1e-9, 1e-9),
-    ("fp64", 1e-8, "r8", 1e-9, 5e-9),
+@pytest.mark.parametrize("precision,rtol,tag,form,tol,tol_u", [
+    ("mixed", 1e-8, "r12", "modal", 1e-6, 1e-6),
+    ("fp64", 1e-12, "r12", "modal", 1e-9, 1e-9),
+    ("fp64", 1e-8, "r8", "product", 1e-9, 1e-9),
+    ("fp64", 1e-8, "r8", "modal", 1e-9, 1e-8),
 ])
-def test_spacetime_fullsize(pkg, name, precision, rtol, tag, tol, tol_g):
-    from sttopt_b200 import spacetime
+def test_spacetime_fullsize(pkg, name, precision, rtol, tag, form, tol, tol_u):
+    from sttopt_b200 import element_form, spacetime
 
     g, x, w = _spacetime_case(name)
     n_stage = int(g["n_stage"])
     info = {}
-    out = spacetime.objective_and_gradient(T(x), T(w), n_stage=n_stage, precision=precision, rtol=rtol, info=info)
-    torch.cuda.synchronize()
+    with element_form(form):
+        out = spacetime.objective_and_gradient(T(x), T(w), n_stage=n_stage, precision=precision, rtol=rtol,
+                                               info=info)
+        torch.cuda.synchronize()
     c_s = out["c_s"].cpu().numpy()
     e_c = rel(c_s, g[f"{tag}_c_s"])
     e_cmax = float(np.max(np.abs(c_s - g[f"{tag}_c_s"]) / np.abs(g[f"{tag}_c_s"])))
@@ -172,7 +188,7 @@ def test_spacetime_fullsize(pkg, name, precision, rtol, tag, tol, tol_g):
     mh = member_hash(out["member"].cpu().numpy())
     member_equal = bool(np.array_equal(mh, g[f"{tag}_member"]))
     count_diff = int(np.abs(mh[:, 0] - g[f"{tag}_member"][:, 0]).max())
-    record(f"{name} {precision} rtol {rtol:g} vs reference rtol {'1e-8' if tag == 'r8' else '1e-12'}",
+    record(f"{name} {precision} {form} rtol {rtol:g} vs reference rtol {'1e-8' if tag == 'r8' else '1e-12'}",
            c_s=e_c, c_s_max=e_cmax, objective=e_L, gradient=max(e_g["proj"], e_g["sub"]),
            tPhys=max(e_t["proj"], e_t["sub"]), U=max(e_u["proj"], e_u["sub"]), member_equal=member_equal,
            member_count_diff=count_diff, iters={k: v for k, v in info.items()},
@@ -188,5 +204,5 @@ def test_spacetime_fullsize(pkg, name, precision, rtol, tag, tol, tol_g):
         assert info["adjoint_n_iter"] == int(g["r8_bwd_iter"])
     assert e_cmax < tol and e_L < tol
     assert e_t["proj"] < tol and e_t["sub"] < tol
-    assert e_u["proj"] < tol and e_u["sub"] < tol
-    assert e_g["proj"] < tol_g and e_g["sub"] < tol_g
+    assert e_u["proj"] < tol_u and e_u["sub"] < tol_u
+    assert e_g["proj"] < tol and e_g["sub"] < tol

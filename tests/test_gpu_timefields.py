@@ -5,7 +5,9 @@ reference's outputs (golden fixtures made by running it on the same seeded input
   point-load row 0 and the device gravity stencil: compliances and displacements 1e-9
   relative, the gradients in xPhys and tPhys 5e-8 (converged FP64 solves at rtol 1e-8).
 * ``whole_compliance``, ``gravity_compliance`` and ``_gravity_load`` (fields 1e-9 /
-  1e-14, gradients 5e-9 / 5e-8 / 1e-13) and the batched call with the hard stage mask.
+  1e-14, gradients 1e-9 / 1e-8 / 1e-13) and the batched call with the hard stage mask,
+  solves at rtol 1e-12 through the patch points on both sides (a nearly disconnected
+  stage, which FP64 fixes only to ~1e-8, at 5e-8).
 * The fused Poisson load and its adjoint, element means: 1e-13 (same arithmetic to
   rounding).
 * ``heat_time_field`` with the ``neg_log`` map (solves at rtol 1e-10): fields 1e-9,
@@ -57,13 +59,40 @@ def test_batched_whole_and_gravity_compliance_smooth(pkg, key, sparse_C):
     assert rel_err(gt.cpu(), g[f"{key}_gt"]) < 5e-8
 
 
-def test_single_solve_glue_and_hard_mask(pkg):
+@pytest.fixture
+def product_form(pkg):
+    """The reference's element form for the duration of a test."""
+    from sttopt_b200 import element_form
+
+    with element_form("product"):
+        yield
+
+
+def test_single_solve_glue_and_hard_mask(pkg, monkeypatch, product_form):
     """whole_compliance, gravity_compliance and _gravity_load with their gradients, and the
     batched call with ``mask_fn=hard_time_mask``, against the reference (the hard mask by
-    replacing its ``time_mask``)."""
-    from sttopt_b200 import compliance, fem, gravity
+    replacing its ``time_mask``).  Both sides solve at rtol 1e-12 through the patch points
+    ``_solve_fe`` / ``_solve_fe_batched`` (one stage is a nearly disconnected build whose
+    compliance an rtol-1e-8 solve fixes only to ~1e-8: the oracle and the reference differ
+    by 1.4e-8 there), in the reference's element form (that stage floats on the void
+    material with large rigid displacements, where the modal form and the reference's
+    float64 KE differ by 3e-8)."""
+    from sttopt_b200 import compliance, fem, gravity, torch_fem, torch_solve
 
     g = golden("compliance_single")
+    rtol = float(g["rtol"])
+
+    def solve_fe(KE_, xPhys, Emin, Emax, penal, edofMat, freedofs, F_, ndof_, *, x0=None):
+        nely_, nelx_ = xPhys.shape
+        density = torch_fem.simp_density(xPhys, Emin, Emax, penal)
+        m = torch_fem.free_mask(ndof_, freedofs, device=xPhys.device)
+        return torch_solve.femsolve(density.flatten(), F_, edofMat, KE_, m, nelx_, nely_, x0=x0, rtol=rtol)
+
+    def solve_fe_batched(KE_, density, edofMat, m, nelx_, nely_, F_, *, x0=None):
+        return torch_solve.femsolve(density, F_, edofMat, KE_, m, nelx_, nely_, x0=x0, rtol=rtol)
+
+    monkeypatch.setattr(compliance, "_solve_fe", solve_fe)
+    monkeypatch.setattr(compliance, "_solve_fe_batched", solve_fe_batched)
     nely, nelx = g["x"].shape
     ndof = 2 * (nelx + 1) * (nely + 1)
     KE, edof = T(fem.plane_stress_KE(NU)), T(fem.element_dof_map(nelx, nely), torch.int64)
@@ -74,14 +103,14 @@ def test_single_solve_glue_and_hard_mask(pkg):
     (gx,) = torch.autograd.grad(c, [x])
     assert abs(float(c) - float(g["whole_c"])) <= 1e-9 * abs(float(g["whole_c"]))
     assert rel_err(U.detach().cpu(), g["whole_U"]) < 1e-9
-    assert rel_err(gx.cpu(), g["whole_gx"]) < 5e-9
+    assert rel_err(gx.cpu(), g["whole_gx"]) < 1e-9
     x, tp = T(g["x"]).requires_grad_(True), T(g["t"]).requires_grad_(True)
     cg, Ug = compliance.gravity_compliance(x, tp, KE, edof, EMIN, EMAX, PENAL, 0.55, C, 12.0, free, ndof)
     gx, gt = torch.autograd.grad(cg, [x, tp])
     assert abs(float(cg) - float(g["grav_c"])) <= 1e-9 * abs(float(g["grav_c"]))
     assert rel_err(Ug.detach().cpu(), g["grav_U"]) < 1e-9
-    assert rel_err(gx.cpu(), g["grav_gx"]) < 5e-8
-    assert rel_err(gt.cpu(), g["grav_gt"]) < 5e-8
+    assert rel_err(gx.cpu(), g["grav_gx"]) < 1e-8
+    assert rel_err(gt.cpu(), g["grav_gt"]) < 1e-8
     x, tp = T(g["x"]).requires_grad_(True), T(g["t"]).requires_grad_(True)
     tm, xj, Fg = compliance._gravity_load(x, tp, 0.4, C, 8.0, ndof)
     J = torch.sum(T(g["wF"]) * Fg) + torch.sum(T(g["wx"]) * xj)
@@ -97,8 +126,15 @@ def test_single_solve_glue_and_hard_mask(pkg):
         mask_fn=compliance.hard_time_mask)
     (gx,) = torch.autograd.grad(c + 2.0 * stages[0] + stages[1] + 0.5 * stages[2], [x])
     assert abs(float(c) - float(g["hard_c"])) <= 1e-9 * abs(float(g["hard_c"]))
-    assert rel_err(torch.stack(stages).detach().cpu(), g["hard_stages"]) < 1e-9
-    assert rel_err(U.detach().cpu(), g["hard_U"]) < 1e-9
+    # stage 2 (t <= 0.6) is the nearly disconnected build: FP64 fixes its compliance and U
+    # only to ~1e-8 (the oracle at rtol 1e-12 or 1e-14 stagnates 1.8e-8 / 9e-9 from the
+    # reference there, its F.U and U.KU 1e-8 apart); the other rows agree to 1e-9
+    st = torch.stack(stages).detach().cpu().numpy()
+    err = np.abs(st / g["hard_stages"] - 1)
+    assert err[0] < 1e-9 and err[2] < 1e-9 and err[1] < 5e-8
+    Uh = U.detach().cpu().numpy()
+    for row, tol in [(0, 1e-9), (1, 1e-9), (2, 5e-8), (3, 1e-9)]:
+        assert rel_err(Uh[row], g["hard_U"][row]) < tol, row
     assert rel_err(gx.cpu(), g["hard_gx"]) < 5e-8
 
 
