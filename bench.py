@@ -5,15 +5,18 @@ One step = one evaluation of the full 16-stage space-time objective and its grad
 on a 2048 x 1024 Q4 grid: the virtual-heat time-field solve, stage membership
 ``t <= s/16``, 16 self-weight stage solves (one batched device PCG, rtol 1e-8, FP32
 V-cycle inside FP64 PCG), the stage adjoints, the heat adjoint and the sensitivity
-field.  Metric: converged stage solves per second (16 per step, summed over ranks);
-the JSON line also carries the time per full gradient.
+field.  Metric: converged stage solves per second (16 per step); the JSON line also
+carries the time per full gradient.
 
-``--impl reference`` times the CPU restatement of the reference algorithm (the
-oracle; the reference itself is Python and is not installed on the GPU box) on a
-bounded sample of the same workload, scaled to the same metric.
+``--impl reference`` times the CPU restatement of the reference algorithm (the oracle;
+the reference itself is Python and is not installed on the GPU box) on the same
+full-size workload with every host core (stages in a process pool, the heat adjoint
+beside them), as many whole evaluations as fit its time budget.
 
-Multi-GPU: the path has no exchange step, so N ranks run N independent replicas
-(weak scaling); the time is the max over ranks.
+Multi-GPU (``--gpus N`` under torchrun): one objective split over the ranks -- rank 0
+solves the heat field and broadcasts tPhys, each rank solves its share of the 16 stages
+and their adjoints, one all-reduce combines the gradient and the stage compliances
+(strong scaling); the time is the max over ranks.
 """
 
 from __future__ import annotations
@@ -35,9 +38,9 @@ NELX, NELY, N_STAGE = 2048, 1024, 16
 SEED = 3
 METRIC = "stage solves/s (space-time objective + full gradient, 2048x1024 Q4, 16 stages, rtol 1e-8)"
 UNIT = "stage solves/s"
-# Per-launch DRAM bytes of the roofline kernels from ncu captures: the FP32 apply at 16 rows
-# (profiles/q4_apply_fp32_2048x1024_16rows.md), and the FP64 p.Ap pass per stage row, from a
-# 2-row capture scaled by the rows (profiles/pcg_pap_fp64_2048x1024.md).
+# Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the roofline
+# kernels from ncu captures: the FP32 level-0 apply over 16 stage rows, and the FP64 p.Ap
+# pass per stage row (a 4-row capture of bench.py --pcg-only, divided by its 4 rows).
 NCU_TRAFFIC = {"l0_apply_fp32_16rows": 687000576, "pcg_pap_fp64_per_row": 198669505}
 
 
@@ -61,6 +64,12 @@ def parse():
                          "seeded densities and loads)")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the batched uneven multi-problem measurement")
+    ap.add_argument("--no-dropin", action="store_true",
+                    help="skip the end-to-end timing through the reference-signature chain")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="seconds of full-size CPU evaluations the reference arm may spend (at least one)")
+    ap.add_argument("--cpu-budget", type=float, default=0.0,
+                    help="seconds of full-size CPU evaluations the cpu_baseline leg may spend (at least one)")
     ap.add_argument("--uneven-only", action="store_true",
                     help="run only the batched uneven multi-problem measurement")
     return ap.parse_args()
@@ -73,28 +82,45 @@ def dist_env():
     return rank, world, local
 
 
-# ---- CPU baseline: the oracle on a bounded sample ------------------------------------
+# ---- CPU baseline: the oracle on the full workload -----------------------------------
 
-def cpu_sample(steps: int, warmup: int):
-    """Times the oracle's full objective + gradient on a smaller grid of the same
-    workload (16 stages) and scales by the element count (MG iterations are
-    mesh-independent here: 20 stage / 9 heat iterations at 256x128 and 512x256)."""
+def cpu_full_evaluations(max_evals: int, budget_s: float) -> dict:
+    """Times the oracle's full space-time objective + gradient at 2048x1024 with 16 stages
+    (the benchmark's seed), at most ``max_evals`` times and no more once ``budget_s`` is
+    spent (at least once).  Every host core works: the 16 stages run in a spawn-started
+    pool of single-threaded processes while the main process runs the heat adjoint, and
+    the oracle's C/OpenMP loops use all threads in the main process.  A 64x32 evaluation
+    first starts the pool's workers (untimed)."""
     import numpy as np
 
     from oracle import sttopt_oracle as O
 
-    nx, ny = (256, 128) if steps + warmup <= 8 else (128, 64)
-    x = O.smoothed_density(nx, ny, SEED)
-    w = np.random.default_rng(SEED).uniform(-1, 1, (ny, nx))
-    t0 = time.perf_counter()
-    out = O.spacetime_objective(x, w, n_stage=N_STAGE)
-    dt = time.perf_counter() - t0
-    scale = (NELX * NELY) / (nx * ny)
-    full_s = dt * scale
-    return dict(value=N_STAGE / full_s, full_gradient_ms=full_s * 1e3, sample=(
-        f"oracle full objective+gradient at {nx}x{ny}, 16 stages ({dt:.2f} s, "
-        f"{out['forward_n_iter']} stage / {out['heat_n_iter']} heat iterations), scaled x{scale:.0f} "
-        "by element count"), seconds=dt)
+    workers = os.cpu_count() or 1
+    pool = O.stage_pool(workers)
+    try:
+        xs = O.smoothed_density(64, 32, SEED)
+        O.spacetime_objective(xs, np.random.default_rng(SEED).uniform(-1, 1, xs.shape), n_stage=N_STAGE, pool=pool)
+        x = O.smoothed_density(NELX, NELY, SEED)
+        w = np.random.default_rng(SEED).uniform(-1, 1, (NELY, NELX))
+        times, t_start = [], time.perf_counter()
+        while len(times) < max(1, max_evals):
+            t0 = time.perf_counter()
+            out = O.spacetime_objective(x, w, n_stage=N_STAGE, pool=pool)
+            times.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_start + times[-1] > budget_s:
+                break
+    finally:
+        pool.close()
+        pool.join()
+    med = statistics.median(times)
+    return dict(value=N_STAGE / med, full_gradient_ms=med * 1e3, evaluations=len(times), seconds=times,
+                cores=workers, c_kernels=O.c_kernels() is not None, iterations=dict(
+                    stage=out["forward_n_iter"], heat=out["heat_n_iter"], adjoint=out["adjoint_n_iter"],
+                    heat_adjoint=out["heat_adjoint_n_iter"]),
+                sample=(f"the full workload: {len(times)} evaluation(s) of the 2048x1024 x 16-stage objective + "
+                        f"gradient ({', '.join(f'{t:.1f}' for t in times)} s), stages in a spawn pool of {workers} "
+                        f"single-thread processes beside the heat adjoint, oracle C/OpenMP loops "
+                        f"{'on' if O.c_kernels() is not None else 'absent (NumPy)'}; no scaling"))
 
 
 def run_reference(args):
@@ -104,22 +130,23 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ.setdefault(k, str(threads))
-    vals, ms, last = [], [], None
-    for i in range(args.warmup + args.steps):
-        s = cpu_sample(args.steps, args.warmup)
-        if i >= args.warmup:
-            vals.append(s["value"])
-            ms.append(s["full_gradient_ms"])
-        last = s
-    v = statistics.median(vals)
+    os.environ.setdefault("OMP_WAIT_POLICY", "passive")
+    s = cpu_full_evaluations(args.steps, args.ref_budget)
+    v = s["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(ms),
+        "steps": s["evaluations"], "warmup": 0, "ms_per_step": s["full_gradient_ms"],
+        "requested": {"steps": args.steps, "warmup": args.warmup,
+                      "note": "each step is a whole full-size CPU evaluation; as many as fit --ref-budget seconds "
+                              "are timed (at least one), no warm-up evaluation at full size"},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded smoothed density, seeded time weights)",
-        "config": {"workload": "space-time full gradient 2048x1024x16 stages, CPU oracle sample",
+        "data": "synthetic (seeded N(0,1) noise, radius-4 cone filter, mapped to [1e-3, 1]; seeded U(-1,1) time weights)",
+        "config": {"workload": "space-time objective + full gradient: heat time field, 16 hard-threshold gravity "
+                               "stages, MG-PCG rtol 1e-8, stage + heat adjoints (CPU oracle, FP64)",
                    "nelx": NELX, "nely": NELY, "n_stage": N_STAGE},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": last["sample"]},
+        "iterations": s["iterations"],
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": s["cores"], "kind": "port", "sample": s["sample"],
+                         "seconds_per_evaluation": s["seconds"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -314,11 +341,9 @@ def main():
     load_package()
     from sttopt_b200 import _lib, sharding, spacetime, synthetic
 
-    # each rank solves its own problem (independent units sharded over the ranks; no
-    # collective on the data path): rank 0 keeps the single-GPU workload's seed
-    seed = sharding.rank_seed(SEED, rank)
-    x = synthetic.smoothed_density(NELX, NELY, seed, device=dev)
-    w = synthetic.time_weights(NELX, NELY, seed, device=dev)
+    # the one workload of every rank (with N ranks its 16 stages are split over them)
+    x = synthetic.smoothed_density(NELX, NELY, SEED, device=dev)
+    w = synthetic.time_weights(NELX, NELY, SEED, device=dev)
     problem = spacetime.SpaceTimeProblem(NELX, NELY, dev)
     if args.roofline_only:
         u = torch.randn(N_STAGE, 2 * problem.nnode, device=dev, dtype=torch.float64)
@@ -341,8 +366,16 @@ def main():
         return spacetime.objective_and_gradient(xx, ww, n_stage=N_STAGE, precision=precision,
                                                 problem=problem, info=info, batched=batched)
 
+    def timed_step(xx, ww):
+        """The measured step: the whole objective, or this rank's share of it split over
+        the ranks (heat field broadcast from rank 0, one all-reduce)."""
+        if world == 1:
+            return step(xx, ww)
+        return sharding.objective_and_gradient_split(xx, ww, n_stage=N_STAGE, precision=args.precision,
+                                                     problem=problem, info=info)
+
     for _ in range(max(args.warmup, 0)):
-        out = step(x, w)
+        out = timed_step(x, w)
     torch.cuda.synchronize()
 
     def barrier():
@@ -366,7 +399,7 @@ def main():
         for k in range(args.steps):
             marks[k].record()
             torch.cuda.nvtx.range_push("timed_step")  # lets a profiler select one step's launches
-            out = step(x, w)
+            out = timed_step(x, w)
             torch.cuda.nvtx.range_pop()
         marks[-1].record()
         end.record()
@@ -384,7 +417,7 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         elapsed_ms = float(t.item())
     ms_per_step = elapsed_ms / args.steps
-    value = N_STAGE * args.steps * world / (elapsed_ms / 1e3)
+    value = N_STAGE * args.steps / (elapsed_ms / 1e3)  # one objective's 16 stages a step, on all ranks together
     iters = dict(info)
 
     # end to end through the public call with host buffers
@@ -398,7 +431,7 @@ def main():
     for _ in range(2):
         xd.copy_(xh, non_blocking=True)
         wd.copy_(wh, non_blocking=True)
-        o = step(xd, wd)
+        o = timed_step(xd, wd)
         gh.copy_(o["gradient"], non_blocking=True)
     torch.cuda.synchronize()
     barrier()
@@ -411,7 +444,7 @@ def main():
         emarks[k].record()
         xd.copy_(xh, non_blocking=True)
         wd.copy_(wh, non_blocking=True)
-        o = step(xd, wd)
+        o = timed_step(xd, wd)
         gh.copy_(o["gradient"], non_blocking=True)
         oh.copy_(o["objective"].reshape(1), non_blocking=True)
     emarks[-1].record()
@@ -425,7 +458,7 @@ def main():
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = N_STAGE * args.steps * world / (e2e_ms / 1e3)
+    e2e_value = N_STAGE * args.steps / (e2e_ms / 1e3)
     h2d = xh.numel() * 8 + wh.numel() * 8
     d2h = gh.numel() * 8 + 8
 
@@ -447,27 +480,32 @@ def main():
                                     "max_rel_err_stage_compliance": c_err, "rel_err_gradient_l2": g_err}
         if not args.no_profile:
             extra["gpu_launches_per_step"], extra["top_kernels"] = profile_step(step, x, w)
+        if not args.no_dropin:
+            extra["e2e_dropin"] = {p: run_dropin(dev, x, w, args.steps, max(args.warmup, 1), p, out)
+                                   for p in ("fp64", "mixed")}
         if not args.no_uneven:
             del ref
             torch.cuda.empty_cache()
             extra["batched_uneven"] = run_uneven(dev)
         if world == 1 and not args.no_cpu_baseline:
-            s = cpu_sample(1, 0)
-            extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": 1, "kind": "port",
-                                     "sample": s["sample"], "full_gradient_ms": s["full_gradient_ms"]}
+            s = cpu_full_evaluations(1, args.cpu_budget)
+            extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "port",
+                                     "sample": s["sample"], "full_gradient_ms": s["full_gradient_ms"],
+                                     "iterations": s["iterations"]}
     if rank == 0:
         launches = extra.pop("gpu_launches_per_step", None)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong", "vs_baseline": None,
             "dtype": "f64 outer PCG + f32 V-cycle" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded N(0,1) noise, radius-4 cone filter, mapped to [1e-3, 1]; seeded U(-1,1) time weights)",
             "config": {"workload": "space-time objective + full gradient: heat time field, 16 hard-threshold "
                                    "gravity stages, batched MG-PCG rtol 1e-8, stage + heat adjoints",
                        "nelx": NELX, "nely": NELY, "n_stage": N_STAGE, "precision": args.precision,
-                       "parallelism": (f"{world} ranks, one seeded problem each (independent units, no "
-                                       "collective on the data path)") if world > 1 else "single GPU",
+                       "parallelism": (f"{world} ranks split the one objective: rank 0 solves the heat field and "
+                                       "broadcasts tPhys, the 16 stages are spread over the ranks, one all-reduce "
+                                       "of gradient and stage compliances") if world > 1 else "single GPU",
                        "l2": "working set (16 stage rows x 4.2M dofs, hierarchy) far above the 126 MB L2; no flush"},
             "full_gradient_ms": ms_per_step,
             "iterations": iters,
@@ -482,6 +520,51 @@ def main():
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_dropin(dev, x, w, steps, warmup, precision, fused):
+    """End to end through the reference-signature chain (``spacetime.DropInChain``:
+    heat_time_field -> batched_whole_and_gravity_compliance(mask_fn=hard_time_mask) ->
+    jacobian_rows) with host buffers: each step copies x and w in from pinned host memory
+    and the gradient and objective out.  Also the chain's agreement with the fused step."""
+    import torch
+
+    from sttopt_b200 import spacetime
+
+    chain = spacetime.DropInChain(NELX, NELY, dev, n_stage=N_STAGE)
+    xh, wh = x.detach().cpu().pin_memory(), w.detach().cpu().pin_memory()
+    gh = torch.empty(NELY, NELX, dtype=torch.float64).pin_memory()
+    oh = torch.empty(1, dtype=torch.float64).pin_memory()
+    xd, wd = torch.empty_like(x), torch.empty_like(w)
+
+    def one():
+        xd.copy_(xh, non_blocking=True)
+        wd.copy_(wh, non_blocking=True)
+        o = chain(xd, wd, precision=precision)
+        gh.copy_(o["gradient"], non_blocking=True)
+        oh.copy_(o["objective"].reshape(1), non_blocking=True)
+        return o
+
+    for _ in range(warmup):
+        o = one()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        o = one()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    c_err = float(((o["c_s"] - fused["c_s"]).abs() / fused["c_s"].abs()).max())
+    g_err = float((o["gradient"] - fused["gradient"]).norm() / fused["gradient"].norm())
+    del chain
+    torch.cuda.empty_cache()
+    return {"value": N_STAGE / (ms / 1e3), "unit": UNIT, "full_gradient_ms": ms, "steps": steps,
+            "h2d_bytes_per_step": 2 * x.numel() * 8, "d2h_bytes_per_step": x.numel() * 8 + 8,
+            "vs_fused_step": {"max_rel_err_stage_compliance": c_err, "rel_err_gradient_l2": g_err},
+            "path": "heat_time_field -> batched_whole_and_gravity_compliance(mask_fn=hard_time_mask) -> "
+                    "jacobian_rows" + (" (stage solve through the _solve_fe_batched patch point, FP32 V-cycle)"
+                                       if precision == "mixed" else " (FP64, the reference's arithmetic)")}
 
 
 def roofline(_lib, P, out, dev, pap_live=None):
@@ -503,7 +586,7 @@ def roofline(_lib, P, out, dev, pap_live=None):
         # the V-cycle's layout: rows padded to 16 bytes
         vs = (ndof + 3) // 4 * 4
         u = torch.zeros(rows, vs, device=dev, dtype=dt)
-        u[:, :ndof] = out["U"].to(dt)
+        u[:, :ndof] = (out["U"] if "U" in out else torch.randn(rows, ndof, device=dev, dtype=torch.float64)).to(dt)
         rho = torch.rand(rows, nel, device=dev, dtype=torch.float64).to(dt)
         o = torch.empty_like(u)
         for _ in range(3):

@@ -1,11 +1,20 @@
-"""Sharding independent space-time problems over ranks (one process per GPU).
+"""Spreading the space-time work over ranks (one process per GPU).
 
-The solve path has no exchange step: stage rows, load cases and whole problems are
-independent units.  Units are given to ranks whole, balanced by their estimated cost
-(elements x stage rows, the work of the batched solves), and each rank solves its own
-with ``spacetime.objective_and_gradient_many``; nothing crosses ranks during a solve.
-``gather`` (optional) collects every rank's results afterwards, for callers that want
-the full list on every rank.
+The solve path has no exchange step inside a solve: stage rows, load cases and whole
+problems are independent units.
+
+* Independent problems (``objective_and_gradient_sharded``): given to ranks whole,
+  balanced by their estimated cost (elements x stage rows, the work of the batched
+  solves); each rank solves its own with ``spacetime.objective_and_gradient_many``;
+  ``gather`` (optional) collects the results afterwards.
+* One objective split over ranks (``objective_and_gradient_split``): the reference's
+  unit is the stage stack of one objective (sttopt/compliance.py:228-242, one batched
+  solve over the stage rows).  Rank 0 solves the heat time field and broadcasts tPhys
+  (one NCCL broadcast of ``nel`` doubles); every rank solves its share of the stages and
+  their adjoints; rank 0 also runs the heat adjoint; one all-reduce (sum) of the
+  gradient and the stage compliances combines them.  Every rank takes the same two
+  collectives in the same order.  Peers' data only arrives through these collectives,
+  into local buffers.
 """
 
 from __future__ import annotations
@@ -107,5 +116,62 @@ def gather(indices: Sequence[int], values: Sequence[Tensor], n: int, group=None)
     return out
 
 
+def stage_partition(n_stage: int, world: int, heat_cost: float = 1.0) -> list[list[int]]:
+    """The stages of each rank when one objective is split: stages have equal cost (one
+    grid, one row each); rank 0 starts loaded with ``heat_cost`` stage-equivalents (the
+    heat solve and its adjoint), and each stage goes to the least loaded rank (ties to the
+    lower rank).  Deterministic; each list ascending."""
+    if world <= 0:
+        raise ValueError("world must be positive")
+    load = [float(heat_cost)] + [0.0] * (world - 1)
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for s in range(n_stage):
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(s)
+        load[r] += 1.0
+    return parts
+
+
+def objective_and_gradient_split(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, group=None,
+                                 solve: Callable | None = None, heat_cost: float = 1.0, **kw) -> dict:
+    """One space-time objective and its gradient with the stages spread over the ranks of
+    ``group``; every rank returns the whole result (``objective``, ``c_s`` of all stages,
+    ``J_t``, ``tPhys``, ``gradient``) and ``stages``, its own share.
+
+    ``solve(x, w, n_stage=, stages=, tphys=, publish=, **kw)`` computes a rank's share: the
+    given stages' compliances and gradient terms, the heat solve (calling ``publish(tPhys)``
+    as soon as it exists) and the heat adjoint when ``tphys`` is None, else the given time
+    field.  It defaults to ``spacetime.objective_and_gradient_part``."""
+    world, rank = world_and_rank(group)
+    mine = stage_partition(n_stage, world, heat_cost)[rank]
+    if solve is None:
+        from . import spacetime
+
+        solve = spacetime.objective_and_gradient_part
+    if world == 1:
+        part = solve(xPhys, w, n_stage=n_stage, stages=mine, tphys=None, publish=None, **kw)
+        return dict(part, stages=mine)
+    dist = _dist()
+    src = dist.get_global_rank(group, 0) if group is not None else 0
+    if rank == 0:
+        part = solve(xPhys, w, n_stage=n_stage, stages=mine, tphys=None,
+                     publish=lambda t: dist.broadcast(t.reshape(-1).contiguous(), src=src, group=group), **kw)
+    else:
+        tphys = torch.empty(xPhys.numel(), dtype=torch.float64, device=xPhys.device)
+        dist.broadcast(tphys, src=src, group=group)
+        part = solve(xPhys, w, n_stage=n_stage, stages=mine, tphys=tphys.reshape(xPhys.shape), publish=None, **kw)
+    nel = xPhys.numel()
+    buf = torch.zeros(nel + n_stage, dtype=torch.float64, device=xPhys.device)
+    buf[:nel] = part["gradient"].reshape(-1).to(torch.float64)
+    if mine:
+        buf[nel + torch.tensor(mine, device=xPhys.device)] = part["c_s"].to(torch.float64)
+    dist.all_reduce(buf, group=group)
+    c_s = buf[nel:]
+    tPhys = part["tPhys"].reshape(xPhys.shape)
+    J_t = (w.to(torch.float64) * tPhys).sum()
+    return dict(objective=c_s.sum() + J_t, c_s=c_s, J_t=J_t, tPhys=tPhys,
+                gradient=buf[:nel].reshape(xPhys.shape), stages=mine)
+
+
 __all__ = ["unit_cost", "partition", "rank_seed", "world_and_rank", "max_over_ranks",
-           "objective_and_gradient_sharded", "gather"]
+           "objective_and_gradient_sharded", "gather", "stage_partition", "objective_and_gradient_split"]

@@ -22,6 +22,8 @@ form the batched one is compared against).
 
 from __future__ import annotations
 
+from typing import Callable
+
 import torch
 from torch import Tensor
 
@@ -103,6 +105,27 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
                 conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
                 max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched, overlap=overlap)
     return _solve_group(P, [xPhys], [w], [n_stage], info=info, **opts)[0]
+
+
+def objective_and_gradient_part(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, stages: list[int],
+                                tphys: Tensor | None = None, publish: Callable[[Tensor], None] | None = None,
+                                precision: str = "mixed", rtol: float = 1e-8, max_iter: int = 500,
+                                drain_beta: float = 25.0, conduction_penal: float = 3.0, Emin: float = EMIN,
+                                Emax: float = EMAX, penal: float = PENAL,
+                                max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS,
+                                problem: SpaceTimeProblem | None = None, info: dict | None = None) -> dict:
+    """A rank's share of one objective split over ranks (``sharding.objective_and_gradient_split``):
+    the compliances ``c_s`` of ``stages`` (in that order) and their gradient terms, plus,
+    when ``tphys`` is None, the heat solve (``publish(tPhys)`` is called as soon as it
+    exists) and the heat adjoint's gradient term; with ``tphys`` given, neither."""
+    _lib.require_cuda(xPhys, w)
+    nely, nelx = xPhys.shape
+    P = problem if problem is not None and (problem.nelx, problem.nely) == (nelx, nely) else \
+        SpaceTimeProblem(nelx, nely, xPhys.device)
+    return _solve_group(P, [xPhys], [w], [n_stage], precision=precision, rtol=rtol, max_iter=max_iter,
+                        drain_beta=drain_beta, conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
+                        max_coarse_elements=max_coarse_elements, gradient=True, batched=True, info=info,
+                        stage_subset=list(stages), tphys=tphys, publish=publish)[0]
 
 
 def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
@@ -251,15 +274,29 @@ class _HeatAdjoint:
 def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stages: list[int], *,
                  precision: str, rtol: float, max_iter: int, drain_beta: float, conduction_penal: float,
                  Emin: float, Emax: float, penal: float, max_coarse_elements: int, gradient: bool,
-                 batched: bool, info: dict | None, overlap: bool = True) -> list[dict]:
-    """G problems on one grid: batched heat solve, all stage rows in one batched solve."""
+                 batched: bool, info: dict | None, overlap: bool = True,
+                 stage_subset: list[int] | None = None, tphys: Tensor | None = None,
+                 publish: Callable[[Tensor], None] | None = None) -> list[dict]:
+    """G problems on one grid: batched heat solve, all stage rows in one batched solve.
+
+    For one problem (G = 1) a share of its work, as the ranks of a split objective do it:
+    ``stage_subset`` solves only those stages (``c_s`` and the gradient then cover them
+    only); ``tphys`` takes the time field as given (no heat solve, no heat adjoint);
+    ``publish(tPhys)`` is called as soon as the heat solve has produced it."""
     L = _lib.lib()
     st = _lib.stream()
     nelx, nely, nel, nnode = P.nelx, P.nely, P.nel, P.nnode
     dev = P.device
     G = len(xs)
+    if (stage_subset is not None or tphys is not None) and G != 1:
+        raise ValueError("stage_subset and tphys apply to a single problem")
     X = torch.stack([x.detach().to(torch.float64).reshape(-1) for x in xs]).contiguous()  # (G, nel)
     W = torch.stack([w.detach().to(torch.float64).reshape(-1) for w in ws]).contiguous()
+    if tphys is not None:
+        return _stage_work(P, X, W, tphys.detach().to(torch.float64).reshape(1, nel).contiguous(), None, n_stages,
+                           stage_subset, precision=precision, rtol=rtol, max_iter=max_iter, Emin=Emin, Emax=Emax,
+                           penal=penal, max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched,
+                           info=info, conduction_penal=conduction_penal, T=None)
 
     # 1. heat time fields (a row per problem)
     chi = torch.clamp(X ** conduction_penal, min=1e-6).contiguous()
@@ -281,6 +318,8 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
     part = X >= X.max(dim=1, keepdim=True).values / 2
     scale = torch.where(part, t_e, torch.full_like(t_e, -torch.inf)).max(dim=1, keepdim=True).values
     tPhys = (t_e / scale).contiguous()
+    if publish is not None:
+        publish(tPhys[0])
 
     # 5b (overlapped). The heat adjoints need only T, tPhys's scale and w, not the stage
     # solves: they run from a host thread on a side stream while this thread launches the
@@ -292,83 +331,194 @@ def _solve_group(P: SpaceTimeProblem, xs: list[Tensor], ws: list[Tensor], n_stag
                                 threaded=overlap)
 
     try:
-        # 2.-3. stage rows of every problem, then the batched stage solves
-        offs = [0]
-        for n in n_stages:
-            offs.append(offs[-1] + n)
-        S = offs[-1]
-        members = []
-        rho = torch.empty(S, nel, dtype=torch.float64, device=dev)
-        F = torch.empty(S, 2 * nnode, dtype=torch.float64, device=dev)
-        for g, n in enumerate(n_stages):
-            m = torch.empty(n, nel, dtype=torch.uint8, device=dev)
-            _lib.check(L.stt_stage_membership(nel, n, _lib.ptr(tPhys[g]), _lib.ptr(m), st))
-            _lib.check(L.stt_stage_rows(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(m), Emin, Emax, penal,
-                                        _lib.ptr(P.fixed2), _lib.ptr(rho[offs[g]]), _lib.ptr(F[offs[g]]), st))
-            members.append(m)
-        if batched:
-            sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
-                                          max_coarse_elements=max_coarse_elements, precision=precision, check=False)
-            U = _pcg(sl, F, None, rtol, max_iter, "stage_n_iter", info)
-            stage_levels = [sl]
-        else:
-            Us, stage_levels = [], []
-            for s in range(S):
-                sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
-                                              max_coarse_elements=max_coarse_elements, precision=precision, check=False)
-                Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
-                stage_levels.append(sl)
-            U = torch.stack(Us)
-        ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
-        c_s = (rho * ce).sum(-1)
-        J_t = (W * tPhys).sum(-1)
-        outs = []
-        for g in range(G):
-            a, b = offs[g], offs[g + 1]
-            outs.append(dict(objective=c_s[a:b].sum() + J_t[g], c_s=c_s[a:b], J_t=J_t[g],
-                             tPhys=tPhys[g].reshape(nely, nelx), U=U[a:b], T=T[g], member=members[g]))
-        if not gradient:
-            return outs
-
-        # 5a. stage adjoints: dL/dU = 2 K U (one apply with 2 KE); warm start alpha U
-        # (exact for compliance)
-        gK = torch.empty_like(U)
-        _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
-                                  2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
-                                  _lib.STT_PROJECT_OUT, P.ke2, st))
-        # U . gK and U . F in one pass over U
-        d2 = torch.empty(S, 2, dtype=torch.float64, device=dev)
-        _lib.check(L.stt_vec_dots(S, 2 * nnode, _lib.ptr(U), _lib.ptr(gK), _lib.ptr(U), _lib.ptr(F), None, None,
-                                  2 * nnode, _lib.ptr(d2), st))
-        a_ = torch_fem.safe_div(d2[:, 0], d2[:, 1])
-        x0 = (a_[:, None] * U).contiguous()
-        if batched:
-            lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
-        else:
-            lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
-                               for s in range(S)])
-        lam = lam.contiguous()
-        gd = torch_fem.element_terms(U, P.edof, P.KE, lam=lam)["gdens"]
-        grads = torch.zeros(G, nel, dtype=torch.float64, device=dev)
-        for g, n in enumerate(n_stages):
-            a = offs[g]
-            _lib.check(L.stt_stage_gradient(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(members[g]), _lib.ptr(ce[a]),
-                                            _lib.ptr(gd[a]), _lib.ptr(lam[a]), Emin, Emax, penal,
-                                            _lib.ptr(grads[g]), st))
-
-        # 5b. the heat adjoints' share of the gradient
-        g_chi = heat_adj.result()
-        q = conduction_penal
-        dpen = torch.where(X ** q >= 1e-6, q * X ** (q - 1), torch.zeros_like(X))
-        grads = grads + g_chi * dpen
-        for g in range(G):
-            outs[g]["gradient"] = grads[g].reshape(nely, nelx)
-            outs[g]["lam"] = lam[offs[g]:offs[g + 1]]
-        return outs
+        return _stage_work(P, X, W, tPhys, heat_adj, n_stages, stage_subset, precision=precision, rtol=rtol,
+                           max_iter=max_iter, Emin=Emin, Emax=Emax, penal=penal,
+                           max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched, info=info,
+                           conduction_penal=conduction_penal, T=T)
     except BaseException:
         if heat_adj is not None:
             heat_adj.abandon()
         raise
+
+
+def _heat_share(heat_adj, X: Tensor, conduction_penal: float, grads: Tensor) -> Tensor:
+    """``grads`` plus the heat adjoints' share of the gradient (none without a heat adjoint:
+    a split objective's ranks that were given the time field)."""
+    if heat_adj is None:
+        return grads
+    g_chi = heat_adj.result()
+    q = conduction_penal
+    dpen = torch.where(X ** q >= 1e-6, q * X ** (q - 1), torch.zeros_like(X))
+    return grads + g_chi * dpen
+
+
+def _stage_work(P: SpaceTimeProblem, X: Tensor, W: Tensor, tPhys: Tensor, heat_adj, n_stages: list[int],
+                stage_subset: list[int] | None, *, precision: str, rtol: float, max_iter: int, Emin: float,
+                Emax: float, penal: float, max_coarse_elements: int, gradient: bool, batched: bool,
+                info: dict | None, conduction_penal: float, T: Tensor | None) -> list[dict]:
+    """Stage membership, the batched stage solves, their adjoints and the gradient (plus
+    the heat adjoints' share when ``heat_adj`` is given); ``stage_subset`` (one problem)
+    restricts the stages solved."""
+    # 2.-3. stage rows of every problem, then the batched stage solves
+    L = _lib.lib()
+    st = _lib.stream()
+    nelx, nely, nel, nnode = P.nelx, P.nely, P.nel, P.nnode
+    dev = P.device
+    G = X.shape[0]
+    counts = list(n_stages) if stage_subset is None else [len(stage_subset)]
+    offs = [0]
+    for n in counts:
+        offs.append(offs[-1] + n)
+    S = offs[-1]
+    members = []
+    rho = torch.empty(S, nel, dtype=torch.float64, device=dev)
+    F = torch.empty(S, 2 * nnode, dtype=torch.float64, device=dev)
+    for g, n in enumerate(n_stages):
+        m = torch.empty(n, nel, dtype=torch.uint8, device=dev)
+        _lib.check(L.stt_stage_membership(nel, n, _lib.ptr(tPhys[g]), _lib.ptr(m), st))
+        if stage_subset is not None:
+            m = m[list(stage_subset)].contiguous()
+        if m.shape[0]:
+            _lib.check(L.stt_stage_rows(nelx, nely, m.shape[0], _lib.ptr(X[g]), _lib.ptr(m), Emin, Emax, penal,
+                                        _lib.ptr(P.fixed2), _lib.ptr(rho[offs[g]]), _lib.ptr(F[offs[g]]), st))
+        members.append(m)
+    if S == 0:  # a share with no stage rows (more ranks than stages)
+        J_t = (W * tPhys).sum(-1)
+        outs = [dict(objective=J_t[g], c_s=rho.new_zeros(0), J_t=J_t[g], tPhys=tPhys[g].reshape(nely, nelx), U=F,
+                     T=None if T is None else T[g], member=members[g]) for g in range(G)]
+        if gradient:
+            grads = _heat_share(heat_adj, X, conduction_penal, torch.zeros(G, nel, dtype=torch.float64, device=dev))
+            for g in range(G):
+                outs[g]["gradient"] = grads[g].reshape(nely, nelx)
+                outs[g]["lam"] = F
+        return outs
+    if batched:
+        sl = torch_mg.build_hierarchy(rho, P.edof, P.KE, P.mask, nelx, nely,
+                                      max_coarse_elements=max_coarse_elements, precision=precision, check=False)
+        U = _pcg(sl, F, None, rtol, max_iter, "stage_n_iter", info)
+        stage_levels = [sl]
+    else:
+        Us, stage_levels = [], []
+        for s in range(S):
+            sl = torch_mg.build_hierarchy(rho[s], P.edof, P.KE, P.mask, nelx, nely,
+                                          max_coarse_elements=max_coarse_elements, precision=precision, check=False)
+            Us.append(_pcg(sl, F[s], None, rtol, max_iter, f"stage{s}_n_iter", info))
+            stage_levels.append(sl)
+        U = torch.stack(Us)
+    ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
+    c_s = (rho * ce).sum(-1)
+    J_t = (W * tPhys).sum(-1)
+    outs = []
+    for g in range(G):
+        a, b = offs[g], offs[g + 1]
+        outs.append(dict(objective=c_s[a:b].sum() + J_t[g], c_s=c_s[a:b], J_t=J_t[g],
+                         tPhys=tPhys[g].reshape(nely, nelx), U=U[a:b], T=None if T is None else T[g],
+                         member=members[g]))
+    if not gradient:
+        return outs
+
+    # 5a. stage adjoints: dL/dU = 2 K U (one apply with 2 KE); warm start alpha U
+    # (exact for compliance)
+    gK = torch.empty_like(U)
+    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
+                              2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
+                              _lib.STT_PROJECT_OUT, P.ke2, st))
+    # U . gK and U . F in one pass over U
+    d2 = torch.empty(S, 2, dtype=torch.float64, device=dev)
+    _lib.check(L.stt_vec_dots(S, 2 * nnode, _lib.ptr(U), _lib.ptr(gK), _lib.ptr(U), _lib.ptr(F), None, None,
+                              2 * nnode, _lib.ptr(d2), st))
+    a_ = torch_fem.safe_div(d2[:, 0], d2[:, 1])
+    x0 = (a_[:, None] * U).contiguous()
+    if batched:
+        lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
+    else:
+        lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
+                           for s in range(S)])
+    lam = lam.contiguous()
+    gd = torch_fem.element_terms(U, P.edof, P.KE, lam=lam)["gdens"]
+    grads = torch.zeros(G, nel, dtype=torch.float64, device=dev)
+    for g, n in enumerate(counts):
+        a = offs[g]
+        _lib.check(L.stt_stage_gradient(nelx, nely, n, _lib.ptr(X[g]), _lib.ptr(members[g]), _lib.ptr(ce[a]),
+                                        _lib.ptr(gd[a]), _lib.ptr(lam[a]), Emin, Emax, penal,
+                                        _lib.ptr(grads[g]), st))
+
+    # 5b. the heat adjoints' share of the gradient
+    grads = _heat_share(heat_adj, X, conduction_penal, grads)
+    for g in range(G):
+        outs[g]["gradient"] = grads[g].reshape(nely, nelx)
+        outs[g]["lam"] = lam[offs[g]:offs[g + 1]]
+    return outs
+
+
+class _HeatConfig:
+    """The fields of ``HeatRunConfig`` that ``heat_time_field`` reads (sttopt/run_config.py:495)."""
+
+    def __init__(self, drain_beta: float, rtol: float):
+        self.chi_contrast = 1000.0  # mu = 1/2 makes chi's contrast factor 1
+        self.drain_beta = drain_beta
+        self.time_map = "one_minus"
+        self.heat_cg_rtol = rtol
+
+
+class DropInChain:
+    """The space-time objective composed only of the reference-signature functions, as a
+    caller of the reference would write it (sttopt/stto_heat.py:192-327 with the hard stage
+    threshold): ``virtual_heat.heat_time_field`` -> ``compliance.batched_whole_and_gravity_compliance``
+    (``mask_fn=hard_time_mask``, the whole-structure row unloaded) -> ``sum_s c_s + sum(w tPhys)``
+    -> ``sensitivity.jacobian_rows``.  The grid-level set-up (meshes, element matrices, the
+    build-plate clamp, the gravity stencil) is built once.  ``precision="mixed"`` routes
+    the stage solve through the ``_solve_fe_batched`` patch point with the FP32 V-cycle
+    (and the heat solve likewise); ``"fp64"`` is the reference's arithmetic."""
+
+    def __init__(self, nelx: int, nely: int, device, *, n_stage: int = 16, drain_beta: float = 25.0,
+                 rtol: float = 1e-8, conduction_penal: float = 3.0):
+        from . import gravity, load_cases, virtual_heat
+
+        self.nelx, self.nely, self.n_stage = nelx, nely, n_stage
+        self.mesh = virtual_heat.ScalarMesh.build(nelx, nely, "bottom_edge", device, torch.float64)
+        self.cfg = _HeatConfig(drain_beta, rtol)
+        self.rtol = rtol
+        self.conduction_penal = conduction_penal
+        self.KE = torch.tensor(fem.plane_stress_KE(NU), dtype=torch.float64, device=device)
+        self.edof = torch_mg.element_dof_map_tensor(nelx, nely, device, 2)
+        F, free = load_cases.build_plate_clamp(nelx, nely)
+        self.F = torch.as_tensor(F, device=device)
+        self.free = torch.as_tensor(free, device=device)
+        self.ndof = F.size
+        self.C = gravity.gravity_load_matrix(nelx, nely)
+        self.mu = torch.full((nely, nelx), 0.5, dtype=torch.float64, device=device)
+        self.times = [s / n_stage for s in range(1, n_stage + 1)]
+
+    def __call__(self, xPhys: Tensor, w: Tensor, precision: str = "fp64") -> dict:
+        from . import compliance, sensitivity, torch_solve, virtual_heat
+
+        x = xPhys.detach().to(torch.float64).requires_grad_(True)
+        prec = None if precision == "fp64" else precision
+        sol = virtual_heat.heat_time_field(self.cfg, self.mesh, x, self.mu, conduction_penal=self.conduction_penal,
+                                           precision=prec)
+        patched = None
+        if prec is not None:
+            rtol = self.rtol
+
+            def solve_fe_batched(KE, density, edofMat, mask, nelx, nely, F, *, x0=None):
+                return torch_solve.femsolve(density, F, edofMat, KE, mask, nelx, nely, x0=x0, rtol=rtol,
+                                            precision=prec)
+
+            patched = compliance._solve_fe_batched
+            compliance._solve_fe_batched = solve_fe_batched
+        try:
+            c, stages, U = compliance.batched_whole_and_gravity_compliance(
+                x, sol.tPhys, self.KE, self.edof, EMIN, EMAX, PENAL, self.free, self.F, self.ndof, self.C, 1.0,
+                self.times, mask_fn=compliance.hard_time_mask)
+        finally:
+            if patched is not None:
+                compliance._solve_fe_batched = patched
+        c_s = torch.stack(stages)
+        L = c_s.sum() + torch.sum(w * sol.tPhys)
+        (g,) = sensitivity.jacobian_rows(L[None], [x])
+        return dict(objective=L.detach(), c_s=c_s.detach(), tPhys=sol.tPhys.detach(), U=U.detach()[1:],
+                    gradient=g.reshape(self.nely, self.nelx))
 
 
 class SpaceTimeObjective(torch.autograd.Function):

@@ -84,3 +84,26 @@ def test_gradient_matches_central_differences(case):
     assert np.all(err <= 2e-3 * np.abs(an) + 5e-5 * scale), (err.max(), scale)
     big = np.abs(an) > 1e-2 * scale
     assert big.sum() >= 8 and np.median(err[big] / np.abs(an[big])) < 1e-3
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 5e-9), ("mixed", 1e-6)])
+def test_dropin_chain_matches_the_reference_and_the_fused_path(case, precision, tol):
+    """The objective composed only of the reference-signature functions
+    (heat_time_field -> batched_whole_and_gravity_compliance(mask_fn=hard_time_mask) ->
+    jacobian_rows, ``spacetime.DropInChain``) against the reference's field and the fused
+    ``objective_and_gradient``: the two device paths to 1e-10 in FP64."""
+    from sttopt_b200 import spacetime
+
+    g, x, w, member = case
+    dev = torch.device("cuda")
+    chain = spacetime.DropInChain(NELX, NELY, dev, n_stage=NSTAGE)
+    xt, wt = torch.tensor(x, device=dev), torch.tensor(w, device=dev)
+    out = chain(xt, wt, precision=precision)
+    assert abs(float(out["objective"]) - float(g["L"])) <= tol * abs(float(g["L"]))
+    assert rel_err(out["c_s"].cpu(), g["c_s"]) < tol
+    assert rel_err(out["gradient"].cpu(), g["grad"]) < tol
+    assert rel_err(out["tPhys"].cpu(), g["tPhys"]) < tol
+    if precision == "fp64":
+        fused = spacetime.objective_and_gradient(xt, wt, n_stage=NSTAGE, precision="fp64")
+        assert rel_err(out["c_s"].cpu(), fused["c_s"].cpu()) < 1e-10
+        assert rel_err(out["gradient"].cpu(), fused["gradient"].cpu()) < 1e-10

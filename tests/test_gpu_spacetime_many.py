@@ -66,3 +66,31 @@ def test_many_sequential_matches_concurrent(pkg):
     for p, q in zip(a, b):
         assert torch.equal(p["gradient"], q["gradient"])
         assert torch.equal(p["c_s"], q["c_s"])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-6)])
+def test_split_objective_shares_add_up_to_the_whole(pkg, precision, tol):
+    """The shares of a split objective (``objective_and_gradient_part``), computed one
+    after another on one GPU as three ranks would: rank 0 solves the heat field (handing
+    tPhys to the others through ``publish``), every share solves its stages, and the sum
+    of the gradient terms and the stage compliances equals the whole objective."""
+    from sttopt_b200 import sharding, spacetime, synthetic
+
+    nelx, nely, n_stage = 128, 64, 16
+    x = synthetic.smoothed_density(nelx, nely, 21)
+    w = synthetic.time_weights(nelx, nely, 21)
+    whole = spacetime.objective_and_gradient(x, w, n_stage=n_stage, precision=precision)
+    parts = sharding.stage_partition(n_stage, 3)
+    got = {}
+    p0 = spacetime.objective_and_gradient_part(x, w, n_stage=n_stage, stages=parts[0], precision=precision,
+                                               publish=lambda t: got.setdefault("tPhys", t.clone()))
+    shares = [p0] + [spacetime.objective_and_gradient_part(x, w, n_stage=n_stage, stages=p, precision=precision,
+                                                           tphys=got["tPhys"].reshape(nely, nelx))
+                     for p in parts[1:]]
+    grad = sum(s["gradient"] for s in shares)
+    c_s = torch.zeros(n_stage, dtype=torch.float64, device=x.device)
+    for p, s in zip(parts, shares):
+        c_s[torch.tensor(p, device=x.device)] = s["c_s"]
+    assert torch.equal(got["tPhys"].reshape(nely, nelx), whole["tPhys"])
+    assert rel_err(c_s.cpu(), whole["c_s"].cpu()) < tol
+    assert rel_err(grad.cpu(), whole["gradient"].cpu()) < tol
