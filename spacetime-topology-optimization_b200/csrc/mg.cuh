@@ -321,14 +321,66 @@ struct FrontRow {
   uint8_t fl;
 };
 
-// Per-row values a stage reads one or two rows after the front.
+// Per-row values a stage reads one or two rows after the front: the right-hand side,
+// w = omega / diag and the free mask mf (1 on free dofs, 0 on fixed and off-grid ones;
+// the diagonal is taken as 1 there, so w stays finite).
 template <int D, typename T, bool RD>
 struct DelayRow {
-  T b[D], dg[D];
+  T b[D], w[D], mf[D];
   T rd[RD ? D : 1];
   T rho;
-  uint8_t fl;
 };
+
+// The chained level-0 stages' per-node results from A x (unprojected, without the
+// reaction term):
+//   SW_FIRST: mf (w b);   SW_SWEEP: mf (x + w (b - A x));   SW_RESID: mf (b - A x).
+// Multiplying by the free mask makes every result the projected one, whatever the input
+// holds on fixed dofs (the reference projects the cycle's input and every smoothing
+// result, torch_mg.py:440-476).  The plane-stress FP32 form pairs the two components.
+template <int D, typename T, int MODE, bool RDT>
+STT_DEV void l0_chain_result(T (&Ax)[D], const T (&w)[D], const T (&mf)[D], const T (&xo)[D], const T (&bv)[D],
+                             const T (&rd)[D], T (&res)[D]) {
+  if constexpr (D == 2 && sizeof(T) == 4 && !RDT) {
+    const float2 W = make_float2(w[0], w[1]), M = make_float2(mf[0], mf[1]), B = make_float2(bv[0], bv[1]);
+    float2 R;
+    if constexpr (MODE == SW_FIRST) {
+      R = __fmul2_rn(__fmul2_rn(W, B), M);
+    } else {
+      const float2 Bm = __fadd2_rn(B, make_float2(-Ax[0], -Ax[1]));
+      if constexpr (MODE == SW_RESID) R = __fmul2_rn(Bm, M);
+      else R = __fmul2_rn(__ffma2_rn(W, Bm, make_float2(xo[0], xo[1])), M);
+    }
+    res[0] = R.x;
+    res[1] = R.y;
+  } else {
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      T a = Ax[i];
+      if constexpr (RDT && MODE != SW_FIRST) a = fma(rd[i], xo[i], a);
+      if constexpr (MODE == SW_FIRST) res[i] = (w[i] * bv[i]) * mf[i];
+      else if constexpr (MODE == SW_RESID) res[i] = (bv[i] - a) * mf[i];
+      else res[i] = fma(w[i], bv[i] - a, xo[i]) * mf[i];
+    }
+  }
+}
+
+// The front row's DelayRow from its loads: mf from the fixed flags (the loaders mark
+// off-grid positions all-fixed), w = omega / diag with diag = kd * (the densities
+// around the node) (+ the reaction), 1 where mf is 0.
+template <int D, typename T, bool RD>
+STT_DEV void l0_delay_row(const FrontRow<D, T, RD>& F, T dsum, const MQ<T>& q, T omega, DelayRow<D, T, RD>& cur) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const bool free = !((F.fl >> d) & 1);
+    cur.mf[d] = free ? T(1) : T(0);
+    T dg = (d == 0 ? q.kd0 : q.kd1) * dsum;
+    if constexpr (RD) dg += F.rd[d];
+    cur.w[d] = sweep_div(omega, free ? dg : T(1));
+    cur.b[d] = F.b[d];
+    if constexpr (RD) cur.rd[d] = F.rd[d];
+  }
+  cur.rho = F.rho;
+}
 
 constexpr int kPreCols = 27;  // output columns per warp strip of l0_presmooth_kernel
 
@@ -372,7 +424,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
 #pragma unroll
       for (int d = 0; d < D; ++d) F.rd[d] = T(0);
     }
-    F.fl = 0;
+    F.fl = 0xFF;  // off the grid: every dof fixed (free mask 0)
     F.rho = (ecol_ok && f >= 0 && f < nely) ? __ldg(rh + (size_t)f * nelx + c) : T(0);
     if (!col_ok || f < 0 || f >= nny) return;
     const long long node = (long long)f * nnx + c;
@@ -398,37 +450,24 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
       const int f = fb + k;
       const FrontRow<D, T, RD> F = qf[k];
       load_front(f + AHEAD, qf[k]);
-      // diagonal of K at row f (kd times the densities around the node)
+      // the row's free mask and w = omega / diag (diag: kd times the densities around the node)
       DelayRow<D, T, RD> cur;
       {
         const T rs = F.rho + rho_prev;
         const T dsum = rs + __shfl_up_sync(0xffffffffu, rs, 1);
-        cur.dg[0] = q.kd0 * dsum;
-        if constexpr (D == 2) cur.dg[1] = q.kd1 * dsum;
+        l0_delay_row<D, T, RD>(F, dsum, q, omega, cur);
       }
       rho_prev = F.rho;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        cur.b[d] = F.b[d];
-        if constexpr (RD) cur.rd[d] = F.rd[d];
-      }
-      cur.rho = F.rho;
-      cur.fl = F.fl;
       // x1 at row f (the first sweep from zero)
       T x1[D];
       {
-        T zero[D], Ax[D], dg[D], rdv[D];
+        T zero[D], rdv[D];
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-          zero[d] = Ax[d] = T(0);
-          dg[d] = cur.dg[d];
-          rdv[d] = RD ? F.rd[d] : T(0);
+          zero[d] = T(0);
+          rdv[d] = RD ? cur.rd[d] : T(0);
         }
-        l0_result<D, T, SW_FIRST, RD>(Ax, dg, zero, F.b, F.fl, rdv, omega, x1);
-        if (!(col_ok && f >= 0 && f < nny)) {
-#pragma unroll
-          for (int d = 0; d < D; ++d) x1[d] = T(0);
-        }
+        l0_chain_result<D, T, SW_FIRST, RD>(zero, cur.w, cur.mf, zero, cur.b, rdv, x1);
       }
       // stage A: element row f - 1 -> second sweep at node row f - 1
       T KA[D], xa[D], xo_a[D];
@@ -436,17 +475,10 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
       for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
       A.step(q, x1, d1.rho, KA);
       {
-        T rd1[D], dg[D];
+        T rd1[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          rd1[d] = RD ? d1.rd[d] : T(0);
-          dg[d] = d1.dg[d];
-        }
-        l0_result<D, T, SW_SWEEP, RD>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
-        if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
-#pragma unroll
-          for (int d = 0; d < D; ++d) xa[d] = T(0);
-        }
+        for (int d = 0; d < D; ++d) rd1[d] = RD ? d1.rd[d] : T(0);
+        l0_chain_result<D, T, SW_SWEEP, RD>(KA, d1.w, d1.mf, xo_a, d1.b, rd1, xa);
       }
       // stage B: element row f - 2 -> residual at node row f - 2
       T KB[D], rb[D], xo_b[D];
@@ -454,13 +486,10 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
       for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
       B.step(q, xa, d2.rho, KB);
       {
-        T rd2[D], dg[D];
+        T rd2[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          rd2[d] = RD ? d2.rd[d] : T(0);
-          dg[d] = d2.dg[d];
-        }
-        l0_result<D, T, SW_RESID, RD>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, rb);
+        for (int d = 0; d < D; ++d) rd2[d] = RD ? d2.rd[d] : T(0);
+        l0_chain_result<D, T, SW_RESID, RD>(KB, d2.w, d2.mf, xo_b, d2.b, rd2, rb);
       }
       if (out_lane) {
         if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);
@@ -522,7 +551,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
 #pragma unroll
       for (int d = 0; d < D; ++d) Q.F.rd[d] = T(0);
     }
-    Q.F.fl = 0;
+    Q.F.fl = 0xFF;  // off the grid: every dof fixed (free mask 0)
     Q.F.rho = (ecol_ok && f >= 0 && f < nely) ? __ldg(rh + (size_t)f * nelx + c) : T(0);
     if (!col_ok || f < 0 || f >= nny) return;
     const long long node = (long long)f * nnx + c;
@@ -553,34 +582,19 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
       {
         const T rs = Q.F.rho + rho_prev;
         const T dsum = rs + __shfl_up_sync(0xffffffffu, rs, 1);
-        cur.dg[0] = q.kd0 * dsum;
-        if constexpr (D == 2) cur.dg[1] = q.kd1 * dsum;
+        l0_delay_row<D, T, RD>(Q.F, dsum, q, omega, cur);
       }
       rho_prev = Q.F.rho;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        cur.b[d] = Q.F.b[d];
-        if constexpr (RD) cur.rd[d] = Q.F.rd[d];
-      }
-      cur.rho = Q.F.rho;
-      cur.fl = Q.F.fl;
       // stage A: element row f - 1 -> first sweep at node row f - 1
       T KA[D], xa[D], xo_a[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
       A.step(q, Q.x, d1.rho, KA);
       {
-        T rd1[D], dg[D];
+        T rd1[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          rd1[d] = RD ? d1.rd[d] : T(0);
-          dg[d] = d1.dg[d];
-        }
-        l0_result<D, T, SW_SWEEP, RD>(KA, dg, xo_a, d1.b, d1.fl, rd1, omega, xa);
-        if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) {
-#pragma unroll
-          for (int d = 0; d < D; ++d) xa[d] = T(0);
-        }
+        for (int d = 0; d < D; ++d) rd1[d] = RD ? d1.rd[d] : T(0);
+        l0_chain_result<D, T, SW_SWEEP, RD>(KA, d1.w, d1.mf, xo_a, d1.b, rd1, xa);
       }
       // stage B: element row f - 2 -> second sweep at node row f - 2
       T KB[D], xb[D], xo_b[D];
@@ -588,13 +602,10 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
       for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
       B.step(q, xa, d2.rho, KB);
       {
-        T rd2[D], dg[D];
+        T rd2[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          rd2[d] = RD ? d2.rd[d] : T(0);
-          dg[d] = d2.dg[d];
-        }
-        l0_result<D, T, SW_SWEEP, RD>(KB, dg, xo_b, d2.b, d2.fl, rd2, omega, xb);
+        for (int d = 0; d < D; ++d) rd2[d] = RD ? d2.rd[d] : T(0);
+        l0_chain_result<D, T, SW_SWEEP, RD>(KB, d2.w, d2.mf, xo_b, d2.b, rd2, xb);
       }
       if (out_lane && f - 2 >= r0 && f - 2 < r1) store_node<D, T>(os, (long long)(f - 2) * nnx + c, xb);
       d2 = d1;
