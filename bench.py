@@ -233,9 +233,10 @@ def run_pcg_small(dev, rows=4):
     return {"rows": rows, "n_iter": n, "ms": a.elapsed_time(b)}
 
 
-def run_uneven(dev, steps=2, warmup=1):
+def run_uneven(dev, steps=2, warmup=1, memory_budget=None):
     """Stage solves per second over the 64 uneven problems (objective + full gradient of
-    each), grouped per grid size into batched solves on concurrent streams."""
+    each), grouped per grid size into batched solves on concurrent streams; with
+    ``memory_budget`` (bytes) the groups run in waves that fit it."""
     import torch
 
     from sttopt_b200 import spacetime
@@ -243,13 +244,16 @@ def run_uneven(dev, steps=2, warmup=1):
     xs, ws, ns = uneven_workload(dev)
     cache: dict = {}
     info: dict = {}
+    torch.cuda.empty_cache()
+    torch.cuda.reset_peak_memory_stats(dev)
+    kw = dict(problems=cache, info=info, memory_budget=memory_budget)
     for _ in range(warmup):
-        spacetime.objective_and_gradient_many(xs, ws, ns, problems=cache, info=info)
+        spacetime.objective_and_gradient_many(xs, ws, ns, **kw)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
     for _ in range(steps):
-        spacetime.objective_and_gradient_many(xs, ws, ns, problems=cache, info=info)
+        spacetime.objective_and_gradient_many(xs, ws, ns, **kw)
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / steps
@@ -266,8 +270,10 @@ def run_uneven(dev, steps=2, warmup=1):
             "problems": len(xs), "stage_rows": sum(ns), "groups": counts,
             "peak_device_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1),
             "iterations": {f"{k[0]}x{k[1]}": v for k, v in info.items()},
+            "memory_budget_gib": None if memory_budget is None else round(memory_budget / 2**30, 1),
             "batching": "one batched device PCG per grid size (heat, stages, adjoints), the size groups "
-                        "on concurrent CUDA streams"}
+                        "on concurrent CUDA streams" + ("" if memory_budget is None else
+                                                        ", in waves whose estimated memory fits the budget")}
 
 
 # ---- clocks -----------------------------------------------------------------------
@@ -487,6 +493,7 @@ def main():
             del ref
             torch.cuda.empty_cache()
             extra["batched_uneven"] = run_uneven(dev)
+            extra["batched_uneven_budget"] = run_uneven(dev, memory_budget=40 << 30)
         if world == 1 and not args.no_cpu_baseline:
             s = cpu_full_evaluations(1, args.cpu_budget)
             extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "port",

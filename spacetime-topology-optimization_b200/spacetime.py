@@ -94,9 +94,18 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
                            penal: float = PENAL, max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS,
                            gradient: bool = True, batched: bool = True,
                            problem: SpaceTimeProblem | None = None, info: dict | None = None,
-                           overlap: bool = True) -> dict:
+                           overlap: bool = True, filter=None, beta: float | None = None,
+                           eta: float = 0.5) -> dict:
     """Objective, stage compliances, ``tPhys`` and (optionally) ``d objective / d xPhys``.
-    ``overlap`` runs the heat adjoint on a side stream concurrently with the stage work."""
+    ``overlap`` runs the heat adjoint on a side stream concurrently with the stage work.
+
+    With ``filter`` (``filters.density_filter``'s ``ConeFilter``) the input is the design
+    variable x and the physical density is ``xPhys = P(H x / Hs)`` (the Heaviside projection
+    with ``beta``, ``eta``; the filter alone when ``beta`` is None), as sttopt/stto_heat.py:177-189
+    forms it: one stencil pass gives ``xTilde`` and ``xPhys``, and the gradient is taken
+    back to x by one pass of the filter's transpose fused with the projection's derivative,
+    ``H (g P'(xTilde) / Hs)``.  The result then also holds ``xPhys``, ``xTilde`` and
+    ``gradient_xPhys``."""
     _lib.require_cuda(xPhys, w)
     nely, nelx = xPhys.shape
     P = problem if problem is not None and (problem.nelx, problem.nely) == (nelx, nely) else \
@@ -104,7 +113,19 @@ def objective_and_gradient(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, preci
     opts = dict(precision=precision, rtol=rtol, max_iter=max_iter, drain_beta=drain_beta,
                 conduction_penal=conduction_penal, Emin=Emin, Emax=Emax, penal=penal,
                 max_coarse_elements=max_coarse_elements, gradient=gradient, batched=batched, overlap=overlap)
-    return _solve_group(P, [xPhys], [w], [n_stage], info=info, **opts)[0]
+    if filter is None:
+        return _solve_group(P, [xPhys], [w], [n_stage], info=info, **opts)[0]
+    from . import filters
+
+    b = 0.0 if beta is None else float(beta)
+    xTilde, xp = filters._filter(xPhys, filter, b, float(eta))
+    xp = xTilde if xp is None else xp
+    out = _solve_group(P, [xp], [w], [n_stage], info=info, **opts)[0]
+    out["xPhys"], out["xTilde"] = xp, xTilde
+    if gradient:
+        out["gradient_xPhys"] = out["gradient"]
+        out["gradient"] = filters._adjoint(out["gradient"], filter, xTilde if b > 0 else None, b, float(eta))
+    return out
 
 
 def objective_and_gradient_part(xPhys: Tensor, w: Tensor, *, n_stage: int = 16, stages: list[int],
@@ -134,7 +155,8 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
                                 Emin: float = EMIN, Emax: float = EMAX, penal: float = PENAL,
                                 max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS,
                                 gradient: bool = True, concurrent: bool = True,
-                                problems: dict | None = None, info: dict | None = None) -> list[dict]:
+                                problems: dict | None = None, info: dict | None = None,
+                                memory_budget: int | None = None) -> list[dict]:
     """Many independent space-time problems of uneven grid sizes and stage counts.
 
     Problems of one grid size form one group: their heat solves are one batched device
@@ -144,6 +166,12 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
     GPU overlaps them.  Results come back in input order, each as
     ``objective_and_gradient`` returns it.  ``problems`` caches ``SpaceTimeProblem`` per
     shape; ``info`` receives per-group iteration counts under ``(nelx, nely)``.
+
+    ``memory_budget`` (bytes) bounds what the solves hold at once: each group's device
+    memory is estimated (``group_bytes``: its hierarchies, solve workspaces and the
+    stage rows' vectors), groups over the budget are split into slices of their problems,
+    and the slices run in waves whose estimates fit the budget (at most one slice per grid
+    size in a wave), one wave after another; without it every group runs at once.
     """
     if not (len(xs) == len(ws) == len(n_stages)):
         raise ValueError("xs, ws and n_stages must have the same length")
@@ -160,6 +188,10 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
         if (nelx, nely) not in cache:
             cache[(nelx, nely)] = SpaceTimeProblem(nelx, nely, dev)
     results: list = [None] * len(xs)
+    if memory_budget is None:
+        waves = [list(groups.items())]
+    else:
+        waves = budget_waves(groups, n_stages, int(memory_budget), precision, max_coarse_elements)
 
     def run(shape, idx):
         nely, nelx = shape
@@ -167,21 +199,90 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
         out = _solve_group(cache[(nelx, nely)], [xs[k] for k in idx], [ws[k] for k in idx],
                            [n_stages[k] for k in idx], info=sub, **opts)
         if info is not None:
-            info[(nelx, nely)] = sub
+            info.setdefault((nelx, nely), {}).update(sub)
         for k, o in zip(idx, out):
             results[k] = o
 
-    if not concurrent or len(groups) == 1:
-        for shape, idx in groups.items():
+    for wave in waves:
+        _run_wave(wave, run, cache, dev, concurrent)
+    if concurrent and any(len(w) > 1 for w in waves):
+        main = torch.cuda.current_stream(_device_index(dev))
+        for o in results:  # made on side streams, used on the caller's
+            for v in o.values():
+                if isinstance(v, torch.Tensor) and v.is_cuda:
+                    v.record_stream(main)
+    return results
+
+
+def group_bytes(nelx: int, nely: int, n_problems: int, stage_rows: int, precision: str,
+                max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS) -> int:
+    """Estimated device bytes of one grid size's batched solves: the stage and heat
+    hierarchies (the library's workspace sizes), the solve workspaces (FP64 PCG vectors and
+    the cycle's per-level vectors, ~100 bytes a dof) and the group's own vectors (densities,
+    loads, U, the adjoint's load, warm start and solution, element terms: ~40 bytes a dof
+    and 40 an element), a quarter added for the allocator's rounding."""
+    L = _lib.lib()
+    prec = _lib.STT_FP32 if precision == "mixed" else _lib.STT_FP64
+    nel, nnode = nelx * nely, (nelx + 1) * (nely + 1)
+    stage = L.stt_hier_workspace_bytes(2, nelx, nely, stage_rows, max_coarse_elements, prec)
+    heat = L.stt_hier_workspace_bytes(1, nelx, nely, n_problems, max_coarse_elements, prec)
+    rows = stage_rows * (2 * nnode * 140 + nel * 40) + n_problems * (nnode * 140 + nel * 40)
+    return int(1.25 * (stage + heat + rows))
+
+
+def budget_waves(groups: dict, n_stages, budget: int, precision: str, max_coarse_elements: int) -> list:
+    """Slices of the shape groups (``{(nely, nelx): [problem indices]}``) packed into waves
+    whose ``group_bytes`` estimates fit ``budget``: a group over the budget is cut into
+    slices of consecutive problems that fit (a single problem over the budget is a slice of
+    its own); slices go first-fit, largest first, into the first wave with room and no
+    slice of the same grid size."""
+    slices = []
+    for shape, idx in groups.items():
+        nely, nelx = shape
+        cur: list = []
+        for k in idx:
+            trial = cur + [k]
+            est = group_bytes(nelx, nely, len(trial), sum(n_stages[i] for i in trial), precision, max_coarse_elements)
+            if cur and est > budget:
+                slices.append((shape, cur))
+                cur = [k]
+            else:
+                cur = trial
+        if cur:
+            slices.append((shape, cur))
+
+    def est(sl):
+        (nely, nelx), idx = sl
+        return group_bytes(nelx, nely, len(idx), sum(n_stages[i] for i in idx), precision, max_coarse_elements)
+
+    waves: list = []  # [load, shapes, slices]
+    for sl in sorted(slices, key=lambda t: -est(t)):
+        e = est(sl)
+        for w in waves:
+            if w[0] + e <= budget and sl[0] not in w[1]:
+                w[0] += e
+                w[1].add(sl[0])
+                w[2].append(sl)
+                break
+        else:
+            waves.append([e, {sl[0]}, [sl]])
+    return [w[2] for w in waves]
+
+
+def _run_wave(wave: list, run, cache: dict, dev, concurrent: bool) -> None:
+    """One wave of ``(shape, problem indices)`` slices: on concurrent CUDA streams from host
+    threads (one slice per grid size), or in order on the caller's stream."""
+    if not concurrent or len(wave) == 1:
+        for shape, idx in wave:
             run(shape, idx)
-        return results
+        return
     import concurrent.futures
 
     dev_i = _device_index(dev)
     main = torch.cuda.current_stream(dev_i)
     ready = torch.cuda.Event()
     ready.record(main)
-    streams = {shape: cache[(shape[1], shape[0])].stream("group") for shape in groups}
+    streams = {shape: cache[(shape[1], shape[0])].stream("group") for shape, _ in wave}
 
     def on_stream(shape, idx):
         torch.cuda.set_device(dev_i)
@@ -191,16 +292,11 @@ def objective_and_gradient_many(xs: list[Tensor], ws: list[Tensor], n_stages: li
             run(shape, idx)
         return s
 
-    with concurrent.futures.ThreadPoolExecutor(max_workers=len(groups)) as ex:
-        futs = [ex.submit(on_stream, shape, idx) for shape, idx in groups.items()]
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(wave)) as ex:
+        futs = [ex.submit(on_stream, shape, idx) for shape, idx in wave]
         done = [f.result() for f in futs]
     for s in done:  # the results were made on the side streams
         main.wait_stream(s)
-    for o in results:
-        for v in o.values():
-            if isinstance(v, torch.Tensor) and v.is_cuda:
-                v.record_stream(main)
-    return results
 
 
 def _device_index(dev) -> int:

@@ -20,18 +20,27 @@ DEFAULT_CG_RTOL = 1e-8  # sttopt/torch_solve.py:49
 
 
 class FemSolve(torch.autograd.Function):
-    """``K @ U = F`` as a differentiable op (sttopt/torch_solve.py:52-173)."""
+    """``K @ U = F`` as a differentiable op (sttopt/torch_solve.py:52-173).
+
+    With ``recompute`` the forward pass keeps the hierarchy but not ``U``: the backward
+    pass solves for ``U`` again (the same kernels on the same inputs, so the same ``U``)
+    before the adjoint, trading one forward solve for the memory of ``U``."""
 
     @staticmethod
     def forward(ctx, density, F, reaction, edofMat, KE, mask, nelx, nely, rtol, max_iter, x0,
-                omega, n_smooth, gamma, max_coarse_elements, info, precision=None):
+                omega, n_smooth, gamma, max_coarse_elements, info, precision=None, recompute=False):
         levels = torch_mg.build_hierarchy(density, edofMat, KE, mask, nelx, nely, reaction=reaction,
                                           max_coarse_elements=max_coarse_elements, precision=precision)
         precond = torch_mg.VCycle(levels, omega=omega, n_smooth=n_smooth, gamma=gamma)
         b = torch_fem.project(F, mask)
         U, n_iter = torch_fem.pcg(levels[0], b, precond, rtol=rtol, max_iter=max_iter, x0=x0)
         U = torch_fem.project(U, mask)
-        ctx.save_for_backward(U, density, F)
+        ctx.recompute = bool(recompute)
+        if ctx.recompute:
+            ctx.x0 = None if x0 is None else x0.detach()
+            ctx.save_for_backward(density, F)
+        else:
+            ctx.save_for_backward(U, density, F)
         ctx.levels = levels
         ctx.edofMat, ctx.KE, ctx.mask = edofMat, KE, mask
         ctx.rtol, ctx.max_iter = rtol, max_iter
@@ -43,7 +52,14 @@ class FemSolve(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, grad_output):
-        U, density, F = ctx.saved_tensors
+        if ctx.recompute:
+            density, F = ctx.saved_tensors
+            precond = torch_mg.VCycle(ctx.levels, omega=ctx.omega, n_smooth=ctx.n_smooth, gamma=ctx.gamma)
+            U, _ = torch_fem.pcg(ctx.levels[0], torch_fem.project(F, ctx.mask), precond, rtol=ctx.rtol,
+                                 max_iter=ctx.max_iter, x0=ctx.x0)
+            U = torch_fem.project(U, ctx.mask)
+        else:
+            U, density, F = ctx.saved_tensors
         Fb = F.expand_as(U)
         UF = torch_fem._dots(U.contiguous(), Fb.contiguous())
         Ug = torch_fem._dots(U.contiguous(), grad_output.expand_as(U).contiguous())
@@ -61,25 +77,26 @@ class FemSolve(torch.autograd.Function):
             grad_density = terms["gdens"] if ctx.needs_input_grad[0] else None
             grad_reaction = terms["greac"] if ctx.needs_input_grad[2] else None
         grad_F = lam if ctx.needs_input_grad[1] else None
-        return (grad_density, grad_F, grad_reaction) + (None,) * 14
+        return (grad_density, grad_F, grad_reaction) + (None,) * 15
 
 
 def femsolve(density: Tensor, F: Tensor, edofMat: Tensor, KE: Tensor, mask: Tensor, nelx: int,
              nely: int, *, rtol: float = DEFAULT_CG_RTOL, max_iter: int = 500,
              x0: Tensor | None = None, omega: float = 0.6, n_smooth: int = 2, gamma: int = 1,
              max_coarse_elements: int = torch_mg.MAX_COARSE_ELEMENTS, info: dict | None = None,
-             reaction: Tensor | None = None, precision: str | None = None) -> Tensor:
+             reaction: Tensor | None = None, precision: str | None = None, recompute: bool = False) -> Tensor:
     """``FemSolve.apply`` with the reference's keyword defaults (sttopt/torch_solve.py:176-243).
 
     ``precision`` ("fp64" default, or "mixed") selects the V-cycle precision; the outer
-    PCG is FP64 either way.
+    PCG is FP64 either way.  ``recompute`` keeps ``U`` out of the autograd graph and solves
+    for it again in the backward pass (memory for one more solve).
     """
     assert x0 is None or not x0.requires_grad, (
-        "x0 must already be detached -- FemSolve.backward returns None for it "
-        "unconditionally, so no caller should be routing gradient through it."
+        "femsolve: the warm start x0 requires grad, but the solve has no gradient for it; "
+        "pass x0.detach()"
     )
     return FemSolve.apply(density, F, reaction, edofMat, KE, mask, nelx, nely, rtol, max_iter, x0,
-                          omega, n_smooth, gamma, max_coarse_elements, info, precision)
+                          omega, n_smooth, gamma, max_coarse_elements, info, precision, recompute)
 
 
 def lifted_femsolve(density: Tensor, F: Tensor, g: Tensor, edofMat: Tensor, KE: Tensor,

@@ -62,3 +62,52 @@ def test_batched_rows_and_a_large_grid(pkg):
     (gu,) = torch.autograd.grad(lhs, [u])
     lhs = lhs.detach()
     assert abs(float(torch.sum(gu * u.detach()) - lhs)) <= 1e-12 * abs(float(lhs))
+
+
+@pytest.mark.parametrize("beta", [None, 4.0])
+def test_filtered_objective_gradient_through_the_filter(pkg, beta):
+    """``objective_and_gradient`` with the density filter (and projection) inside: the
+    objective of ``P(H x / Hs)`` and its gradient in the design variable x equal the
+    autograd composition of ``filters.filter_and_project`` (or ``apply_density_filter``)
+    with the objective node, and central differences of the FP64 objective on seeded
+    elements."""
+    import numpy as np
+
+    from sttopt_b200 import filters, spacetime, synthetic
+
+    nelx, nely, n_stage = 96, 48, 8
+    dev = torch.device("cuda")
+    x = synthetic.smoothed_density(nelx, nely, 31, device=dev)
+    w = synthetic.time_weights(nelx, nely, 31, device=dev)
+    H, Hs = filters.density_filter(nelx, nely, 2.5)
+    kw = dict(n_stage=n_stage, precision="fp64", rtol=1e-12)
+    fused = spacetime.objective_and_gradient(x, w, filter=H, beta=beta, **kw)
+    xv = x.clone().requires_grad_(True)
+    xp = filters.apply_density_filter(xv, H) if beta is None else filters.filter_and_project(xv, H, beta, 0.5)[0]
+    L = spacetime.objective(xp, w, **kw)
+    (g,) = torch.autograd.grad(L, [xv])
+    assert abs(float(fused["objective"]) - float(L)) <= 1e-12 * abs(float(L))
+    assert float((fused["gradient"] - g).norm() / g.norm()) < 1e-12
+    assert torch.equal(fused["xPhys"], xp.detach())
+    # central differences (h = 1e-6) on elements whose perturbation moves no stage
+    # membership; their noise floor is the objective's solve noise over 2h, as in the
+    # differentiation configuration's check
+    rng = np.random.default_rng(5)
+    h = 1e-6
+    grad = fused["gradient"].reshape(-1)
+    scale = float(grad.abs().max())
+    fd, an = [], []
+    for e in rng.choice(nelx * nely, 24, replace=False):
+        xs = []
+        for sgn in (1, -1):
+            xe = x.clone().reshape(-1)
+            xe[e] += sgn * h
+            xs.append(spacetime.objective_and_gradient(xe.reshape(nely, nelx), w, filter=H, beta=beta, gradient=False,
+                                                       **kw))
+        if not torch.equal(xs[0]["member"], fused["member"]) or not torch.equal(xs[1]["member"], fused["member"]):
+            continue
+        fd.append((float(xs[0]["objective"]) - float(xs[1]["objective"])) / (2 * h))
+        an.append(float(grad[e]))
+    fd, an = np.array(fd), np.array(an)
+    assert len(fd) >= 16
+    assert np.all(np.abs(fd - an) <= 2e-3 * np.abs(an) + 5e-5 * scale), (np.abs(fd - an).max(), scale)

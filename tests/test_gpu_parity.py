@@ -431,3 +431,22 @@ def test_stage_membership_bit_exact(pkg):
         _lib.check(_lib.lib().stt_stage_membership(t.numel(), n_stage, _lib.ptr(t), _lib.ptr(member),
                                                    _lib.stream()))
         np.testing.assert_array_equal(member.cpu().numpy(), g[f"{k}_member"])
+
+
+def test_femsolve_recompute_gives_the_same_gradient(m):
+    """``femsolve(..., recompute=True)`` drops U after the forward solve and solves for it
+    again in the backward pass: the same U (same kernels, same inputs), so the same
+    gradients, bit for bit."""
+    nelx, nely = 64, 32
+    F, mask = O.cantilever_point_load(nelx, nely)
+    KE, edof = T(O.plane_stress_KE(0.3)), T(O.element_dof_map(nelx, nely), torch.int64)
+    x = T(O.smoothed_density(nelx, nely, 3))
+    grads = []
+    for recompute in (False, True):
+        xPhys = x.clone().requires_grad_(True)
+        density = m.fem.simp_density(xPhys, EMIN, EMAX, PENAL).flatten()
+        U = m.solve.femsolve(density, T(F), edof, KE, T(mask, torch.bool), nelx, nely, recompute=recompute)
+        ce = m.comp._element_strain_energy(U, edof, KE, nely, nelx)
+        c = torch.sum(m.fem.simp_density(xPhys, EMIN, EMAX, PENAL) * ce)
+        grads.append(torch.autograd.grad(c, [xPhys])[0])
+    assert torch.equal(grads[0], grads[1])

@@ -94,3 +94,31 @@ def test_split_objective_shares_add_up_to_the_whole(pkg, precision, tol):
     assert torch.equal(got["tPhys"].reshape(nely, nelx), whole["tPhys"])
     assert rel_err(c_s.cpu(), whole["c_s"].cpu()) < tol
     assert rel_err(grad.cpu(), whole["gradient"].cpu()) < tol
+
+
+def test_memory_budget_waves_give_the_same_results(pkg):
+    """A memory budget below the whole batch's estimate runs the groups in waves (a group
+    cut into slices where it alone exceeds the budget): every problem's result equals the
+    unbounded call's, and the waves' estimates fit the budget."""
+    from sttopt_b200 import spacetime, synthetic
+
+    dev = torch.device("cuda")
+    shapes = [(96, 48), (64, 32), (96, 48), (128, 64), (64, 32), (128, 64)]
+    xs = [synthetic.smoothed_density(nx, ny, 40 + k, device=dev) for k, (nx, ny) in enumerate(shapes)]
+    ws = [synthetic.time_weights(nx, ny, 40 + k, device=dev) for k, (nx, ny) in enumerate(shapes)]
+    ns = [4, 6, 5, 8, 7, 4]
+    full = spacetime.objective_and_gradient_many(xs, ws, ns, precision="fp64")
+    groups: dict = {}
+    for k, x in enumerate(xs):
+        groups.setdefault(tuple(x.shape), []).append(k)
+    biggest = max(spacetime.group_bytes(s[1], s[0], len(i), sum(ns[k] for k in i), "fp64") for s, i in groups.items())
+    budget = int(0.7 * biggest)
+    waves = spacetime.budget_waves(groups, ns, budget, "fp64", 700)
+    assert len(waves) > 1
+    assert sorted(k for w in waves for _, idx in w for k in idx) == list(range(len(xs)))
+    for w in waves:
+        assert len({shape for shape, _ in w}) == len(w)
+    got = spacetime.objective_and_gradient_many(xs, ws, ns, precision="fp64", memory_budget=budget)
+    for a, b in zip(full, got):
+        assert rel_err(b["c_s"].cpu(), a["c_s"].cpu()) < 1e-12
+        assert rel_err(b["gradient"].cpu(), a["gradient"].cpu()) < 1e-12
