@@ -64,6 +64,8 @@ def parse():
                          "seeded densities and loads)")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the batched uneven multi-problem measurement")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the library's launch-shape heuristics instead of the autotuner's measured choices")
     ap.add_argument("--no-dropin", action="store_true",
                     help="skip the end-to-end timing through the reference-signature chain")
     ap.add_argument("--ref-budget", type=float, default=240.0,
@@ -247,6 +249,15 @@ def run_uneven(dev, steps=2, warmup=1, memory_budget=None):
     torch.cuda.empty_cache()
     torch.cuda.reset_peak_memory_stats(dev)
     kw = dict(problems=cache, info=info, memory_budget=memory_budget)
+    from sttopt_b200 import autotune
+
+    if autotune.mode() != "off":
+        # the grid sizes' launch shapes tuned with the groups one after another (clean timings)
+        prev = autotune.mode()
+        autotune.enable()
+        spacetime.objective_and_gradient_many(xs, ws, ns, problems=cache, concurrent=False)
+        if prev == "frozen":
+            autotune.freeze()
     for _ in range(warmup):
         spacetime.objective_and_gradient_many(xs, ws, ns, **kw)
     torch.cuda.synchronize()
@@ -367,6 +378,15 @@ def main():
               flush=True)
         return 0
     info: dict = {}
+    from sttopt_b200 import autotune
+
+    if not args.no_autotune:
+        # launch shapes picked by measurement on one clean evaluation (the heat adjoint in
+        # order, not beside the stage solves), then only reused
+        autotune.enable()
+        spacetime.objective_and_gradient(x, w, n_stage=N_STAGE, precision=args.precision, problem=problem,
+                                         overlap=False)
+        autotune.freeze()
 
     def step(xx, ww, precision=args.precision, batched=True):
         return spacetime.objective_and_gradient(xx, ww, n_stage=N_STAGE, precision=precision,
@@ -520,6 +540,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "full_gradient_ms": e2e_ms / args.steps, "detail": e2e_detail},
             "timed_detail": timed_detail,
+            "autotune": {"mode": autotune.mode(),
+                         "choices": {k: {kk: v[kk] for kk in ("pcg_band", "level_waves")}
+                                     for k, v in autotune.cache().items()}},
             "gpu_launches": None if launches is None else launches * args.steps,
         }
         line.update(extra)

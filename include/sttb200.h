@@ -158,6 +158,15 @@ int stt_hier_destroy(stt_hier* h);
 /* nlevels, and per level (nelx, nely, kx, ky) into dims[4 * level]. */
 int stt_hier_info(const stt_hier* h, int* nlevels, int* dims, int max_levels);
 
+/* Launch shapes of the solves on h (stt_vcycle, stt_pcg_mg, stt_level_apply; views made
+ * afterwards inherit them): pcg_band, the grid rows a block of the PCG's level-0 passes
+ * marches (8, 16 or 32; 0: the built-in choice, 32 or shorter while the rows give fewer
+ * than two waves of blocks), and level_waves, the blocks the stencil levels' kernels aim
+ * at in waves of one block per SM (1..64; 0: four).  Results do not depend on them beyond
+ * the order of the block reductions.  No reference counterpart: set by this library's
+ * autotuner (sttopt_b200.autotune), which times the candidates on the hierarchy. */
+int stt_hier_tune(stt_hier* h, int pcg_band, int level_waves);
+
 /* Copies of a level's Jacobi diagonal (FP64, [hrows][ndof]) and fixed flags. */
 int stt_hier_level_diag(const stt_hier* h, int level, double* out, stt_stream_t stream);
 int stt_hier_level_fixed(const stt_hier* h, int level, uint8_t* out, stt_stream_t stream);

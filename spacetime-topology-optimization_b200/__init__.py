@@ -12,7 +12,7 @@ from . import _lib  # noqa: F401
 from ._lib import element_form, set_element_form  # noqa: F401
 
 __all__ = ["torch_fem", "torch_mg", "torch_solve", "sensitivity", "virtual_heat", "compliance",
-           "spacetime", "fem", "gravity", "filters", "load_cases", "sharding"]
+           "spacetime", "fem", "gravity", "filters", "load_cases", "sharding", "autotune"]
 
 
 def __getattr__(name):

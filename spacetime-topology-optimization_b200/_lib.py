@@ -61,6 +61,7 @@ _SIGS = {
     "stt_pap_timing": (_c_int, [_c_int]),
     "stt_pap_timing_read": (_c_int, [_pd, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_ll)]),
     "stt_hier_destroy": (_c_int, [_p]),
+    "stt_hier_tune": (_c_int, [_p, _c_int, _c_int]),
     "stt_hier_info": (_c_int, [_p, _pi, _pi, _c_int]),
     "stt_hier_level_diag": (_c_int, [_p, _c_int, _p, _p]),
     "stt_hier_level_fixed": (_c_int, [_p, _c_int, _p, _p]),

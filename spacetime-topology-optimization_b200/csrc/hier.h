@@ -79,6 +79,8 @@ struct stt_hier_impl {
   int* status;         // device status word of the build (bit 0: pivot <= 0, bit 1: band)
   CoarseSync* sync;    // the coarse factorisation's stream and completion event
   long long ws_bytes;
+  int tune_pcg_band = 0;  // launch tuning of the solves on this hierarchy (stt_hier_tune; 0: heuristics)
+  int tune_waves = 0;
 };
 
 inline int level_node_count(int nelx, int nely) { return (nelx + 1) * (nely + 1); }

@@ -614,14 +614,33 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
   }
 }
 
+// The launch shapes a solve uses, tunable per hierarchy (stt_hier_tune) and set on the
+// calling host thread for the duration of a solve entry point: pcg_band, the rows a block
+// of the PCG's level-0 passes marches (8, 16 or 32; 0: the heuristic of pcg_tile_grid);
+// waves, the blocks band_rows aims at in units of one block per SM (0: four).
+struct LaunchTuning {
+  int pcg_band = 0;
+  int waves = 0;
+};
+inline LaunchTuning& launch_tuning() {
+  static thread_local LaunchTuning t;
+  return t;
+}
+struct ScopedTuning {
+  LaunchTuning saved;
+  ScopedTuning(int pcg_band, int waves) : saved(launch_tuning()) { launch_tuning() = LaunchTuning{pcg_band, waves}; }
+  ~ScopedTuning() { launch_tuning() = saved; }
+};
+
 // Rows a block marches on the coarse levels: 32 where the grid then fills the GPU,
 // shorter bands on small grids (the heat solve's single row, the coarse levels), whose
 // launches are otherwise latency-bound by the sequential march down 32 rows.  The
 // kernels derive their band from gridDim.y, so any grid.y covers the rows.
 inline int band_rows(int xblocks, int nny, int rows) {
-  constexpr int kTarget = 4 * 148;  // blocks: four waves of one block per B200 SM
+  const int waves = launch_tuning().waves > 0 ? launch_tuning().waves : 4;
+  const long long target = (long long)waves * 148;  // blocks: waves of one block per B200 SM
   for (int band = 32; band > 4; band /= 2)
-    if ((long long)xblocks * ((nny + band - 1) / band) * rows >= kTarget) return band;
+    if ((long long)xblocks * ((nny + band - 1) / band) * rows >= target) return band;
   return 4;
 }
 

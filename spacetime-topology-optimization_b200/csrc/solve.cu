@@ -51,11 +51,17 @@ static dim3 tile_grid(int nelx, int nely, int rows) { return q4_grid(nelx, nely,
 // ones (down to 8) while the rows give fewer blocks than two waves of six 128-thread
 // blocks on each of the 148 SMs (a single scalar row: the heat solves).  The kernels
 // take the band from the launch (BAND = 0).
-static dim3 pcg_tile_grid(int nelx, int nely, int rows) {
+static dim3 pcg_tile_grid(int nelx, int nely, int rows, int min_band = 0) {
   const dim3 g = q4_grid(nelx, nely, rows);
   const int nny = nely + 1;
   int band = kQRows;
-  while (band > 8 && (long long)g.x * ((nny + band - 1) / band) * rows < 2LL * 148 * 6) band /= 2;
+  if (min_band > 0) {
+    band = min_band;  // the most blocks any tuning can ask for (sizes the reduction partials)
+  } else if (launch_tuning().pcg_band > 0) {
+    band = launch_tuning().pcg_band;
+  } else {
+    while (band > 8 && (long long)g.x * ((nny + band - 1) / band) * rows < 2LL * 148 * 6) band /= 2;
+  }
   return dim3(g.x, (nny + band - 1) / band, rows);
 }
 
@@ -103,7 +109,7 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
   const int es = h->precision == STT_FP32 ? 4 : 8;
   const LevelDesc& l0 = h->lv[0];
   if (pcg) {
-    const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows);
+    const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows, 8);
     w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
     w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
     w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
@@ -1151,6 +1157,8 @@ extern "C" long long stt_vcycle_workspace_bytes(const stt_hier* h, int nrows, in
 extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long long r_rs, double* z,
                           long long z_rs, double omega, int n_smooth, int gamma, void* workspace,
                           long long ws_bytes, stt_stream_t stream) {
+  if (!h) return set_error(STT_ERR_INVALID, "null hierarchy");
+  ScopedTuning tuning(h->tune_pcg_band, h->tune_waves);
   if (!h || !r || !z || !workspace || nrows <= 0 || nrows > 65535 || n_smooth < 1 || gamma < 1)
     return set_error(STT_ERR_INVALID, "stt_vcycle: bad arguments");
   if (h->d == 2 && (!aligned16(r) || !aligned16(z) || (r_rs % 2) || (z_rs % 2)))
@@ -1179,6 +1187,8 @@ extern "C" int stt_vcycle(const stt_hier* h, int nrows, const double* r, long lo
 
 extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const double* v, long long v_rs,
                                double* out, long long out_rs, stt_stream_t stream) {
+  if (!h) return set_error(STT_ERR_INVALID, "null hierarchy");
+  ScopedTuning tuning(h->tune_pcg_band, h->tune_waves);
   if (!h || !v || !out || level < 0 || level >= h->nlevels || nrows <= 0 || nrows > 65535)
     return set_error(STT_ERR_INVALID, "stt_level_apply: bad arguments");
   if (h->d == 2 && (!aligned16(v) || !aligned16(out) || (v_rs % 2) || (out_rs % 2)))
@@ -1226,6 +1236,8 @@ extern "C" int stt_pcg_mg(const stt_hier* h, int nrows, const double* b, long lo
                           int n_smooth, int gamma, int flexible, int replace_every, int retire,
                           double* rel_resid, int* conv_iter, int* n_iter, void* workspace, long long ws_bytes,
                           stt_stream_t stream) {
+  if (!h) return set_error(STT_ERR_INVALID, "null hierarchy");
+  ScopedTuning tuning(h->tune_pcg_band, h->tune_waves);
   if (!h || !b || !x || !workspace || !rel_resid || !conv_iter || !n_iter || nrows <= 0 ||
       nrows > 65535 || max_iter < 0 || n_smooth < 1 || gamma < 1)
     return set_error(STT_ERR_INVALID, "stt_pcg_mg: bad arguments");
@@ -1306,6 +1318,15 @@ extern "C" int stt_vcycle_noalloc(const stt_hier* h, int nrows, const double* r,
   void* scratch = nullptr;
   STT_TRY(vcycle_scratch_address(&scratch));
   return stt_vcycle(h, nrows, r, r_rs, z, z_rs, omega, n_smooth, gamma, scratch, kVCycleScratchBytes, stream);
+}
+
+extern "C" int stt_hier_tune(stt_hier* h, int pcg_band, int level_waves) {
+  if (!h || !(pcg_band == 0 || pcg_band == 8 || pcg_band == 16 || pcg_band == 32) || level_waves < 0 ||
+      level_waves > 64)
+    return set_error(STT_ERR_INVALID, "stt_hier_tune: pcg_band must be 0, 8, 16 or 32 and level_waves in [0, 64]");
+  h->tune_pcg_band = pcg_band;
+  h->tune_waves = level_waves;
+  return STT_OK;
 }
 
 extern "C" int stt_pap_timing(int enable) {

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 from torch import Tensor
 
-from . import _geom, _lib, fem, torch_fem
+from . import _geom, _lib, autotune, fem, torch_fem
 
 MAX_COARSE_ELEMENTS = 700  # sttopt/torch_mg.py:50
 #: "fp64" or "mixed"; the precision ``build_hierarchy`` uses when none is given.
@@ -224,6 +224,7 @@ class _Level:
         x = torch.empty_like(flat)
         if x0 is not None:
             x.copy_(x0.detach().to(torch.float64).expand(*batch, n).reshape(-1, n))
+        autotune.apply(h, flat, rows, n, M.gamma, M.omega, M.n_smooth)
         nbytes = _lib.lib().stt_solve_workspace_bytes(h.handle, rows, M.gamma)
         ws = _lib.workspace(nbytes, flat.device)
         rel = (ctypes.c_double * rows)()
