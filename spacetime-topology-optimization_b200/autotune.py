@@ -81,7 +81,7 @@ def _key(h, rows: int, gamma: int) -> tuple:
     return (h.d, nelx, nely, h.precision or "fp64", int(rows), int(gamma))
 
 
-def _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, mixed, band, waves, ws, x) -> float:
+def _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, band, waves, ws, x) -> float:
     L = _lib.lib()
     _lib.check(L.stt_hier_tune(h.handle, band, waves))
     rel = (ctypes.c_double * rows)()
@@ -91,7 +91,7 @@ def _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, mixed, band, waves
     a.record()
     # rtol 0: every row with a nonzero right-hand side iterates ITERS times
     rc = L.stt_pcg_mg(h.handle, rows, _lib.ptr(flat), n, _lib.ptr(x), n, 0, 0.0, ITERS, omega, n_smooth, gamma,
-                      1 if mixed else 0, 0, 0, rel, conv, ctypes.byref(n_iter), _lib.ptr(ws), ws.numel(),
+                      0, 0, 0, rel, conv, ctypes.byref(n_iter), _lib.ptr(ws), ws.numel(),
                       _lib.stream())
     b.record()
     if rc not in (_lib.STT_OK, _lib.STT_ERR_NOT_CONVERGED):
@@ -104,15 +104,14 @@ def tune(h, flat: torch.Tensor, rows: int, n: int, gamma: int, omega: float, n_s
     """Times the candidates on hierarchy ``h`` with right-hand side rows ``flat`` and
     applies the fastest; returns the cache entry."""
     L = _lib.lib()
-    mixed = h.precision == "mixed"
     ws = _lib.workspace(L.stt_solve_workspace_bytes(h.handle, rows, gamma), flat.device)
     x = torch.empty_like(flat)
     cands = [(b, w) for b in PCG_BANDS for w in LEVEL_WAVES]
-    _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, mixed, 0, 0, ws, x)  # warm-up
+    _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, 0, 0, ws, x)  # warm-up
     times = {c: float("inf") for c in cands}
     for _ in range(2):
         for band, waves in cands:
-            t = _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, mixed, band, waves, ws, x)
+            t = _time_candidate(h, rows, flat, n, gamma, omega, n_smooth, band, waves, ws, x)
             times[(band, waves)] = min(times[(band, waves)], t)
     best = min(cands, key=lambda c: (times[c], c != (0, 0)))
     _lib.check(L.stt_hier_tune(h.handle, best[0], best[1]))

@@ -46,6 +46,13 @@ struct RowState {
   int conv;           // rel <= rtol at the last check (the reference's retirement schedule)
 };
 
+// Coefficients a node in an FP32 stored stencil (node-major): the 5 D^2 of the half
+// stencil rounded up to a multiple of 4 (16-byte aligned node records).
+template <int D>
+__host__ __device__ constexpr int st32_nsp() {
+  return (5 * D * D + 3) & ~3;
+}
+
 STT_DEV int hier_row(const int* row_map, int hrows, int s) {
   return row_map ? row_map[s] : (hrows == 1 ? 0 : s);
 }

@@ -6,6 +6,8 @@
 // _interp_axis/_restrict_axis/_on_node_grid (:75-109).
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "q4.cuh"
 
@@ -382,6 +384,36 @@ STT_DEV void l0_delay_row(const FrontRow<D, T, RD>& F, T dsum, const MQ<T>& q, T
   cur.rho = F.rho;
 }
 
+// The PCG's beta from the dots of a preconditioned residual, t[0] = r.z and t[1] =
+// r.z_old (flexible form): the first call of a solve only records rz; later ones set
+// beta = safe_div(rz - rz_mix, rz_old) (or rz / rz_old) and rz_old = rz.
+STT_DEV void pcg_rz_finish(RowState& S, const double* t, int first, int flexible) {
+  if (first) {
+    S.rz = t[0];
+  } else {
+    const double num = flexible ? t[0] - t[1] : t[0];
+    S.beta = safe_div(num, S.rz);
+    S.rz = t[0];
+    if (!isfinite(S.beta)) S.status = STT_ERR_BREAKDOWN;
+  }
+}
+
+// The PCG's dots taken by the level-0 chained passes of its preconditioner cycle z = M r,
+// whose right-hand side b is the r the dots read (the FP32 copy of r in a mixed cycle):
+// the pre-smoothing pass takes the flexible beta's r.z_old (into RowState::rz_mix, with
+// z_old loaded beside b), the post-smoothing pass r.z as it writes z and finishes beta,
+// so neither needs a pass of its own.  A node's terms are summed in the cycle's
+// precision (one rounding of each FP32 product, ~1e-7 relative, the FP32 cycle's own
+// level) and accumulated in FP64 per thread, reduced over the pass's blocks.
+template <typename T>
+struct RzFuse {
+  RowState* rst;    // null: no dots
+  const T* zold;    // the previous z (the flexible beta's r.z_old), else null
+  long long zo_rs;
+  GridRed red;      // nblk = the pass's blocks a row (set at launch)
+  int first, flexible;
+};
+
 constexpr int kPreCols = 27;  // output columns per warp strip of l0_presmooth_kernel
 
 inline dim3 presmooth_grid(int nelx, int nely, int rows) {
@@ -392,12 +424,13 @@ inline dim3 presmooth_grid(int nelx, int nely, int rows) {
 // FP32: 6 blocks of 128 threads an SM (<= 80 registers), measured fastest on B200 at
 // 2048x1024 x 16 rows (333 us against 351 us at the compiler's 80-95 registers with
 // fewer blocks).  FP64 needs twice the registers for the same state: 3 blocks.
-template <int D, typename T, bool RD, int AHEAD = 2>
+// MX: also r.z_old of the PCG (mx.zold), z_old loaded with the front row's b.
+template <int D, typename T, bool RD, bool MX = false, int AHEAD = 2>
 __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmooth_kernel(
     const T* __restrict__ b, long long b_rs, T* __restrict__ out_x, long long ox_rs, T* __restrict__ out_r,
     long long or_rs, const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag,
     long long rd_rs, const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows,
-    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q) {
+    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q, RzFuse<T> mx = RzFuse<T>{}) {
   constexpr int LO = 3, HI = 29;
   static_assert(HI - LO + 1 == kPreCols, "strip width");
   const int s = blockIdx.z;
@@ -417,6 +450,14 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
   const bool ecol_ok = c >= 0 && c < nelx;
   const int r0 = blockIdx.y * kQRows;
   const int r1 = min(r0 + kQRows, nny);
+  const T* zos = MX ? mx.zold + (size_t)s * mx.zo_rs : nullptr;
+  T zq[MX ? AHEAD : 1][D];  // MX: z_old at the front rows in flight
+  double mix[1] = {0.0};
+  auto load_zo = [&](int f, T(&zv)[D]) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) zv[d] = T(0);
+    if (col_ok && f >= 0 && f < nny) load_node<D, T>(zos, (long long)f * nnx + c, zv);
+  };
   auto load_front = [&](int f, FrontRow<D, T, RD>& F) {
 #pragma unroll
     for (int d = 0; d < D; ++d) F.b[d] = T(0);
@@ -443,13 +484,26 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
   T rho_prev = (ecol_ok && f0 - 1 >= 0 && f0 - 1 < nely) ? __ldg(rh + (size_t)(f0 - 1) * nelx + c) : T(0);
   FrontRow<D, T, RD> qf[AHEAD];
 #pragma unroll
-  for (int k = 0; k < AHEAD; ++k) load_front(f0 + k, qf[k]);
+  for (int k = 0; k < AHEAD; ++k) {
+    load_front(f0 + k, qf[k]);
+    if constexpr (MX) load_zo(f0 + k, zq[k]);
+  }
   for (int fb = f0; fb <= f1; fb += AHEAD) {
 #pragma unroll
     for (int k = 0; k < AHEAD; ++k) {
       const int f = fb + k;
       const FrontRow<D, T, RD> F = qf[k];
       load_front(f + AHEAD, qf[k]);
+      if constexpr (MX) {
+        // b z_old at the front row, each node once (output lanes, the block's rows)
+        if (out_lane && f >= r0 && f < r1) {
+          T t = F.b[0] * zq[k][0];
+#pragma unroll
+          for (int d = 1; d < D; ++d) t = fma(F.b[d], zq[k][d], t);
+          mix[0] += (double)t;
+        }
+        load_zo(f + AHEAD, zq[k]);
+      }
       // the row's free mask and w = omega / diag (diag: kd times the densities around the node)
       DelayRow<D, T, RD> cur;
       {
@@ -499,6 +553,10 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_presmoot
       d1 = cur;
     }
   }
+  if constexpr (MX) {
+    grid_reduce<1, kQThreads>(mx.red, s, blockIdx.y * gridDim.x + blockIdx.x, mix,
+                              [&](const double* t) { mx.rst[s].rz_mix = t[0]; });
+  }
 }
 
 // ---- level 0: post-smoothing in one pass (modal form, n_smooth = 2) -------------------
@@ -515,12 +573,12 @@ inline dim3 postsmooth_grid(int nelx, int nely, int rows) {
   return dim3((strips + kQWarps - 1) / kQWarps, (nely + 1 + kQRows - 1) / kQRows, rows);
 }
 
-template <int D, typename T, bool RD, int AHEAD = 2>
+template <int D, typename T, bool RD, bool RZ = false, int AHEAD = 2>
 __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmooth_kernel(
     const T* __restrict__ x0, long long x_rs, const T* __restrict__ b, long long b_rs, T* __restrict__ out,
     long long o_rs, const T* __restrict__ rho, long long rho_rs, const T* __restrict__ rdiag, long long rd_rs,
     const uint8_t* __restrict__ fixed, const int* __restrict__ row_map, int hrows,
-    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q) {
+    const RowState* __restrict__ rst, int nelx, int nely, T omega, MQ<T> q, RzFuse<T> rz = RzFuse<T>{}) {
   constexpr int LO = 2, HI = 29;
   static_assert(HI - LO + 1 == kPostCols, "strip width");
   const int s = blockIdx.z;
@@ -569,6 +627,8 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
   DelayRow<D, T, RD> d1{}, d2{};  // rows f - 1 and f - 2
   const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
   T rho_prev = (ecol_ok && f0 - 1 >= 0 && f0 - 1 < nely) ? __ldg(rh + (size_t)(f0 - 1) * nelx + c) : T(0);
+  // RZ: the sum of b z over the nodes this thread writes
+  double dots[1] = {0.0};
   Front qf[AHEAD];
 #pragma unroll
   for (int k = 0; k < AHEAD; ++k) load_front(f0 + k, qf[k]);
@@ -578,6 +638,7 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
       const int f = fb + k;
       const Front Q = qf[k];
       load_front(f + AHEAD, qf[k]);
+      const bool emit = out_lane && f - 2 >= r0 && f - 2 < r1;
       DelayRow<D, T, RD> cur;
       {
         const T rs = Q.F.rho + rho_prev;
@@ -607,10 +668,26 @@ __global__ void __launch_bounds__(kQThreads, sizeof(T) == 4 ? 6 : 3) l0_postsmoo
         for (int d = 0; d < D; ++d) rd2[d] = RD ? d2.rd[d] : T(0);
         l0_chain_result<D, T, SW_SWEEP, RD>(KB, d2.w, d2.mf, xo_b, d2.b, rd2, xb);
       }
-      if (out_lane && f - 2 >= r0 && f - 2 < r1) store_node<D, T>(os, (long long)(f - 2) * nnx + c, xb);
+      if (emit) {
+        store_node<D, T>(os, (long long)(f - 2) * nnx + c, xb);
+        if constexpr (RZ) {
+          T t = d2.b[0] * xb[0];
+#pragma unroll
+          for (int d = 1; d < D; ++d) t = fma(d2.b[d], xb[d], t);
+          dots[0] += (double)t;
+        }
+      }
       d2 = d1;
       d1 = cur;
     }
+  }
+  if constexpr (RZ) {
+    if (rz.rst)
+      grid_reduce<1, kQThreads>(rz.red, s, blockIdx.y * gridDim.x + blockIdx.x, dots, [&](const double* t) {
+        RowState& S = rz.rst[s];
+        const double t2[2] = {t[0], S.rz_mix};
+        pcg_rz_finish(S, t2, rz.first, rz.flexible);
+      });
   }
 }
 
@@ -651,6 +728,59 @@ inline dim3 coarse_grid(int nelx, int nely, int rows) {
   return dim3(xb, (nely + 1 + band - 1) / band, rows);
 }
 
+// ---- stored stencils: layout ---------------------------------------------------------
+//
+// A level's half stencil holds 5 D^2 coefficients a node (centre, E, S, SE, SW blocks,
+// row-major D x D each).  FP64 stencils (the coarse factorisation's input, FP64 cycles)
+// are stored by coefficient planes, [rows][5 D^2][nnode].  FP32 stencils (the FP32
+// cycle's) are node-major, [rows][nnode][NSP] with NSP = 5 D^2 rounded up to a multiple
+// of 4, so a node's coefficients are 16-byte aligned vectors: the column-marching
+// kernels load a row's coefficients with 128-bit loads from one address instead of one
+// load (and one address) a coefficient.  A level swept from the level-0 densities keeps
+// only its centre diagonal, compact in FP32: [rows][nnode][D] within the same extent.
+template <int D, typename T>
+STT_DEV const T* st_row(const T* st, int h, long long nnode) {
+  return st + (size_t)h * (sizeof(T) == 4 ? st32_nsp<D>() : 5 * D * D) * nnode;
+}
+// coefficient k of node `node` in a row's stencil sth
+template <int D, typename T>
+STT_DEV T st_coef(const T* sth, long long nnode, long long node, int k) {
+  if constexpr (sizeof(T) == 4) return __ldg(sth + node * st32_nsp<D>() + k);
+  else return __ldg(sth + (size_t)k * nnode + node);
+}
+// all 5 D^2 coefficients of a node
+template <int D, typename T>
+STT_DEV void st_coefs(const T* sth, long long nnode, long long node, T (&co)[5 * D * D]) {
+  constexpr int NS = 5 * D * D;
+  if constexpr (sizeof(T) == 4) {
+    const float4* v = reinterpret_cast<const float4*>(sth + node * st32_nsp<D>());
+#pragma unroll
+    for (int q = 0; q < (NS + 3) / 4; ++q) {
+      const float4 t = __ldg(v + q);
+      const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * q + e < NS) co[4 * q + e] = tv[e];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NS; ++k) co[k] = __ldg(sth + (size_t)k * nnode + node);
+  }
+}
+// the centre block's diagonal of a level swept from the level-0 densities (plane stress)
+template <typename T>
+STT_DEV void st_diag2(const T* st, int h, long long nnode, long long node, T (&dg)[2]) {
+  if constexpr (sizeof(T) == 4) {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(st_row<2, T>(st, h, nnode)) + node);
+    dg[0] = t.x;
+    dg[1] = t.y;
+  } else {
+    const T* sth = st_row<2, T>(st, h, nnode);
+    dg[0] = __ldg(sth + node);
+    dg[1] = __ldg(sth + 3 * nnode + node);
+  }
+}
+
 // ---- stencil levels: column-marching sweeps -----------------------------------------
 //
 // The symmetric half stencil stores, per node, the centre, E, S, SE, SW blocks; the W,
@@ -671,7 +801,7 @@ __global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
   if (rst && !rst[s].active) return;
   const long long nnode = (long long)nnx * nny;
   const int h = hier_row(row_map, hrows, s);
-  const T* sth = st + (size_t)h * NS * nnode;
+  const T* sth = st_row<D, T>(st, h, nnode);
   const T* xs = x + (size_t)s * vec_rs;
   const T* bs = b + (size_t)s * vec_rs;
   T* os = out + (size_t)s * vec_rs;
@@ -700,7 +830,7 @@ __global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
     }
   };
   auto CO = [&](int r, int k) -> T {
-    return (col_ok && r >= 0 && r < nny) ? __ldg(sth + (size_t)k * nnode + (size_t)r * nnx + c) : T(0);
+    return (col_ok && r >= 0 && r < nny) ? st_coef<D, T>(sth, nnode, (long long)r * nnx + c, k) : T(0);
   };
   auto up = [](T v) { return __shfl_up_sync(0xffffffffu, v, 1); };
   auto dn = [](T v) { return __shfl_down_sync(0xffffffffu, v, 1); };
@@ -840,7 +970,7 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
   if (rst && !rst[s].active) return;
   const long long nnode = (long long)nnx * nny;
   const int h = hier_row(row_map, hrows, s);
-  const T* sth = st + (size_t)h * NS * nnode;
+  const T* sth = st_row<D, T>(st, h, nnode);
   const T* xs = x + (size_t)s * vec_rs;
   const T* bs = b + (size_t)s * vec_rs;
   T* os = out + (size_t)s * vec_rs;
@@ -873,7 +1003,7 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
     if (!col_ok || r < 0 || r >= nny) return;
     const long long node = (long long)r * nnx + c;
 #pragma unroll
-    for (int k = 0; k < NC; ++k) R.co[k] = __ldg(sth + (size_t)k * nnode + node);
+    for (int k = 0; k < NC; ++k) R.co[k] = st_coef<D, T>(sth, nnode, node, k);
     if (MODE != SW_APPLY) load_node<D, T>(bs, node, R.b);
     R.fl = __ldg(fixed + node);
   };
@@ -907,9 +1037,9 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
       const long long node = (long long)(r0 - 1) * nnx + c;
 #pragma unroll
       for (int q = 0; q < DD; ++q) {
-        Sp[q] = ok ? __ldg(sth + (size_t)(2 * DD + q) * nnode + node) : T(0);
-        SEp[q] = ok ? __ldg(sth + (size_t)(3 * DD + q) * nnode + node) : T(0);
-        SWp[q] = ok ? __ldg(sth + (size_t)(4 * DD + q) * nnode + node) : T(0);
+        Sp[q] = ok ? st_coef<D, T>(sth, nnode, node, 2 * DD + q) : T(0);
+        SEp[q] = ok ? st_coef<D, T>(sth, nnode, node, 3 * DD + q) : T(0);
+        SWp[q] = ok ? st_coef<D, T>(sth, nnode, node, 4 * DD + q) : T(0);
       }
       T pse[D], psw[D];
 #pragma unroll
@@ -1082,7 +1212,7 @@ __global__ void __launch_bounds__(kQThreads, 6) st_chain_kernel(
   if (rst && !rst[s].active) return;
   const long long nnode = (long long)nnx * nny;
   const int h = hier_row(row_map, hrows, s);
-  const T* sth = st + (size_t)h * NS * nnode;
+  const T* sth = st_row<D, T>(st, h, nnode);
   const T* xs = PRE ? nullptr : x0 + (size_t)s * vec_rs;
   const T* bs = b + (size_t)s * vec_rs;
   T* ox = out_x + (size_t)s * vec_rs;
@@ -1109,8 +1239,7 @@ __global__ void __launch_bounds__(kQThreads, 6) st_chain_kernel(
     R.fl = 0;
     if (!col_ok || r < 0 || r >= nny) return;
     const long long node = (long long)r * nnx + c;
-#pragma unroll
-    for (int k = 0; k < NS; ++k) R.co[k] = __ldg(sth + (size_t)k * nnode + node);
+    st_coefs<D, T>(sth, nnode, node, R.co);
     load_node<D, T>(bs, node, R.b);
     R.fl = __ldg(fixed + node);
   };
@@ -1134,7 +1263,7 @@ __global__ void __launch_bounds__(kQThreads, 6) st_chain_kernel(
     if constexpr (PRE) {
       load_node<D, T>(bs, node, F.v);
 #pragma unroll
-      for (int d = 0; d < D; ++d) F.dg[d] = __ldg(sth + (size_t)(d * D + d) * nnode + node);
+      for (int d = 0; d < D; ++d) F.dg[d] = st_coef<D, T>(sth, nnode, node, d * D + d);
       F.fl = __ldg(fixed + node);
     } else {
       load_node<D, T>(xs, node, F.v);
@@ -1247,7 +1376,6 @@ __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
   const long long nnode = (long long)nnx * nny;
   const int h = hier_row(row_map, hrows, s);
   const T* rh = rho0 + (size_t)h * rho_rs;
-  const T* dgh = st + (size_t)h * 5 * D * D * nnode;  // centre block: coefficients 0 and 3
   const T* xs = x + (size_t)s * vec_rs;
   const T* bs = b + (size_t)s * vec_rs;
   T* os = out + (size_t)s * vec_rs;
@@ -1283,8 +1411,7 @@ __global__ void __launch_bounds__(kQThreads) l1_sweep_kernel(
     if (!(out_lane && r < r1)) return;
     const long long node = (long long)r * nnx + c;
     load_node<D, T>(bs, node, e.b);
-    e.dg[0] = __ldg(dgh + node);
-    e.dg[1] = __ldg(dgh + 3 * nnode + node);
+    st_diag2<T>(st, h, nnode, node, e.dg);
     e.fl = __ldg(fixed + node);
   };
   T ut[D], sT[D], dT[D], co[D], cr[D];
@@ -1501,7 +1628,6 @@ __global__ void __launch_bounds__(kQThreads, 4) l1_chain_kernel(
   const long long nnode = (long long)nnx * nny;
   const int h = hier_row(row_map, hrows, s);
   const T* rh = rho0 + (size_t)h * rho_rs;
-  const T* dgh = st + (size_t)h * 5 * D * D * nnode;  // centre block: coefficients 0 and 3
   const T* xs = PRE ? nullptr : x0 + (size_t)s * vec_rs;
   const T* bs = b + (size_t)s * vec_rs;
   T* ox = out_x + (size_t)s * vec_rs;
@@ -1530,38 +1656,42 @@ __global__ void __launch_bounds__(kQThreads, 4) l1_chain_kernel(
   auto load_front = [&](int f, Front& Q) {
 #pragma unroll
     for (int d = 0; d < D; ++d) Q.b[d] = Q.dg[d] = Q.x[d] = T(0);
-    Q.fl = 0;
+    Q.fl = 0xFF;  // off-grid positions count as fixed: their results are masked to zero
     load_rm(f, Q.rm);
     if (!col_ok || f < 0 || f >= nny) return;
     const long long node = (long long)f * nnx + c;
     Q.fl = __ldg(fixed + node);
     load_node<D, T>(bs, node, Q.b);
-    Q.dg[0] = __ldg(dgh + node);
-    Q.dg[1] = __ldg(dgh + 3 * nnode + node);
+    st_diag2<T>(st, h, nnode, node, Q.dg);
     if constexpr (!PRE) load_node<D, T>(xs, node, Q.x);
   };
+  // per node row, formed once at the front: b, w = omega / diag and the free mask mf (1 on
+  // free dofs, 0 on fixed and off-grid ones, where the diagonal is taken as 1)
   struct Delay {
-    T b[D], dg[D];
-    uint8_t fl;
+    T b[D], w[D], mf[D];
   };
-  // the sweep / residual at a node from K x there
-  auto result = [&](bool sweep, const T(&Kx)[D], const T(&xo)[D], const Delay& e, T(&res)[D]) {
+  auto delay_of = [&](const Front& Q, Delay& e) {
 #pragma unroll
-    for (int i = 0; i < D; ++i) {
-      const bool fx = (e.fl >> i) & 1;
-      const T Ax = fx ? T(0) : Kx[i];
-      if (sweep) {
-        const T dg = fx ? T(1) : e.dg[i];
-        res[i] = xo[i] + sweep_div(omega * (e.b[i] - Ax), dg);
-      } else {
-        res[i] = e.b[i] - Ax;
-      }
+    for (int d = 0; d < D; ++d) {
+      const bool fr = !((Q.fl >> d) & 1);
+      e.mf[d] = fr ? T(1) : T(0);
+      e.w[d] = sweep_div(omega, fr ? Q.dg[d] : T(1));
+      e.b[d] = Q.b[d];
     }
   };
+  // the first sweep from zero, a sweep or the residual at a node from K x there (masked)
+  auto result = [&](auto mode, const T(&Kx)[D], const T(&xo)[D], const Delay& e, T(&res)[D]) {
+    T Ax[D] = {Kx[0], Kx[1]};
+    const T rd[D] = {T(0), T(0)};
+    l0_chain_result<D, T, decltype(mode)::value, false>(Ax, e.w, e.mf, xo, e.b, rd, res);
+  };
+  using First = std::integral_constant<int, SW_FIRST>;
+  using Sweep = std::integral_constant<int, SW_SWEEP>;
+  using Resid = std::integral_constant<int, SW_RESID>;
   L1Stage<T> A, B;
   A.reset();
   B.reset();
-  Delay d1{}, d2{};  // node rows f - 1 and f - 2
+  Delay d1{}, d2{};  // node rows f - 1 and f - 2 (all-zero: masked out)
   const int f0 = r0 - 2, f1 = r1 + 1;  // front rows, inclusive
   T rm_prev[4];  // children of element row f - 1
   load_rm(f0 - 1, rm_prev);
@@ -1577,20 +1707,13 @@ __global__ void __launch_bounds__(kQThreads, 4) l1_chain_kernel(
       const int f = fb + k;
       const Front Q = qf[k];
       load_front(f + AHEAD, qf[k]);
-      const bool row_f = col_ok && f >= 0 && f < nny;
       Delay cur;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        cur.b[d] = Q.b[d];
-        cur.dg[d] = Q.dg[d];
-      }
-      cur.fl = Q.fl;
+      delay_of(Q, cur);
       // stage A's input at row f: the first sweep from zero (PRE) or the loaded x0
       T xin[D];
       if constexpr (PRE) {
         const T zero[D] = {T(0), T(0)};
-        result(true, zero, zero, cur, xin);
-        if (!row_f) xin[0] = xin[1] = T(0);
+        result(First{}, zero, zero, cur, xin);
       } else {
 #pragma unroll
         for (int d = 0; d < D; ++d) xin[d] = Q.x[d];
@@ -1602,14 +1725,14 @@ __global__ void __launch_bounds__(kQThreads, 4) l1_chain_kernel(
 #pragma unroll
       for (int d = 0; d < D; ++d) xo_a[d] = A.ut[d];
       A.step(MeA, xin, KA);
-      result(true, KA, xo_a, d1, xa);
-      if (!(col_ok && f - 1 >= 0 && f - 1 < nny)) xa[0] = xa[1] = T(0);
+      result(Sweep{}, KA, xo_a, d1, xa);
       // stage B: element row f - 2 -> the residual (PRE) or a second sweep at node row f - 2
       T KB[D], xbr[D], xo_b[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) xo_b[d] = B.ut[d];
       B.step(MeB, xa, KB);
-      result(!PRE, KB, xo_b, d2, xbr);
+      if constexpr (PRE) result(Resid{}, KB, xo_b, d2, xbr);
+      else result(Sweep{}, KB, xo_b, d2, xbr);
       if (out_lane) {
         if constexpr (PRE) {
           if (f - 1 >= r0 && f - 1 < r1) store_node<D, T>(ox, (long long)(f - 1) * nnx + c, xa);

@@ -205,7 +205,8 @@ long long plan_hierarchy(stt_hier_impl& h, char* base) {
     }
     if (l > 0 || L == 1) {
       lv.st64 = (double*)carve(p, used, 8LL * h.hrows * NS * lv.nnode);
-      if (f32 && l > 0) lv.st32 = (float*)carve(p, used, 4LL * h.hrows * NS * lv.nnode);
+      if (f32 && l > 0)
+        lv.st32 = (float*)carve(p, used, 4LL * h.hrows * (d == 2 ? st32_nsp<2>() : st32_nsp<1>()) * lv.nnode);
     }
   }
   // coarse factor
@@ -546,6 +547,18 @@ struct DensitySource {  // rho_e KE (+ reaction_e I / 4), level 0 used as the co
   }
 };
 
+// The FP32 copy of stencil entry (blk, i, j) of node n in row h (st32 may be null):
+// node-major records of st32_nsp<D>() coefficients, or with diag32 only the centre
+// block's diagonal, [nnode][D], within the same extent.
+template <int D>
+__device__ __forceinline__ void st32_store(float* st32, int h, long long nnode, int n, int blk, int i, int j,
+                                           int diag32, double v) {
+  if (!st32) return;
+  float* s32 = st32 + (size_t)h * st32_nsp<D>() * nnode;
+  if (!diag32) s32[(size_t)n * st32_nsp<D>() + blk * D * D + i * D + j] = (float)v;
+  else if (blk == 0 && i == j) s32[(size_t)n * D + i] = (float)v;
+}
+
 // Symmetric, projected 9-point block stencil from element matrices: block (N, M)
 // sums the (corner N, corner M) blocks of the elements holding both nodes, averaged
 // with the transpose of (M, N) as the reference symmetrises its dense coarse matrix
@@ -608,7 +621,7 @@ __global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int n
         if (((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
         const size_t o = (size_t)(blk * D * D + i * D + j) * nnode;
         out[o] = v;
-        if (st32 && (!diag32 || (blk == 0 && i == j))) st32[(size_t)h * NS * nnode + n + o] = (float)v;
+        st32_store<D>(st32, h, nnode, n, blk, i, j, diag32, v);
       }
   }
 }
@@ -676,7 +689,7 @@ __global__ void __launch_bounds__(256) stencil_children_kernel(
       if (!m_ok || ((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
       const size_t o = (size_t)(blk * DD + q) * nnode;
       out[o] = v;
-      if (st32 && (!diag32 || (blk == 0 && i == j))) st32[(size_t)h * NS * nnode + n + o] = (float)v;
+      st32_store<D>(st32, h, nnode, n, blk, i, j, diag32, v);
     }
   }
 }

@@ -110,7 +110,9 @@ static long long plan_solve(const stt_hier* h, int nrows, int gamma, char* base,
   const LevelDesc& l0 = h->lv[0];
   if (pcg) {
     const dim3 tg = pcg_tile_grid(h->nelx, h->nely, nrows, 8);
-    w.nblk_max = std::max<int>(tg.x * tg.y, ew_blocks(l0.ndof));
+    // the level-0 chained passes' blocks may take the r.z reductions
+    const dim3 pg = postsmooth_grid(h->nelx, h->nely, nrows), qg = presmooth_grid(h->nelx, h->nely, nrows);
+    w.nblk_max = std::max<int>(std::max<int>(tg.x * tg.y, std::max(pg.x * pg.y, qg.x * qg.y)), ew_blocks(l0.ndof));
     w.rs = (RowState*)carve(base, used, sizeof(RowState) * nrows);
     w.partials = (double*)carve(base, used, 8LL * nrows * w.nblk_max * 3);
     w.counters = (unsigned*)carve(base, used, 4LL * nrows);
@@ -153,6 +155,9 @@ struct Cycle {
   MQ<T> mq;
   T* final_out = nullptr;  // where level 0's last sweep writes (row stride vstride(ndof0))
   bool coarse_waited = false;  // the stream has waited for the coarse factorisation
+  RzFuse<T> rzf{};         // the PCG's dots for level 0's chained passes to take (rzf.rst set)
+  bool mix_done = false;   // the pre-smoothing pass took r . z_old
+  bool rz_done = false;    // the post-smoothing pass took r . z and set beta
 
   T* X(int l) const { return (T*)w.x[l]; }
   T* Tt(int l) const { return (T*)w.t[l]; }
@@ -300,12 +305,20 @@ struct Cycle {
     const LevelDesc& lv = h->lv[0];
     const long long nd = vstride(lv.ndof);
     const dim3 g = presmooth_grid(lv.nelx, lv.nely, nrows);
-#define STT_PRE(RD)                                                                                  \
-  l0_presmooth_kernel<D, T, RD><<<g, kQThreads, 0, st>>>(b, b_rs, out_x, nd, out_r, nd, rho0(), lv.rs_rho, \
-                                                       rdiag0(), lv.ndof, lv.fixed, h->row_map, h->hrows,  \
-                                                       rst, lv.nelx, lv.nely, omega, mq)
-    if (h->has_reaction) STT_PRE(true);
-    else STT_PRE(false);
+    RzFuse<T> mx = rzf;
+    mx.red.nblk = (int)(g.x * g.y);
+#define STT_PRE(RD, MX)                                                                                  \
+  l0_presmooth_kernel<D, T, RD, MX><<<g, kQThreads, 0, st>>>(b, b_rs, out_x, nd, out_r, nd, rho0(), lv.rs_rho, \
+                                                           rdiag0(), lv.ndof, lv.fixed, h->row_map, h->hrows,  \
+                                                           rst, lv.nelx, lv.nely, omega, mq, mx)
+    if (rzf.rst && rzf.zold) {
+      if (h->has_reaction) STT_PRE(true, true);
+      else STT_PRE(false, true);
+      mix_done = true;
+    } else {
+      if (h->has_reaction) STT_PRE(true, false);
+      else STT_PRE(false, false);
+    }
 #undef STT_PRE
   }
 
@@ -362,16 +375,26 @@ struct Cycle {
   }
 
   // Level 0's two post-smoothing sweeps in one pass: x0 (the prolonged iterate) -> out.
+  // With rzf set, the pass also takes the PCG's r.z (and r.z_old) from b and what it writes.
   void postsmooth(const T* x0, const T* b, long long b_rs, T* out) {
     const LevelDesc& lv = h->lv[0];
     const long long nd = vstride(lv.ndof);
     const dim3 g = postsmooth_grid(lv.nelx, lv.nely, nrows);
-#define STT_POST(RD)                                                                                  \
-  l0_postsmooth_kernel<D, T, RD><<<g, kQThreads, 0, st>>>(x0, nd, b, b_rs, out, nd, rho0(), lv.rs_rho,     \
-                                                        rdiag0(), lv.ndof, lv.fixed, h->row_map, h->hrows, \
-                                                        rst, lv.nelx, lv.nely, omega, mq)
-    if (h->has_reaction) STT_POST(true);
-    else STT_POST(false);
+    RzFuse<T> rz = rzf;
+    rz.red.nblk = (int)(g.x * g.y);
+    const bool fuse = rzf.rst && (!rzf.zold || mix_done);
+#define STT_POST(RD, RZ)                                                                                  \
+  l0_postsmooth_kernel<D, T, RD, RZ><<<g, kQThreads, 0, st>>>(x0, nd, b, b_rs, out, nd, rho0(), lv.rs_rho,     \
+                                                            rdiag0(), lv.ndof, lv.fixed, h->row_map, h->hrows, \
+                                                            rst, lv.nelx, lv.nely, omega, mq, rz)
+    if (fuse) {
+      if (h->has_reaction) STT_POST(true, true);
+      else STT_POST(false, true);
+      rz_done = true;
+    } else {
+      if (h->has_reaction) STT_POST(true, false);
+      else STT_POST(false, false);
+    }
 #undef STT_POST
   }
 
@@ -852,17 +875,8 @@ __global__ void __launch_bounds__(kEwThreads) pcg_rz_kernel(
     for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n;
          i += (long long)gridDim.x * kEwThreads)
       one(i);
-  grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) {
-    RowState& S = rst[s];
-    if (first) {
-      S.rz = t[0];
-    } else {
-      const double num = flexible ? t[0] - t[1] : t[0];
-      S.beta = safe_div(num, S.rz);
-      S.rz = t[0];
-      if (!isfinite(S.beta)) S.status = STT_ERR_BREAKDOWN;
-    }
-  });
+  grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals,
+                             [&](const double* t) { pcg_rz_finish(rst[s], t, first, flexible); });
 }
 
 
@@ -887,8 +901,10 @@ static KEq<D, T> ke_of(const stt_hier* h) {
 template <int D, typename T>
 static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r, long long r_rs,
                       T* zout, double omega, int n_smooth,
-                      int gamma, const RowState* rst, cudaStream_t st, bool b0_ready = false) {
+                      int gamma, const RowState* rst, cudaStream_t st, bool b0_ready = false,
+                      const RzFuse<T>* rzf = nullptr, bool* rz_done = nullptr) {
   Cycle<D, T> cyc{h, w, nrows, T(omega), n_smooth, gamma, rst, st, ke_of<D, T>(h), mq_cast<T>(h->mq)};
+  if (rzf) cyc.rzf = *rzf;
   const long long n = h->lv[0].ndof, vs = vstride(n);
   const T* b0;
   long long b_rs;
@@ -905,6 +921,7 @@ static int run_vcycle(const stt_hier* h, SolveWS& w, int nrows, const double* r,
   }
   cyc.final_out = zout;
   T* res = cyc.cycle(0, b0, b_rs);
+  if (rz_done) *rz_done = cyc.rz_done;
   if (res != zout)
     rows_convert_kernel<T, T><<<dim3(ew_blocks(n), nrows), kEwThreads, 0, st>>>(res, vs, zout, vs, n, rst);
   return check_launch("vcycle");
@@ -1053,9 +1070,20 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
       pcg_xclear_kernel<<<(nrows + 127) / 128, 128, 0, st>>>(w.rs, nrows);
     };
     bool pending = false;  // the rows still iterating have an x update pending
-    STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st));
     // r . z: the mixed cycle's z carries FP32 rounding, so its dots read the FP32 copy of r
-    // the cycle itself read (written by the update, or by the cycle's own conversion)
+    // the cycle itself read (written by the update, or by the cycle's own conversion).
+    // Level 0's chained passes take them where the cycle runs them (r . z_old beside the
+    // pre-smoothing, r . z as the post-smoothing writes z); otherwise a pass of their own.
+    auto fuse_of = [&](int first) {
+      RzFuse<T> f{};
+      f.rst = w.rs;
+      f.zold = (flexible && !first) ? zold : nullptr;
+      f.zo_rs = vstride(nd);
+      f.red = GridRed{w.partials, w.counters, 0};
+      f.first = first;
+      f.flexible = flexible;
+      return f;
+    };
     auto rz = [&](int first) {
       if constexpr (sizeof(T) == 4)
         pcg_rz_kernel<T, float><<<dim3(rzb, nrows), kEwThreads, 0, st>>>(
@@ -1064,7 +1092,12 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
         pcg_rz_kernel<T, double><<<dim3(ewb, nrows), kEwThreads, 0, st>>>(w.r, z, zold, nullptr, nd, vstride(nd),
                                                                            nd, w.rs, red_ew, first, flexible);
     };
-    rz(1);
+    {
+      const RzFuse<T> f = fuse_of(1);
+      bool done = false;
+      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, false, &f, &done));
+      if (!done) rz(1);
+    }
     int check_every = 1;
     for (it = 1; it <= max_iter; ++it) {
       pp.it = it;
@@ -1107,8 +1140,13 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
         init(x, pp, 1);
       }
       if (flexible) std::swap(z, zold);
-      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced));
-      rz(0);
+      {
+        const RzFuse<T> f = fuse_of(0);
+        bool done = false;
+        STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, r32 && !replaced, &f,
+                                 &done));
+        if (!done) rz(0);
+      }
       STT_TRY(check_launch("pcg iteration"));
       if (it % check_every == 0 || it == max_iter) {
         STT_TRY(pull(true));

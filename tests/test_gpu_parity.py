@@ -316,6 +316,37 @@ def test_cantilever_config_shapes(m):
         assert rel_err(dc.cpu(), g[f"{k}_dc"]) < 5e-9
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_flexible_and_standard_beta_agree(m, precision):
+    """The device PCG with the reference's beta (default) and with the flexible beta
+    (VCycle(flexible=True)): both reach rtol on the true residual and take the same
+    iterations to within one; the mixed solves agree with an FP64 rtol-1e-12 solve to
+    1e-6, and the two FP64 solves with each other to 1e-10 (the cycle is symmetric up to
+    its rounding, so the betas differ only there)."""
+    rng = np.random.default_rng(21)
+    nelx, nely, rows = 256, 128, 6
+    F, mask = O.cantilever_point_load(nelx, nely)
+    x = np.stack([O.smoothed_density(nelx, nely, 40 + k) for k in range(rows)]).reshape(rows, -1)
+    dens = O.simp_density(x, EMIN, EMAX, PENAL)
+    KE, edof = T(O.plane_stress_KE(0.3)), T(O.element_dof_map(nelx, nely), torch.int64)
+    Fr = T(np.tile(F, (rows, 1)) * rng.uniform(0.5, 2.0, (rows, 1)))
+    ref_lv = m.mg.build_hierarchy(T(dens), edof, KE, T(mask, torch.bool), nelx, nely, precision="fp64")
+    ref, _ = m.fem.pcg(ref_lv[0], Fr, m.mg.VCycle(ref_lv), rtol=1e-12, max_iter=400)
+    lv = m.mg.build_hierarchy(T(dens), edof, KE, T(mask, torch.bool), nelx, nely, precision=precision)
+    iters, sol = {}, {}
+    for flexible in (False, True):
+        U, n = m.fem.pcg(lv[0], Fr, m.mg.VCycle(lv, flexible=flexible), rtol=1e-8, max_iter=400)
+        res = (Fr - ref_lv[0](U)).norm(dim=1) / Fr.norm(dim=1)
+        assert float(res.max()) <= 1.5e-8, (flexible, res)
+        if precision == "mixed":
+            err = float(((U - ref).norm(dim=1) / ref.norm(dim=1)).max())
+            assert err < 1e-6, (flexible, err)
+        iters[flexible], sol[flexible] = n, U
+    assert abs(iters[True] - iters[False]) <= 1, iters
+    if precision == "fp64":
+        assert float(((sol[True] - sol[False]).norm(dim=1) / sol[False].norm(dim=1)).max()) < 1e-10
+
+
 def test_retirement_zero_rows_and_nonconvergence(m):
     g = golden("pcg_cases")
     nelx, nely = 18, 12
