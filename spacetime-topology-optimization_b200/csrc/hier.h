@@ -10,6 +10,7 @@
 #pragma once
 
 #include <atomic>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -58,6 +59,11 @@ struct CoarseSync {
   cudaStream_t side = nullptr;
   cudaEvent_t built = nullptr, ready = nullptr;
   std::atomic<int> refs{1};
+  // level 1's FP64 stencil not yet assembled (an FP32 hierarchy swept from the densities
+  // builds only the FP32 diagonal its cycle reads); the first entry point that reads the
+  // FP64 stencil assembles it, under l1_mu.  Shared by the hierarchy's views.
+  std::atomic<int> l1_pending{0};
+  std::mutex l1_mu;
 };
 
 struct stt_hier_impl {
@@ -91,6 +97,8 @@ long long plan_hierarchy(stt_hier_impl& h, char* base);
 
 // The build's device status word (copied to the host) as an STT error code.
 int hier_status_code(int s);
+// Assembles level 1's deferred FP64 stencil (see CoarseSync::l1_pending) before a read of it.
+int ensure_level1_fp64(const stt_hier* h, int level, cudaStream_t st);
 
 }  // namespace stt
 

@@ -956,12 +956,14 @@ __global__ void __launch_bounds__(kQThreads) st_sweep_kernel(
 // 2 shuffles of x plus 3 of products per component (10 for D = 2) instead of a shuffle
 // per coefficient (16), and only the coefficients of the row being emitted are held.
 // AHEAD rows of raw loads (coefficients, rhs, flags, and x one row further) stay in
-// flight.  Modes as st_sweep_kernel, SW_POST excepted.
+// flight.  Modes as st_sweep_kernel, SW_POST excepted.  dcompact: the level keeps only its
+// centre diagonal (FP32, swept from the level-0 densities otherwise), which the first
+// sweep from zero, the one pass that reaches such a level here, reads (st_diag2).
 template <int D, typename T, int MODE, int AHEAD = 1>
 __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
     const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ out, long long vec_rs,
     const T* __restrict__ st, const uint8_t* __restrict__ fixed, int nnx, int nny,
-    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega) {
+    const int* __restrict__ row_map, int hrows, const RowState* __restrict__ rst, T omega, int dcompact = 0) {
   static_assert(MODE != SW_POST, "no folded prolongation on stencil levels");
   constexpr int DD = D * D, NS = 5 * DD;
   constexpr bool KU = MODE != SW_FIRST;
@@ -1002,8 +1004,20 @@ __global__ void __launch_bounds__(kQThreads) st_sweep2_kernel(
     load_x(r + 1, R.xn);
     if (!col_ok || r < 0 || r >= nny) return;
     const long long node = (long long)r * nnx + c;
+    if constexpr (MODE == SW_FIRST && D == 2) {
+      if (dcompact) {
+        T dg[2];
+        st_diag2<T>(st, h, nnode, node, dg);
+        R.co[0] = dg[0];
+        R.co[3] = dg[1];  // (the off-diagonal centre entries stay zero: the first sweep reads none)
+      } else {
 #pragma unroll
-    for (int k = 0; k < NC; ++k) R.co[k] = st_coef<D, T>(sth, nnode, node, k);
+        for (int k = 0; k < NC; ++k) R.co[k] = st_coef<D, T>(sth, nnode, node, k);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; ++k) R.co[k] = st_coef<D, T>(sth, nnode, node, k);
+    }
     if (MODE != SW_APPLY) load_node<D, T>(bs, node, R.b);
     R.fl = __ldg(fixed + node);
   };

@@ -634,8 +634,10 @@ __global__ void stencil_kernel(Src src, const uint8_t* __restrict__ fixed, int n
 // S_m^T KE S_m (the reference averages its coarse matrix with its transpose,
 // torch_mg.py:286).  The table sits in shared memory; a thread per node loads the
 // 4 x NM child densities once and forms its 5 D^2 coefficients, rows and columns of
-// fixed dofs zeroed.  RD adds the reaction's share with its own table.
-template <int D, bool RD, int NM>
+// fixed dofs zeroed.  RD adds the reaction's share with its own table.  DIAG: only the
+// centre block's diagonal, into st32 (a level swept from the level-0 densities reads no
+// other coefficient; st is not written).
+template <int D, bool RD, int NM, bool DIAG = false>
 __global__ void __launch_bounds__(256) stencil_children_kernel(
     const double* __restrict__ rho, long long rho_rs, const double* __restrict__ reac, long long r_rs,
     const double* __restrict__ Wg, int fnelx, int kx, int ky, const uint8_t* __restrict__ fixed, int nelx,
@@ -677,6 +679,9 @@ __global__ void __launch_bounds__(256) stencil_children_kernel(
 #pragma unroll
     for (int q = 0; q < DD; ++q) {
       const int i = q / D, j = q % D;
+      if constexpr (DIAG) {
+        if (blk != 0 || i != j) continue;
+      }
       const double* w = W + (size_t)(blk * DD + q) * 4 * NM;
       double v = 0.0;
 #pragma unroll
@@ -688,7 +693,7 @@ __global__ void __launch_bounds__(256) stencil_children_kernel(
         }
       if (!m_ok || ((fN >> i) & 1) || ((fM >> j) & 1)) v = 0.0;
       const size_t o = (size_t)(blk * DD + q) * nnode;
-      out[o] = v;
+      if constexpr (!DIAG) out[o] = v;
       st32_store<D>(st32, h, nnode, n, blk, i, j, diag32, v);
     }
   }
@@ -1105,19 +1110,37 @@ extern "C" long long stt_hier_workspace_bytes(int d, int nelx, int nely, int hro
 
 // Level 1's stencil: keff[E] = sum_m rho_m G_m (+ reaction), assembled from the level-0
 // densities (level 1's flags must be built).
+// Level 1's stencil from the level-0 densities.  mode 0: the FP64 stencil and the FP32 copy
+// the cycle reads (all of it, or with h->l1 the centre diagonal); mode 1: only that FP32
+// diagonal (an FP32 hierarchy swept from the densities: nothing in its cycle reads the
+// FP64 stencil); mode 2: only the FP64 stencil (assembled on first use after mode 1).
 template <int D>
-static int level1_stencil(stt_hier* h, const double* reaction, long long r_rs, cudaStream_t st) {
+static int level1_stencil(stt_hier* h, const double* reaction, long long r_rs, cudaStream_t st, int mode = 0) {
   const int H = h->hrows;
   const bool f32 = h->precision == STT_FP32;
   const LevelDesc& f = h->lv[0];
   LevelDesc& c = h->lv[1];
   const double* S = h->tables;  // the level 0 -> 1 transition's tables
   const int nm = f.kx * f.ky;
+  float* s32 = (f32 && mode != 2) ? c.st32 : nullptr;
+  if (mode == 1) {
+    if (!(h->l1 && f32 && !reaction && (nm == 4 || nm == 6 || nm == 9)))
+      return set_error(STT_ERR_INVALID, "level-1 diagonal alone: not a level swept from the densities");
+#define STT_CHILD_DG(NM)                                                                                        \
+  stencil_children_kernel<D, false, NM, true><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                         \
+      f.rho64, f.rs_rho, nullptr, 0, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, c.nelx, c.nely, \
+      nullptr, s32, 1)
+    if (nm == 4) STT_CHILD_DG(4);
+    else if (nm == 6) STT_CHILD_DG(6);
+    else STT_CHILD_DG(9);
+#undef STT_CHILD_DG
+    return check_launch("level-1 diagonal");
+  }
   if (nm == 4 || nm == 6 || nm == 9) {
 #define STT_CHILD_ST(RD, NM)                                                                          \
   stencil_children_kernel<D, RD, NM><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(                        \
       f.rho64, f.rs_rho, reaction, r_rs, h->gtables + 2 * kGrandStride, f.nelx, f.kx, f.ky, c.fixed, \
-      c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, h->l1)
+      c.nelx, c.nely, c.st64, s32, h->l1)
     if (reaction) {
       if (nm == 4) STT_CHILD_ST(true, 4);
       else if (nm == 6) STT_CHILD_ST(true, 6);
@@ -1132,7 +1155,7 @@ static int level1_stencil(stt_hier* h, const double* reaction, long long r_rs, c
     stencil_kernel<D, ChildSource<D>><<<dim3(grid1(c.nnode), H), 256, 0, st>>>(
         ChildSource<D>{f.rho64, f.rs_rho, reaction, r_rs, S + kTableStride, S + 2 * kTableStride, f.nelx,
                        f.kx, f.ky, c.nelx},
-        c.fixed, c.nelx, c.nely, c.st64, f32 ? c.st32 : nullptr, 0);
+        c.fixed, c.nelx, c.nely, c.st64, s32, 0);
   }
   return check_launch("level-1 stencil");
 }
@@ -1518,6 +1541,7 @@ static int acquire_sync(CoarseSync** out) {
         CoarseSync* s = g_sync_free[i];
         g_sync_free.erase(g_sync_free.begin() + (long)i);
         s->refs.store(1);
+        s->l1_pending.store(0);
         *out = s;
         return STT_OK;
       }
@@ -1629,9 +1653,15 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   if (rc == STT_OK) rc = check_cuda(cudaStreamWaitEvent(h->sync->side, h->sync->built, 0), "side wait");
   if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, h->sync->side) : build_coarse<1>(h, h->sync->side);
   if (rc == STT_OK) rc = check_cuda(cudaEventRecord(h->sync->ready, h->sync->side), "record coarse");
-  // level 1's stencil (deferred by build_levels) beside the factorisation
-  if (rc == STT_OK && h->nlevels > 2)
-    rc = d == 2 ? level1_stencil<2>(h, reaction, r_rs, st) : level1_stencil<1>(h, reaction, r_rs, st);
+  // level 1's stencil (deferred by build_levels) beside the factorisation; an FP32
+  // hierarchy swept from the densities only its FP32 diagonal, the FP64 stencil on first use
+  if (rc == STT_OK && h->nlevels > 2) {
+    const int nm = h->lv[0].kx * h->lv[0].ky;
+    const bool diag_only = h->l1 && precision == STT_FP32 && !reaction && (nm == 4 || nm == 6 || nm == 9);
+    rc = d == 2 ? level1_stencil<2>(h, reaction, r_rs, st, diag_only ? 1 : 0)
+                : level1_stencil<1>(h, reaction, r_rs, st, diag_only ? 1 : 0);
+    if (rc == STT_OK && diag_only) h->sync->l1_pending.store(1);
+  }
   if (rc != STT_OK) {
     if (h->sync) release_sync(h->sync);
     delete h;
@@ -1640,6 +1670,18 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   // no synchronisation here: the build's device checks (coarse pivots, band) are read by
   // stt_hier_status, and by the first convergence check after a solve's first V-cycle
   *out = h;
+  return STT_OK;
+}
+
+// Level 1's FP64 stencil of an FP32 hierarchy swept from the densities, assembled on the
+// first use (on `st`) by the entry points that read it.
+int stt::ensure_level1_fp64(const stt_hier* h, int level, cudaStream_t st) {
+  if (level != 1 || !h->sync->l1_pending.load()) return STT_OK;
+  std::lock_guard<std::mutex> lock(h->sync->l1_mu);
+  if (!h->sync->l1_pending.load()) return STT_OK;
+  stt_hier* hh = const_cast<stt_hier*>(h);
+  STT_TRY(h->d == 2 ? level1_stencil<2>(hh, nullptr, 0, st, 2) : level1_stencil<1>(hh, nullptr, 0, st, 2));
+  h->sync->l1_pending.store(0);
   return STT_OK;
 }
 
@@ -1711,6 +1753,7 @@ extern "C" int stt_hier_level_diag(const stt_hier* h, int level, double* out, st
     return stt_q4_diag(h->d, h->nelx, h->nely, h->hrows, lv.rho64, lv.rs_rho,
                        h->has_reaction ? lv.rdiag64 : nullptr, lv.ndof,
                        lv.fixed, out, lv.ndof, h->KE, stream);
+  STT_TRY(ensure_level1_fp64(h, level, st));
   if (h->d == 2)
     stencil_diag_kernel<2><<<dim3(grid1(lv.nnode), h->hrows), 256, 0, st>>>(lv.st64, lv.fixed, lv.nnode, out);
   else

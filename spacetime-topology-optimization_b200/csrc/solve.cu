@@ -266,7 +266,8 @@ struct Cycle {
             pro);
       else
         st_sweep2_kernel<D, T, MODE><<<coarse_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
-            x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega);
+            x, b, out, vstride(lv.ndof), stl(l), lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, rst, omega,
+            (sizeof(T) == 4 && l == 1 && h->l1) ? 1 : 0);
     }
   }
 
@@ -1260,6 +1261,7 @@ extern "C" int stt_level_apply(const stt_hier* h, int level, int nrows, const do
   }
   if (v_rs != out_rs)
     return set_error(STT_ERR_INVALID, "stt_level_apply: coarse levels need equal row strides");
+  STT_TRY(ensure_level1_fp64(h, level, st));
   if (h->d == 2)
     st_sweep2_kernel<2, double, SW_APPLY><<<tile_grid(lv.nelx, lv.nely, nrows), kQThreads, 0, st>>>(
         v, nullptr, out, v_rs, lv.st64, lv.fixed, lv.nnx, lv.nny, h->row_map, h->hrows, nullptr, 1.0);

@@ -202,6 +202,41 @@ def test_vcycle_fp32_matches_fp64(m, nelx, nely, mce):
     assert abs(a - b) <= 1e-4 * abs(a)
 
 
+@pytest.mark.parametrize("n_smooth,gamma", [(1, 1), (3, 1), (2, 2)])
+def test_vcycle_fp32_unchained_paths_match_fp64(m, n_smooth, gamma):
+    """Sweep counts and W-cycles that the chained level-0 / level-1 passes do not take:
+    the FP32 cycle runs the separate first sweep, sweeps and residuals, on a level 1 that
+    keeps only its centre diagonal (swept from the level-0 densities); against the FP64
+    cycle with the same n_smooth and gamma, to FP32 rounding."""
+    rng = np.random.default_rng(11)
+    nelx, nely = 128, 64
+    x = rng.uniform(1e-3, 1.0, nelx * nely)
+    F, mask = O.cantilever_point_load(nelx, nely)
+    M64 = m.mg.VCycle(_levels(m, nelx, nely, x, mask, 700), n_smooth=n_smooth, gamma=gamma)
+    M32 = m.mg.VCycle(_levels(m, nelx, nely, x, mask, 700, precision="mixed"), n_smooth=n_smooth, gamma=gamma)
+    u = O.project(rng.standard_normal((3, len(F))), mask)
+    z64, z32 = M64(T(u)).cpu().numpy(), M32(T(u)).cpu().numpy()
+    assert rel_err(z32, z64) < 1e-4
+
+
+def test_mixed_level1_fp64_stencil_assembled_on_first_use(m):
+    """An FP32 hierarchy swept from the level-0 densities builds only level 1's FP32
+    diagonal; its FP64 stencil is assembled by the first entry point that reads it (a
+    view's apply first, then the parent's diagonal) and equals the FP64 hierarchy's."""
+    rng = np.random.default_rng(13)
+    nelx, nely, rows = 96, 48, 3
+    x = rng.uniform(1e-3, 1.0, (rows, nelx * nely))
+    F, mask = O.cantilever_point_load(nelx, nely)
+    lv64, lv32 = (_levels(m, nelx, nely, x, mask, 300, precision=p) for p in ("fp64", "mixed"))
+    assert len(lv32) > 2
+    u = T(O.project(rng.standard_normal((rows, lv32[1].ndof)), lv32[1].mask.cpu().numpy()))
+    sel = torch.tensor([2, 0], device=DEV)
+    got = lv32[1].select(sel)(u[sel])
+    assert rel_err(got.cpu().numpy(), lv64[1](u)[sel].cpu().numpy()) < 1e-13
+    assert rel_err(lv32[1].diag.cpu().numpy(), lv64[1].diag.cpu().numpy()) < 1e-14
+    assert rel_err(lv32[1](u).cpu().numpy(), lv64[1](u).cpu().numpy()) < 1e-13
+
+
 @pytest.mark.parametrize("kx,ky,d", [(2, 2, 2), (3, 2, 2), (2, 3, 1), (3, 3, 1), (1, 2, 2)])
 def test_grid_transfer_helpers_match_oracle_and_are_adjoint(m, kx, ky, d):
     """torch_mg._on_node_grid with _interp_axis / _restrict_axis (stt_grid_transfer) against
