@@ -58,7 +58,11 @@ struct CoarseSync {
   int device = 0;
   cudaStream_t side = nullptr;
   cudaEvent_t built = nullptr, ready = nullptr;
+  cudaEvent_t factored = nullptr;  // the band factor is done (the inverse may still run)
   std::atomic<int> refs{1};
+  // an FP32 hierarchy's first coarse solve takes the block solves, which need only the
+  // factor, so it does not wait for the explicit inverse (set at the build, taken once)
+  std::atomic<int> first_cycle{0};
   // level 1's FP64 stencil not yet assembled (an FP32 hierarchy swept from the densities
   // builds only the FP32 diagonal its cycle reads); the first entry point that reads the
   // FP64 stencil assembles it, under l1_mu.  Shared by the hierarchy's views.

@@ -1542,6 +1542,7 @@ static int acquire_sync(CoarseSync** out) {
         g_sync_free.erase(g_sync_free.begin() + (long)i);
         s->refs.store(1);
         s->l1_pending.store(0);
+        s->first_cycle.store(0);
         *out = s;
         return STT_OK;
       }
@@ -1553,7 +1554,9 @@ static int acquire_sync(CoarseSync** out) {
   if (rc == STT_OK) rc = check_cuda(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi), "side stream");
   if (rc == STT_OK) rc = check_cuda(cudaEventCreateWithFlags(&s->built, cudaEventDisableTiming), "event");
   if (rc == STT_OK) rc = check_cuda(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event");
+  if (rc == STT_OK) rc = check_cuda(cudaEventCreateWithFlags(&s->factored, cudaEventDisableTiming), "event");
   if (rc != STT_OK) {
+    if (s->factored) cudaEventDestroy(s->factored);
     if (s->ready) cudaEventDestroy(s->ready);
     if (s->built) cudaEventDestroy(s->built);
     if (s->side) cudaStreamDestroy(s->side);
@@ -1594,6 +1597,7 @@ static int build_coarse(stt_hier* h, cudaStream_t st) {
   else
     band_factor_kernel<<<H, 256, smem, st>>>(co.blocks, co.B, co.nb, h->status);
   STT_TRY(check_launch("band factor"));
+  STT_TRY(check_cuda(cudaEventRecord(h->sync->factored, st), "record factor"));
   if (co.inv) {
     if (co.B == 32 || co.B == 64) {
       const size_t tsm = (size_t)3 * co.B * (co.B + 1) * sizeof(double);
@@ -1653,6 +1657,7 @@ extern "C" int stt_hier_create(stt_hier** out, void* workspace, long long ws_byt
   if (rc == STT_OK) rc = check_cuda(cudaStreamWaitEvent(h->sync->side, h->sync->built, 0), "side wait");
   if (rc == STT_OK) rc = d == 2 ? build_coarse<2>(h, h->sync->side) : build_coarse<1>(h, h->sync->side);
   if (rc == STT_OK) rc = check_cuda(cudaEventRecord(h->sync->ready, h->sync->side), "record coarse");
+  if (rc == STT_OK) h->sync->first_cycle.store(h->co.inv ? 1 : 0);
   // level 1's stencil (deferred by build_levels) beside the factorisation; an FP32
   // hierarchy swept from the densities only its FP32 diagonal, the FP64 stencil on first use
   if (rc == STT_OK && h->nlevels > 2) {

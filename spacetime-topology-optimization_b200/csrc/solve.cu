@@ -154,7 +154,8 @@ struct Cycle {
   KEq<D, T> ke;
   MQ<T> mq;
   T* final_out = nullptr;  // where level 0's last sweep writes (row stride vstride(ndof0))
-  bool coarse_waited = false;  // the stream has waited for the coarse factorisation
+  bool waited_factor = false;  // the stream has waited for the coarse factorisation
+  bool waited_ready = false;   // ... and for the explicit inverse
   RzFuse<T> rzf{};         // the PCG's dots for level 0's chained passes to take (rzf.rst set)
   bool mix_done = false;   // the pre-smoothing pass took r . z_old
   bool rz_done = false;    // the post-smoothing pass took r . z and set beta
@@ -271,14 +272,23 @@ struct Cycle {
     }
   }
 
+  // The factorisation (and an FP32 hierarchy's explicit inverse after it) runs on the
+  // hierarchy's side stream.  The first coarse solve on a fresh FP32 hierarchy takes the
+  // block solves, which need only the factor, so the first cycle does not wait for the
+  // inverse; every later one takes the inverse's GEMV (equal to FP64 rounding).
   void coarse(int l, const T* b, T* x) {
     const LevelDesc& lv = h->lv[l];
     const CoarseDesc& co = h->co;
-    if (!coarse_waited) {  // the factorisation runs on the hierarchy's side stream
+    bool use_inv = sizeof(T) == 4 && co.inv;
+    if (use_inv && h->sync->first_cycle.load() && h->sync->first_cycle.exchange(0) == 1) use_inv = false;
+    if (use_inv && !waited_ready) {
       cudaStreamWaitEvent(st, h->sync->ready, 0);
-      coarse_waited = true;
+      waited_ready = waited_factor = true;
+    } else if (!use_inv && !waited_factor) {
+      cudaStreamWaitEvent(st, h->sync->factored, 0);
+      waited_factor = true;
     }
-    if (sizeof(T) == 4 && co.inv) {
+    if (use_inv) {
       const int np = co.nb * co.B;
       coarse_inv_solve_kernel<D, T><<<dim3((np + kInvRowsPerCta - 1) / kInvRowsPerCta, nrows), 256,
                                       sizeof(double) * np, st>>>(b, x, vstride(lv.ndof), co.inv, np, co.by_col,

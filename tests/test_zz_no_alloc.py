@@ -48,23 +48,27 @@ def test_vcycle_noalloc_matches_the_workspace_entry_point(pkg):
 
     lib = _lib.lib()
     for precision in ("fp64", "mixed"):
-        levels, r = _hierarchy(48, 36, 3, precision, 5)
+        # the workspace entry point on a workspace of NaN bytes against one of zeros, on two
+        # identical hierarchies: no word is read unwritten.  Two cycles each, as an FP32
+        # hierarchy's first coarse solve takes the block solves and later ones its inverse.
+        (levels, r), (twin, _) = _hierarchy(48, 36, 3, precision, 5), _hierarchy(48, 36, 3, precision, 5)
         h, n = levels[0]._hier, levels[0].ndof
-        # the workspace entry point on a workspace of NaN bytes: no word is read unwritten
-        ws = _lib.workspace(lib.stt_vcycle_workspace_bytes(h.handle, 3, 1), r.device)
-        ws.fill_(255)
-        z_ref = torch.empty_like(r)
-        _lib.check(lib.stt_vcycle(h.handle, 3, _lib.ptr(r), n, _lib.ptr(z_ref), n, 0.6, 2, 1,
-                                  _lib.ptr(ws), ws.numel(), _lib.stream()))
+        outs = {}
+        for key, hh, fill in (("nan", h, 255), ("zero", twin[0]._hier, 0)):
+            ws = _lib.workspace(lib.stt_vcycle_workspace_bytes(hh.handle, 3, 1), r.device)
+            ws.fill_(fill)
+            zs = []
+            for _ in range(2):
+                z = torch.empty_like(r)
+                _lib.check(lib.stt_vcycle(hh.handle, 3, _lib.ptr(r), n, _lib.ptr(z), n, 0.6, 2, 1,
+                                          _lib.ptr(ws), ws.numel(), _lib.stream()))
+                zs.append(z)
+            outs[key] = zs
         torch.cuda.synchronize()
-        assert torch.isfinite(z_ref).all()
-        ws2 = _lib.workspace(lib.stt_vcycle_workspace_bytes(h.handle, 3, 1), r.device)
-        ws2.zero_()
-        z_zero = torch.empty_like(r)
-        _lib.check(lib.stt_vcycle(h.handle, 3, _lib.ptr(r), n, _lib.ptr(z_zero), n, 0.6, 2, 1,
-                                  _lib.ptr(ws2), ws2.numel(), _lib.stream()))
-        torch.cuda.synchronize()
-        assert torch.equal(z_ref, z_zero)
+        for k in range(2):
+            assert torch.isfinite(outs["nan"][k]).all()
+            assert torch.equal(outs["nan"][k], outs["zero"][k])
+        z_ref = outs["nan"][1]
         # a larger hierarchy with a NaN residual fills the shared scratch with NaN first
         big, rb = _hierarchy(160, 96, 4, precision, 6)
         hb, nb = big[0]._hier, big[0].ndof
