@@ -929,6 +929,7 @@ __global__ void __launch_bounds__(256) band_factor_tiled_kernel(double* __restri
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   double* bh = blocks + (size_t)blockIdx.x * nb * 4 * B * B;
   __shared__ int bad;
+  __shared__ double rp[B];  // reciprocals of the current block's pivots
   if (tid == 0) bad = 0;
   auto stage = [&](double* dst, const double* src) {
     for (int t = tid; t < B * B / 2; t += 256) cp_async16(dst + 2 * t, src + 2 * t);
@@ -975,52 +976,87 @@ __global__ void __launch_bounds__(256) band_factor_tiled_kernel(double* __restri
       stage(P1, Dn + (size_t)2 * B * B);  // A_{k+1,k}
       cp_async_commit();
     }
-    // Cholesky, columns j and j + 1 per step
-    for (int j = 0; j < B; j += 2) {
-      const double p0 = A[j * ld + j];
-      const double piv0 = sqrt(p0 > 0.0 ? p0 : 1.0), r0 = 1.0 / piv0;
-      const double c1 = A[(j + 1) * ld + j] * r0;  // scaled (j + 1, j)
-      const double p1 = A[(j + 1) * ld + j + 1] - c1 * c1;
-      const double piv1 = sqrt(p1 > 0.0 ? p1 : 1.0), r1 = 1.0 / piv1;
-      double ci[NA], di[NA], cl[NA], dl[NA];
+    // Cholesky, a panel of four columns per step: every thread factors the 4 x 4 pivot
+    // block (one rsqrt a pivot, L_jj = t rsqrt(t), its reciprocal kept for the
+    // substitution), then the panel entries of its rows and a rank-4 update
+    for (int j = 0; j < B; j += 4) {
+      double a[4][4];
 #pragma unroll
-      for (int a = 0; a < NA; ++a) {
-        const int i = ty + 16 * a;
-        const double c = i > j ? A[i * ld + j] * r0 : 0.0;
-        ci[a] = c;
-        di[a] = i > j + 1 ? (A[i * ld + j + 1] - c * c1) * r1 : 0.0;
-      }
+      for (int p = 0; p < 4; ++p)
 #pragma unroll
-      for (int b = 0; b < NA; ++b) {
-        const int l = tx + 16 * b;
-        const double c = l > j ? A[l * ld + j] * r0 : 0.0;
-        cl[b] = c;
-        dl[b] = l > j + 1 ? (A[l * ld + j + 1] - c * c1) * r1 : 0.0;
+        for (int q = 0; q <= p; ++q) a[p][q] = A[(j + p) * ld + j + q];
+      double l[4][4], r[4];
+      bool ok = true;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double t = a[q][q];
+#pragma unroll
+        for (int m = 0; m < q; ++m) t = fma(-l[q][m], l[q][m], t);
+        ok = ok && t > 0.0;
+        const double tt = t > 0.0 ? t : 1.0;
+        r[q] = rsqrt(tt);
+        l[q][q] = tt * r[q];
+#pragma unroll
+        for (int p = q + 1; p < 4; ++p) {
+          double v = a[p][q];
+#pragma unroll
+          for (int m = 0; m < q; ++m) v = fma(-l[p][m], l[q][m], v);
+          l[p][q] = v * r[q];
+        }
       }
+      // the panel columns of rows i (this thread's rows) and of rows c (its columns)
+      auto panel = [&](int i, double (&cv)[4]) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          double v = 0.0;
+          if (i > j + q) {
+            v = A[i * ld + j + q];
+#pragma unroll
+            for (int m = 0; m < q; ++m) v = fma(-cv[m], l[q][m], v);
+            v *= r[q];
+          }
+          cv[q] = v;
+        }
+      };
+      double ci[NA][4], cl[NA][4];
+#pragma unroll
+      for (int a2 = 0; a2 < NA; ++a2) panel(ty + 16 * a2, ci[a2]);
+#pragma unroll
+      for (int b = 0; b < NA; ++b) panel(tx + 16 * b, cl[b]);
       __syncthreads();
       if (tx == 0) {
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-          const int i = ty + 16 * a;
-          if (i > j) A[i * ld + j] = ci[a];
-          if (i > j + 1) A[i * ld + j + 1] = di[a];
+        for (int a2 = 0; a2 < NA; ++a2) {
+          const int i = ty + 16 * a2;
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (i > j + q) A[i * ld + j + q] = ci[a2][q];
         }
       }
       if (tid == 0) {
-        if (!(p0 > 0.0) || !(p1 > 0.0)) bad = 1;
-        A[j * ld + j] = piv0;
-        A[(j + 1) * ld + j + 1] = piv1;
+        if (!ok) bad = 1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          A[(j + q) * ld + j + q] = l[q][q];
+          rp[j + q] = r[q];
+        }
       }
 #pragma unroll
-      for (int a = 0; a < NA; ++a)
+      for (int a2 = 0; a2 < NA; ++a2)
 #pragma unroll
         for (int b = 0; b < NA; ++b) {
-          const int i = ty + 16 * a, l = tx + 16 * b;
-          if (i > j + 1 && l > j + 1) A[i * ld + l] = fma(-di[a], dl[b], fma(-ci[a], cl[b], A[i * ld + l]));
+          const int i = ty + 16 * a2, c = tx + 16 * b;
+          if (i > j + 3 && c > j + 3) {
+            double v = A[i * ld + c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v = fma(-ci[a2][q], cl[b][q], v);
+            A[i * ld + c] = v;
+          }
         }
       __syncthreads();
     }
-    // X = A^{-1}: forward substitution, a quad of threads per column (as band_factor_kernel)
+    // X = A^{-1}: forward substitution with the pivots' reciprocals, a quad of threads a
+    // column, each thread's share of a dot product in two independent chains
     {
       const int q = tid & 3;
       for (int c0 = 0; c0 < B; c0 += 64) {
@@ -1028,16 +1064,23 @@ __global__ void __launch_bounds__(256) band_factor_tiled_kernel(double* __restri
         const bool col = c < B;
         if (col && q == 0) {
           for (int i = 0; i < c; ++i) X[i * ld + c] = 0.0;
-          X[c * ld + c] = 1.0 / A[c * ld + c];
+          X[c * ld + c] = rp[c];
         }
         __syncwarp();
         for (int i = c0 + 1; i < B; ++i) {
-          double sacc = 0.0;
-          if (col && i > c)
-            for (int l = c + q; l < i; l += 4) sacc = fma(A[i * ld + l], X[l * ld + c], sacc);
+          double s0 = 0.0, s1 = 0.0;
+          if (col && i > c) {
+            int l2 = c + q;
+            for (; l2 + 4 < i; l2 += 8) {
+              s0 = fma(A[i * ld + l2], X[l2 * ld + c], s0);
+              s1 = fma(A[i * ld + l2 + 4], X[(l2 + 4) * ld + c], s1);
+            }
+            if (l2 < i) s0 = fma(A[i * ld + l2], X[l2 * ld + c], s0);
+          }
+          double sacc = s0 + s1;
           sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
           sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
-          if (col && i > c && q == 0) X[i * ld + c] = -sacc / A[i * ld + i];
+          if (col && i > c && q == 0) X[i * ld + c] = -sacc * rp[i];
           __syncwarp();
         }
       }
