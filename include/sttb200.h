@@ -32,6 +32,8 @@
  *   stt_stage_glue_*    sttopt/compliance.py:33-46 (time_mask), :137-161 (_gravity_load),
  *                       :164-253 (gravity_compliance, batched_whole_and_gravity_compliance)
  *   stt_lumped_reaction_adjoint  sttopt/torch_fem.py:117-132 (lumped_reaction's gradient)
+ *   stt_q4_apply_dots, stt_adjoint_warm_start  sttopt/torch_solve.py:117-140 (FemSolve.backward:
+ *                       the adjoint load and its warm start alpha U, alpha = (U.g)/(U.F))
  *   stt_heat_*          sttopt/virtual_heat.py:162-166,189-201,404-462
  */
 #ifndef STTB200_H
@@ -72,6 +74,22 @@ int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
                  const void* u, long long u_rs, void* out, long long out_rs,
                  const void* rho, long long rho_rs, const void* rdiag, long long rdiag_rs,
                  const uint8_t* fixed, int flags, const double* KE, stt_stream_t stream);
+
+/* out[s] = P K(rho[s]) u[s] (FP64, fixed dofs zeroed; u projected already) and in the same
+ * pass dots[s][0] = u[s] . out[s], dots[s][1] = u[s] . f[s]: an adjoint load (KE = 2 KE
+ * gives dL/dU = 2 K U) with its warm-start factor's dots, one pass over u.  The dots are
+ * reduced in a fixed order through ws (stt_q4_apply_dots_workspace_bytes; 256-byte
+ * aligned; its counters are reset on the stream).  Any KE (modal or the 8 x 8 product). */
+long long stt_q4_apply_dots_workspace_bytes(int nelx, int nely, int nrows);
+int stt_q4_apply_dots(int d, int nelx, int nely, int nrows, const double* u, long long u_rs,
+                      double* out, long long out_rs, const double* rho, long long rho_rs,
+                      const uint8_t* fixed, const double* KE, const double* f, long long f_rs,
+                      double* dots, void* ws, long long ws_bytes, stt_stream_t stream);
+
+/* out[s] = safe_div(dots[s][0], dots[s][1]) v[s] (FP64, dots [nrows][2] as written by
+ * stt_q4_apply_dots): the adjoint's warm start alpha U, alpha = (U . g) / (U . F). */
+int stt_adjoint_warm_start(int nrows, long long n, const double* dots, const double* v, long long v_rs,
+                           double* out, long long o_rs, stt_stream_t stream);
 
 /* The adjoint of stt_lumped_reaction: out[s][e] = (1/4) sum over e's 4 corners and their
  * d dofs of g[s].  FP64. */

@@ -43,6 +43,10 @@ _SIGS = {
     "stt_q4_diag": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _p, _c_ll, _pd, _p]),
     "stt_lumped_reaction": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
     "stt_lumped_reaction_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_q4_apply_dots_workspace_bytes": (_c_ll, [_c_int, _c_int, _c_int]),
+    "stt_q4_apply_dots": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _c_ll, _p, _pd, _p,
+                                   _c_ll, _p, _p, _c_ll, _p]),
+    "stt_adjoint_warm_start": (_c_int, [_c_int, _c_ll, _p, _p, _c_ll, _p, _c_ll, _p]),
     "stt_stage_glue_rows": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p,
                                      _c_double, _c_double, _c_double, _p, _p, _p, _p]),
     "stt_stage_glue_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p, _p,

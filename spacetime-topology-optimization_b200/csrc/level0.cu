@@ -1,4 +1,5 @@
 // Level-0 operator entry points: K(rho) u (projected or not), diag(K), lumped reaction.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -81,6 +82,71 @@ __global__ void __launch_bounds__(kQThreads) q4_apply_modal_kernel(
         }
         store_node<D, T>(outr, node, acc);
       });
+}
+
+// out = K(rho) u with the fixed dofs zeroed (FP64), and per row the dots u . out and
+// u . f taken in the same pass (f read beside the output node), reduced over the blocks
+// in a fixed order (grid_reduce): one pass over u for an adjoint load and its warm-start
+// factor (torch_solve.py:121-126).  MODAL: KE in modal form, else the 8 x 8 product.
+template <int D, bool MODAL>
+__global__ void __launch_bounds__(kQThreads) q4_apply_dots_kernel(
+    const double* __restrict__ u, long long u_rs, double* __restrict__ out, long long out_rs,
+    const double* __restrict__ rho, long long rho_rs, const uint8_t* __restrict__ fixed,
+    const double* __restrict__ f, long long f_rs, double* __restrict__ dots, GridRed red, int nelx, int nely,
+    KEq<D, double> ke, MQ<double> mq) {
+  const int nnx = nelx + 1, nny = nely + 1;
+  const int row = blockIdx.z;
+  const double* ur = u + (size_t)row * u_rs;
+  const double* rr = rho + (size_t)row * rho_rs;
+  const double* fr = f + (size_t)row * f_rs;
+  double* outr = out + (size_t)row * out_rs;
+  double vals[2] = {0.0, 0.0};
+  auto finish = [&](int r, int c, double(&acc)[D], const double(&uc)[D], const RhsX<D, double>& ex) {
+    const int node = r * nnx + c;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      if ((ex.fl >> i) & 1) acc[i] = 0.0;
+      vals[0] = fma(uc[i], acc[i], vals[0]);
+      vals[1] = fma(uc[i], ex.b[i], vals[1]);
+    }
+    store_node<D, double>(outr, node, acc);
+  };
+  auto loadx = [&](int r, int c) {
+    RhsX<D, double> e;
+    const int node = r * nnx + c;
+    load_node<D, double>(fr, node, e.b);
+    e.fl = __ldg(fixed + node);
+    return e;
+  };
+  auto loadr = [&](int r, int c) { return __ldg(rr + (size_t)r * nelx + c); };
+  if constexpr (MODAL) {
+    march_modal<D, double, true, false, false, RhsX<D, double>>(
+        mq, nnx, nny, [&](int r, int c) -> uint8_t { return __ldg(fixed + r * nnx + c); },
+        [&](int r, int c, uint8_t, double(&v)[D]) { load_node<D, double>(ur, r * nnx + c, v); }, loadr, loadx,
+        [&](int r, int c, double(&acc)[D], double(&)[D], const double(&uc)[D], uint8_t,
+            const RhsX<D, double>& ex) { finish(r, c, acc, uc, ex); });
+  } else {
+    march<D, double, true, false, RhsX<D, double>>(
+        ke, nnx, nny, [&](int r, int c, double(&v)[D]) { load_node<D, double>(ur, r * nnx + c, v); }, loadr,
+        loadx, [&](int r, int c, double(&acc)[D], double(&)[D], const double(&uc)[D],
+                   const RhsX<D, double>& ex) { finish(r, c, acc, uc, ex); });
+  }
+  grid_reduce<2, kQThreads>(red, row, blockIdx.y * gridDim.x + blockIdx.x, vals, [&](const double* t) {
+    dots[(size_t)row * 2] = t[0];
+    dots[(size_t)row * 2 + 1] = t[1];
+  });
+}
+
+// out[s] = safe_div(dots[s][0], dots[s][1]) v[s]: the adjoint's warm start alpha U with
+// alpha = (U . g) / (U . F) (torch_solve.py:121-126), written where the solve starts.
+__global__ void rows_warm_start_kernel(long long n, const double* __restrict__ dots, const double* __restrict__ v,
+                                       long long v_rs, double* __restrict__ out, long long o_rs) {
+  const int s = blockIdx.y;
+  const double a = safe_div(dots[(size_t)s * 2], dots[(size_t)s * 2 + 1]);
+  const double* vs = v + (size_t)s * v_rs;
+  double* os = out + (size_t)s * o_rs;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    os[i] = a * vs[i];
 }
 
 template <int D>
@@ -192,6 +258,53 @@ extern "C" int stt_q4_apply(int precision, int d, int nelx, int nely, int nrows,
     if (d == 1) return launch_apply<1, float>(nelx, nely, nrows, u, u_rs, out, out_rs, rho, rho_rs, rdiag, rdiag_rs, fixed, flags, KE, st);
   }
   return set_error(STT_ERR_INVALID, "stt_q4_apply: d must be 1 or 2, precision FP64 or FP32");
+}
+
+extern "C" long long stt_q4_apply_dots_workspace_bytes(int nelx, int nely, int nrows) {
+  if (nelx <= 0 || nely <= 0 || nrows <= 0) return 0;
+  const dim3 g = q4_grid(nelx, nely, nrows);
+  const long long partials = 16LL * nrows * g.x * g.y;  // two doubles a block and row
+  return ((partials + 255) & ~255LL) + ((4LL * nrows + 255) & ~255LL);
+}
+
+extern "C" int stt_q4_apply_dots(int d, int nelx, int nely, int nrows, const double* u, long long u_rs,
+                                 double* out, long long out_rs, const double* rho, long long rho_rs,
+                                 const uint8_t* fixed, const double* KE, const double* f, long long f_rs,
+                                 double* dots, void* ws, long long ws_bytes, stt_stream_t stream) {
+  if (nelx <= 0 || nely <= 0 || nrows <= 0 || nrows > 65535 || !u || !out || !rho || !fixed || !KE || !f ||
+      !dots || !ws || (d != 1 && d != 2))
+    return set_error(STT_ERR_INVALID, "stt_q4_apply_dots: bad sizes or null pointer");
+  if (ws_bytes < stt_q4_apply_dots_workspace_bytes(nelx, nely, nrows) || ((uintptr_t)ws & 255) != 0)
+    return set_error(STT_ERR_WORKSPACE, "stt_q4_apply_dots: workspace too small or not 256-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  const dim3 grid = q4_grid(nelx, nely, nrows);
+  const long long partials = 16LL * nrows * grid.x * grid.y;
+  GridRed red{(double*)ws, (unsigned*)((char*)ws + ((partials + 255) & ~255LL)), (int)(grid.x * grid.y)};
+  STT_TRY(check_cuda(cudaMemsetAsync(red.counters, 0, 4LL * nrows, st), "memset counters"));
+  double m[8];
+  const bool modal = modal_from_ke(d, KE, m);
+  const MQ<double> mq = mq_cast<double>(m);
+#define STT_APD(D, MODAL)                                                                                    \
+  q4_apply_dots_kernel<D, MODAL><<<grid, kQThreads, 0, st>>>(u, u_rs, out, out_rs, rho, rho_rs, fixed, f, f_rs, \
+                                                             dots, red, nelx, nely, make_ke<D, double>(KE), mq)
+  if (d == 2) {
+    if (modal) STT_APD(2, true);
+    else STT_APD(2, false);
+  } else {
+    if (modal) STT_APD(1, true);
+    else STT_APD(1, false);
+  }
+#undef STT_APD
+  return check_launch("q4_apply_dots");
+}
+
+extern "C" int stt_adjoint_warm_start(int nrows, long long n, const double* dots, const double* v, long long v_rs,
+                                      double* out, long long o_rs, stt_stream_t stream) {
+  if (nrows <= 0 || nrows > 65535 || n <= 0 || !dots || !v || !out)
+    return set_error(STT_ERR_INVALID, "stt_adjoint_warm_start: bad arguments");
+  const long long bx = std::min<long long>((n + 255) / 256, 4LL * 148 * 4 / nrows + 1);
+  rows_warm_start_kernel<<<dim3((unsigned)bx, nrows), 256, 0, (cudaStream_t)stream>>>(n, dots, v, v_rs, out, o_rs);
+  return check_launch("adjoint_warm_start");
 }
 
 extern "C" int stt_set_element_form(int form) {

@@ -79,10 +79,16 @@ class SpaceTimeProblem:
         return s
 
 
-def _pcg(levels, b, x0, rtol, max_iter, info_key, info):
+def _pcg(levels, b, x0, rtol, max_iter, info_key, info, x0_inplace=False):
+    """The device MG-PCG solve (``x0_inplace``: the warm start's own buffer becomes the
+    solution, for the package's warm starts)."""
     M = torch_mg.VCycle(levels)
     sub = {}
-    x, n = torch_fem.pcg(levels[0], b, M, rtol=rtol, max_iter=max_iter, x0=x0, info=sub)
+    out = levels[0]._native_pcg(b, M, rtol=rtol, max_iter=max_iter, x0=x0, info=sub,
+                                x0_inplace=x0_inplace) if x0_inplace else None
+    if out is None:
+        out = torch_fem.pcg(levels[0], b, M, rtol=rtol, max_iter=max_iter, x0=x0, info=sub)
+    x, n = out
     if info is not None:
         info[info_key] = n
     return x
@@ -502,8 +508,8 @@ def _stage_work(P: SpaceTimeProblem, X: Tensor, W: Tensor, tPhys: Tensor, heat_a
             stage_levels.append(sl)
         U = torch.stack(Us)
     ce = torch_fem.element_terms(U, P.edof, P.KE)["ce"]
-    c_s = (rho * ce).sum(-1)
-    J_t = (W * tPhys).sum(-1)
+    c_s = torch_fem._dots(rho, ce)
+    J_t = (W * tPhys).sum(-1)  # (G rows of nel: one row is too small for the cluster dot kernel)
     outs = []
     for g in range(G):
         a, b = offs[g], offs[g + 1]
@@ -513,20 +519,20 @@ def _stage_work(P: SpaceTimeProblem, X: Tensor, W: Tensor, tPhys: Tensor, heat_a
     if not gradient:
         return outs
 
-    # 5a. stage adjoints: dL/dU = 2 K U (one apply with 2 KE); warm start alpha U
-    # (exact for compliance)
+    # 5a. stage adjoints: dL/dU = 2 K U (one apply with 2 KE), with the warm-start factor's
+    # dots U . gK and U . F in the same pass over U; the warm start alpha U (exact for
+    # compliance) is written where the adjoint solve starts
     gK = torch.empty_like(U)
-    _lib.check(L.stt_q4_apply(_lib.STT_FP64, 2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK),
-                              2 * nnode, _lib.ptr(rho), nel, None, 0, _lib.ptr(P.fixed2),
-                              _lib.STT_PROJECT_OUT, P.ke2, st))
-    # U . gK and U . F in one pass over U
     d2 = torch.empty(S, 2, dtype=torch.float64, device=dev)
-    _lib.check(L.stt_vec_dots(S, 2 * nnode, _lib.ptr(U), _lib.ptr(gK), _lib.ptr(U), _lib.ptr(F), None, None,
-                              2 * nnode, _lib.ptr(d2), st))
-    a_ = torch_fem.safe_div(d2[:, 0], d2[:, 1])
-    x0 = (a_[:, None] * U).contiguous()
+    ws = _lib.workspace(L.stt_q4_apply_dots_workspace_bytes(nelx, nely, S), dev)
+    _lib.check(L.stt_q4_apply_dots(2, nelx, nely, S, _lib.ptr(U), 2 * nnode, _lib.ptr(gK), 2 * nnode,
+                                   _lib.ptr(rho), nel, _lib.ptr(P.fixed2), P.ke2, _lib.ptr(F), 2 * nnode,
+                                   _lib.ptr(d2), _lib.ptr(ws), ws.numel(), st))
+    x0 = torch.empty_like(U)
+    _lib.check(L.stt_adjoint_warm_start(S, 2 * nnode, _lib.ptr(d2), _lib.ptr(U), 2 * nnode, _lib.ptr(x0),
+                                        2 * nnode, st))
     if batched:
-        lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info)
+        lam = _pcg(stage_levels[0], gK, x0, rtol, max_iter, "adjoint_n_iter", info, x0_inplace=True)
     else:
         lam = torch.stack([_pcg(stage_levels[s], gK[s], x0[s], rtol, max_iter, f"adjoint{s}_n_iter", info)
                            for s in range(S)])

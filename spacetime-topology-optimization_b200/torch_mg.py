@@ -213,17 +213,23 @@ class _Level:
         lv._mask = self._mask
         return lv
 
-    def _native_pcg(self, b: Tensor, M: "VCycle", *, rtol, max_iter, x0, info):
-        """The whole MG-PCG solve on the device when ``M`` cycles this hierarchy."""
+    def _native_pcg(self, b: Tensor, M: "VCycle", *, rtol, max_iter, x0, info, x0_inplace: bool = False):
+        """The whole MG-PCG solve on the device when ``M`` cycles this hierarchy.
+        ``x0_inplace``: ``x0`` (contiguous FP64 rows of this solve's shape) becomes the
+        solution buffer instead of being copied (for the package's own warm starts)."""
         h = self._hier
         if self._index != 0 or M._is_vcycle_of is not h or b.ndim > 2:
             return None
         _lib.require_cuda(b, x0)
         flat, rows, batch = _rows_for(h, b.detach().to(torch.float64))
         n = self.ndof
-        x = torch.empty_like(flat)
-        if x0 is not None:
-            x.copy_(x0.detach().to(torch.float64).expand(*batch, n).reshape(-1, n))
+        if (x0_inplace and x0 is not None and x0.dtype == torch.float64 and x0.is_contiguous()
+                and x0.numel() == flat.numel() and x0.device == flat.device):
+            x = x0.detach().view(-1, n)
+        else:
+            x = torch.empty_like(flat)
+            if x0 is not None:
+                x.copy_(x0.detach().to(torch.float64).expand(*batch, n).reshape(-1, n))
         autotune.apply(h, flat, rows, n, M.gamma, M.omega, M.n_smooth)
         nbytes = _lib.lib().stt_solve_workspace_bytes(h.handle, rows, M.gamma)
         ws = _lib.workspace(nbytes, flat.device)
