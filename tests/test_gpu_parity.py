@@ -149,6 +149,29 @@ def test_coarse_levels_are_exact_galerkin(m):
         assert rel_err(lv(T(v)).cpu(), olv(v)) < 1e-12, i
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_two_by_two_hierarchy_is_exact_galerkin(m, precision):
+    """2 x 2 coarsening on every level (64x32 -> 4x2, five levels: level 1 from the
+    densities, level 2 from its grandchildren, levels 3-4 by Galerkin products): every
+    level's FP64 apply equals the oracle's R A P of the level above to 1e-12, and the
+    mixed hierarchy's FP32 cycle the FP64 one to FP32 rounding."""
+    rng = np.random.default_rng(17)
+    nelx, nely = 64, 32
+    x = rng.uniform(1e-3, 1.0, nelx * nely)
+    F, mask = O.cantilever_point_load(nelx, nely)
+    levels = _levels(m, nelx, nely, x, mask, 8, precision=precision)
+    assert [(lv.nelx, lv.nely) for lv in levels] == [(64, 32), (32, 16), (16, 8), (8, 4), (4, 2)]
+    ol = O.build_hierarchy(O.simp_density(x, EMIN, EMAX, PENAL), O.element_dof_map(nelx, nely),
+                           O.plane_stress_KE(0.3), mask, nelx, nely, max_coarse_elements=8)
+    for i, (lv, olv) in enumerate(zip(levels, ol)):
+        v = O.project(rng.standard_normal((2, lv.ndof)), olv.mask)
+        assert rel_err(lv(T(v)).cpu(), olv(v)) < 1e-12, i
+    if precision == "mixed":
+        M64 = m.mg.VCycle(_levels(m, nelx, nely, x, mask, 8))
+        u = O.project(rng.standard_normal((2, len(F))), mask)
+        assert rel_err(m.mg.VCycle(levels)(T(u)).cpu().numpy(), M64(T(u)).cpu().numpy()) < 1e-4
+
+
 def test_scalar_hierarchy_with_reaction(m):
     g = golden("hierarchy")
     hx, hy = 18, 12
