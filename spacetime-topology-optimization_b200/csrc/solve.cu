@@ -521,6 +521,22 @@ STT_DEV void pcg_converged(RowState& S, const PcgParams& pp) {
   }
 }
 
+// A row's state after the initial residual: t[0] = ||r||^2, t[1] = ||b||^2 (kept across a
+// true-residual replacement, replace = 1).
+STT_DEV void pcg_init_finish(RowState& S, const double* t, const PcgParams& pp, int replace) {
+  if (!replace) {
+    const double bn = sqrt(t[1]);
+    S.bnorm_safe = bn > 0.0 ? bn : 1.0;
+    S.conv_iter = -1;
+    S.status = STT_OK;
+    S.active = 1;
+    S.conv = 0;
+  }
+  S.rel = sqrt(t[0]) / S.bnorm_safe;
+  if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
+  pcg_converged(S, pp);
+}
+
 // r = b - A x (or r = b when x is null), reductions ||r||^2 and ||b||^2.
 // replace: keep bnorm and only re-test convergence (true-residual replacement).
 template <int D, bool MODAL, bool RD>
@@ -602,20 +618,27 @@ __global__ void __launch_bounds__(kQThreads) pcg_init_kernel(
       march<D, double, false, false, RhsX<D, double>, 0>(ke, nnx, nny, loadu, loadr, loadx, emit);
   }
   const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-  grid_reduce<2, kQThreads>(red, s, bid, vals, [&](const double* t) {
-    RowState& S = rst[s];
-    if (!replace) {
-      const double bn = sqrt(t[1]);
-      S.bnorm_safe = bn > 0.0 ? bn : 1.0;
-      S.conv_iter = -1;
-      S.status = STT_OK;
-      S.active = 1;
-      S.conv = 0;
-    }
-    S.rel = sqrt(t[0]) / S.bnorm_safe;
-    if (!isfinite(S.rel)) S.status = STT_ERR_BREAKDOWN;
-    pcg_converged(S, pp);
-  });
+  grid_reduce<2, kQThreads>(red, s, bid, vals, [&](const double* t) { pcg_init_finish(rst[s], t, pp, replace); });
+}
+
+// r = b, its FP32 copy (r32 may be null) and ||b||^2: the initialisation from x = 0 as one
+// elementwise pass (no operator apply).
+__global__ void __launch_bounds__(kEwThreads) pcg_init_b_kernel(
+    const double* __restrict__ b, long long b_rs, double* __restrict__ r, long long r_rs, long long n,
+    float* __restrict__ r32, long long r32_rs, RowState* __restrict__ rst, GridRed red, PcgParams pp) {
+  const int s = blockIdx.y;
+  const double* bs = b + (size_t)s * b_rs;
+  double* rs_ = r + (size_t)s * r_rs;
+  float* r32s = r32 ? r32 + (size_t)s * r32_rs : nullptr;
+  double vals[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)kEwThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kEwThreads) {
+    const double v = bs[i];
+    rs_[i] = v;
+    if (r32s) r32s[i] = (float)v;
+    vals[0] = fma(v, v, vals[0]);
+  }
+  vals[1] = vals[0];
+  grid_reduce<2, kEwThreads>(red, s, blockIdx.x, vals, [&](const double* t) { pcg_init_finish(rst[s], t, pp, 0); });
 }
 
 // The search direction and its operator product in one pass:
@@ -1022,7 +1045,16 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
   }
   PapEvents pev;
   // r = b - A x (x may be null: r = b); replace = 1 keeps ||b|| (true-residual replacement)
+  // the initialisation from x = 0 also writes (FP32 cycle) r's FP32 copy, the first
+  // V-cycle's right-hand side; after a warm start, which often converges at once (the
+  // adjoints' alpha U), and after a true-residual replacement the cycle converts r itself
+  float* r32init = sizeof(T) == 4 ? (float*)w.b0 : nullptr;
   auto init = [&](const double* xx, const PcgParams& pq, int replace) {
+    if (!xx && !replace) {
+      pcg_init_b_kernel<<<dim3(upb, nrows), kEwThreads, 0, st>>>(b, b_rs, w.r, nd, nd, r32init, vstride(nd), w.rs,
+                                                                  red_up, pq);
+      return;
+    }
 #define STT_INIT(MODAL, RD)                                                                              \
   pcg_init_kernel<D, MODAL, RD><<<tg, kQThreads, 0, st>>>(b, b_rs, xx, x_rs, w.r, nd, l0.rho64, l0.rs_rho, rd0, \
                                                           l0.ndof, l0.fixed, h->row_map, h->hrows, w.rs,        \
@@ -1106,7 +1138,8 @@ static int run_pcg(const stt_hier* h, SolveWS& w, int nrows, const double* b, lo
     {
       const RzFuse<T> f = fuse_of(1);
       bool done = false;
-      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st, false, &f, &done));
+      STT_TRY(run_vcycle<D, T>(h, w, nrows, w.r, nd, z, omega, n_smooth, gamma, w.rs, st,
+                               r32init != nullptr && !has_x0, &f, &done));
       if (!done) rz(1);
     }
     int check_every = 1;
