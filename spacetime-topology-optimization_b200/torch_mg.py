@@ -243,7 +243,8 @@ class _Level:
         retire = 0 if mixed else 1
         rc = _lib.lib().stt_pcg_mg(
             h.handle, rows, _lib.ptr(flat), n, _lib.ptr(x), n, 1 if x0 is not None else 0, rtol, max_iter,
-            M.omega, M.n_smooth, M.gamma, 1 if M.flexible else 0, 0, retire, rel, conv, ctypes.byref(n_iter),
+            M.omega, M.n_smooth, M.gamma, 1 if M.flexible else 0, M.replace_every, retire, rel, conv,
+            ctypes.byref(n_iter),
             _lib.ptr(ws), ws.numel(), _lib.stream())
         conv_list = list(conv)
         n_rows_ref = b.shape[0] if b.ndim == 2 else 1
@@ -291,10 +292,13 @@ class VCycle:
     (Polak-Ribiere) beta, r_new . (z_new - z_old) / (r . z), instead of the reference's
     r_new . z_new / (r . z).  The cycle is symmetric, in FP32 up to its rounding, so the
     two agree to that rounding (~1e-7 relative in the mixed form); the flexible form costs
-    the extra dot r_new . z_old an iteration."""
+    the extra dot r_new . z_old an iteration.
+
+    ``replace_every``: that PCG recomputes the true residual b - A x in FP64 every k
+    iterations (0: never; each costs an operator apply and an x flush)."""
 
     def __init__(self, levels: list[_Level], *, omega: float = 0.6, n_smooth: int = 2,
-                 gamma: int = 1, flexible: bool = False) -> None:
+                 gamma: int = 1, flexible: bool = False, replace_every: int = 0) -> None:
         if not levels or not isinstance(levels[0], _Level):
             raise TypeError("VCycle needs levels from sttopt_b200.torch_mg.build_hierarchy")
         self.levels = levels
@@ -302,11 +306,13 @@ class VCycle:
         self.n_smooth = n_smooth
         self.gamma = gamma
         self.flexible = flexible
+        self.replace_every = int(replace_every)
         self._is_vcycle_of = levels[0]._hier
 
     def select(self, rows: Tensor) -> "VCycle":
         return VCycle([lv.select(rows) for lv in self.levels], omega=self.omega,
-                      n_smooth=self.n_smooth, gamma=self.gamma, flexible=self.flexible)
+                      n_smooth=self.n_smooth, gamma=self.gamma, flexible=self.flexible,
+                      replace_every=self.replace_every)
 
     def __call__(self, r: Tensor) -> Tensor:
         _lib.require_cuda(r)
