@@ -268,6 +268,22 @@ def run_uneven(dev, steps=2, warmup=1, memory_budget=None):
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / steps
+    # comparator (unbudgeted run only): the same problems one after another through the
+    # single-problem entry point, each with its own hierarchies and solves
+    single = None
+    if memory_budget is None:
+        for x, w, n in zip(xs[:4], ws[:4], ns[:4]):
+            spacetime.objective_and_gradient(x, w, n_stage=n)
+        torch.cuda.synchronize()
+        a.record()
+        for x, w, n in zip(xs, ws, ns):
+            spacetime.objective_and_gradient(x, w, n_stage=n)
+        b.record()
+        torch.cuda.synchronize()
+        ms1 = a.elapsed_time(b)
+        single = {"value": sum(ns) / (ms1 / 1e3), "unit": UNIT, "ms_per_step": ms1,
+                  "speedup_of_batching": ms1 / ms,
+                  "path": "spacetime.objective_and_gradient per problem, one after another (1 pass)"}
     counts: dict = {}
     for x, n in zip(xs, ns):
         key = f"{x.shape[1]}x{x.shape[0]}"
@@ -282,6 +298,7 @@ def run_uneven(dev, steps=2, warmup=1, memory_budget=None):
             "peak_device_gib": round(torch.cuda.max_memory_allocated() / 2**30, 1),
             "iterations": {f"{k[0]}x{k[1]}": v for k, v in info.items()},
             "memory_budget_gib": None if memory_budget is None else round(memory_budget / 2**30, 1),
+            "one_problem_at_a_time": single,
             "batching": "one batched device PCG per grid size (heat, stages, adjoints), the size groups "
                         "on concurrent CUDA streams" + ("" if memory_budget is None else
                                                         ", in waves whose estimated memory fits the budget")}
