@@ -9,7 +9,7 @@ translation a stiffness of ~1e-16 per element, so on a large-displacement proble
 FP64 discretisations differ by ~1e-9 relative in compliance (measured: 7.5e-10 on the
 1024x512 cantilever, whose tip moves ~400 units; the oracle, a third FP64 code with the
 product form, agrees with the reference to 3e-12).  The product form therefore carries
-the north star's 1e-9 FP64 parity; the modal form is held to the bounds measured for it.
+the 1e-9 FP64 parity bound; the modal form is held to the bounds measured for it.
 
 * Config 2, the 1024x512 cantilever in FP64 (6 levels, 1122-dof coarse Cholesky): product
   form at the config's rtol 1e-8 (iteration counts equal to the reference's) and at rtol
