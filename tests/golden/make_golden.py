@@ -758,12 +758,58 @@ def gen_pcg_cases():
          fail_resid=resid, fail_msg=np.array(msg))
 
 
+def _mma_problem(rng, m, n, iteration):
+    """A seeded MMA subproblem of the shape the optimisation loop builds: variables in
+    [0, 1] away from the bounds, gradients of both signs, some constraints violated."""
+    xmin, xmax = np.zeros(n), np.ones(n)
+    xval = rng.uniform(0.05, 0.95, n)
+    xold1 = np.clip(xval + rng.normal(0, 0.02, n), 0.0, 1.0)
+    xold2 = np.clip(xold1 + rng.normal(0, 0.02, n), 0.0, 1.0)
+    low = xval - rng.uniform(0.1, 0.4, n)
+    upp = xval + rng.uniform(0.1, 0.4, n)
+    return dict(m=m, n=n, iteration=iteration, xval=xval, xmin=xmin, xmax=xmax, xold1=xold1, xold2=xold2,
+                f0val=float(rng.normal()), df0dx=rng.normal(0, 1.0, n), fval=rng.normal(0, 0.5, m),
+                dfdx=rng.normal(0, 1.0, (m, n)), low=low, upp=upp, a0=1.0, a=np.zeros(m),
+                c=np.full(m, 1000.0), d=rng.uniform(0.0, 1.0, m))
+
+
+def gen_mma():
+    """``mma.mmasub`` (asymptotes, the separable approximation and ``subsolv``'s
+    primal-dual Newton solve) on seeded subproblems: the first-iteration asymptotes
+    (m = 1), the adaptive branch with per-variable trust regions from
+    ``trust_region_params`` (m = 3), more constraints (m = 12), and the m >= n
+    elimination (m = 6, n = 4)."""
+    import sttopt.mma as mma
+
+    rng = np.random.default_rng(11)
+    cases = [("first", 1, 2000, 0, None), ("adapt", 3, 5000, 5, "trust"), ("wide", 12, 3000, 3, None),
+             ("mgen", 6, 4, 4, None)]
+    out = {}
+    names = ("xmma", "ymma", "zmma", "lam", "xsi", "eta", "mu", "zet", "s", "low", "upp")
+    for tag, m, n, it, kind in cases:
+        p = _mma_problem(rng, m, n, it)
+        kw = {}
+        if kind == "trust":
+            tr = mma.trust_region_params(t(rng.uniform(0.02, 0.1, n)), t(p["xmax"] - p["xmin"]))
+            kw = dict(tr)
+            for k, v in tr.items():
+                out[f"{tag}_{k}"] = v.numpy()
+        res = mma.mmasub(m, n, it, t(p["xval"]), t(p["xmin"]), t(p["xmax"]), t(p["xold1"]), t(p["xold2"]),
+                         p["f0val"], t(p["df0dx"]), t(p["fval"]), t(p["dfdx"]), t(p["low"]), t(p["upp"]), p["a0"],
+                         t(p["a"]), t(p["c"]), t(p["d"]), **kw)
+        for k, v in p.items():
+            out[f"{tag}_in_{k}"] = np.asarray(v)
+        for k, v in zip(names, res):
+            out[f"{tag}_{k}"] = np.asarray(v.detach().cpu().numpy() if torch.is_tensor(v) else v)
+    save("mma", **out)
+
+
 GENERATORS = {
     "fem_basic": gen_fem_basic, "load_cases": gen_load_cases, "operator": gen_operator, "transfers": gen_transfers,
     "hierarchy": gen_hierarchy, "pcg_cases": gen_pcg_cases, "mbb120x40": gen_mbb_config,
     "cantilever": gen_cantilever, "heat": gen_heat, "spacetime": gen_spacetime, "filters": gen_filters,
     "compliance_smooth": gen_compliance_smooth, "compliance_single": gen_compliance_single,
-    "time_maps": gen_time_maps, "neg_log": gen_neg_log,
+    "time_maps": gen_time_maps, "neg_log": gen_neg_log, "mma": gen_mma,
 }
 OPTIONAL = {
     "spacetime512": gen_spacetime_512,
