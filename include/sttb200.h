@@ -35,10 +35,13 @@
  *   stt_q4_apply_dots, stt_adjoint_warm_start  sttopt/torch_solve.py:117-140 (FemSolve.backward:
  *                       the adjoint load and its warm start alpha U, alpha = (U.g)/(U.F))
  *   stt_heat_*          sttopt/virtual_heat.py:162-166,189-201,404-462
+ *   stt_mma_sub         sttopt/mma.py:150-285 (mmasub: asymptotes, approximation, subsolv)
+ *   stt_mma_subsolv     sttopt/mma.py:346-557 (subsolv)
  */
 #ifndef STTB200_H
 #define STTB200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -370,6 +373,44 @@ int stt_poisson_load_adjoint(int nelx, int nely, int nrows, const double* s, lon
                              const double* w, long long w_rs, const double* gF, long long gF_rs,
                              double* gs, long long gs_rs, double* gw, long long gw_rs,
                              stt_stream_t stream);
+
+/* ---- MMA subproblem (sttopt/mma.py:150-557) -----------------------------------------
+ *
+ * n-sized vectors and the m x n matrices (row stride ld >= n, in elements) are device
+ * pointers; m-sized vectors (fval, a, b, c, d and the m-sized results y, lam, mu, s) and
+ * the scalars z, zet are HOST pointers, since the m-sized algebra runs on the host.  The
+ * calls synchronise the stream.  With m < n (at most 64 constraints) the per-variable
+ * work runs on the device; with m >= n the whole solve runs in the library's host code.
+ * counts (optional, 3 ints) receives the number of barrier levels whose Newton loop
+ * stopped at its 200-iteration cap, the Newton steps taken and the line-search
+ * candidates tried; cap_epsi (optional) the last capped level's epsi.  Workspace:
+ * stt_mma_workspace_bytes (256-byte aligned device memory). */
+size_t stt_mma_workspace_bytes(int m, long long n);
+
+/* mmasub (sttopt/mma.py:150-285) with epsimin 1e-7: low / upp are read (iteration >= 2)
+ * and overwritten with the new asymptotes; each of asyinit, asyclamp_min, asyclamp_max
+ * and move is a device n-vector, or NULL for the scalar beside it.  Outputs xmma, xsi,
+ * eta (device n) and ymma, zmma, lam, mu, zet, s (host). */
+int stt_mma_sub(int m, long long n, int iteration, const double* xval, const double* xmin,
+                const double* xmax, const double* xold1, const double* xold2, const double* df0dx,
+                const double* fval, const double* dfdx, long long dfdx_ld, double* low, double* upp,
+                double a0, const double* a, const double* c, const double* d,
+                const double* asyinit, double asyinit_v, const double* asyclamp_min,
+                double asyclamp_min_v, const double* asyclamp_max, double asyclamp_max_v,
+                const double* move, double move_v, double raa0, double albefa, double asyincr,
+                double asydecr, double* xmma, double* xsi, double* eta, double* ymma, double* zmma,
+                double* lam, double* mu, double* zet, double* s, int* counts, double* cap_epsi,
+                void* ws, size_t ws_bytes, stt_stream_t stream);
+
+/* subsolv (sttopt/mma.py:346-557) on a given subproblem: low, upp, alfa, beta, p0, q0
+ * (device n), P, Q (device m x n, row stride ld), a0 and a, b, c, d (host m). */
+int stt_mma_subsolv(int m, long long n, double epsimin, const double* low, const double* upp,
+                    const double* alfa, const double* beta, const double* p0, const double* q0,
+                    const double* P, const double* Q, long long ld, double a0, const double* a,
+                    const double* b, const double* c, const double* d, double* xmma, double* xsi,
+                    double* eta, double* ymma, double* zmma, double* lam, double* mu, double* zet,
+                    double* s, int* counts, double* cap_epsi, void* ws, size_t ws_bytes,
+                    stt_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -47,6 +47,13 @@ _SIGS = {
     "stt_q4_apply_dots": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _c_ll, _p, _c_ll, _p, _c_ll, _p, _pd, _p,
                                    _c_ll, _p, _p, _c_ll, _p]),
     "stt_adjoint_warm_start": (_c_int, [_c_int, _c_ll, _p, _p, _c_ll, _p, _c_ll, _p]),
+    "stt_mma_workspace_bytes": (ctypes.c_size_t, [_c_int, _c_ll]),
+    "stt_mma_sub": (_c_int, [_c_int, _c_ll, _c_int, _p, _p, _p, _p, _p, _p, _p, _p, _c_ll, _p, _p, _c_double, _p, _p,
+                             _p, _p, _c_double, _p, _c_double, _p, _c_double, _p, _c_double, _c_double, _c_double,
+                             _c_double, _c_double, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.c_size_t,
+                             _p]),
+    "stt_mma_subsolv": (_c_int, [_c_int, _c_ll, _c_double, _p, _p, _p, _p, _p, _p, _p, _p, _c_ll, _c_double, _p, _p,
+                                 _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.c_size_t, _p]),
     "stt_stage_glue_rows": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p,
                                      _c_double, _c_double, _c_double, _p, _p, _p, _p]),
     "stt_stage_glue_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p, _p,

@@ -20,6 +20,9 @@ LIB = HERE / "libsttb200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-Wall", "-Xptxas", "-warn-spills"]
+# Per-file flags.  The MMA subproblem rounds a * b + c twice, as the reference's tensor
+# arithmetic does, and fuses only its dot products (explicit fma()).
+FILE_FLAGS = {"mma.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -34,7 +37,7 @@ def _compile(src: Path, verbose: bool, extra: list[str]) -> Path:
     deps = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [HERE.parent / "include" / "sttb200.h"]
     if obj.exists() and obj.stat().st_mtime > max(p.stat().st_mtime for p in [src, *deps]):
         return obj
-    cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), *extra, "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

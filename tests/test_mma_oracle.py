@@ -59,3 +59,23 @@ def test_oracle_subsolv_meets_barrier_target(m, n):
     epsi_last = 1e-7  # 0.1 ** 7, the last level above epsimin
     assert np.abs(_kkt_residual(sol, epsi_last, args)).max() <= 0.9 * epsi_last * 1.0001
     assert np.all(sol[0] > alfa) and np.all(sol[0] < beta)
+
+
+def test_trust_region_and_floor_share_host_logic(pkg):
+    """The drop-in's small torch wrappers (sttopt/mma.py:22-147) on CPU tensors."""
+    import torch
+    from sttopt_b200 import mma
+
+    move = torch.tensor([0.01, 0.05, 0.1, 0.2], dtype=torch.float64)
+    tr = mma.trust_region_params(move, torch.full_like(move, 2.0))
+    assert torch.equal(tr["asyinit"], move / 2.0) and torch.equal(tr["move"], move / 2.0)
+    assert torch.equal(tr["asyclamp_min"], 0.02 * (move / 2.0))
+    assert torch.equal(tr["asyclamp_max"], 20.0 * (move / 2.0))
+    h = mma.History.initial(torch.full((4,), 0.5, dtype=torch.float64))
+    assert torch.equal(h.xold1, h.xold2) and h.xold1 is not h.xold2 and float(h.low.abs().sum()) == 0.0
+    floor = 0.02 * move
+    half = torch.tensor([1.0, 1.0, 1.0, 1.0], dtype=torch.float64) * floor
+    half[2] *= 3.0
+    hist = mma.History(xold1=h.xold1, xold2=h.xold2, low=0.5 - half, upp=0.5 + half)
+    assert mma.floor_share(hist, move, torch.tensor([True, True, True, False])) == pytest.approx(2 / 3)
+    assert mma.floor_share(hist, move, torch.zeros(4, dtype=torch.bool)) == 0.0
