@@ -20,6 +20,7 @@
 // reference's tensor arithmetic; the dot products use fma() explicitly.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -28,7 +29,6 @@
 namespace stt {
 
 constexpr int kMmaThreads = 256;  // a tile is kMmaThreads variables, one a thread
-constexpr int kMmaLd = kMmaThreads + 1;
 constexpr int kMmaMaxM = 64;
 
 // A per-variable parameter of mmasub: a vector (p) or one value for all (v).
@@ -91,20 +91,44 @@ STT_DEV ColFixed load_fixed(const MmaCols& c, long long j) {
   return f;
 }
 
+// Rows are read in chunks: the CH entries of column j in rows [i0, i0 + CH), the row
+// clamped to m - 1 so that the loads are unconditional and issue back to back before
+// any of them is used (a guarded load per row would wait out one memory latency a row).
+template <int MB>
+constexpr int row_chunk() {
+  return MB <= 24 ? MB : 16;
+}
+template <int CH, bool G>
+STT_DEV void load_rows(const MmaCols& c, int i0, long long j, double (&a)[CH], double (&b)[CH]) {
+  const int nv = min(CH, c.m - i0);  // rows past m - 1 reread row i0
+  const long long o0 = (long long)i0 * c.ld + j;
+#pragma unroll
+  for (int u = 0; u < CH; ++u) {
+    const long long o = u < nv ? o0 + u * c.ld : o0;
+    if constexpr (G) {
+      a[u] = __ldg(c.dfdx + o);
+      b[u] = 0.0;
+    } else {
+      a[u] = __ldg(c.P + o);
+      b[u] = __ldg(c.Q + o);
+    }
+  }
+}
 template <bool G>
-STT_DEV void load_pq(const MmaCols& c, const ColFixed& f, int i, long long j, double& P, double& Q) {
-  const long long o = (long long)i * c.ld + j;
+STT_DEV void rows_pq(const ColFixed& f, double a, double b, double& P, double& Q) {
   if constexpr (G) {
-    approx_pq(__ldg(c.dfdx + o), f.r, f.ux2f, f.xl2f, P, Q);
+    approx_pq(a, f.r, f.ux2f, f.xl2f, P, Q);
   } else {
-    P = __ldg(c.P + o);
-    Q = __ldg(c.Q + o);
+    P = a;
+    Q = b;
   }
 }
 
 // The point's distances to the asymptotes and their inverses (sttopt/mma.py:443-452).
+// Divisions by the point's four distances are multiplications by these reciprocals (one
+// division each), which rounds within an ulp of the reference's quotients.
 struct ColPoint {
-  double ux1, xl1, ux2, xl2, uxinv1, xlinv1, uxinv2, xlinv2, xa, bx;
+  double ux1, xl1, ux2, xl2, uxinv1, xlinv1, uxinv2, xlinv2, xa, bx, xainv, bxinv;
 };
 STT_DEV ColPoint point_of(const ColFixed& f, double x) {
   ColPoint p;
@@ -118,6 +142,8 @@ STT_DEV ColPoint point_of(const ColFixed& f, double x) {
   p.xlinv2 = 1.0 / p.xl2;
   p.xa = x - f.alfa;
   p.bx = f.beta - x;
+  p.xainv = 1.0 / p.xa;
+  p.bxinv = 1.0 / p.bx;
   return p;
 }
 
@@ -125,26 +151,35 @@ STT_DEV ColPoint point_of(const ColFixed& f, double x) {
 // (sttopt/mma.py:520-521).
 STT_DEV void step_point(double& x, double& xsi, double& eta, double dx, double t, double epsi, double alfa,
                         double beta) {
-  const double xa = x - alfa, bx = beta - x;
-  const double dxsi = -xsi + epsi / xa - (xsi * dx) / xa;
-  const double deta = -eta + epsi / bx + (eta * dx) / bx;
+  const double xainv = 1.0 / (x - alfa), bxinv = 1.0 / (beta - x);
+  const double dxsi = -xsi + epsi * xainv - (xsi * dx) * xainv;
+  const double deta = -eta + epsi * bxinv + (eta * dx) * bxinv;
   x = x + t * dx;
   xsi = xsi + t * dxsi;
   eta = eta + t * deta;
 }
 
+// The Newton terms of one variable (sttopt/mma.py:453-465): delx and diagx.
+STT_DEV void newton_col(double plam, double qlam, const ColPoint& p, double xsi, double eta, double epsi,
+                        double& delx, double& diagx) {
+  const double dpsidx = plam * p.uxinv2 - qlam * p.xlinv2;
+  delx = dpsidx - epsi * p.xainv + epsi * p.bxinv;
+  diagx = 2.0 * (plam * p.uxinv2 * p.uxinv1 + qlam * p.xlinv2 * p.xlinv1) + xsi * p.xainv + eta * p.bxinv;
+}
+
 // The n-sized parts of the barrier residual (rex, rexsi, reeta; sttopt/mma.py:409-417):
-// their sum of squares and largest magnitude.
+// their sum of squares and largest magnitude.  A NaN part makes the sum of squares NaN,
+// from which the host restores the NaN maximum the reference's max would give.
 STT_DEV void resid_n(double plam, double qlam, const ColPoint& p, double xsi, double eta, double epsi, double& ss,
                      double& mx) {
-  const double dpsidx = plam / p.ux2 - qlam / p.xl2;
+  const double dpsidx = plam * p.uxinv2 - qlam * p.xlinv2;
   const double rex = dpsidx - xsi + eta;
   const double rexsi = xsi * p.xa - epsi;
   const double reeta = eta * p.bx - epsi;
   ss = fma(rex, rex, ss);
   ss = fma(rexsi, rexsi, ss);
   ss = fma(reeta, reeta, ss);
-  mx = nanmax(mx, nanmax(fabs(rex), nanmax(fabs(rexsi), fabs(reeta))));
+  mx = fmax(mx, fmax(fabs(rex), fmax(fabs(rexsi), fabs(reeta))));
 }
 
 // ---- deterministic block partials and the last block's finalisation --------------------
@@ -173,9 +208,14 @@ STT_DEV double block_nanmax(double v, double* red) {
   return t;
 }
 
+// Block partials are stored entry-major: entry e of block b at partials[e * grid + b].
+STT_DEV double* part(double* partials, int e) { return partials + (size_t)e * gridDim.x + blockIdx.x; }
+
 // After this block wrote its kp partials (the first ks summed, the rest max-reduced):
-// the last block to arrive reduces all blocks' partials in block order into fin[kp]
-// (shared memory) and returns true.
+// the last block to arrive folds every entry over all blocks into fin[kp] (shared
+// memory) and returns true.  A warp folds an entry: lane l takes blocks l, l + 32, ... in
+// order, then the lanes combine in a fixed butterfly, so the result does not depend on
+// which block finished last.
 STT_DEV bool finish_blocks(const double* partials, unsigned* counter, int kp, int ks, double* fin) {
   __shared__ bool is_last;
   __threadfence();
@@ -184,13 +224,20 @@ STT_DEV bool finish_blocks(const double* partials, unsigned* counter, int kp, in
   __syncthreads();
   if (!is_last) return false;
   __threadfence();
-  for (int e = threadIdx.x; e < kp; e += kMmaThreads) {
-    double t = e < ks ? 0.0 : -INFINITY;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      const double v = __ldcg(partials + (size_t)b * kp + e);
-      t = e < ks ? t + v : nanmax(t, v);
+  const int lane = threadIdx.x & 31, nb = gridDim.x;
+  for (int e = threadIdx.x >> 5; e < kp; e += kMmaThreads / 32) {
+    const bool sum = e < ks;
+    double t = sum ? 0.0 : -INFINITY;
+    for (int b = lane; b < nb; b += 32) {
+      const double v = __ldcg(partials + (size_t)e * nb + b);
+      t = sum ? t + v : nanmax(t, v);
     }
-    fin[e] = t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, t, o);
+      t = sum ? t + u : nanmax(t, u);
+    }
+    if (lane == 0) fin[e] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) *counter = 0u;
@@ -265,17 +312,106 @@ __global__ void __launch_bounds__(kMmaThreads) mma_apply_kernel(long long n, con
 
 // ---- subsolv's Newton passes ---------------------------------------------------------------
 
-// Index of the upper-triangular 4 x 4 block row bi's first block, nb blocks a side.
-STT_DEV int blk_offset(int bi, int nb) { return bi * nb - bi * (bi - 1) / 2; }
-
-// Dynamic shared memory of the assemble pass, in doubles.
-__host__ __device__ inline int assemble_kp(int m) {
-  const int nb = ((m + 4) & ~3) >> 2;
-  return m + 2 + nb * (nb + 1) / 2 * 16;
+// A warp's sum in a fixed butterfly order; every lane gets it.
+STT_DEV double warp_allsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
-inline size_t assemble_smem(int m) {
-  const size_t mp = (size_t)((m + 4) & ~3);
-  return 8 * std::max({mp * kMmaLd + kMmaThreads, (size_t)kMmaThreads * 17 + 8, (size_t)assemble_kp(m)});
+
+// Per-row sums over all variables without a register a row: for row i the warp sums
+// its 32 variables' terms and lane i mod 32 keeps the running total in acc[i / 32].
+// Called by whole warps (lanes past n add zeros).
+template <int MB>
+struct RowSums {
+  static constexpr int K = (MB + 31) / 32;
+  double acc[K];
+  STT_DEV void zero() {
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  }
+  STT_DEV void add(int i, double v) {
+    v = warp_allsum(v);
+    if ((threadIdx.x & 31) == (i & 31)) acc[i >> 5] += v;
+  }
+  // The block's row sums (warp by warp, in warp order) into its partial entries
+  // e0 .. e0 + m - 1; sh holds kMmaThreads / 32 x kMmaMaxM doubles.
+  STT_DEV void write(int m, double* partials, int e0, double* sh) const {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int i = k * 32 + lane;
+      if (i < m) sh[warp * kMmaMaxM + i] = acc[k];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += kMmaThreads) {
+      double t = 0.0;
+      for (int w = 0; w < kMmaThreads / 32; ++w) t += sh[w * kMmaMaxM + i];
+      *part(partials, e0 + i) = t;
+    }
+    __syncthreads();
+  }
+};
+
+// The same row sums kept in shared memory, one slot a row and thread: a thread adds its
+// own variables' terms to its slots (no synchronisation, no shuffles) and the block
+// folds the slots once at the end.  slots: [MB][kMmaThreads] doubles.
+template <int MB>
+struct SlotSums {
+  double* slots;
+  STT_DEV void zero() {
+#pragma unroll
+    for (int i = 0; i < MB; ++i) slots[i * kMmaThreads + threadIdx.x] = 0.0;
+  }
+  STT_DEV void add(int i, double v) { slots[i * kMmaThreads + threadIdx.x] += v; }
+  STT_DEV void write(int m, double* partials, int e0, double*) const {
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < m; i += kMmaThreads / 32) {
+      double t = 0.0;
+#pragma unroll
+      for (int k = 0; k < kMmaThreads / 32; ++k) t += slots[i * kMmaThreads + k * 32 + lane];
+      t = warp_allsum(t);
+      if (lane == 0) *part(partials, e0 + i) = t;
+    }
+    __syncthreads();
+  }
+};
+// Slots where they fit beside the assemble pass's tile at two blocks an SM.
+template <int MB>
+constexpr bool use_slots() {
+  return MB <= 24;
+}
+template <int MB>
+using RowAcc = std::conditional_t<use_slots<MB>(), SlotSums<MB>, RowSums<MB>>;
+
+// The m x m product GG diag(1/diagx) GG^T is formed on the FP64 tensor cores: tcgen05 has
+// no FP64 kind, so this is mma.sync m8n8k4 (DMMA), 8 x 8 tiles of the (m + 1)-row tile of
+// GG with delx appended (row m, which gives h), k running over a tile's variables.
+constexpr int kMmaLd8 = kMmaThreads + 4;  // row stride of the GG tile: fragment loads hit distinct banks
+
+STT_DEV void dmma_f64(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Upper-triangular 8 x 8 tiles (I <= K) of the (m + 1) x (m + 1) product, t8 a side.
+__host__ __device__ inline int gram_side(int m) { return (m + 8) >> 3; }
+__host__ __device__ inline int gram_tiles(int m) { return gram_side(m) * (gram_side(m) + 1) / 2; }
+__host__ __device__ inline int tile_index(int I, int K, int t8) { return I * t8 - I * (I - 1) / 2 + (K - I); }
+// Partial entries of the assemble pass: [gvec (m) | sum of squares | tiles x 64 | max].
+__host__ __device__ inline int assemble_kp(int m) { return m + 2 + gram_tiles(m) * 64; }
+// Its dynamic shared memory: the GG tile (or, later, the folded entries), 1/diagx, a
+// block-sum scratch, and the row-sum slots or shuffle scratch.
+inline size_t assemble_smem(int m, int mb) {
+  const size_t rows = (size_t)gram_side(m) * 8;
+  const size_t tail = mb <= 24 ? (size_t)mb * kMmaThreads : (size_t)(kMmaThreads / 32) * kMmaMaxM;
+  return 8 * (std::max(rows * kMmaLd8, (size_t)assemble_kp(m)) + kMmaThreads + 8 + tail);
+}
+inline int mma_bucket(int m) {
+  return m <= 4 ? 4 : m <= 8 ? 8 : m <= 12 ? 12 : m <= 16 ? 16 : m <= 20 ? 20 : m <= 24 ? 24 : m <= 32 ? 32
+         : m <= 48 ? 48 : 64;
 }
 
 // The assemble pass (sttopt/mma.py:399-489, m < n): applies a pending accepted step,
@@ -283,134 +419,185 @@ inline size_t assemble_smem(int m) {
 //   gvec = P (1/ux1) + Q (1/xl1),  h = GG (delx / diagx),  A = GG diag(1/diagx) GG^T
 // with GG = P diag(1/ux2) - Q diag(1/xl2), and the sum of squares and largest magnitude
 // of the residual's n-sized parts.  A block's 256 variables write their GG column and
-// delx into a shared tile [m + 1 rows][256]; the tile's upper-triangular 4 x 4 blocks
-// of GG' diag(1/diagx) GG'^T (GG' = GG with delx appended as row m, which gives h) are
-// accumulated by groups of threads, one block a thread.
+// delx into a shared tile; A and h come from DMMA tiles of that tile.  Up to 31
+// constraints each warp takes 32 of the tile's variables for every 8 x 8 tile and the
+// warps' sums are folded in warp order; above that the tiles are split among the warps.
 // res = [gvec (m) | h (m) | A (m x m) | sum of squares | max].
 template <int MB, bool G>
-__global__ void __launch_bounds__(kMmaThreads) mma_assemble_kernel(
+__global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
     MmaCols c, double* __restrict__ x, double* __restrict__ xsi, double* __restrict__ eta,
     const double* __restrict__ dx, int pend, double t_pend, double eps_pend, MVec lam, double epsi,
     double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ res) {
   extern __shared__ double sm[];
-  const int m = c.m, mp = (m + 4) & ~3, nb = mp >> 2, nblk = nb * (nb + 1) / 2;
-  double* gs = sm;                              // [mp][kMmaLd]
-  double* ws = sm + (size_t)mp * kMmaLd;        // [kMmaThreads]: 1 / diagx
-  const int tid = threadIdx.x, ngrp = kMmaThreads / nblk, grp = tid / nblk;
-  int bi = 0, rem = tid % nblk;
-  while (rem >= nb - bi) {
-    rem -= nb - bi;
-    ++bi;
-  }
-  const int bk = bi + rem;
-  double acc[4][4];
+  constexpr int T8 = (MB + 8) / 8;  // tile side for the largest m of the bucket
+  constexpr int NT = T8 * (T8 + 1) / 2;
+  constexpr bool KSPLIT = T8 <= 4;
+  constexpr int TPW = KSPLIT ? NT : (NT + 7) / 8;  // tiles a warp accumulates
+  const int m = c.m, t8 = gram_side(m), rows = t8 * 8, ntile = gram_tiles(m);
+  const int head = max(rows * kMmaLd8, assemble_kp(m));
+  double* gs = sm;                 // [rows][kMmaLd8]
+  double* ws = sm + head;          // [kMmaThreads]: 1 / diagx
+  double* wred = ws + kMmaThreads; // [8]
+  double* tail = wred + 8;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int fr = lane >> 2, fc = lane & 3;  // DMMA fragment row and column
+  double acc[TPW][2];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int s = 0; s < 4; ++s) acc[r][s] = 0.0;
-  double gv[MB];
-#pragma unroll
-  for (int i = 0; i < MB; ++i) gv[i] = 0.0;
+  for (int q = 0; q < TPW; ++q) acc[q][0] = acc[q][1] = 0.0;
+  RowAcc<MB> gv;
+  if constexpr (use_slots<MB>()) gv.slots = tail;
+  gv.zero();
   double ss = 0.0, mx = 0.0;
-  for (int r = m + 1; r < mp; ++r) gs[r * kMmaLd + tid] = 0.0;
+  for (int r = m + 1; r < rows; ++r) gs[r * kMmaLd8 + tid] = 0.0;
 
   const long long ntiles = (c.n + kMmaThreads - 1) / kMmaThreads;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long j = tile * kMmaThreads + tid;
-    double w = 0.0;
-    if (j < c.n) {
-      const ColFixed f = load_fixed<G>(c, j);
-      double xv = x[j], xs = xsi[j], et = eta[j];
+    const bool ok = j < c.n;
+    ColFixed f{};
+    ColPoint p{};
+    double xs = 0.0, et = 0.0;
+    if (ok) {
+      f = load_fixed<G>(c, j);
+      double xv = x[j];
+      xs = xsi[j];
+      et = eta[j];
       if (pend) {
         step_point(xv, xs, et, dx[j], t_pend, eps_pend, f.alfa, f.beta);
         x[j] = xv;
         xsi[j] = xs;
         eta[j] = et;
       }
-      const ColPoint p = point_of(f, xv);
-      double plam = 0.0, qlam = 0.0;
+      p = point_of(f, xv);
+    }
+    double plam = 0.0, qlam = 0.0;
+    constexpr int CH = row_chunk<MB>();
 #pragma unroll
-      for (int i = 0; i < MB; ++i) {
-        if (i < m) {
-          double P, Q;
-          load_pq<G>(c, f, i, j, P, Q);
-          plam = fma(lam.v[i], P, plam);
-          qlam = fma(lam.v[i], Q, qlam);
-          gv[i] = fma(P, p.uxinv1, gv[i]);
-          gv[i] = fma(Q, p.xlinv1, gv[i]);
-          gs[i * kMmaLd + tid] = P * p.uxinv2 - Q * p.xlinv2;
+    for (int i0 = 0; i0 < MB; i0 += CH) {
+      if (i0 < m) {
+        double ra[CH], rb[CH];
+        if (ok) {
+          load_rows<CH, G>(c, i0, j, ra, rb);
+        } else {
+#pragma unroll
+          for (int u = 0; u < CH; ++u) ra[u] = rb[u] = 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 + u;
+          if (i < m) {
+            double P, Q;
+            rows_pq<G>(f, ra[u], rb[u], P, Q);
+            plam = fma(lam.v[i], P, plam);
+            qlam = fma(lam.v[i], Q, qlam);
+            gv.add(i, fma(P, p.uxinv1, Q * p.xlinv1));
+            gs[i * kMmaLd8 + tid] = P * p.uxinv2 - Q * p.xlinv2;
+          }
         }
       }
+    }
+    double w = 0.0, delx = 0.0;
+    if (ok) {
       plam = f.p0 + plam;
       qlam = f.q0 + qlam;
       resid_n(plam, qlam, p, xs, et, epsi, ss, mx);
-      const double dpsidx = plam / p.ux2 - qlam / p.xl2;
-      const double delx = dpsidx - epsi / p.xa + epsi / p.bx;
-      const double diagx = 2.0 * (plam / (p.ux1 * p.ux2) + qlam / (p.xl1 * p.xl2)) + xs / p.xa + et / p.bx;
-      gs[m * kMmaLd + tid] = delx;
+      double diagx;
+      newton_col(plam, qlam, p, xs, et, epsi, delx, diagx);
       w = 1.0 / diagx;
-    } else {
-      for (int i = 0; i <= m; ++i) gs[i * kMmaLd + tid] = 0.0;
     }
+    gs[m * kMmaLd8 + tid] = delx;
     ws[tid] = w;
     __syncthreads();
-    if (grp < ngrp) {
-      for (int cc = grp; cc < kMmaThreads; cc += ngrp) {
-        const double wc = ws[cc];
-        double a[4], b[4];
+    if constexpr (KSPLIT) {
+#pragma unroll 2
+      for (int k4 = 0; k4 < 8; ++k4) {
+        const int col = warp * 32 + k4 * 4 + fc;
+        const double wc = ws[col];
+        double a[T8], b[T8];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          a[r] = gs[(4 * bi + r) * kMmaLd + cc];
-          b[r] = gs[(4 * bk + r) * kMmaLd + cc] * wc;
+        for (int I = 0; I < T8; ++I) {
+          a[I] = I < t8 ? gs[(8 * I + fr) * kMmaLd8 + col] : 0.0;
+          b[I] = a[I] * wc;
         }
+        int q = 0;
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int I = 0; I < T8; ++I)
 #pragma unroll
-          for (int s = 0; s < 4; ++s) acc[r][s] = fma(a[r], b[s], acc[r][s]);
+          for (int K = I; K < T8; ++K, ++q)
+            if (K < t8) dmma_f64(acc[q], a[I], b[K]);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < TPW; ++q) {
+        const int t = warp + 8 * q;
+        if (t < ntile) {
+          int I = 0, rem = t;
+          while (rem >= t8 - I) {
+            rem -= t8 - I;
+            ++I;
+          }
+          const int K = I + rem;
+          const double* ga = gs + (8 * I + fr) * kMmaLd8 + fc;
+          const double* gb = gs + (8 * K + fr) * kMmaLd8 + fc;
+#pragma unroll 4
+          for (int k4 = 0; k4 < kMmaThreads / 4; ++k4)
+            dmma_f64(acc[q], ga[4 * k4], gb[4 * k4] * ws[4 * k4 + fc]);
+        }
       }
     }
     __syncthreads();
   }
 
-  // Block partials: [gvec (m) | sum of squares | Gram blocks (nblk x 16) | max].
-  const int kp = assemble_kp(m), ks = kp - 1;
-  double* dst = partials + (size_t)blockIdx.x * kp;
+  // Gram partials: entry m + 1 + t * 64 + r * 8 + c of tile t = (I, K) holds the
+  // product's (8 I + r, 8 K + c).
+  if constexpr (KSPLIT) {
+    double* red8 = sm;  // [8 warps][ntile][64]
+    int q = 0;
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+    for (int I = 0; I < T8; ++I)
 #pragma unroll
-    for (int s = 0; s < 4; ++s) sm[tid * 17 + r * 4 + s] = acc[r][s];
-  __syncthreads();
-  for (int e = tid; e < nblk * 16; e += kMmaThreads) {
-    const int b = e >> 4, rs = e & 15;
-    double t = 0.0;
-    for (int g = 0; g < ngrp; ++g) t += sm[(g * nblk + b) * 17 + rs];
-    dst[m + 1 + e] = t;
-  }
-  double* wred = sm + kMmaThreads * 17;
+      for (int K = I; K < T8; ++K, ++q)
+        if (K < t8) {
+          double* d = red8 + ((size_t)warp * ntile + tile_index(I, K, t8)) * 64 + fr * 8 + fc * 2;
+          d[0] = acc[q][0];
+          d[1] = acc[q][1];
+        }
+    __syncthreads();
+    for (int e = tid; e < ntile * 64; e += kMmaThreads) {
+      double t = 0.0;
+      for (int w8 = 0; w8 < kMmaThreads / 32; ++w8) t += red8[(size_t)w8 * ntile * 64 + e];
+      *part(partials, m + 1 + e) = t;
+    }
+  } else {
 #pragma unroll
-  for (int i = 0; i < MB; ++i) {
-    if (i < m) {
-      const double t = block_total(gv[i], wred);
-      if (tid == 0) dst[i] = t;
+    for (int q = 0; q < TPW; ++q) {
+      const int t = warp + 8 * q;
+      if (t < ntile) {
+        *part(partials, m + 1 + t * 64 + fr * 8 + fc * 2) = acc[q][0];
+        *part(partials, m + 1 + t * 64 + fr * 8 + fc * 2 + 1) = acc[q][1];
+      }
     }
   }
+  const int kp = assemble_kp(m), ks = kp - 1;
+  gv.write(m, partials, 0, tail);
   {
     const double t = block_total(ss, wred);
-    if (tid == 0) dst[m] = t;
+    if (tid == 0) *part(partials, m) = t;
     const double u = block_nanmax(mx, wred);
-    if (tid == 0) dst[ks] = u;
+    if (tid == 0) *part(partials, ks) = u;
   }
   double* fin = sm;
   if (!finish_blocks(partials, counter, kp, ks, fin)) return;
+  auto gram = [&](int lo, int hi) {
+    return fin[m + 1 + tile_index(lo >> 3, hi >> 3, t8) * 64 + (lo & 7) * 8 + (hi & 7)];
+  };
   for (int e = tid; e < m * m; e += kMmaThreads) {
-    const int i = e / m, k = e % m, lo = min(i, k), hi = max(i, k);
-    const int b = blk_offset(lo >> 2, nb) + (hi >> 2) - (lo >> 2);
-    res[2 * m + e] = fin[m + 1 + b * 16 + (lo & 3) * 4 + (hi & 3)];
+    const int i = e / m, k = e % m;
+    res[2 * m + e] = gram(min(i, k), max(i, k));
   }
   for (int i = tid; i < m; i += kMmaThreads) {
     res[i] = fin[i];
-    const int b = blk_offset(i >> 2, nb) + (m >> 2) - (i >> 2);
-    res[m + i] = fin[m + 1 + b * 16 + (i & 3) * 4 + (m & 3)];
+    res[m + i] = gram(i, m);
   }
   if (tid == 0) {
     res[2 * m + m * m] = fin[m];
@@ -423,7 +610,7 @@ __global__ void __launch_bounds__(kMmaThreads) mma_assemble_kernel(
 // fraction-to-the-boundary limits max(-1.01 dx / (x - alfa)), max(1.01 dx / (beta - x))
 // and max(-1.01 dxsi / xsi, -1.01 deta / eta).  res = those three maxima.
 template <int MB, bool G>
-__global__ void __launch_bounds__(kMmaThreads) mma_step_kernel(
+__global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
     MVec lam, MVec dlam, double epsi, double* __restrict__ dx, double* __restrict__ partials,
     unsigned* __restrict__ counter, double* __restrict__ res) {
@@ -437,97 +624,119 @@ __global__ void __launch_bounds__(kMmaThreads) mma_step_kernel(
     const double xv = x[j], xs = xsi[j], et = eta[j];
     const ColPoint p = point_of(f, xv);
     double plam = 0.0, qlam = 0.0, gd = 0.0;
+    constexpr int CH = row_chunk<MB>();
 #pragma unroll
-    for (int i = 0; i < MB; ++i) {
-      if (i < m) {
-        double P, Q;
-        load_pq<G>(c, f, i, j, P, Q);
-        plam = fma(lam.v[i], P, plam);
-        qlam = fma(lam.v[i], Q, qlam);
-        gd = fma(P * p.uxinv2 - Q * p.xlinv2, dlam.v[i], gd);
+    for (int i0 = 0; i0 < MB; i0 += CH) {
+      if (i0 < m) {
+        double ra[CH], rb[CH];
+        load_rows<CH, G>(c, i0, j, ra, rb);
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 + u;
+          if (i < m) {
+            double P, Q;
+            rows_pq<G>(f, ra[u], rb[u], P, Q);
+            plam = fma(lam.v[i], P, plam);
+            qlam = fma(lam.v[i], Q, qlam);
+            gd = fma(P * p.uxinv2 - Q * p.xlinv2, dlam.v[i], gd);
+          }
+        }
       }
     }
     plam = f.p0 + plam;
     qlam = f.q0 + qlam;
-    const double dpsidx = plam / p.ux2 - qlam / p.xl2;
-    const double delx = dpsidx - epsi / p.xa + epsi / p.bx;
-    const double diagx = 2.0 * (plam / (p.ux1 * p.ux2) + qlam / (p.xl1 * p.xl2)) + xs / p.xa + et / p.bx;
-    const double d = -delx / diagx - gd / diagx;
+    double delx, diagx;
+    newton_col(plam, qlam, p, xs, et, epsi, delx, diagx);
+    const double w = 1.0 / diagx;
+    const double d = -delx * w - gd * w;
     dx[j] = d;
-    const double dxsi = -xs + epsi / p.xa - (xs * d) / p.xa;
-    const double deta = -et + epsi / p.bx + (et * d) / p.bx;
-    m1 = nanmax(m1, (-1.01 * d) / p.xa);
-    m2 = nanmax(m2, (1.01 * d) / p.bx);
+    const double dxsi = -xs + epsi * p.xainv - (xs * d) * p.xainv;
+    const double deta = -et + epsi * p.bxinv + (et * d) * p.bxinv;
+    m1 = nanmax(m1, (-1.01 * d) * p.xainv);
+    m2 = nanmax(m2, (1.01 * d) * p.bxinv);
     m3 = nanmax(m3, nanmax((-1.01 * dxsi) / xs, (-1.01 * deta) / et));
   }
-  double* dst = partials + (size_t)blockIdx.x * 3;
   const double b1 = block_nanmax(m1, red);
   const double b2 = block_nanmax(m2, red);
   const double b3 = block_nanmax(m3, red);
   if (threadIdx.x == 0) {
-    dst[0] = b1;
-    dst[1] = b2;
-    dst[2] = b3;
+    *part(partials, 0) = b1;
+    *part(partials, 1) = b2;
+    *part(partials, 2) = b3;
   }
   if (!finish_blocks(partials, counter, 3, 0, fin)) return;
   if (threadIdx.x < 3) res[threadIdx.x] = fin[threadIdx.x];
 }
 
-// The search pass: at the point (x, xsi, eta) + t (dx, dxsi, dxsi) (when dx is given)
+// The search pass: at the point (x, xsi, eta) + t (dx, dxsi, deta) (when dx is given)
 // and multipliers lam, gvec = P (1/ux1) + Q (1/xl1) and, when resid, the sum of squares
 // and largest magnitude of the residual's n-sized parts (sttopt/mma.py:399-434).  With
 // x = xval and no step it gives mmasub's b + fval (:285).
 // res = [gvec (m) | sum of squares | max].
 template <int MB, bool G>
-__global__ void __launch_bounds__(kMmaThreads) mma_search_kernel(
+__global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
     const double* __restrict__ dx, double t, MVec lam, double epsi, int resid, double* __restrict__ partials,
     unsigned* __restrict__ counter, double* __restrict__ res) {
-  __shared__ double red[kMmaThreads / 32];
+  __shared__ double red[kMmaThreads / 32 * (kMmaMaxM + 1)];
   __shared__ double fin[kMmaMaxM + 2];
+  constexpr bool kSlots = MB <= 20;  // static shared memory stays under 48 KB
+  __shared__ double slots[kSlots ? MB * kMmaThreads : 1];
   const int m = c.m;
-  double gv[MB];
-#pragma unroll
-  for (int i = 0; i < MB; ++i) gv[i] = 0.0;
+  std::conditional_t<kSlots, SlotSums<MB>, RowSums<MB>> gv;
+  if constexpr (kSlots) gv.slots = slots;
+  gv.zero();
   double ss = 0.0, mx = 0.0;
-  for (long long j = blockIdx.x * (long long)kMmaThreads + threadIdx.x; j < c.n;
-       j += (long long)gridDim.x * kMmaThreads) {
-    const ColFixed f = load_fixed<G>(c, j);
-    double xv = x[j], xs = 0.0, et = 0.0;
-    if (resid) {
-      xs = xsi[j];
-      et = eta[j];
+  for (long long base = blockIdx.x * (long long)kMmaThreads; base < c.n; base += (long long)gridDim.x * kMmaThreads) {
+    const long long j = base + threadIdx.x;
+    const bool ok = j < c.n;
+    ColFixed f{};
+    ColPoint p{};
+    double xs = 0.0, et = 0.0;
+    if (ok) {
+      f = load_fixed<G>(c, j);
+      double xv = x[j];
+      if (resid) {
+        xs = xsi[j];
+        et = eta[j];
+      }
+      if (dx) step_point(xv, xs, et, dx[j], t, epsi, f.alfa, f.beta);
+      p = point_of(f, xv);
     }
-    if (dx) step_point(xv, xs, et, dx[j], t, epsi, f.alfa, f.beta);
-    const ColPoint p = point_of(f, xv);
     double plam = 0.0, qlam = 0.0;
+    constexpr int CH = row_chunk<MB>();
 #pragma unroll
-    for (int i = 0; i < MB; ++i) {
-      if (i < m) {
-        double P, Q;
-        load_pq<G>(c, f, i, j, P, Q);
-        plam = fma(lam.v[i], P, plam);
-        qlam = fma(lam.v[i], Q, qlam);
-        gv[i] = fma(P, p.uxinv1, gv[i]);
-        gv[i] = fma(Q, p.xlinv1, gv[i]);
+    for (int i0 = 0; i0 < MB; i0 += CH) {
+      if (i0 < m) {
+        double ra[CH], rb[CH];
+        if (ok) {
+          load_rows<CH, G>(c, i0, j, ra, rb);
+        } else {
+#pragma unroll
+          for (int u = 0; u < CH; ++u) ra[u] = rb[u] = 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 + u;
+          if (i < m) {
+            double P, Q;
+            rows_pq<G>(f, ra[u], rb[u], P, Q);
+            plam = fma(lam.v[i], P, plam);
+            qlam = fma(lam.v[i], Q, qlam);
+            gv.add(i, fma(P, p.uxinv1, Q * p.xlinv1));
+          }
+        }
       }
     }
-    if (resid) resid_n(f.p0 + plam, f.q0 + qlam, p, xs, et, epsi, ss, mx);
+    if (ok && resid) resid_n(f.p0 + plam, f.q0 + qlam, p, xs, et, epsi, ss, mx);
   }
   const int kp = m + 2, ks = m + 1;
-  double* dst = partials + (size_t)blockIdx.x * kp;
-#pragma unroll
-  for (int i = 0; i < MB; ++i) {
-    if (i < m) {
-      const double v = block_total(gv[i], red);
-      if (threadIdx.x == 0) dst[i] = v;
-    }
-  }
+  gv.write(m, partials, 0, red + kMmaThreads / 32);
   const double v = block_total(ss, red);
   const double u = block_nanmax(mx, red);
   if (threadIdx.x == 0) {
-    dst[m] = v;
-    dst[ks] = u;
+    *part(partials, m) = v;
+    *part(partials, ks) = u;
   }
   if (!finish_blocks(partials, counter, kp, ks, fin)) return;
   for (int e = threadIdx.x; e < kp; e += kMmaThreads) res[e] = fin[e];
@@ -537,7 +746,7 @@ __global__ void __launch_bounds__(kMmaThreads) mma_search_kernel(
 
 namespace {
 
-constexpr int kAsmBlocks = 2 * 148, kPassBlocks = 4 * 148;
+constexpr int kAsmBlocks = 2 * 148, kPassBlocks = 2 * 148;  // the resident blocks, 2 an SM
 constexpr int kMaxHalvings = 50;   // sttopt/mma.py:289
 constexpr int kMaxNewton = 200;    // sttopt/mma.py:442
 
@@ -558,11 +767,17 @@ Kernels kernels_of() {
 }
 template <bool G>
 Kernels pick_kernels(int m) {
-  if (m <= 4) return kernels_of<4, G>();
-  if (m <= 8) return kernels_of<8, G>();
-  if (m <= 16) return kernels_of<16, G>();
-  if (m <= 32) return kernels_of<32, G>();
-  return kernels_of<64, G>();
+  switch (mma_bucket(m)) {
+    case 4: return kernels_of<4, G>();
+    case 8: return kernels_of<8, G>();
+    case 12: return kernels_of<12, G>();
+    case 16: return kernels_of<16, G>();
+    case 20: return kernels_of<20, G>();
+    case 24: return kernels_of<24, G>();
+    case 32: return kernels_of<32, G>();
+    case 48: return kernels_of<48, G>();
+    default: return kernels_of<64, G>();
+  }
 }
 
 // Workspace: [alfa | beta | rxm | dx] (n each), block partials, results, counters.
@@ -583,10 +798,10 @@ size_t carve(int m, long long n, char* base, MmaWs* w) {
   };
   double* v[4];
   for (auto& p : v) p = reinterpret_cast<double*>(take(8 * (size_t)n));
-  double* part = reinterpret_cast<double*>(take(8 * partial_doubles(m)));
+  double* parts = reinterpret_cast<double*>(take(8 * partial_doubles(m)));
   double* res = reinterpret_cast<double*>(take(8 * ((size_t)m * m + 2 * m + 8)));
   unsigned* cnt = reinterpret_cast<unsigned*>(take(4 * sizeof(unsigned)));
-  if (w) *w = {v[0], v[1], v[2], v[3], part, res, cnt};
+  if (w) *w = {v[0], v[1], v[2], v[3], parts, res, cnt};
   return off;
 }
 
@@ -758,7 +973,7 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
   const long long tiles = (c.n + kMmaThreads - 1) / kMmaThreads;
   const int ga = (int)std::min<long long>(tiles, kAsmBlocks), gp = (int)std::min<long long>(tiles, kPassBlocks);
   const Kernels k = pick_kernels<G>(m);
-  const size_t smem = assemble_smem(m);
+  const size_t smem = assemble_smem(m, mma_bucket(m));
   STT_TRY(check_cuda(cudaFuncSetAttribute((const void*)k.assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem),
                      "mma: assemble shared memory"));
@@ -785,7 +1000,7 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
     std::copy(R.begin() + m, R.begin() + 2 * m, h.begin());
     std::copy(R.begin() + 2 * m, R.begin() + 2 * m + (size_t)m * m, A.begin());
     ssn = R[nres - 2];
-    mxn = R[nres - 1];
+    mxn = ssn != ssn ? NAN : R[nres - 1];
     return STT_OK;
   };
 
@@ -840,7 +1055,7 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
                                              w.counters + 2, w.res);
         STT_TRY(check_launch("mma_search_kernel"));
         STT_TRY(fetch((size_t)m + 2, "mma: line search"));
-        double ssc = R[m], mxcn = R[m + 1], ssmc = 0.0, mxmc = -INFINITY;
+        double ssc = R[m], mxcn = ssc != ssc ? NAN : R[m + 1], ssmc = 0.0, mxmc = -INFINITY;
         resid_m(D, C, R.data(), epsi, ssmc, mxmc);
         resinew = std::sqrt(ssc + ssmc);
         mxc = hmax(mxcn, mxmc);
