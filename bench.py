@@ -66,6 +66,10 @@ def parse():
                     help="skip the batched uneven multi-problem measurement")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the library's launch-shape heuristics instead of the autotuner's measured choices")
+    ap.add_argument("--no-mma", action="store_true", help="skip the MMA step measurement")
+    ap.add_argument("--mma-only", action="store_true", help="only the MMA step measurement")
+    ap.add_argument("--mma-vars", type=int, default=2 * NELX * NELY,
+                    help="design variables of the MMA step (default 2 x 2048 x 1024; smaller for profiling)")
     ap.add_argument("--no-dropin", action="store_true",
                     help="skip the end-to-end timing through the reference-signature chain")
     ap.add_argument("--ref-budget", type=float, default=240.0,
@@ -304,6 +308,92 @@ def run_uneven(dev, steps=2, warmup=1, memory_budget=None):
                                                         ", in waves whose estimated memory fits the budget")}
 
 
+# ---- the MMA step the optimisation loop takes after each evaluation ----------------------
+
+MMA_M = 17  # constraint rows of the space-time problem (volume, start points, stage bounds, ...)
+
+
+def mma_workload(n, m, seed=SEED):
+    """A seeded unit-box MMA step of the space-time problem's shape: n design variables
+    (density and time field), m constraint rows, per-variable trust regions, the
+    adaptive-asymptote branch (iteration 2)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    xval = rng.uniform(0.05, 0.95, n)
+    xold1 = np.clip(xval + rng.normal(0, 0.02, n), 0, 1)
+    xold2 = np.clip(xold1 + rng.normal(0, 0.02, n), 0, 1)
+    return dict(xval=xval, xold1=xold1, xold2=xold2, df0dx=rng.normal(0, 1e-6, n), fval=rng.normal(0, 0.1, m),
+                dfdx=rng.normal(0, 1e-6, (m, n)), move=rng.uniform(0.02, 0.1, n), low=xval - 0.2, upp=xval + 0.2)
+
+
+def run_mma(dev, steps=3, warmup=1, cpu_sample=1 << 18, n=2 * NELX * NELY):
+    """``mma.mmasub`` on 2 x 2048 x 1024 variables and 17 constraints (the step after each
+    evaluation), timed with CUDA events; the HBM roofline of its passes (algorithmic bytes:
+    one m x n read and the n-vectors of each pass); the oracle's mmasub on a sample of
+    ``cpu_sample`` variables on the host."""
+    import numpy as np
+    import torch
+
+    from sttopt_b200 import mma
+
+    m = MMA_M
+    p = mma_workload(n, m)
+    t = {k: torch.as_tensor(v).to(dev) for k, v in p.items()}
+    zeros = torch.zeros(m, dtype=torch.float64, device=dev)
+    cc = torch.full((m,), 1000.0, dtype=torch.float64, device=dev)
+    one, zero = torch.ones(n, dtype=torch.float64, device=dev), torch.zeros(n, dtype=torch.float64, device=dev)
+    tr = mma.trust_region_params(t["move"], one)
+
+    def call(stats=None):
+        return mma.mmasub(m, n, 2, t["xval"], zero, one, t["xold1"], t["xold2"], 0.0, t["df0dx"], t["fval"],
+                          t["dfdx"], t["low"], t["upp"], 1.0, zeros, cc, zeros, raa0=1e-5 / n, stats=stats, **tr)
+
+    for _ in range(warmup):
+        call()
+    stats: dict = {}
+    call(stats)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        call()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    newton, tries = stats["subsolv_newton_steps"], stats["subsolv_line_search_tries"]
+    # bytes a variable: assemble 8m + 112 (with the pending step), step 8m + 88, search 8m + 88
+    per_var = newton * (8 * m + 112 + 8 * m + 88) + tries * (8 * m + 88) + (8 * m + 112)
+    achieved = per_var * n / (ms / 1e3) / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    # CPU: the oracle's mmasub (NumPy, FP64) on a sample of the same workload
+    from oracle import mma_oracle
+
+    q = mma_workload(cpu_sample, m)
+    trq = {"asyinit": q["move"], "asyclamp_min": 0.02 * q["move"], "asyclamp_max": 20.0 * q["move"],
+           "move": q["move"]}
+    from threadpoolctl import threadpool_limits
+
+    t0 = time.perf_counter()
+    with threadpool_limits(limits=1):
+        mma_oracle.mmasub(m, cpu_sample, 2, q["xval"], np.zeros(cpu_sample), np.ones(cpu_sample), q["xold1"],
+                          q["xold2"], 0.0, q["df0dx"], q["fval"], q["dfdx"], q["low"], q["upp"], 1.0, np.zeros(m),
+                          np.full(m, 1000.0), np.zeros(m), raa0=1e-5 / cpu_sample, **trq)
+    cpu_s = time.perf_counter() - t0
+    return {"metric": f"mmasub calls/s (unit-box MMA step: {n} variables, 17 constraints, FP64)",
+            "value": 1e3 / ms, "unit": "calls/s", "ms_per_call": ms, "steps": steps, "warmup": warmup,
+            "newton_steps": newton, "line_search_tries": tries,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback",
+                         "bytes_per_variable": per_var,
+                         "basis": "algorithmic bytes of all passes of the call (dfdx once a pass, the n-vectors a "
+                                  "pass reads and writes) over the call's device time"},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "calls/s", "cores": 1, "kind": "port",
+                             "sample": f"the oracle's mmasub (NumPy) on {cpu_sample} variables of the same workload "
+                                       f"({cpu_s:.2f} s; the full call has {n // cpu_sample}x the variables)"}}
+
+
 # ---- clocks -----------------------------------------------------------------------
 
 class ClockSampler:
@@ -393,6 +483,10 @@ def main():
     if args.uneven_only:
         print(json.dumps({"batched_uneven": run_uneven(dev, steps=max(args.steps, 1), warmup=max(args.warmup, 1))}),
               flush=True)
+        return 0
+    if args.mma_only:
+        print(json.dumps({"mma_unit_box_step": run_mma(dev, steps=max(args.steps, 1), warmup=max(args.warmup, 1),
+                                                       n=args.mma_vars)}), flush=True)
         return 0
     info: dict = {}
     from sttopt_b200 import autotune
@@ -531,6 +625,8 @@ def main():
             torch.cuda.empty_cache()
             extra["batched_uneven"] = run_uneven(dev)
             extra["batched_uneven_budget"] = run_uneven(dev, memory_budget=40 << 30)
+        if not args.no_mma:
+            extra["mma_unit_box_step"] = run_mma(dev)
         if world == 1 and not args.no_cpu_baseline:
             s = cpu_full_evaluations(1, args.cpu_budget)
             extra["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": s["cores"], "kind": "port",

@@ -56,17 +56,20 @@ struct MmaCols {
 
 STT_DEV double nanmax(double a, double b) { return (a != a || b != b) ? NAN : (a > b ? a : b); }
 
-// The separable approximation's coefficients of one gradient entry g
-// (sttopt/mma.py:263-284): p = (max(g,0) + 0.001 |g| + r) ux2, q = (max(-g,0) + ...) xl2.
-STT_DEV void approx_pq(double g, double r, double ux2, double xl2, double& p, double& q) {
+// The separable approximation of one gradient entry g (sttopt/mma.py:263-284), factored
+// as P = P' ux2 and Q = Q' xl2 with P' = max(g, 0) + (0.001 |g| + r) and
+// Q' = max(-g, 0) + (0.001 |g| + r): the reference's own operations before its
+// multiplication by ux2 / xl2, which the passes fold into per-variable constants.
+STT_DEV void approx_pq1(double g, double r, double& p1, double& q1) {
   const double pp = fmax(g, 0.0), qq = fmax(-g, 0.0);
   const double pq = 0.001 * (pp + qq) + r;
-  p = (pp + pq) * ux2;
-  q = (qq + pq) * xl2;
+  p1 = pp + pq;
+  q1 = qq + pq;
 }
 
+// A variable's fixed data; P = P' sp and Q = Q' sq (sp = sq = 1 when P, Q are given).
 struct ColFixed {
-  double low, upp, alfa, beta, p0, q0, ux2f, xl2f, r;
+  double low, upp, alfa, beta, p0, q0, sp, sq, r;
 };
 
 template <bool G>
@@ -79,52 +82,68 @@ STT_DEV ColFixed load_fixed(const MmaCols& c, long long j) {
   if constexpr (G) {
     const double xv = c.xval[j];
     const double ux1 = f.upp - xv, xl1 = xv - f.low;
-    f.ux2f = ux1 * ux1;
-    f.xl2f = xl1 * xl1;
+    f.sp = ux1 * ux1;
+    f.sq = xl1 * xl1;
     f.r = c.rxm[j];
-    approx_pq(c.df0dx[j], f.r, f.ux2f, f.xl2f, f.p0, f.q0);
+    double p1, q1;
+    approx_pq1(c.df0dx[j], f.r, p1, q1);
+    f.p0 = p1 * f.sp;
+    f.q0 = q1 * f.sq;
   } else {
     f.p0 = c.p0[j];
     f.q0 = c.q0[j];
-    f.ux2f = f.xl2f = f.r = 0.0;
+    f.sp = f.sq = 1.0;
+    f.r = 0.0;
   }
   return f;
 }
 
-// Rows are read in chunks: the CH entries of column j in rows [i0, i0 + CH), the row
-// clamped to m - 1 so that the loads are unconditional and issue back to back before
-// any of them is used (a guarded load per row would wait out one memory latency a row).
-template <int MB>
+// Rows are read in chunks: the CH entries of column j in rows [i0, i0 + CH), all loads
+// issued before any is used (a load guarded together with its use would wait out one
+// memory latency a row).  Rows past m - 1 read as 0.
+template <int MB, bool G>
 constexpr int row_chunk() {
-  return MB <= 24 ? MB : 16;
+  if constexpr (G) {
+    return MB <= 20 ? MB : (MB % 16 == 0 ? 16 : 8);
+  } else {
+    return MB <= 12 ? MB : (MB % 8 == 0 ? 8 : 4);  // two loads an entry
+  }
 }
 template <int CH, bool G>
 STT_DEV void load_rows(const MmaCols& c, int i0, long long j, double (&a)[CH], double (&b)[CH]) {
-  const int nv = min(CH, c.m - i0);  // rows past m - 1 reread row i0
-  const long long o0 = (long long)i0 * c.ld + j;
+  const int nv = c.m - i0;
+  long long o = (long long)i0 * c.ld + j;
 #pragma unroll
   for (int u = 0; u < CH; ++u) {
-    const long long o = u < nv ? o0 + u * c.ld : o0;
-    if constexpr (G) {
-      a[u] = __ldg(c.dfdx + o);
-      b[u] = 0.0;
-    } else {
-      a[u] = __ldg(c.P + o);
-      b[u] = __ldg(c.Q + o);
+    a[u] = b[u] = 0.0;
+    if (u < nv) {
+      if constexpr (G) {
+        a[u] = __ldg(c.dfdx + o);
+      } else {
+        a[u] = __ldg(c.P + o);
+        b[u] = __ldg(c.Q + o);
+      }
     }
+    o += c.ld;
   }
 }
+// P', Q' of one entry from what load_rows read.
 template <bool G>
-STT_DEV void rows_pq(const ColFixed& f, double a, double b, double& P, double& Q) {
+STT_DEV void rows_pq1(const ColFixed& f, double a, double b, double& p1, double& q1) {
   if constexpr (G) {
-    approx_pq(a, f.r, f.ux2f, f.xl2f, P, Q);
+    approx_pq1(a, f.r, p1, q1);
   } else {
-    P = a;
-    Q = b;
+    p1 = a;
+    q1 = b;
   }
 }
 
-// The point's distances to the asymptotes and their inverses (sttopt/mma.py:443-452).
+// The per-variable factors of a gradient entry's terms at a point: gvec's
+// P / ux1 + Q / xl1 = P' A + Q' B and GG's P / ux2 - Q / xl2 = P' C - Q' D.
+struct ColFactors {
+  double A, B, C, D;
+};
+
 // Divisions by the point's four distances are multiplications by these reciprocals (one
 // division each), which rounds within an ulp of the reference's quotients.
 struct ColPoint {
@@ -145,6 +164,9 @@ STT_DEV ColPoint point_of(const ColFixed& f, double x) {
   p.xainv = 1.0 / p.xa;
   p.bxinv = 1.0 / p.bx;
   return p;
+}
+STT_DEV ColFactors factors_of(const ColFixed& f, const ColPoint& p) {
+  return {f.sp * p.uxinv1, f.sq * p.xlinv1, f.sp * p.uxinv2, f.sq * p.xlinv2};
 }
 
 // old + t * d for x, xsi, eta, with dxsi / deta formed from dx as subsolv does
@@ -470,8 +492,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
       }
       p = point_of(f, xv);
     }
-    double plam = 0.0, qlam = 0.0;
-    constexpr int CH = row_chunk<MB>();
+    const ColFactors k = factors_of(f, p);
+    double lp = 0.0, lq = 0.0;  // sum of lam_i P'_i, lam_i Q'_i
+    constexpr int CH = row_chunk<MB, G>();
 #pragma unroll
     for (int i0 = 0; i0 < MB; i0 += CH) {
       if (i0 < m) {
@@ -486,20 +509,20 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
         for (int u = 0; u < CH; ++u) {
           const int i = i0 + u;
           if (i < m) {
-            double P, Q;
-            rows_pq<G>(f, ra[u], rb[u], P, Q);
-            plam = fma(lam.v[i], P, plam);
-            qlam = fma(lam.v[i], Q, qlam);
-            gv.add(i, fma(P, p.uxinv1, Q * p.xlinv1));
-            gs[i * kMmaLd8 + tid] = P * p.uxinv2 - Q * p.xlinv2;
+            double p1, q1;
+            rows_pq1<G>(f, ra[u], rb[u], p1, q1);
+            lp = fma(lam.v[i], p1, lp);
+            lq = fma(lam.v[i], q1, lq);
+            gv.add(i, fma(p1, k.A, q1 * k.B));
+            gs[i * kMmaLd8 + tid] = fma(p1, k.C, -(q1 * k.D));
           }
         }
       }
     }
     double w = 0.0, delx = 0.0;
     if (ok) {
-      plam = f.p0 + plam;
-      qlam = f.q0 + qlam;
+      const double plam = f.p0 + f.sp * lp;
+      const double qlam = f.q0 + f.sq * lq;
       resid_n(plam, qlam, p, xs, et, epsi, ss, mx);
       double diagx;
       newton_col(plam, qlam, p, xs, et, epsi, delx, diagx);
@@ -623,8 +646,8 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
     const ColFixed f = load_fixed<G>(c, j);
     const double xv = x[j], xs = xsi[j], et = eta[j];
     const ColPoint p = point_of(f, xv);
-    double plam = 0.0, qlam = 0.0, gd = 0.0;
-    constexpr int CH = row_chunk<MB>();
+    double lp = 0.0, lq = 0.0, dp = 0.0, dq = 0.0;  // lam . P', lam . Q', dlam . P', dlam . Q'
+    constexpr int CH = row_chunk<MB, G>();
 #pragma unroll
     for (int i0 = 0; i0 < MB; i0 += CH) {
       if (i0 < m) {
@@ -634,17 +657,19 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
         for (int u = 0; u < CH; ++u) {
           const int i = i0 + u;
           if (i < m) {
-            double P, Q;
-            rows_pq<G>(f, ra[u], rb[u], P, Q);
-            plam = fma(lam.v[i], P, plam);
-            qlam = fma(lam.v[i], Q, qlam);
-            gd = fma(P * p.uxinv2 - Q * p.xlinv2, dlam.v[i], gd);
+            double p1, q1;
+            rows_pq1<G>(f, ra[u], rb[u], p1, q1);
+            lp = fma(lam.v[i], p1, lp);
+            lq = fma(lam.v[i], q1, lq);
+            dp = fma(dlam.v[i], p1, dp);
+            dq = fma(dlam.v[i], q1, dq);
           }
         }
       }
     }
-    plam = f.p0 + plam;
-    qlam = f.q0 + qlam;
+    const ColFactors k = factors_of(f, p);
+    const double plam = f.p0 + f.sp * lp, qlam = f.q0 + f.sq * lq;
+    const double gd = fma(dp, k.C, -(dq * k.D));  // GG^T dlam
     double delx, diagx;
     newton_col(plam, qlam, p, xs, et, epsi, delx, diagx);
     const double w = 1.0 / diagx;
@@ -703,8 +728,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
       if (dx) step_point(xv, xs, et, dx[j], t, epsi, f.alfa, f.beta);
       p = point_of(f, xv);
     }
-    double plam = 0.0, qlam = 0.0;
-    constexpr int CH = row_chunk<MB>();
+    const ColFactors k = factors_of(f, p);
+    double lp = 0.0, lq = 0.0;
+    constexpr int CH = row_chunk<MB, G>();
 #pragma unroll
     for (int i0 = 0; i0 < MB; i0 += CH) {
       if (i0 < m) {
@@ -719,16 +745,16 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
         for (int u = 0; u < CH; ++u) {
           const int i = i0 + u;
           if (i < m) {
-            double P, Q;
-            rows_pq<G>(f, ra[u], rb[u], P, Q);
-            plam = fma(lam.v[i], P, plam);
-            qlam = fma(lam.v[i], Q, qlam);
-            gv.add(i, fma(P, p.uxinv1, Q * p.xlinv1));
+            double p1, q1;
+            rows_pq1<G>(f, ra[u], rb[u], p1, q1);
+            lp = fma(lam.v[i], p1, lp);
+            lq = fma(lam.v[i], q1, lq);
+            gv.add(i, fma(p1, k.A, q1 * k.B));
           }
         }
       }
     }
-    if (ok && resid) resid_n(f.p0 + plam, f.q0 + qlam, p, xs, et, epsi, ss, mx);
+    if (ok && resid) resid_n(f.p0 + f.sp * lp, f.q0 + f.sq * lq, p, xs, et, epsi, ss, mx);
   }
   const int kp = m + 2, ks = m + 1;
   gv.write(m, partials, 0, red + kMmaThreads / 32);
