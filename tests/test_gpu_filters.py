@@ -86,6 +86,7 @@ def test_filtered_objective_gradient_through_the_filter(pkg, beta):
     xp = filters.apply_density_filter(xv, H) if beta is None else filters.filter_and_project(xv, H, beta, 0.5)[0]
     L = spacetime.objective(xp, w, **kw)
     (g,) = torch.autograd.grad(L, [xv])
+    L = L.detach()
     assert abs(float(fused["objective"]) - float(L)) <= 1e-12 * abs(float(L))
     assert float((fused["gradient"] - g).norm() / g.norm()) < 1e-12
     assert torch.equal(fused["xPhys"], xp.detach())

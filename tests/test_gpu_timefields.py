@@ -16,6 +16,8 @@ reference's outputs (golden fixtures made by running it on the same seeded input
   poisson maps; solves at rtol 1e-10): fields 1e-8, gradients 1e-7.
 """
 
+import warnings
+
 import numpy as np
 import pytest
 import torch
@@ -42,8 +44,11 @@ def test_batched_whole_and_gravity_compliance_smooth(pkg, key, sparse_C):
     C = gravity.gravity_load_matrix(nelx, nely)
     if sparse_C:  # the production loop's torch CSR form of the matrix (a library SpMV)
         csr = C.tocsr()
-        C = torch.sparse_csr_tensor(torch.as_tensor(csr.indptr), torch.as_tensor(csr.indices),
-                                    torch.as_tensor(csr.data), size=csr.shape).to(DEV)
+        with warnings.catch_warnings():  # torch's beta notice for CSR tensors
+            warnings.simplefilter("ignore", UserWarning)
+            C = torch.sparse_csr_tensor(torch.as_tensor(csr.indptr), torch.as_tensor(csr.indices),
+                                        torch.as_tensor(csr.data), size=csr.shape,
+                                        check_invariants=True).to(DEV)
     x = T(g[f"{key}_x"]).requires_grad_(True)
     tp = T(g[f"{key}_t"]).requires_grad_(True)
     c, stages, U = compliance.batched_whole_and_gravity_compliance(
