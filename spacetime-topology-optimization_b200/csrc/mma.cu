@@ -101,6 +101,15 @@ STT_DEV ColFixed load_fixed(const MmaCols& c, long long j) {
 // Rows are read in chunks: the CH entries of column j in rows [i0, i0 + CH), all loads
 // issued before any is used (a load guarded together with its use would wait out one
 // memory latency a row).  Rows past m - 1 read as 0.
+// The step and search passes take smaller chunks, for three blocks an SM.
+template <int MB, bool G>
+constexpr int pass_chunk() {
+  if constexpr (G) {
+    return MB <= 12 ? MB : (MB % 10 == 0 ? 10 : 8);
+  } else {
+    return MB <= 8 ? MB : 4;
+  }
+}
 template <int MB, bool G>
 constexpr int row_chunk() {
   if constexpr (G) {
@@ -233,11 +242,32 @@ STT_DEV double block_nanmax(double v, double* red) {
 // Block partials are stored entry-major: entry e of block b at partials[e * grid + b].
 STT_DEV double* part(double* partials, int e) { return partials + (size_t)e * gridDim.x + blockIdx.x; }
 
+constexpr int kFoldMax = 16;  // a lane folds up to 16 blocks: grids of at most 512 blocks
+
+// One partial entry over all nb blocks (p: its nb values): lane l takes blocks l, l + 32,
+// ... with every load issued before the first is used, then the lanes combine in a fixed
+// butterfly.  The result does not depend on the order the blocks ran in.
+STT_DEV double fold_entry(const double* p, int nb, bool sum, int lane) {
+  double v[kFoldMax];
+#pragma unroll
+  for (int q = 0; q < kFoldMax; ++q) {
+    const int b = lane + 32 * q;
+    v[q] = b < nb ? __ldcg(p + b) : (sum ? 0.0 : -INFINITY);
+  }
+  double t = v[0];
+#pragma unroll
+  for (int q = 1; q < kFoldMax; ++q) t = sum ? t + v[q] : nanmax(t, v[q]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double u = __shfl_xor_sync(0xffffffffu, t, o);
+    t = sum ? t + u : nanmax(t, u);
+  }
+  return t;
+}
+
 // After this block wrote its kp partials (the first ks summed, the rest max-reduced):
 // the last block to arrive folds every entry over all blocks into fin[kp] (shared
-// memory) and returns true.  A warp folds an entry: lane l takes blocks l, l + 32, ... in
-// order, then the lanes combine in a fixed butterfly, so the result does not depend on
-// which block finished last.
+// memory), a warp an entry, and returns true.
 STT_DEV bool finish_blocks(const double* partials, unsigned* counter, int kp, int ks, double* fin) {
   __shared__ bool is_last;
   __threadfence();
@@ -248,17 +278,7 @@ STT_DEV bool finish_blocks(const double* partials, unsigned* counter, int kp, in
   __threadfence();
   const int lane = threadIdx.x & 31, nb = gridDim.x;
   for (int e = threadIdx.x >> 5; e < kp; e += kMmaThreads / 32) {
-    const bool sum = e < ks;
-    double t = sum ? 0.0 : -INFINITY;
-    for (int b = lane; b < nb; b += 32) {
-      const double v = __ldcg(partials + (size_t)e * nb + b);
-      t = sum ? t + v : nanmax(t, v);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double u = __shfl_xor_sync(0xffffffffu, t, o);
-      t = sum ? t + u : nanmax(t, u);
-    }
+    const double t = fold_entry(partials + (size_t)e * nb, nb, e < ks, lane);
     if (lane == 0) fin[e] = t;
   }
   __syncthreads();
@@ -422,8 +442,10 @@ STT_DEV void dmma_f64(double (&d)[2], double a, double b) {
 __host__ __device__ inline int gram_side(int m) { return (m + 8) >> 3; }
 __host__ __device__ inline int gram_tiles(int m) { return gram_side(m) * (gram_side(m) + 1) / 2; }
 __host__ __device__ inline int tile_index(int I, int K, int t8) { return I * t8 - I * (I - 1) / 2 + (K - I); }
-// Partial entries of the assemble pass: [gvec (m) | sum of squares | tiles x 64 | max].
-__host__ __device__ inline int assemble_kp(int m) { return m + 2 + gram_tiles(m) * 64; }
+// The product's upper triangle (i <= k <= m, row m being delx), packed row by row.
+__host__ __device__ inline int packed_index(int i, int k, int m1) { return i * m1 - i * (i - 1) / 2 + (k - i); }
+// Partial entries of the assemble pass: [gvec (m) | sum of squares | packed product | max].
+__host__ __device__ inline int assemble_kp(int m) { return m + 2 + (m + 1) * (m + 2) / 2; }
 // Its dynamic shared memory: the GG tile (or, later, the folded entries), 1/diagx, a
 // block-sum scratch, and the row-sum slots or shuffle scratch.
 inline size_t assemble_smem(int m, int mb) {
@@ -449,7 +471,7 @@ template <int MB, bool G>
 __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
     MmaCols c, double* __restrict__ x, double* __restrict__ xsi, double* __restrict__ eta,
     const double* __restrict__ dx, int pend, double t_pend, double eps_pend, MVec lam, double epsi,
-    double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ res) {
+    double* __restrict__ partials) {
   extern __shared__ double sm[];
   constexpr int T8 = (MB + 8) / 8;  // tile side for the largest m of the bucket
   constexpr int NT = T8 * (T8 + 1) / 2;
@@ -530,7 +552,13 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
     }
     gs[m * kMmaLd8 + tid] = delx;
     ws[tid] = w;
-    __syncthreads();
+    // Up to 31 constraints a warp's tiles read only the 32 variables the warp wrote, so
+    // the warps need not wait for one another.
+    if constexpr (KSPLIT) {
+      __syncwarp();
+    } else {
+      __syncthreads();
+    }
     if constexpr (KSPLIT) {
 #pragma unroll 2
       for (int k4 = 0; k4 < 8; ++k4) {
@@ -568,12 +596,18 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
         }
       }
     }
-    __syncthreads();
+    if constexpr (KSPLIT) {
+      __syncwarp();
+    } else {
+      __syncthreads();
+    }
   }
 
-  // Gram partials: entry m + 1 + t * 64 + r * 8 + c of tile t = (I, K) holds the
-  // product's (8 I + r, 8 K + c).
+  // Product partials: entry m + 1 + packed_index(i, k) holds (i, k), i <= k <= m; tile
+  // t = (I, K) holds (8 I + r, 8 K + c) at r * 8 + c.
+  const int m1 = m + 1;
   if constexpr (KSPLIT) {
+    __syncthreads();    // every warp's tiles are done before the tile memory is reused
     double* red8 = sm;  // [8 warps][ntile][64]
     int q = 0;
 #pragma unroll
@@ -586,45 +620,70 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
           d[1] = acc[q][1];
         }
     __syncthreads();
-    for (int e = tid; e < ntile * 64; e += kMmaThreads) {
+    for (int e = tid; e < m1 * m1; e += kMmaThreads) {
+      const int i = e / m1, k = e % m1;
+      if (i > k) continue;
+      const size_t at = (size_t)tile_index(i >> 3, k >> 3, t8) * 64 + (i & 7) * 8 + (k & 7);
       double t = 0.0;
-      for (int w8 = 0; w8 < kMmaThreads / 32; ++w8) t += red8[(size_t)w8 * ntile * 64 + e];
-      *part(partials, m + 1 + e) = t;
+      for (int w8 = 0; w8 < kMmaThreads / 32; ++w8) t += red8[(size_t)w8 * ntile * 64 + at];
+      *part(partials, m + 1 + packed_index(i, k, m1)) = t;
     }
   } else {
 #pragma unroll
     for (int q = 0; q < TPW; ++q) {
       const int t = warp + 8 * q;
       if (t < ntile) {
-        *part(partials, m + 1 + t * 64 + fr * 8 + fc * 2) = acc[q][0];
-        *part(partials, m + 1 + t * 64 + fr * 8 + fc * 2 + 1) = acc[q][1];
+        int I = 0, rem = t;
+        while (rem >= t8 - I) {
+          rem -= t8 - I;
+          ++I;
+        }
+        const int K = I + rem;
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int i = 8 * I + fr, k = 8 * K + fc * 2 + v;
+          if (i <= k && k <= m) *part(partials, m + 1 + packed_index(i, k, m1)) = acc[q][v];
+        }
       }
     }
   }
-  const int kp = assemble_kp(m), ks = kp - 1;
+  const int ks = assemble_kp(m) - 1;
   gv.write(m, partials, 0, tail);
-  {
-    const double t = block_total(ss, wred);
-    if (tid == 0) *part(partials, m) = t;
-    const double u = block_nanmax(mx, wred);
-    if (tid == 0) *part(partials, ks) = u;
-  }
-  double* fin = sm;
-  if (!finish_blocks(partials, counter, kp, ks, fin)) return;
-  auto gram = [&](int lo, int hi) {
-    return fin[m + 1 + tile_index(lo >> 3, hi >> 3, t8) * 64 + (lo & 7) * 8 + (hi & 7)];
-  };
-  for (int e = tid; e < m * m; e += kMmaThreads) {
-    const int i = e / m, k = e % m;
-    res[2 * m + e] = gram(min(i, k), max(i, k));
-  }
-  for (int i = tid; i < m; i += kMmaThreads) {
-    res[i] = fin[i];
-    res[m + i] = gram(i, m);
-  }
-  if (tid == 0) {
-    res[2 * m + m * m] = fin[m];
-    res[2 * m + m * m + 1] = fin[ks];
+  const double t = block_total(ss, wred);
+  if (tid == 0) *part(partials, m) = t;
+  const double u = block_nanmax(mx, wred);
+  if (tid == 0) *part(partials, ks) = u;
+}
+
+// Folds the assemble pass's block partials (entry-major, nb blocks) in block order, a
+// warp an entry on as many SMs as there are entries / 8, and writes
+// res = [gvec (m) | h (m) | A (m x m) | sum of squares | max].
+__global__ void __launch_bounds__(kMmaThreads) mma_fold_kernel(const double* __restrict__ partials, int nb, int m,
+                                                               double* __restrict__ res) {
+  const int kp = assemble_kp(m), ks = kp - 1, m1 = m + 1, lane = threadIdx.x & 31;
+  const int e = blockIdx.x * (kMmaThreads / 32) + (threadIdx.x >> 5);
+  if (e >= kp) return;
+  const double t = fold_entry(partials + (size_t)e * nb, nb, e < ks, lane);
+  if (lane != 0) return;
+  if (e < m) {
+    res[e] = t;
+  } else if (e == m) {
+    res[2 * m + m * m] = t;
+  } else if (e == ks) {
+    res[2 * m + m * m + 1] = t;
+  } else {
+    int i = 0, pe = e - m - 1;
+    while (pe >= m1 - i) {
+      pe -= m1 - i;
+      ++i;
+    }
+    const int k = i + pe;
+    if (k == m) {
+      if (i < m) res[m + i] = t;  // (m, m), delx' diag(1/diagx) delx, is not needed
+    } else {
+      res[2 * m + i * m + k] = t;
+      res[2 * m + k * m + i] = t;
+    }
   }
 }
 
@@ -633,7 +692,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
 // fraction-to-the-boundary limits max(-1.01 dx / (x - alfa)), max(1.01 dx / (beta - x))
 // and max(-1.01 dxsi / xsi, -1.01 deta / eta).  res = those three maxima.
 template <int MB, bool G>
-__global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
+__global__ void __launch_bounds__(kMmaThreads, 3) mma_step_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
     MVec lam, MVec dlam, double epsi, double* __restrict__ dx, double* __restrict__ partials,
     unsigned* __restrict__ counter, double* __restrict__ res) {
@@ -647,7 +706,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
     const double xv = x[j], xs = xsi[j], et = eta[j];
     const ColPoint p = point_of(f, xv);
     double lp = 0.0, lq = 0.0, dp = 0.0, dq = 0.0;  // lam . P', lam . Q', dlam . P', dlam . Q'
-    constexpr int CH = row_chunk<MB, G>();
+    constexpr int CH = pass_chunk<MB, G>();
 #pragma unroll
     for (int i0 = 0; i0 < MB; i0 += CH) {
       if (i0 < m) {
@@ -699,7 +758,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_step_kernel(
 // x = xval and no step it gives mmasub's b + fval (:285).
 // res = [gvec (m) | sum of squares | max].
 template <int MB, bool G>
-__global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
+__global__ void __launch_bounds__(kMmaThreads, 3) mma_search_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
     const double* __restrict__ dx, double t, MVec lam, double epsi, int resid, double* __restrict__ partials,
     unsigned* __restrict__ counter, double* __restrict__ res) {
@@ -730,7 +789,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
     }
     const ColFactors k = factors_of(f, p);
     double lp = 0.0, lq = 0.0;
-    constexpr int CH = row_chunk<MB, G>();
+    constexpr int CH = pass_chunk<MB, G>();
 #pragma unroll
     for (int i0 = 0; i0 < MB; i0 += CH) {
       if (i0 < m) {
@@ -772,12 +831,12 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_search_kernel(
 
 namespace {
 
-constexpr int kAsmBlocks = 2 * 148, kPassBlocks = 2 * 148;  // the resident blocks, 2 an SM
+constexpr int kAsmBlocks = 2 * 148, kPassBlocks = 3 * 148;  // the resident blocks: 2 and 3 an SM
+static_assert(kAsmBlocks <= 32 * kFoldMax && kPassBlocks <= 32 * kFoldMax, "a fold lane takes at most kFoldMax blocks");
 constexpr int kMaxHalvings = 50;   // sttopt/mma.py:289
 constexpr int kMaxNewton = 200;    // sttopt/mma.py:442
 
-using AsmFn = void (*)(MmaCols, double*, double*, double*, const double*, int, double, double, MVec, double, double*,
-                       unsigned*, double*);
+using AsmFn = void (*)(MmaCols, double*, double*, double*, const double*, int, double, double, MVec, double, double*);
 using StepFn = void (*)(MmaCols, const double*, const double*, const double*, MVec, MVec, double, double*, double*,
                         unsigned*, double*);
 using SearchFn = void (*)(MmaCols, const double*, const double*, const double*, const double*, double, MVec, double,
@@ -1018,9 +1077,12 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
   double t_pend = 0.0, eps_pend = 0.0;
   auto assemble = [&](double epsi, double& ssn, double& mxn) -> int {
     k.assemble<<<ga, kMmaThreads, smem, st>>>(c, x, xsi, eta, w.dx, pend, t_pend, eps_pend, mvec(S.lam), epsi,
-                                              w.partials, w.counters + 0, w.res);
+                                              w.partials);
     pend = 0;
     STT_TRY(check_launch("mma_assemble_kernel"));
+    const int kp = assemble_kp(m), per = kMmaThreads / 32;
+    mma_fold_kernel<<<(kp + per - 1) / per, kMmaThreads, 0, st>>>(w.partials, ga, m, w.res);
+    STT_TRY(check_launch("mma_fold_kernel"));
     STT_TRY(fetch(nres, "mma: assemble"));
     std::copy(R.begin(), R.begin() + m, gvec.begin());
     std::copy(R.begin() + m, R.begin() + 2 * m, h.begin());
