@@ -11,10 +11,11 @@
 //
 // One Newton step is three passes over the variables: assemble (the residual at the
 // current point, the Newton right-hand side and the m x m matrix GG diag(1/diagx) GG^T,
-// which is accumulated from a shared-memory tile of GG), step (dx and the
+// formed on the FP64 tensor cores from a shared-memory tile of GG), step (dx and the
 // fraction-to-the-boundary limits) and one search pass per line-search candidate.  The
 // accepted step is applied by the next pass's prologue.  Reductions are deterministic:
-// one partial a block, summed by the last block in block order.
+// one partial a block, folded in block order (by the step and search passes' last block,
+// and for the assemble pass's larger product by a separate fold kernel).
 //
 // The file is compiled with -fmad=false, so that a * b + c rounds twice as in the
 // reference's tensor arithmetic; the dot products use fma() explicitly.
