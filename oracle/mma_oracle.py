@@ -55,14 +55,14 @@ def approximation(xval, xmin, xmax, low, upp, df0dx, fval, dfdx, move, raa0, alb
 
 def mmasub(m, n, iteration, xval, xmin, xmax, xold1, xold2, f0val, df0dx, fval, dfdx, low, upp, a0, a, c, d,
            asyinit=0.5, asyclamp_min=0.01, asyclamp_max=10.0, move=0.5, raa0=1e-5, albefa=0.1, asyincr=1.2,
-           asydecr=0.7):
+           asydecr=0.7, stats=None):
     """One MMA step (sttopt/mma.py:150-285): ``(xmma, ymma, zmma, lam, xsi, eta, mu, zet, s,
-    low, upp)``."""
+    low, upp)``; ``stats`` as in ``subsolv``."""
     low, upp = asymptotes(iteration, xval, xmin, xmax, xold1, xold2, low, upp, asyinit, asyclamp_min,
                           asyclamp_max, asyincr, asydecr)
     alfa, beta, p0, q0, P, Q, b = approximation(xval, xmin, xmax, low, upp, df0dx, fval, dfdx, move, raa0,
                                                 albefa)
-    return subsolv(m, n, EPSIMIN, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d) + (low, upp)
+    return subsolv(m, n, EPSIMIN, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d, stats) + (low, upp)
 
 
 def _residual(pt, epsi, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
@@ -80,10 +80,14 @@ def _residual(pt, epsi, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
                            mu * y - epsi, [zet * z - epsi], lam * s - epsi])
 
 
-def subsolv(m, n, epsimin, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
+def subsolv(m, n, epsimin, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d, stats=None):
     """The subproblem's primal-dual Newton solve along the barrier path epsi = 1, 0.1, ...
     (sttopt/mma.py:346-557): both eliminations of the bordered KKT system (m < n and
-    m >= n), the fraction-to-the-boundary step limit and the residual-norm line search."""
+    m >= n), the fraction-to-the-boundary step limit and the residual-norm line search.
+    ``stats`` (a dict) gathers the levels stopped at the Newton cap as the reference does
+    (``subsolv_cap_hits``), and the Newton steps and line-search candidates tried
+    (``subsolv_newton_steps``, ``subsolv_line_search_tries``)."""
+    counts = {"subsolv_cap_hits": 0, "subsolv_newton_steps": 0, "subsolv_line_search_tries": 0}
     x = 0.5 * (alfa + beta)
     y, z, lam = np.ones(m), 1.0, np.ones(m)
     xsi = np.maximum(1.0 / (x - alfa), 1.0)
@@ -99,6 +103,7 @@ def subsolv(m, n, epsimin, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
         ittt = 0
         while residumax > 0.9 * epsi and ittt < MAX_NEWTON:
             ittt += 1
+            counts["subsolv_newton_steps"] += 1
             ux1, xl1 = upp - x, x - low
             ux2, xl2 = ux1 * ux1, xl1 * xl1
             ux3, xl3 = ux1 * ux2, xl1 * xl2
@@ -143,6 +148,7 @@ def subsolv(m, n, epsimin, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
             old = (x, y, z, lam, xsi, eta, mu, zet, s)
             dirs = (dx, dy, dz, dlam, dxsi, deta, dmu, dzet, ds)
             for j in range(MAX_HALVINGS):
+                counts["subsolv_line_search_tries"] += 1
                 t = steg / 2.0 ** j
                 pt = tuple(o + t * dv for o, dv in zip(old, dirs))
                 residu = _residual(pt, epsi, *args)
@@ -151,5 +157,10 @@ def subsolv(m, n, epsimin, low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d):
                     break
             x, y, z, lam, xsi, eta, mu, zet, s = pt
             residunorm, residumax = resinew, np.abs(residu).max()
+        if ittt > MAX_NEWTON - 2:  # sttopt/mma.py:540
+            counts["subsolv_cap_hits"] += 1
         epsi = 0.1 * epsi
+    if stats is not None:
+        for k, v in counts.items():
+            stats[k] = stats.get(k, 0) + v
     return x, y, z, lam, xsi, eta, mu, zet, s

@@ -50,13 +50,19 @@ def run_device(mma, args, kw, stats=None):
 
 @pytest.mark.parametrize("tag", TAGS)
 def test_mmasub_matches_reference_outputs(mma, tag):
+    """The outputs, and the same Newton path as the oracle: as many Newton steps and
+    line-search candidates."""
     g = golden("mma")
     args, kw = mma_case(g, tag)
-    got = run_device(mma, args, kw)
-    oracle = M.mmasub(*args, **kw)
+    got_stats, want_stats = {}, {}
+    got = run_device(mma, args, kw, got_stats)
+    oracle = M.mmasub(*args, **kw, stats=want_stats)
     for name, v, o in zip(NAMES, got, oracle):
         assert rel_max(v, g[f"{tag}_{name}"]) < TOL, (name, rel_max(v, g[f"{tag}_{name}"]))
         assert rel_max(v, o) < TOL, name
+    for key in ("subsolv_newton_steps", "subsolv_line_search_tries"):
+        assert got_stats[key] == want_stats[key], (key, got_stats, want_stats)
+    assert got_stats.get("subsolv_cap_hits", 0) == want_stats["subsolv_cap_hits"] == 0
 
 
 def _subproblem(rng, m, n):
@@ -117,13 +123,16 @@ def test_mmasub_oracle_at_a_quarter_million_variables(mma):
     tr = M_trust(p["move"], np.ones(n))
     args = (m, n, 4, p["xval"], np.zeros(n), np.ones(n), p["xold1"], p["xold2"], 0.0, p["df0dx"], p["fval"],
             p["dfdx"], p["xval"] - 0.2, p["xval"] + 0.2, 1.0, np.zeros(m), np.full(m, 1000.0), np.zeros(m))
-    want = M.mmasub(*args, raa0=1e-5 / n, **tr)
+    want_stats, got_stats = {}, {}
+    want = M.mmasub(*args, raa0=1e-5 / n, stats=want_stats, **tr)
     t = [dev(v) for v in args[3:8]]
     got = mma.mmasub(m, n, 4, *t, 0.0, dev(p["df0dx"]), dev(p["fval"]), dev(p["dfdx"]), dev(args[12]),
                      dev(args[13]), 1.0, dev(np.zeros(m)), dev(np.full(m, 1000.0)), dev(np.zeros(m)),
-                     raa0=1e-5 / n, **{k: dev(v) for k, v in tr.items()})
+                     raa0=1e-5 / n, stats=got_stats, **{k: dev(v) for k, v in tr.items()})
     for name, gv, wv in zip(NAMES, got, want):
         assert rel_max(gv, wv) < TOL, (name, rel_max(gv, wv))
+    assert got_stats["subsolv_newton_steps"] == want_stats["subsolv_newton_steps"]
+    assert got_stats["subsolv_line_search_tries"] == want_stats["subsolv_line_search_tries"]
 
 
 def M_trust(move, xrange):
