@@ -166,3 +166,39 @@ def test_host_conversions_are_memoised_per_tensor_object(pkg):
     assert _geom.grid_shape(e1, 2 * 7 * 5, 2) == (6, 4)
     e2 = torch.as_tensor(O.element_dof_map(4, 6))
     assert _geom.grid_shape(e2, 2 * 5 * 7, 2) == (4, 6)
+
+
+def test_mma_entry_points_size_and_validate_without_a_device(pkg):
+    """``stt_mma_*``: the workspace grows with the variables and the constraints, and bad
+    sizes, null pointers or a short workspace are refused before any CUDA call."""
+    from sttopt_b200 import _lib
+
+    lib = _lib.lib()
+    a, b, c = (lib.stt_mma_workspace_bytes(m, n) for m, n in ((17, 1 << 20), (17, 1 << 22), (40, 1 << 22)))
+    assert 0 < a < b < c
+    assert b >= 4 * 8 * (1 << 22)  # alfa, beta, raa0 / range and dx
+    assert lib.stt_mma_workspace_bytes(0, 100) == 0 and lib.stt_mma_workspace_bytes(3, 0) == 0
+    need = lib.stt_mma_workspace_bytes(3, 1000)
+
+    def subsolv(m, ws_bytes):
+        # m, n, epsimin, low upp alfa beta p0 q0 P Q, ld, a0, a b c d, x xsi eta y z lam mu zet s,
+        # counts, cap_epsi, ws, ws_bytes, stream
+        return lib.stt_mma_subsolv(m, 1000, 1e-7, *[None] * 8, 1000, 1.0, *[None] * 4, *[None] * 9, None, None,
+                                   None, ws_bytes, None)
+
+    def sub(m, ws_bytes):
+        # m, n, iteration, xval xmin xmax xold1 xold2 df0dx fval dfdx, ld, low upp, a0, a c d,
+        # four (pointer, value) keywords, raa0 albefa asyincr asydecr, 9 outputs, counts,
+        # cap_epsi, ws, ws_bytes, stream
+        return lib.stt_mma_sub(m, 1000, 0, *[None] * 8, 1000, None, None, 1.0, None, None, None, None, 0.5, None,
+                               0.01, None, 10.0, None, 0.5, 1e-5, 0.1, 1.2, 0.7, *[None] * 9, None, None, None,
+                               ws_bytes, None)
+
+    assert subsolv(65, 1 << 30) == _lib.STT_ERR_INVALID  # m < n beyond 64 constraints
+    assert b"64" in lib.stt_last_error()
+    assert subsolv(3, need - 1) == _lib.STT_ERR_WORKSPACE
+    assert subsolv(3, need) == _lib.STT_ERR_INVALID  # null pointers
+    assert b"null pointer" in lib.stt_last_error()
+    assert sub(3, need - 1) == _lib.STT_ERR_WORKSPACE
+    assert sub(3, need) == _lib.STT_ERR_INVALID
+    assert sub(0, need) == _lib.STT_ERR_INVALID
