@@ -53,7 +53,7 @@ _SIGS = {
                              _c_double, _c_double, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.c_size_t,
                              _p]),
     "stt_mma_subsolv": (_c_int, [_c_int, _c_ll, _c_double, _p, _p, _p, _p, _p, _p, _p, _p, _c_ll, _c_double, _p, _p,
-                                 _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.c_size_t, _p]),
+                                 _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, ctypes.c_size_t, _p]),
     "stt_stage_glue_rows": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p,
                                      _c_double, _c_double, _c_double, _p, _p, _p, _p]),
     "stt_stage_glue_adjoint": (_c_int, [_c_int, _c_int, _c_int, _c_int, _p, _p, _pd, _c_double, _p, _p, _p, _p,

@@ -30,6 +30,27 @@ def test_library_exports_every_declared_symbol(pkg):
     assert sorted(_lib.exported_symbols()) == declared_symbols()
 
 
+def declared_arity():
+    """Parameter count of every prototype in the header."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(stt_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_the_header(pkg):
+    """Every ctypes signature has as many arguments as its C prototype (an argument past
+    the declared ones would be passed as a 32-bit int)."""
+    from sttopt_b200 import _lib
+
+    arity = declared_arity()
+    assert set(arity) == set(declared_symbols())
+    wrong = {n: (len(args), arity[n]) for n, (_, args) in _lib._SIGS.items() if len(args) != arity[n]}
+    assert not wrong, wrong
+
+
 def test_workspace_planning_follows_the_reference_policy(pkg):
     from sttopt_b200 import _lib
 

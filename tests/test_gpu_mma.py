@@ -90,6 +90,24 @@ def test_subsolv_matches_oracle(mma, m, n):
         assert rel_max(gv, wv) < TOL, (k, rel_max(gv, wv))
 
 
+def test_subsolv_on_a_side_stream(mma):
+    """The call runs on the caller's current stream, here not the default one."""
+    rng = np.random.default_rng(17)
+    m, n = 5, 3000
+    args = _subproblem(rng, m, n)
+    low, upp, alfa, beta, p0, q0, P, Q, a0, a, b, c, d = args
+    dargs = [dev(v) for v in (low, upp, alfa, beta, p0, q0, P, Q)]
+    rest = [dev(v) for v in (a, b, c, d)]
+    want = mma.subsolv(m, n, M.EPSIMIN, *dargs, a0, *rest)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        got = mma.subsolv(m, n, M.EPSIMIN, *dargs, a0, *rest)
+    torch.cuda.current_stream().wait_stream(side)
+    for gv, wv in zip(got, want):
+        assert torch.equal(gv, wv)
+
+
 def test_subsolv_strided_rows(mma):
     """P and Q as row views with a row stride larger than n."""
     rng = np.random.default_rng(5)
