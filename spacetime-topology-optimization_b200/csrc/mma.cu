@@ -448,10 +448,10 @@ __host__ __device__ inline int packed_index(int i, int k, int m1) { return i * m
 // Partial entries of the assemble pass: [gvec (m) | sum of squares | packed product | max].
 __host__ __device__ inline int assemble_kp(int m) { return m + 2 + (m + 1) * (m + 2) / 2; }
 // Its dynamic shared memory: the GG tile (or, later, the folded entries), 1/diagx, a
-// block-sum scratch, and the row-sum slots or shuffle scratch.
-inline size_t assemble_smem(int m, int mb) {
+// block-sum scratch, and when it forms gvec the row-sum slots or shuffle scratch.
+inline size_t assemble_smem(int m, int mb, bool need_g) {
   const size_t rows = (size_t)gram_side(m) * 8;
-  const size_t tail = mb <= 24 ? (size_t)mb * kMmaThreads : (size_t)(kMmaThreads / 32) * kMmaMaxM;
+  const size_t tail = !need_g ? 0 : mb <= 24 ? (size_t)mb * kMmaThreads : (size_t)(kMmaThreads / 32) * kMmaMaxM;
   return 8 * (std::max(rows * kMmaLd8, (size_t)assemble_kp(m)) + kMmaThreads + 8 + tail);
 }
 inline int mma_bucket(int m) {
@@ -467,11 +467,13 @@ inline int mma_bucket(int m) {
 // delx into a shared tile; A and h come from DMMA tiles of that tile.  Up to 31
 // constraints each warp takes 32 of the tile's variables for every 8 x 8 tile and the
 // warps' sums are folded in warp order; above that the tiles are split among the warps.
-// res = [gvec (m) | h (m) | A (m x m) | sum of squares | max].
+// gvec is formed only with need_g: after a line search it is the accepted candidate's,
+// which the search pass formed at this same point.
+// res = [gvec (m), or zeros | h (m) | A (m x m) | sum of squares | max].
 template <int MB, bool G>
 __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
     MmaCols c, double* __restrict__ x, double* __restrict__ xsi, double* __restrict__ eta,
-    const double* __restrict__ dx, int pend, double t_pend, double eps_pend, MVec lam, double epsi,
+    const double* __restrict__ dx, int pend, double t_pend, double eps_pend, MVec lam, double epsi, int need_g,
     double* __restrict__ partials) {
   extern __shared__ double sm[];
   constexpr int T8 = (MB + 8) / 8;  // tile side for the largest m of the bucket
@@ -490,8 +492,10 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
 #pragma unroll
   for (int q = 0; q < TPW; ++q) acc[q][0] = acc[q][1] = 0.0;
   RowAcc<MB> gv;
-  if constexpr (use_slots<MB>()) gv.slots = tail;
-  gv.zero();
+  if (need_g) {
+    if constexpr (use_slots<MB>()) gv.slots = tail;
+    gv.zero();
+  }
   double ss = 0.0, mx = 0.0;
   for (int r = m + 1; r < rows; ++r) gs[r * kMmaLd8 + tid] = 0.0;
 
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
             rows_pq1<G>(f, ra[u], rb[u], p1, q1);
             lp = fma(lam.v[i], p1, lp);
             lq = fma(lam.v[i], q1, lq);
-            gv.add(i, fma(p1, k.A, q1 * k.B));
+            if (need_g) gv.add(i, fma(p1, k.A, q1 * k.B));
             gs[i * kMmaLd8 + tid] = fma(p1, k.C, -(q1 * k.D));
           }
         }
@@ -649,7 +653,11 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mma_assemble_kernel(
     }
   }
   const int ks = assemble_kp(m) - 1;
-  gv.write(m, partials, 0, tail);
+  if (need_g) {
+    gv.write(m, partials, 0, tail);
+  } else {
+    for (int i = tid; i < m; i += kMmaThreads) *part(partials, i) = 0.0;
+  }
   const double t = block_total(ss, wred);
   if (tid == 0) *part(partials, m) = t;
   const double u = block_nanmax(mx, wred);
@@ -837,7 +845,8 @@ static_assert(kAsmBlocks <= 32 * kFoldMax && kPassBlocks <= 32 * kFoldMax, "a fo
 constexpr int kMaxHalvings = 50;   // sttopt/mma.py:289
 constexpr int kMaxNewton = 200;    // sttopt/mma.py:442
 
-using AsmFn = void (*)(MmaCols, double*, double*, double*, const double*, int, double, double, MVec, double, double*);
+using AsmFn = void (*)(MmaCols, double*, double*, double*, const double*, int, double, double, MVec, double, int,
+                       double*);
 using StepFn = void (*)(MmaCols, const double*, const double*, const double*, MVec, MVec, double, double*, double*,
                         unsigned*, double*);
 using SearchFn = void (*)(MmaCols, const double*, const double*, const double*, const double*, double, MVec, double,
@@ -1059,9 +1068,9 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
   const long long tiles = (c.n + kMmaThreads - 1) / kMmaThreads;
   const int ga = (int)std::min<long long>(tiles, kAsmBlocks), gp = (int)std::min<long long>(tiles, kPassBlocks);
   const Kernels k = pick_kernels<G>(m);
-  const size_t smem = assemble_smem(m, mma_bucket(m));
+  const size_t smem_g = assemble_smem(m, mma_bucket(m), true), smem = assemble_smem(m, mma_bucket(m), false);
   STT_TRY(check_cuda(cudaFuncSetAttribute((const void*)k.assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem),
+                                          (int)smem_g),
                      "mma: assemble shared memory"));
   STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4 * sizeof(unsigned), st), "mma: counters"));
   mma_init_kernel<<<gp, kMmaThreads, 0, st>>>(c.n, c.alfa, c.beta, x, xsi, eta);
@@ -1076,16 +1085,21 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
   };
   int pend = 0;
   double t_pend = 0.0, eps_pend = 0.0;
+  // gvec at the current point: formed by the first assemble, then taken from each
+  // accepted line-search candidate, whose point the next assemble starts from
+  bool have_g = false;
   auto assemble = [&](double epsi, double& ssn, double& mxn) -> int {
-    k.assemble<<<ga, kMmaThreads, smem, st>>>(c, x, xsi, eta, w.dx, pend, t_pend, eps_pend, mvec(S.lam), epsi,
-                                              w.partials);
+    const int need_g = have_g ? 0 : 1;
+    k.assemble<<<ga, kMmaThreads, need_g ? smem_g : smem, st>>>(c, x, xsi, eta, w.dx, pend, t_pend, eps_pend,
+                                                                mvec(S.lam), epsi, need_g, w.partials);
     pend = 0;
     STT_TRY(check_launch("mma_assemble_kernel"));
     const int kp = assemble_kp(m), per = kMmaThreads / 32;
     mma_fold_kernel<<<(kp + per - 1) / per, kMmaThreads, 0, st>>>(w.partials, ga, m, w.res);
     STT_TRY(check_launch("mma_fold_kernel"));
     STT_TRY(fetch(nres, "mma: assemble"));
-    std::copy(R.begin(), R.begin() + m, gvec.begin());
+    if (!have_g) std::copy(R.begin(), R.begin() + m, gvec.begin());
+    have_g = true;
     std::copy(R.begin() + m, R.begin() + 2 * m, h.begin());
     std::copy(R.begin() + 2 * m, R.begin() + 2 * m + (size_t)m * m, A.begin());
     ssn = R[nres - 2];
@@ -1151,6 +1165,7 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
         if (!(resinew > residunorm)) break;
       }
       S = C;
+      std::copy(R.begin(), R.begin() + m, gvec.begin());  // the accepted candidate's gvec
       pend = 1;
       t_pend = t;
       eps_pend = epsi;
