@@ -699,11 +699,13 @@ __global__ void __launch_bounds__(kMmaThreads) mma_fold_kernel(const double* __r
 // The step pass (sttopt/mma.py:490-535, m < n): with the Newton step's dlam from the
 // host, dx = -delx / diagx - (GG^T dlam) / diagx (stored), dxsi and deta, and the
 // fraction-to-the-boundary limits max(-1.01 dx / (x - alfa)), max(1.01 dx / (beta - x))
-// and max(-1.01 dxsi / xsi, -1.01 deta / eta).  res = those three maxima.
+// and max(-1.01 dxsi / xsi, -1.01 deta / eta).  res = those three maxima and the step
+// length steg = 1 / max(them, stm_host (the m-sized variables' limit), 1), formed as the
+// host forms it, for a search pass launched right behind this one.
 template <int MB, bool G>
 __global__ void __launch_bounds__(kMmaThreads, 3) mma_step_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
-    MVec lam, MVec dlam, double epsi, double* __restrict__ dx, double* __restrict__ partials,
+    MVec lam, MVec dlam, double epsi, double stm_host, double* __restrict__ dx, double* __restrict__ partials,
     unsigned* __restrict__ counter, double* __restrict__ res) {
   __shared__ double red[kMmaThreads / 32];
   __shared__ double fin[3];
@@ -759,20 +761,26 @@ __global__ void __launch_bounds__(kMmaThreads, 3) mma_step_kernel(
   }
   if (!finish_blocks(partials, counter, 3, 0, fin)) return;
   if (threadIdx.x < 3) res[threadIdx.x] = fin[threadIdx.x];
+  if (threadIdx.x == 0) res[3] = 1.0 / nanmax(nanmax(nanmax(fin[0], fin[1]), nanmax(fin[2], stm_host)), 1.0);
 }
 
 // The search pass: at the point (x, xsi, eta) + t (dx, dxsi, deta) (when dx is given)
-// and multipliers lam, gvec = P (1/ux1) + Q (1/xl1) and, when resid, the sum of squares
-// and largest magnitude of the residual's n-sized parts (sttopt/mma.py:399-434).  With
-// x = xval and no step it gives mmasub's b + fval (:285).
+// and multipliers lam + t dlam, gvec = P (1/ux1) + Q (1/xl1) and, when resid, the sum of
+// squares and largest magnitude of the residual's n-sized parts (sttopt/mma.py:399-434).
+// t is read from tdev when given (the step pass's steg, the line search's first
+// candidate).  With x = xval and no step it gives mmasub's b + fval (:285).
 // res = [gvec (m) | sum of squares | max].
 template <int MB, bool G>
 __global__ void __launch_bounds__(kMmaThreads, 3) mma_search_kernel(
     MmaCols c, const double* __restrict__ x, const double* __restrict__ xsi, const double* __restrict__ eta,
-    const double* __restrict__ dx, double t, MVec lam, double epsi, int resid, double* __restrict__ partials,
-    unsigned* __restrict__ counter, double* __restrict__ res) {
+    const double* __restrict__ dx, double t_arg, const double* tdev, MVec lam0, MVec dlam, double epsi, int resid,
+    double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ res) {
   __shared__ double red[kMmaThreads / 32 * (kMmaMaxM + 1)];
   __shared__ double fin[kMmaMaxM + 2];
+  __shared__ MVec lam;  // the candidate's multipliers, lam0 + t dlam as the host forms them
+  const double t = tdev ? *tdev : t_arg;
+  for (int i = threadIdx.x; i < c.m; i += kMmaThreads) lam.v[i] = lam0.v[i] + t * dlam.v[i];
+  __syncthreads();
   constexpr bool kSlots = MB <= 20;  // static shared memory stays under 48 KB
   __shared__ double slots[kSlots ? MB * kMmaThreads : 1];
   const int m = c.m;
@@ -847,10 +855,10 @@ constexpr int kMaxNewton = 200;    // sttopt/mma.py:442
 
 using AsmFn = void (*)(MmaCols, double*, double*, double*, const double*, int, double, double, MVec, double, int,
                        double*);
-using StepFn = void (*)(MmaCols, const double*, const double*, const double*, MVec, MVec, double, double*, double*,
-                        unsigned*, double*);
-using SearchFn = void (*)(MmaCols, const double*, const double*, const double*, const double*, double, MVec, double,
-                          int, double*, unsigned*, double*);
+using StepFn = void (*)(MmaCols, const double*, const double*, const double*, MVec, MVec, double, double, double*,
+                        double*, unsigned*, double*);
+using SearchFn = void (*)(MmaCols, const double*, const double*, const double*, const double*, double, const double*,
+                          MVec, MVec, double, int, double*, unsigned*, double*);
 struct Kernels {
   AsmFn assemble;
   StepFn step;
@@ -1077,8 +1085,10 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
   STT_TRY(check_launch("mma_init_kernel"));
   init_state(D, S);
 
+  // results of one fetch: the assemble's [gvec | h | A | ss | mx] or the search's
+  // [gvec | ss | mx] with the step's [3 maxima | steg] behind it
   const size_t nres = (size_t)m * m + 2 * m + 2;
-  std::vector<double> R(nres), gvec(m), h(m), A((size_t)m * m);
+  std::vector<double> R(std::max(nres, (size_t)m + 6)), gvec(m), h(m), A((size_t)m * m);
   auto fetch = [&](size_t count, const char* what) -> int {
     STT_TRY(check_cuda(cudaMemcpyAsync(R.data(), w.res, 8 * count, cudaMemcpyDeviceToHost, st), what));
     return check_cuda(cudaStreamSynchronize(st), what);
@@ -1139,13 +1149,20 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
       MStep T;
       T.dlam.assign(bb.begin(), bb.begin() + m);
       T.dz = bb[m];
-      k.step<<<gp, kMmaThreads, 0, st>>>(c, x, xsi, eta, mvec(S.lam), mvec(T.dlam), epsi, w.dx, w.partials,
-                                         w.counters + 1, w.res);
+      // The step pass forms steg on the device and the line search's first candidate
+      // (t = steg) is evaluated right behind it: one sync for both.  The step's results sit
+      // behind the search's in res: [search (m + 2) | step maxima (3) | steg].
+      const double stm_m = step_m(D, S, N, epsi, T);
+      const MVec lam_now = mvec(S.lam), dlam = mvec(T.dlam);
+      double* const res_step = w.res + m + 2;
+      k.step<<<gp, kMmaThreads, 0, st>>>(c, x, xsi, eta, lam_now, dlam, epsi, stm_m, w.dx, w.partials,
+                                         w.counters + 1, res_step);
       STT_TRY(check_launch("mma_step_kernel"));
-      STT_TRY(fetch(3, "mma: step"));
-      const double stmalfa = R[0], stmbeta = R[1];
-      const double stmxx = hmax(R[2], step_m(D, S, N, epsi, T));
-      const double steg = 1.0 / hmax(hmax(hmax(stmalfa, stmbeta), stmxx), 1.0);
+      k.search<<<gp, kMmaThreads, 0, st>>>(c, x, xsi, eta, w.dx, 0.0, res_step + 3, lam_now, dlam, epsi, 1,
+                                           w.partials, w.counters + 2, w.res);
+      STT_TRY(check_launch("mma_search_kernel"));
+      STT_TRY(fetch((size_t)m + 6, "mma: step and first candidate"));
+      const double steg = R[m + 5];  // 1 / max(stmalfa, stmbeta, stmxx, 1), as formed on the device
       // Backtracking on the residual norm: the first halving whose norm does not exceed
       // the current one, else the last (sttopt/mma.py:297-343).
       MState C;
@@ -1154,10 +1171,12 @@ int device_subsolv(const MmaCols& c, const MData& D, double epsimin, const MmaWs
         t = steg / std::ldexp(1.0, jj);
         C = moved(S, T, t);
         ++cap.tries;
-        k.search<<<gp, kMmaThreads, 0, st>>>(c, x, xsi, eta, w.dx, t, mvec(C.lam), epsi, 1, w.partials,
-                                             w.counters + 2, w.res);
-        STT_TRY(check_launch("mma_search_kernel"));
-        STT_TRY(fetch((size_t)m + 2, "mma: line search"));
+        if (jj > 0) {
+          k.search<<<gp, kMmaThreads, 0, st>>>(c, x, xsi, eta, w.dx, t, nullptr, lam_now, dlam, epsi, 1, w.partials,
+                                               w.counters + 2, w.res);
+          STT_TRY(check_launch("mma_search_kernel"));
+          STT_TRY(fetch((size_t)m + 2, "mma: line search"));
+        }
         double ssc = R[m], mxcn = ssc != ssc ? NAN : R[m + 1], ssmc = 0.0, mxmc = -INFINITY;
         resid_m(D, C, R.data(), epsi, ssmc, mxmc);
         resinew = std::sqrt(ssc + ssmc);
@@ -1420,8 +1439,8 @@ extern "C" int stt_mma_sub(int m, long long n, int iteration, const double* xval
   if (m < n) {
     STT_TRY(check_cuda(cudaMemsetAsync(w.counters, 0, 4 * sizeof(unsigned), st), "mma: counters"));
     const Kernels k = pick_kernels<true>(m);
-    k.search<<<gp, kMmaThreads, 0, st>>>(cols, xval, nullptr, nullptr, nullptr, 0.0, MVec{}, 0.0, 0, w.partials,
-                                         w.counters + 3, w.res);
+    k.search<<<gp, kMmaThreads, 0, st>>>(cols, xval, nullptr, nullptr, nullptr, 0.0, nullptr, MVec{}, MVec{}, 0.0,
+                                         0, w.partials, w.counters + 3, w.res);
     STT_TRY(check_launch("mma_search_kernel"));
     std::vector<double> g;
     STT_TRY(d2h(g, w.res, (size_t)m, st));
